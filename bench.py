@@ -1,0 +1,323 @@
+"""Benchmark of the supernodal numeric factorization (one JSON line on stdout, rank 0).
+
+A step is one numeric factorization of the workload matrix (default grid3d_60: the 3D
+7-point Laplacian on 60^3 plus 1e-3 I, n = 216,000, ordered by geometric nested dissection
+and analysed by the reference's own symbolic phase; the supernode partition and final
+permutation come from tests/golden/sym_grid3d_60.npz).  The metric is the reference's flop
+measure fl = sum_j c_j^2 (exact column counts) divided by the factorization time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Our arm: values already resident in HBM, K factorizations timed with CUDA events on the
+library's stream, bracketed by barrier + synchronize; max over ranks.  `e2e` times the
+reference-facing C-ABI call sw_cholesky_left_par_05 with host buffers (upload of the
+structure and values, factorization, download of L).  The reference arm (--impl reference)
+times the reference's own CPU executor (oracle/_ref) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "factorization GFLOP/s (fl = sum c_j^2), FP64 supernodal numeric factor"
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def load_problem(name):
+    from swcholesky_b200 import workloads as W
+    g = dict(np.load(os.path.join(GOLDEN, f"sym_{name}.npz")))
+    A, perm_in, meta = W.build(name)
+    P = W.assemble(A, g["perm"], g["super"])
+    return A, perm_in, meta, P, float(g["fl"])
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def fp64_gemm_peak(torch, dev):
+    """Dense FP64 GEMM throughput of this GPU measured with cuBLAS (torch.matmul, 8192^3),
+    best of 5 after 2 warm-ups; the FP64 roofline denominator (MEASURED_PEAKS.json has
+    none for FP64)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        best = max(best, 2.0 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+def reference_time(A, perm_in, threads, budget_s, max_reps, min_reps=1):
+    """Times the reference's own FP64 executor; returns (median seconds, reps, symbolic)."""
+    from oracle import oracle as O
+    R = O.RefSymbolic(A, perm_in)
+    times = []
+    t0 = time.time()
+    while len(times) < max_reps and (len(times) < min_reps or time.time() - t0 < budget_s):
+        _, t, ret = R.factor(threads=threads)
+        if ret != 1:
+            raise RuntimeError("reference factorization failed")
+        times.append(t)
+    sym = R.sym
+    R.close()
+    return float(np.median(times)), len(times), sym
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    A, perm_in, meta, P, fl = load_problem(args.workload)
+    threads = os.cpu_count() or 1
+    from oracle import oracle as O
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libswref.so not built"}))
+        return
+    R = O.RefSymbolic(A, perm_in)
+    for _ in range(args.warmup):
+        R.factor(threads=threads)
+    times = []
+    for _ in range(args.steps):
+        _, t, ret = R.factor(threads=threads)
+        assert ret == 1
+        times.append(t)
+    R.close()
+    t = float(np.mean(times))
+    val = fl / t / 1e9
+    line = {
+        "metric": METRIC, "value": round(val, 3), "unit": "GFLOP/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator, reference symbolic phase)",
+        "config": {"workload": args.workload, "n": P.n, "nnz_lower": int(P.A2p[-1]),
+                   "fl": fl, "parallelism": "host cores"},
+        "impl": "reference",
+        "cpu_baseline": {"value": round(val, 3), "unit": "GFLOP/s", "cores": threads,
+                         "kind": "reference",
+                         "sample": f"full {args.workload} factorization per step "
+                                   f"(sw_cholesky_left_par_05_check + OpenBLAS, {threads} threads)"},
+        "e2e": {"value": round(val, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    import swcholesky_b200 as swc
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    A, perm_in, meta, P, fl = load_problem(args.workload)
+
+    h = swc.Handle(local_rank)
+    h.analyze(P.n, P.A2p, P.A2i, P.lC, P.Ls, P.Li_ptr, P.super, P.prunePtr, P.pruneSet,
+              P.levelPtr, P.parPtr, P.partition)
+    vals = torch.from_numpy(P.A2x).to(dev)
+    stream = torch.cuda.ExternalStream(h.stream, device=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        info = h.factor(vals)
+        assert info == 0, f"not SPD at column {info - 1}"
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        h.factor(vals)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * fl / (ms * 1e-3) / 1e9
+
+    # ---- per-kernel roofline (a separate profiled factorization, untimed) ----
+    prof = h.profile(vals)
+    kinds = {k: v for k, v in prof.items() if k != "memset"}
+    dom = max(kinds, key=lambda k: kinds[k][1])
+    la, kms, kfl, kby = kinds[dom]
+    peak64 = fp64_gemm_peak(torch, dev) if rank == 0 else None
+
+    # ---- end to end through the reference-facing C-ABI call, host buffers ----
+    e2e = None
+    if rank == 0:
+        L_host = np.zeros(P.xsize, np.float64)
+        e2e_steps = max(1, min(3, args.steps))
+        t_e2e = []
+        for i in range(e2e_steps + 1):
+            t0 = time.perf_counter()
+            ret = swc.sw_cholesky_left_par_05(
+                P.n, P.A2p, P.A2i, P.A2x, P.lC, P.Ls, P.Li_ptr, L_host, P.super, P.nsuper,
+                None, P.prunePtr, P.pruneSet, P.levelPtr.size - 1, P.levelPtr, None, 0,
+                P.parPtr, P.partition, 0, 1, 0, 0, None)
+            dt = time.perf_counter() - t0
+            assert ret == 1
+            if i > 0:          # the first call also creates the library's default handle
+                t_e2e.append(dt)
+        h2d = (P.A2x.nbytes + P.A2p.nbytes + P.A2i.nbytes + P.Ls.nbytes + P.super.nbytes +
+               P.prunePtr.nbytes + P.pruneSet.nbytes + 8 * 2 * P.nsuper)
+        te = float(np.mean(t_e2e))
+        e2e = {"value": round(fl / te / 1e9, 3), "unit": "GFLOP/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(8 * P.xsize),
+               "ms_per_step": round(te * 1e3, 3),
+               "note": "sw_cholesky_left_par_05 with host arrays: host validation + plan, "
+                       "upload of structure and values, factorization, download of L"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        if O.ref_available():
+            threads = os.cpu_count() or 1
+            tref, reps, _ = reference_time(A, perm_in, threads, budget_s=15.0, max_reps=5)
+            cpu = {"value": round(fl / tref / 1e9, 3), "unit": "GFLOP/s", "cores": threads,
+                   "kind": "reference",
+                   "sample": f"{reps} full {args.workload} factorizations, median "
+                             f"(reference sw_cholesky_left_par_05_check + OpenBLAS)"}
+        else:
+            cpu = {"value": None, "unit": "GFLOP/s", "cores": 0, "kind": "reference",
+                   "sample": "unavailable: oracle/_ref/libswref.so not built"}
+
+    if rank == 0:
+        achieved = kfl / (kms * 1e-3) / 1e12
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator; reference symbolic phase via fixture)",
+            "config": {"workload": args.workload, "n": P.n, "nnz_lower": int(P.A2p[-1]),
+                       "nsuper": P.nsuper, "xsize": P.xsize, "fl": fl,
+                       "parallelism": "replicas only" if world > 1 else "single GPU",
+                       "l2": f"inputs larger than L2 (L = {P.xsize * 8 / 1e9:.2f} GB)"},
+            "roofline": {"bound": "tensor", "kernel": dom, "achieved": round(achieved, 4),
+                         "peak": round(peak64, 3) if peak64 else None, "unit": "TFLOP/s",
+                         "frac": round(achieved / peak64, 4) if peak64 else None,
+                         "traffic": None,
+                         "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run",
+                         "launches": la, "kernel_ms": round(kms, 4),
+                         "algorithmic_flops": kfl,
+                         "classes": {k: {"launches": v[0], "ms": round(v[1], 4),
+                                         "gflop": round(v[2] / 1e9, 4)}
+                                     for k, v in prof.items()}},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(h.launches * args.steps),
+            "clocks": clk,
+        }
+        print(json.dumps(line))
+    h.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="grid3d_60")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

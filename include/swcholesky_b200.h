@@ -1,0 +1,119 @@
+/* libswchol_b200 -- supernodal sparse Cholesky numeric factorization on NVIDIA B200.
+ *
+ * C ABI.  Plain pointers and sizes; no CUDA or PyTorch types in any signature (streams and
+ * device pointers travel as void*).  Every function that can fail returns an int status
+ * (SWC_OK = 0) and leaves a message for swc_last_error(), except the drop-in
+ * sw_cholesky_left_par_05, which keeps the reference's "1 = success" convention.
+ *
+ * Layout conventions are the reference's BCSC (swCholesky common/def.h:123-210):
+ *   blockSet[s] .. blockSet[s+1]-1 are the columns of supernode s (supNo supernodes);
+ *   Ls[Li_ptr[j] ..] is the sorted row list of the supernode holding column j;
+ *   lValues[lC[j] ..] holds column j; a supernode is an nsrow x nscol column-major block.
+ */
+#ifndef SWCHOLESKY_B200_H
+#define SWCHOLESKY_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define SWC_OK 0
+#define SWC_NOT_SPD 1          /* a pivot was <= 0 or NaN; *info = failing column + 1 */
+#define SWC_INVALID_INPUT 2    /* symbolic arrays rejected by host-side validation */
+#define SWC_CUDA_ERROR 3
+#define SWC_STRUCTURE_ERROR 4  /* pattern of A does not fit the supernodal structure */
+#define SWC_NOT_READY 5        /* call order violated (e.g. factor before analyze) */
+
+/* factorization modes */
+#define SWC_MODE_FP64 0        /* every operation in FP64 */
+
+typedef struct swc_handle *swc_handle_t;
+
+/* ---- drop-in for the reference numeric executor ------------------------------------
+ * Replaces sw_cholesky_left_par_05 (PRUNE build), cholesky/sw_parallel_PB_Cholesky_05.h:52-66,
+ * called from examples/sw_choleskyTest01.cpp:223-232.  Same arguments, same meaning: A2 =
+ * lower CSC of P A P^T (c, r, values), the BCSC layout (lC, Ls, Li_ptr, blockSet, supNo),
+ * the prune sets and the H-level schedule from analyze_p2; lValues (L->xsize doubles, zeroed
+ * by the caller) receives L in place.  timing, levelSet, nPar, chunk, threads, super_max,
+ * col_max and nodCost are accepted and ignored, as in the reference (levelSet is never
+ * allocated by its inspector: cholesky/InspectionLevel_06.h:28).  The factorization runs on
+ * the current CUDA device through a process-wide handle; inputs are uploaded, L is
+ * downloaded before returning.  Returns 1 on success and 0 on failure (non-SPD matrix or
+ * invalid input); swc_last_info() gives the failing column + 1 of a non-SPD matrix. */
+int sw_cholesky_left_par_05(int n, int *c, int *r, double *values, size_t *lC, int *Ls,
+                            size_t *Li_ptr, double *lValues, int *blockSet, int supNo,
+                            double *timing, int *prunePtr, int *pruneSet, int nLevels,
+                            int *levelPtr, int *levelSet, int nPar, int *parPtr,
+                            int *partition, int chunk, int threads, int super_max,
+                            int col_max, double *nodCost);
+
+/* Info of the last sw_cholesky_left_par_05 call: 0, or failing column + 1. */
+int swc_last_info(void);
+
+/* Message of the last failing call on this thread ("" if none). */
+const char *swc_last_error(void);
+
+/* ---- handle API: device-resident factorization -----------------------------------
+ * No reference counterpart: the reference re-reads host arrays on every call.  A handle
+ * keeps the symbolic structure and L on one GPU so that refactorization, solves and
+ * refinement need no host traffic. */
+int swc_create(swc_handle_t *handle, int device);
+int swc_destroy(swc_handle_t handle);
+/* Stream used by every later call on the handle (a cudaStream_t; NULL restores the
+ * handle's own stream). */
+int swc_set_stream(swc_handle_t handle, void *stream);
+void *swc_get_stream(swc_handle_t handle);
+
+/* Uploads and validates the structure.  Arguments as in sw_cholesky_left_par_05
+ * (values excluded).  levelPtr/parPtr/partition may be NULL: the executor derives its own
+ * level schedule from the supernodal etree. */
+int swc_analyze(swc_handle_t handle, int n, const int *c, const int *r, const size_t *lC,
+                const int *Ls, const size_t *Li_ptr, const int *blockSet, int supNo,
+                const int *prunePtr, const int *pruneSet, int nLevels, const int *levelPtr,
+                const int *parPtr, const int *partition);
+
+/* Numeric factorization with the A2 values (nnz(A2) doubles, in the order of r).
+ * values_on_device != 0: values is a device pointer on the handle's GPU.  *info = 0, or
+ * the failing column + 1 (status SWC_NOT_SPD). */
+int swc_factor(swc_handle_t handle, const double *values, int values_on_device, int mode,
+               int *info);
+
+/* Copies L (xsize doubles, reference layout) to host (to_device == 0) or device memory. */
+int swc_get_L(swc_handle_t handle, double *lValues, int to_device);
+
+/* Device pointer to the handle's L (xsize doubles), valid until the next analyze. */
+const double *swc_device_L(swc_handle_t handle);
+
+/* sizes[0..5] = n, nsuper, xsize, kernel launches per factorization, host-to-device and
+ * device-to-host bytes of the last factor / get_L call. */
+int swc_sizes(swc_handle_t handle, long long *sizes);
+
+/* Kernel classes reported by swc_profile (arrays of SWC_NKINDS entries, in this order). */
+#define SWC_NKINDS 6   /* memset, small, assemble, update, panel, syrk */
+
+/* One factorization, as swc_factor, with a CUDA event pair around every kernel launch:
+ * per kernel class the number of launches, the summed device milliseconds, and the
+ * algorithmic flops and DRAM bytes of one factorization.  Any output may be NULL. */
+int swc_profile(swc_handle_t handle, const double *values, int values_on_device, int *info,
+                int *launches, double *ms, double *flops, double *bytes);
+
+/* ---- host layout builder ---------------------------------------------------------
+ * Builds the BCSC layout the reference's analyze_p2 produces for a given supernode
+ * partition (cholesky/sw_LSparsity.h:598-665): Li_ptr, lC and Ls, the prune sets
+ * (descendants in increasing order), the supernodal etree, and a level schedule in the
+ * H-level array format (one partition per supernode, levels by etree height).
+ * swc_layout_sizes gives sizes[0..3] = len(Ls), len(pruneSet), xsize, nLevels. */
+int swc_layout_sizes(int n, const int *c, const int *r, const int *blockSet, int supNo,
+                     long long *sizes);
+int swc_layout(int n, const int *c, const int *r, const int *blockSet, int supNo,
+               size_t *lC, int *Ls, size_t *Li_ptr, int *sparent, int *prunePtr,
+               int *pruneSet, int *levelPtr, int *parPtr, int *partition);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SWCHOLESKY_B200_H */

@@ -1,0 +1,243 @@
+"""swcholesky_b200 -- supernodal sparse Cholesky numeric factorization on NVIDIA B200.
+
+Host-side mirror of the reference's numeric-phase interface over the C ABI of
+``libswchol_b200.so`` (``include/swcholesky_b200.h``):
+
+* ``sw_cholesky_left_par_05`` -- the reference entry point
+  (``cholesky/sw_parallel_PB_Cholesky_05.h:52-66``) with the same argument names and
+  meaning, taking numpy arrays; returns 1 on success and 0 on failure.
+* ``Handle`` -- device-resident factorization (analyze once, factor many times, keep L on
+  the GPU).
+* ``layout`` -- the BCSC layout, prune sets and a level schedule for a supernode partition.
+
+The CUDA library is the only compute path: importing works without a GPU, but every
+numeric call raises if the library is missing or no CUDA device is present.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = ["lib", "SWCError", "sw_cholesky_left_par_05", "Handle", "layout", "LIB_PATH",
+           "SWC_OK", "SWC_NOT_SPD", "SWC_MODE_FP64"]
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libswchol_b200.so")
+
+SWC_OK = 0
+SWC_NOT_SPD = 1
+SWC_INVALID_INPUT = 2
+SWC_CUDA_ERROR = 3
+SWC_STRUCTURE_ERROR = 4
+SWC_NOT_READY = 5
+SWC_MODE_FP64 = 0
+
+# every symbol include/swcholesky_b200.h declares
+EXPORTS = (
+    "sw_cholesky_left_par_05", "swc_last_info", "swc_last_error", "swc_create", "swc_destroy",
+    "swc_set_stream", "swc_get_stream", "swc_analyze", "swc_factor", "swc_get_L",
+    "swc_device_L", "swc_sizes", "swc_profile", "swc_layout_sizes", "swc_layout",
+)
+KERNEL_CLASSES = ("memset", "small", "assemble", "update", "panel", "syrk")
+
+_lib = None
+_VP = ctypes.c_void_p
+_I = ctypes.c_int
+
+
+class SWCError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"swc error {code}: {msg}")
+        self.code = code
+
+
+def lib() -> ctypes.CDLL:
+    """Loads libswchol_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m swcholesky_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        L.sw_cholesky_left_par_05.restype = _I
+        L.sw_cholesky_left_par_05.argtypes = ([_I] + [_VP] * 8 + [_I, _VP, _VP, _VP, _I] +
+                                              [_VP] * 2 + [_I] + [_VP] * 2 + [_I] * 4 + [_VP])
+        L.swc_last_info.restype = _I
+        L.swc_last_error.restype = ctypes.c_char_p
+        L.swc_create.argtypes = [ctypes.POINTER(_VP), _I]
+        L.swc_destroy.argtypes = [_VP]
+        L.swc_set_stream.argtypes = [_VP, _VP]
+        L.swc_get_stream.restype = _VP
+        L.swc_get_stream.argtypes = [_VP]
+        L.swc_analyze.argtypes = [_VP, _I] + [_VP] * 7 + [_I] + [_VP] * 2 + [_I] + [_VP] * 3
+        L.swc_factor.argtypes = [_VP, _VP, _I, _I, ctypes.POINTER(_I)]
+        L.swc_get_L.argtypes = [_VP, _VP, _I]
+        L.swc_device_L.restype = _VP
+        L.swc_device_L.argtypes = [_VP]
+        L.swc_sizes.argtypes = [_VP, _VP]
+        L.swc_profile.argtypes = [_VP, _VP, _I, ctypes.POINTER(_I), _VP, _VP, _VP, _VP]
+        L.swc_layout_sizes.argtypes = [_I] + [_VP] * 3 + [_I, _VP]
+        L.swc_layout.argtypes = [_I] + [_VP] * 3 + [_I] + [_VP] * 9
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return ctypes.c_void_p(a.data_ptr())
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _check(rc: int):
+    if rc != SWC_OK:
+        raise SWCError(rc, lib().swc_last_error().decode())
+
+
+def _c(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+def sw_cholesky_left_par_05(n, c, r, values, lC, Ls, Li_ptr, lValues, blockSet, supNo,
+                            timing, prunePtr, pruneSet, nLevels, levelPtr, levelSet, nPar,
+                            parPtr, partition, chunk, threads, super_max, col_max, nodCost):
+    """The reference numeric executor's interface; fills ``lValues`` (float64 numpy array of
+    L->xsize entries) in place.  Returns 1 on success, 0 on failure (as the reference's
+    driver expects, ``examples/sw_choleskyTest01.cpp:240-244``)."""
+    L = lib()
+    assert lValues.dtype == np.float64 and lValues.flags.c_contiguous
+    args = dict(c=_c(c, np.int32), r=_c(r, np.int32), values=_c(values, np.float64),
+                lC=_c(lC, np.uint64), Ls=_c(Ls, np.int32), Li_ptr=_c(Li_ptr, np.uint64),
+                blockSet=_c(blockSet, np.int32), prunePtr=_c(prunePtr, np.int32),
+                pruneSet=_c(pruneSet, np.int32), levelPtr=_c(levelPtr, np.int32),
+                parPtr=_c(parPtr, np.int32), partition=_c(partition, np.int32))
+    return L.sw_cholesky_left_par_05(
+        int(n), _p(args["c"]), _p(args["r"]), _p(args["values"]), _p(args["lC"]),
+        _p(args["Ls"]), _p(args["Li_ptr"]), _p(lValues), _p(args["blockSet"]), int(supNo),
+        _p(timing), _p(args["prunePtr"]), _p(args["pruneSet"]), int(nLevels),
+        _p(args["levelPtr"]), _p(levelSet), int(nPar), _p(args["parPtr"]),
+        _p(args["partition"]), int(chunk), int(threads), int(super_max), int(col_max),
+        _p(nodCost))
+
+
+def last_info() -> int:
+    return int(lib().swc_last_info())
+
+
+def layout(n, c, r, blockSet):
+    """BCSC layout of a supernode partition: dict with lC, Ls, Li_ptr, sparent, prunePtr,
+    pruneSet, levelPtr, parPtr, partition, xsize."""
+    L = lib()
+    c = _c(c, np.int32)
+    r = _c(r, np.int32)
+    bs = _c(blockSet, np.int32)
+    ns = bs.size - 1
+    sz = np.zeros(4, np.int64)
+    _check(L.swc_layout_sizes(int(n), _p(c), _p(r), _p(bs), ns, _p(sz)))
+    nls, nprune, xsize, nlev = (int(v) for v in sz)
+    out = dict(lC=np.zeros(n + 1, np.uint64), Ls=np.zeros(nls, np.int32),
+               Li_ptr=np.zeros(n + 1, np.uint64), sparent=np.zeros(ns, np.int32),
+               prunePtr=np.zeros(ns + 1, np.int32), pruneSet=np.zeros(nprune, np.int32),
+               levelPtr=np.zeros(nlev + 1, np.int32), parPtr=np.zeros(ns + 1, np.int32),
+               partition=np.zeros(ns, np.int32))
+    _check(L.swc_layout(int(n), _p(c), _p(r), _p(bs), ns, *[_p(out[k]) for k in (
+        "lC", "Ls", "Li_ptr", "sparent", "prunePtr", "pruneSet", "levelPtr", "parPtr",
+        "partition")]))
+    out["xsize"] = xsize
+    return out
+
+
+class Handle:
+    """A device-resident factorization on one GPU (``swc_create`` ... ``swc_destroy``)."""
+
+    def __init__(self, device: int = 0):
+        self._lib = lib()
+        h = ctypes.c_void_p()
+        _check(self._lib.swc_create(ctypes.byref(h), int(device)))
+        self._h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.swc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self) -> int:
+        """cudaStream_t of the handle, as an integer (for torch.cuda.ExternalStream)."""
+        return int(self._lib.swc_get_stream(self._h) or 0)
+
+    def set_stream(self, stream_ptr: int | None):
+        _check(self._lib.swc_set_stream(self._h, ctypes.c_void_p(stream_ptr or 0)))
+
+    def analyze(self, n, c, r, lC, Ls, Li_ptr, blockSet, prunePtr, pruneSet,
+                levelPtr=None, parPtr=None, partition=None):
+        self._keep = [_c(c, np.int32), _c(r, np.int32), _c(lC, np.uint64), _c(Ls, np.int32),
+                      _c(Li_ptr, np.uint64), _c(blockSet, np.int32), _c(prunePtr, np.int32),
+                      _c(pruneSet, np.int32)]
+        c, r, lC, Ls, Li_ptr, bs, pp, ps = self._keep
+        sched = [None, None, None]
+        nlev = 0
+        if levelPtr is not None:
+            sched = [_c(levelPtr, np.int32), _c(parPtr, np.int32), _c(partition, np.int32)]
+            nlev = sched[0].size - 1
+        _check(self._lib.swc_analyze(self._h, int(n), _p(c), _p(r), _p(lC), _p(Ls), _p(Li_ptr),
+                                     _p(bs), bs.size - 1, _p(pp), _p(ps), nlev, _p(sched[0]),
+                                     _p(sched[1]), _p(sched[2])))
+        self._keep = None
+        sz = np.zeros(6, np.int64)
+        _check(self._lib.swc_sizes(self._h, _p(sz)))
+        self.n, self.nsuper, self.xsize, self.launches = (int(v) for v in sz[:4])
+
+    def factor(self, values, mode: int = SWC_MODE_FP64) -> int:
+        """Factor with A2 values: a numpy array (host) or a CUDA tensor on this device.
+        Returns info (0 = success, else failing column + 1); raises on other errors."""
+        on_dev = hasattr(values, "data_ptr")
+        if not on_dev:
+            values = _c(values, np.float64)
+        info = ctypes.c_int(0)
+        rc = self._lib.swc_factor(self._h, _p(values), 1 if on_dev else 0, int(mode),
+                                  ctypes.byref(info))
+        if rc not in (SWC_OK, SWC_NOT_SPD):
+            _check(rc)
+        return int(info.value)
+
+    def transfer_bytes(self):
+        """(host-to-device, device-to-host) bytes of the last factor / get_L call."""
+        sz = np.zeros(6, np.int64)
+        _check(self._lib.swc_sizes(self._h, _p(sz)))
+        return int(sz[4]), int(sz[5])
+
+    def profile(self, values):
+        """One factorization with per-kernel-class event timing.  Returns a dict
+        class -> (launches, ms, algorithmic flops, algorithmic bytes)."""
+        on_dev = hasattr(values, "data_ptr")
+        if not on_dev:
+            values = _c(values, np.float64)
+        k = len(KERNEL_CLASSES)
+        la = np.zeros(k, np.int32)
+        ms, fl, by = np.zeros(k), np.zeros(k), np.zeros(k)
+        info = ctypes.c_int(0)
+        rc = self._lib.swc_profile(self._h, _p(values), 1 if on_dev else 0, ctypes.byref(info),
+                                   _p(la), _p(ms), _p(fl), _p(by))
+        if rc not in (SWC_OK, SWC_NOT_SPD):
+            _check(rc)
+        return {name: (int(la[i]), float(ms[i]), float(fl[i]), float(by[i]))
+                for i, name in enumerate(KERNEL_CLASSES)}
+
+    def get_L(self, out=None):
+        """L in the reference layout: into ``out`` (numpy or CUDA tensor) or a new numpy array."""
+        if out is None:
+            out = np.zeros(self.xsize, np.float64)
+        _check(self._lib.swc_get_L(self._h, _p(out), 1 if hasattr(out, "data_ptr") else 0))
+        return out
+
+    def device_L_ptr(self) -> int:
+        return int(self._lib.swc_device_L(self._h) or 0)

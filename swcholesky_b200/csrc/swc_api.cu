@@ -1,0 +1,222 @@
+// C ABI of libswchol_b200 (declared in include/swcholesky_b200.h).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/swcholesky_b200.h"
+#include "swc_engine.h"
+
+struct swc_handle {
+  std::unique_ptr<swc::Engine> eng;
+  int device = 0;
+  bool analyzed = false;
+  bool factored = false;
+};
+
+namespace {
+
+thread_local std::string g_err;
+int g_last_info = 0;
+std::mutex g_default_mu;
+swc_handle *g_default = nullptr;
+
+int fail(int code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+
+std::vector<int64_t> to_i64(const size_t *p, int count) {
+  std::vector<int64_t> v(count);
+  for (int i = 0; i < count; ++i) v[i] = (int64_t)p[i];
+  return v;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *swc_last_error(void) { return g_err.c_str(); }
+int swc_last_info(void) { return g_last_info; }
+
+int swc_create(swc_handle_t *handle, int device) {
+  if (!handle) return fail(SWC_INVALID_INPUT, "null handle pointer");
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0)
+    return fail(SWC_CUDA_ERROR, std::string("no CUDA device: ") + cudaGetErrorString(e));
+  if (device < 0 || device >= ndev) return fail(SWC_INVALID_INPUT, "device out of range");
+  swc_handle *h = new swc_handle;
+  h->device = device;
+  h->eng.reset(new swc::Engine(device));
+  *handle = h;
+  return SWC_OK;
+}
+
+int swc_destroy(swc_handle_t handle) {
+  delete handle;
+  return SWC_OK;
+}
+
+int swc_set_stream(swc_handle_t h, void *stream) {
+  if (!h) return fail(SWC_INVALID_INPUT, "null handle");
+  h->eng->set_stream((cudaStream_t)stream);
+  return SWC_OK;
+}
+
+void *swc_get_stream(swc_handle_t h) { return h ? (void *)h->eng->stream() : nullptr; }
+
+int swc_analyze(swc_handle_t h, int n, const int *c, const int *r, const size_t *lC,
+                const int *Ls, const size_t *Li_ptr, const int *blockSet, int supNo,
+                const int *prunePtr, const int *pruneSet, int nLevels, const int *levelPtr,
+                const int *parPtr, const int *partition) {
+  if (!h) return fail(SWC_INVALID_INPUT, "null handle");
+  if (n <= 0 || !lC || !Li_ptr) return fail(SWC_INVALID_INPUT, "null or empty symbolic input");
+  // The H-level schedule, when given, must cover every supernode exactly once.
+  if (levelPtr && parPtr && partition && nLevels > 0) {
+    int nparts = levelPtr[nLevels];
+    if (levelPtr[0] != 0 || nparts < 0 || parPtr[0] != 0 || parPtr[nparts] != supNo)
+      return fail(SWC_INVALID_INPUT, "H-level schedule does not cover the supernodes");
+    std::vector<char> seen(supNo, 0);
+    for (int k = 0; k < supNo; ++k) {
+      int s = partition[k];
+      if (s < 0 || s >= supNo || seen[s]) return fail(SWC_INVALID_INPUT, "partition is not a permutation");
+      seen[s] = 1;
+    }
+  }
+  std::vector<int64_t> lc = to_i64(lC, n + 1), lip = to_i64(Li_ptr, n + 1);
+  std::string err;
+  h->analyzed = false;
+  h->factored = false;
+  if (!h->eng->analyze(n, c, r, lc.data(), Ls, lip.data(), blockSet, supNo, prunePtr, pruneSet, err))
+    return fail(err.rfind("device", 0) == 0 ? SWC_CUDA_ERROR : SWC_INVALID_INPUT, err);
+  h->analyzed = true;
+  return SWC_OK;
+}
+
+int swc_factor(swc_handle_t h, const double *values, int values_on_device, int mode, int *info) {
+  if (!h) return fail(SWC_INVALID_INPUT, "null handle");
+  if (!h->analyzed) return fail(SWC_NOT_READY, "factor before analyze");
+  if (mode != SWC_MODE_FP64) return fail(SWC_INVALID_INPUT, "unknown factorization mode");
+  if (!values) return fail(SWC_INVALID_INPUT, "null values");
+  std::string err;
+  int lin = 0;
+  int rc = h->eng->factor(values, values_on_device != 0, &lin, err);
+  if (info) *info = lin;
+  if (rc == 0) {
+    h->factored = true;
+    return SWC_OK;
+  }
+  h->factored = (rc == 1);
+  if (rc == 1) return fail(SWC_NOT_SPD, err);
+  if (rc == -2) return fail(SWC_STRUCTURE_ERROR, err);
+  return fail(SWC_CUDA_ERROR, err);
+}
+
+int swc_get_L(swc_handle_t h, double *lValues, int to_device) {
+  if (!h) return fail(SWC_INVALID_INPUT, "null handle");
+  if (!h->analyzed) return fail(SWC_NOT_READY, "no factor");
+  std::string err;
+  if (!h->eng->download(lValues, to_device != 0, err)) return fail(SWC_CUDA_ERROR, err);
+  return SWC_OK;
+}
+
+const double *swc_device_L(swc_handle_t h) { return h ? h->eng->device_L() : nullptr; }
+
+int swc_sizes(swc_handle_t h, long long *sizes) {
+  if (!h || !sizes) return fail(SWC_INVALID_INPUT, "null argument");
+  sizes[0] = h->eng->n();
+  sizes[1] = h->eng->nsuper();
+  sizes[2] = h->eng->xsize();
+  sizes[3] = h->eng->launches_per_factor();
+  sizes[4] = h->eng->h2d_bytes();
+  sizes[5] = h->eng->d2h_bytes();
+  return SWC_OK;
+}
+
+int swc_profile(swc_handle_t h, const double *values, int values_on_device, int *info,
+                int *launches, double *ms, double *flops, double *bytes) {
+  if (!h) return fail(SWC_INVALID_INPUT, "null handle");
+  if (!h->analyzed) return fail(SWC_NOT_READY, "profile before analyze");
+  if (!values) return fail(SWC_INVALID_INPUT, "null values");
+  swc::KernelStats ks;
+  std::string err;
+  int lin = 0;
+  int rc = h->eng->factor_profiled(values, values_on_device != 0, &lin, ks, err);
+  if (info) *info = lin;
+  for (int k = 0; k < swc::K_NKINDS; ++k) {
+    if (launches) launches[k] = ks.launches[k];
+    if (ms) ms[k] = ks.ms[k];
+    if (flops) flops[k] = ks.flops[k];
+    if (bytes) bytes[k] = ks.bytes[k];
+  }
+  if (rc == 0) return SWC_OK;
+  if (rc == 1) return fail(SWC_NOT_SPD, err);
+  if (rc == -2) return fail(SWC_STRUCTURE_ERROR, err);
+  return fail(SWC_CUDA_ERROR, err);
+}
+
+int sw_cholesky_left_par_05(int n, int *c, int *r, double *values, size_t *lC, int *Ls,
+                            size_t *Li_ptr, double *lValues, int *blockSet, int supNo,
+                            double *timing, int *prunePtr, int *pruneSet, int nLevels,
+                            int *levelPtr, int *levelSet, int nPar, int *parPtr,
+                            int *partition, int chunk, int threads, int super_max,
+                            int col_max, double *nodCost) {
+  (void)timing; (void)levelSet; (void)nPar; (void)chunk; (void)threads;
+  (void)super_max; (void)col_max; (void)nodCost;
+  std::lock_guard<std::mutex> lock(g_default_mu);
+  g_last_info = 0;
+  if (!g_default) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    swc_handle_t h = nullptr;
+    if (swc_create(&h, dev) != SWC_OK) return 0;
+    g_default = h;
+  }
+  if (swc_analyze(g_default, n, c, r, lC, Ls, Li_ptr, blockSet, supNo, prunePtr, pruneSet,
+                  nLevels, levelPtr, parPtr, partition) != SWC_OK)
+    return 0;
+  int info = 0;
+  int rc = swc_factor(g_default, values, 0, SWC_MODE_FP64, &info);
+  g_last_info = info;
+  if (rc != SWC_OK && rc != SWC_NOT_SPD) return 0;
+  if (swc_get_L(g_default, lValues, 0) != SWC_OK) return 0;
+  return rc == SWC_OK ? 1 : 0;
+}
+
+int swc_layout_sizes(int n, const int *c, const int *r, const int *blockSet, int supNo,
+                     long long *sizes) {
+  swc::Layout L;
+  std::string err;
+  if (!sizes) return fail(SWC_INVALID_INPUT, "null sizes");
+  if (!swc::build_layout(n, c, r, blockSet, supNo, L, err)) return fail(SWC_INVALID_INPUT, err);
+  sizes[0] = (long long)L.Ls.size();
+  sizes[1] = (long long)L.pruneSet.size();
+  sizes[2] = (long long)L.xsize;
+  sizes[3] = (long long)(L.levelPtr.size() - 1);
+  return SWC_OK;
+}
+
+int swc_layout(int n, const int *c, const int *r, const int *blockSet, int supNo,
+               size_t *lC, int *Ls, size_t *Li_ptr, int *sparent, int *prunePtr,
+               int *pruneSet, int *levelPtr, int *parPtr, int *partition) {
+  swc::Layout L;
+  std::string err;
+  if (!swc::build_layout(n, c, r, blockSet, supNo, L, err)) return fail(SWC_INVALID_INPUT, err);
+  if (lC) for (int j = 0; j <= n; ++j) lC[j] = (size_t)L.lC[j];
+  if (Li_ptr) for (int j = 0; j <= n; ++j) Li_ptr[j] = (size_t)L.Li_ptr[j];
+  if (Ls) std::memcpy(Ls, L.Ls.data(), sizeof(int) * L.Ls.size());
+  if (sparent) std::memcpy(sparent, L.sparent.data(), sizeof(int) * supNo);
+  if (prunePtr) std::memcpy(prunePtr, L.prunePtr.data(), sizeof(int) * (supNo + 1));
+  if (pruneSet) std::memcpy(pruneSet, L.pruneSet.data(), sizeof(int) * L.pruneSet.size());
+  if (levelPtr) std::memcpy(levelPtr, L.levelPtr.data(), sizeof(int) * L.levelPtr.size());
+  if (parPtr) std::memcpy(parPtr, L.parPtr.data(), sizeof(int) * L.parPtr.size());
+  if (partition) std::memcpy(partition, L.partition.data(), sizeof(int) * L.partition.size());
+  return SWC_OK;
+}
+
+}  // extern "C"

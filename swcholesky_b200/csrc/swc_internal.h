@@ -1,0 +1,36 @@
+// Internal declarations shared by the host code and the CUDA kernels of libswchol_b200.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace swc {
+
+// Supernodal layout in the reference's BCSC conventions plus derived schedule arrays.
+struct Layout {
+  int n = 0, nsuper = 0;
+  int64_t xsize = 0;
+  std::vector<int64_t> rowptr;   // per supernode: start of its row list in Ls (nsuper+1)
+  std::vector<int> Ls;           // row lists
+  std::vector<int64_t> Li_ptr;   // per column (n+1)
+  std::vector<int64_t> lC;       // per column (n+1)
+  std::vector<int> sparent;      // supernodal etree, -1 = root
+  std::vector<int> prunePtr, pruneSet;
+  std::vector<int> levelPtr, parPtr, partition;
+};
+
+bool build_layout(int n, const int *c, const int *r, const int *blockSet, int supNo,
+                  Layout &out, std::string &err);
+
+// Tile edge used by every tiled kernel.
+constexpr int TB = 64;
+
+// Size classes of the executor (the B200 counterpart of the reference's triple queue,
+// cholesky/tripleQueue.c:17-170): a supernode whose whole panel fits in shared memory is
+// factored by one CTA, updates included; every other supernode goes through the tiled
+// path (tile-owner updates, then a blocked right-looking dense factorization).
+constexpr int SMALL_MAX_W = 64;
+constexpr int SMALL_MAX_ELEMS = 12288;  // panel doubles held in shared memory (96 KB)
+constexpr int SMALL_MAX_M = 2048;
+
+}  // namespace swc

@@ -1,0 +1,99 @@
+"""Named workloads and their assembly into the numeric-phase inputs.
+
+Each workload is a seeded synthetic SPD matrix plus the geometric nested-dissection user
+permutation for it.  They stand in for the reference's SuiteSparse inputs, which it does
+not ship:
+
+=============  ===========================================================================
+grid2d_100     2D 5-point Laplacian, 100 x 100, Dirichlet (n = 10,000)
+grid3d_60      3D 7-point Laplacian, 60^3, diagonal shift 1e-3 (n = 216,000)
+stencil27_40   3-dof 27-point weighted stencil, 40^3 (n = 192,000), shift for cond ~ 1e6
+stencil27_40c10  the same operator with the shift for cond ~ 1e10
+gmrf_500       GMRF precision 0.1 I + weighted 5-point Laplacian, 500 x 500 (n = 250,000)
+grid2d_20, grid3d_8, stencil27_4   small cases of the same families, for tests
+=============  ===========================================================================
+
+``assemble(A, perm, super)`` turns a matrix, the final permutation and a supernode
+partition (what the reference's symbolic phase produces) into every array the numeric
+entry point takes, using the library's layout builder.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import matrices as M
+
+__all__ = ["build", "assemble", "Problem", "cond_shift"]
+
+
+def cond_shift(L: M.LowerCSC, cond: float) -> float:
+    """Diagonal shift giving cond(L + shift*I) = cond for a singular PSD graph Laplacian L
+    (lambda_min = 0), from a Lanczos estimate of lambda_max."""
+    import scipy.sparse.linalg as sla
+    lmax = float(sla.eigsh(L.to_scipy_full(), k=1, which="LA", return_eigenvectors=False,
+                           tol=1e-6)[0])
+    return lmax / (cond - 1.0)
+
+
+def build(name: str):
+    """Returns (A as LowerCSC in the original order, user permutation, meta dict)."""
+    if name.startswith("grid2d_"):
+        k = int(name.split("_")[1])
+        return M.laplacian_2d(k), M.nested_dissection((k, k)), dict(kind="laplacian2d", k=k)
+    if name.startswith("grid3d_"):
+        k = int(name.split("_")[1])
+        shift = 1e-3
+        return (M.laplacian_3d(k, shift), M.nested_dissection((k, k, k)),
+                dict(kind="laplacian3d", k=k, shift=shift))
+    if name.startswith("stencil27_"):
+        tag = name.split("_")[1]
+        cond = 1e10 if tag.endswith("c10") else 1e6
+        k = int(tag.replace("c10", ""))
+        L0 = M.stencil27_3dof(k, sigma=1.0, shift=0.0, seed=0)
+        shift = cond_shift(L0, cond)
+        A = M.stencil27_3dof(k, sigma=1.0, shift=shift, seed=0)
+        return A, M.nested_dissection((k, k, k), dof=3), dict(kind="stencil27x3", k=k,
+                                                                   cond=cond, shift=shift)
+    if name.startswith("gmrf_"):
+        k = int(name.split("_")[1])
+        A = M.weighted_grid_2d(k, sigma=0.7, shift=0.1, seed=0)
+        return A, M.nested_dissection((k, k)), dict(kind="gmrf", k=k, kappa2=0.1)
+    raise KeyError(name)
+
+
+@dataclass
+class Problem:
+    n: int
+    A2p: np.ndarray
+    A2i: np.ndarray
+    A2x: np.ndarray
+    super: np.ndarray
+    lC: np.ndarray
+    Ls: np.ndarray
+    Li_ptr: np.ndarray
+    sparent: np.ndarray
+    prunePtr: np.ndarray
+    pruneSet: np.ndarray
+    levelPtr: np.ndarray
+    parPtr: np.ndarray
+    partition: np.ndarray
+    xsize: int
+    perm: np.ndarray
+
+    @property
+    def nsuper(self) -> int:
+        return int(self.super.size - 1)
+
+
+def assemble(A: M.LowerCSC, perm, super_) -> Problem:
+    from . import layout
+    perm = np.asarray(perm)
+    A2 = M.permute_lower(A, perm)
+    lay = layout(A2.n, A2.indptr, A2.indices, super_)
+    return Problem(n=A2.n, A2p=A2.indptr, A2i=A2.indices, A2x=A2.data,
+                   super=np.ascontiguousarray(super_, np.int32), lC=lay["lC"], Ls=lay["Ls"],
+                   Li_ptr=lay["Li_ptr"], sparent=lay["sparent"], prunePtr=lay["prunePtr"],
+                   pruneSet=lay["pruneSet"], levelPtr=lay["levelPtr"], parPtr=lay["parPtr"],
+                   partition=lay["partition"], xsize=int(lay["xsize"]), perm=perm)

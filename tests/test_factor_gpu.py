@@ -1,0 +1,148 @@
+"""GPU parity of the FP64 numeric factorization against the reference's factor (golden
+vectors) and against the oracle, through the C ABI.
+
+Tolerance: the north-star bar for FP64, max |L_gpu - L_ref| <= 1e-12 * max |L_ref|, plus the
+backward error ||Ax - b|| / (||A|| ||x||) <= 1e-13 on the seeded right-hand side."""
+import numpy as np
+import pytest
+
+from conftest import SMALL_CASES, load_small, load_sym
+import swcholesky_b200 as swc
+from swcholesky_b200 import workloads as W
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+RTOL_L = 1e-12
+
+
+def rel_diff(a, b):
+    return float(np.abs(a - b).max() / np.abs(b).max())
+
+
+def backward_error(n, A2p, A2i, A2x, x, b):
+    r = O.oracle_symv(n, A2p, A2i, A2x, x) - b
+    # ||A||_inf of the symmetric matrix from its lower triangle
+    rowsum = np.zeros(n)
+    cols = np.repeat(np.arange(n), np.diff(A2p))
+    np.add.at(rowsum, A2i, np.abs(A2x))
+    off = A2i != cols
+    np.add.at(rowsum, cols[off], np.abs(A2x[off]))
+    return float(np.abs(r).max() / (rowsum.max() * np.abs(x).max()))
+
+
+def dropin(g, values=None, prune=None):
+    n = int(g["n"])
+    L = np.zeros(g["L"].size if "L" in g else int(g["xsize"]), np.float64)
+    pp, ps = prune if prune is not None else (g["prunePtr"], g["pruneSet"])
+    ret = swc.sw_cholesky_left_par_05(
+        n, g["A2p"], g["A2i"], g["A2x"] if values is None else values, g["lC"], g["Ls"],
+        g["Li_ptr"], L, g["super"], g["super"].size - 1, None, pp, ps,
+        g["levelPtr"].size - 1, g["levelPtr"], None, 0, g["parPtr"], g["partition"], 0, 1,
+        int(g["maxSupWid"]) + 1, int(g["maxCol"]) + 1, None)
+    return ret, L
+
+
+@pytest.mark.parametrize("name", SMALL_CASES)
+def test_dropin_matches_reference_factor(cuda_ok, name):
+    g = load_small(name)
+    ret, L = dropin(g)
+    assert ret == 1
+    assert rel_diff(L, g["L"]) <= RTOL_L
+    # every entry the reference leaves at zero (upper triangles of diagonal blocks) is zero
+    assert np.all(L[g["L"] == 0.0] == 0.0)
+    n = int(g["n"])
+    x = O.oracle_solve(n, g["lC"], g["Ls"], g["Li_ptr"], L, g["super"], g["b"])
+    assert backward_error(n, g["A2p"], g["A2i"], g["A2x"], x, g["b"]) <= 1e-13
+
+
+def test_handle_device_values_and_determinism(cuda_ok):
+    import torch
+    g = load_small("grid2d_100")
+    h = swc.Handle(0)
+    h.analyze(int(g["n"]), g["A2p"], g["A2i"], g["lC"], g["Ls"], g["Li_ptr"], g["super"],
+              g["prunePtr"], g["pruneSet"], g["levelPtr"], g["parPtr"], g["partition"])
+    vals = torch.from_numpy(g["A2x"]).cuda()
+    assert h.factor(vals) == 0
+    L1 = h.get_L()
+    out = torch.zeros(h.xsize, dtype=torch.float64, device="cuda")
+    assert h.factor(g["A2x"]) == 0
+    h.get_L(out)
+    L2 = out.cpu().numpy()
+    assert np.array_equal(L1, L2), "factorization must be deterministic"
+    assert rel_diff(L1, g["L"]) <= RTOL_L
+
+
+@pytest.mark.parametrize("name", ["grid3d_24", "stencil27_12"])
+def test_tiled_path_matches_oracle(cuda_ok, name):
+    """Wide supernodes (several 64-column blocks, partial last block) against the oracle."""
+    gs = load_sym(name)
+    A, _, _ = W.build(name)
+    P = W.assemble(A, gs["perm"], gs["super"])
+    Lo, ok, info = O.oracle_factor(P.n, P.A2p, P.A2i, P.A2x, P.lC, P.Ls, P.Li_ptr, P.super,
+                                   P.prunePtr, P.pruneSet, P.levelPtr, P.parPtr, P.partition,
+                                   P.xsize)
+    assert ok == 1
+    h = swc.Handle(0)
+    h.analyze(P.n, P.A2p, P.A2i, P.lC, P.Ls, P.Li_ptr, P.super, P.prunePtr, P.pruneSet)
+    assert h.factor(P.A2x) == 0
+    L = h.get_L()
+    assert rel_diff(L, Lo) <= RTOL_L
+    assert np.all(L[Lo == 0.0] == 0.0)
+
+
+def test_not_spd_reports_failing_column(cuda_ok):
+    g = load_small("grid2d_100")
+    vals = g["A2x"].copy()
+    col = 4321
+    p = g["A2p"][col]
+    assert g["A2i"][p] == col
+    vals[p] = -5.0
+    _, ok, info_o = O.oracle_factor(int(g["n"]), g["A2p"], g["A2i"], vals, g["lC"], g["Ls"],
+                                    g["Li_ptr"], g["super"], g["prunePtr"], g["pruneSet"],
+                                    g["levelPtr"], g["parPtr"], g["partition"], g["L"].size)
+    ret, _ = dropin(g, values=vals)
+    assert ret == 0 and ok == 0
+    assert swc.last_info() == info_o == col + 1
+
+
+def test_invalid_prune_set_rejected(cuda_ok):
+    g = load_small("grid2d_20")
+    ps = g["pruneSet"].copy()
+    ps[0] = g["super"].size + 5   # out of range
+    ret, _ = dropin(g, prune=(g["prunePtr"], ps))
+    assert ret == 0
+    assert "pruneSet" in swc.lib().swc_last_error().decode()
+
+
+def test_structure_mismatch_flagged(cuda_ok):
+    """A matrix entry outside the supernodal pattern is reported, not written out of bounds."""
+    g = load_small("grid2d_20")
+    h = swc.Handle(0)
+    A2i = g["A2i"].copy()
+    # move one off-diagonal entry of column 0 to a row outside its supernode's pattern
+    rows0 = set(g["Ls"][g["Li_ptr"][0]:g["Li_ptr"][1]].tolist())
+    cand = [i for i in range(int(g["n"])) if i not in rows0 and i > 0]
+    p = g["A2p"][0] + 1
+    A2i[p] = cand[-1]
+    h.analyze(int(g["n"]), g["A2p"], A2i, g["lC"], g["Ls"], g["Li_ptr"], g["super"],
+              g["prunePtr"], g["pruneSet"])
+    with pytest.raises(swc.SWCError) as e:
+        h.factor(g["A2x"])
+    assert e.value.code == swc.SWC_STRUCTURE_ERROR
+
+
+def test_full_size_grid3d_60_backward_error(cuda_ok):
+    """The benchmark workload at full size: size-independent checks (backward error of the
+    solve with the GPU factor; symmetric-positive diagonal)."""
+    gs = load_sym("grid3d_60")
+    A, _, _ = W.build("grid3d_60")
+    P = W.assemble(A, gs["perm"], gs["super"])
+    h = swc.Handle(0)
+    h.analyze(P.n, P.A2p, P.A2i, P.lC, P.Ls, P.Li_ptr, P.super, P.prunePtr, P.pruneSet)
+    assert h.factor(P.A2x) == 0
+    L = h.get_L()
+    assert np.isfinite(L).all()
+    b = np.random.default_rng(0).standard_normal(P.n)
+    x = O.oracle_solve(P.n, P.lC, P.Ls, P.Li_ptr, L, P.super, b)
+    assert backward_error(P.n, P.A2p, P.A2i, P.A2x, x, b) <= 1e-13
