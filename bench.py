@@ -223,7 +223,7 @@ def run_ours(args, rank, world, local_rank):
 
     # ---- end to end through the reference-facing C-ABI call, host buffers ----
     e2e = None
-    if rank == 0:
+    if rank == 0 and not args.no_e2e:
         L_host = np.zeros(P.xsize, np.float64)
         e2e_steps = max(1, min(3, args.steps))
         t_e2e = []
@@ -298,6 +298,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="grid3d_60")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -69,7 +69,7 @@ def lib() -> ctypes.CDLL:
         L.swc_set_stream.argtypes = [_VP, _VP]
         L.swc_get_stream.restype = _VP
         L.swc_get_stream.argtypes = [_VP]
-        L.swc_analyze.argtypes = [_VP, _I] + [_VP] * 7 + [_I] + [_VP] * 2 + [_I] + [_VP] * 3
+        L.swc_analyze.argtypes = [_VP, _I] + [_VP] * 6 + [_I] + [_VP] * 2 + [_I] + [_VP] * 3
         L.swc_factor.argtypes = [_VP, _VP, _I, _I, ctypes.POINTER(_I)]
         L.swc_get_L.argtypes = [_VP, _VP, _I]
         L.swc_device_L.restype = _VP

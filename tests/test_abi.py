@@ -34,3 +34,21 @@ def test_create_without_gpu_fails_cleanly():
     with pytest.raises(swc.SWCError) as e:
         swc.Handle(0)
     assert e.value.code == swc.SWC_CUDA_ERROR
+
+
+def test_null_handle_calls_fail_cleanly():
+    """Every handle entry point rejects a NULL handle with SWC_INVALID_INPUT (this also
+    checks that the Python argument lists match the C signatures)."""
+    import ctypes
+    L = swc.lib()
+    info = ctypes.c_int(0)
+    assert L.swc_analyze(None, 10, None, None, None, None, None, None, 1, None, None, 0,
+                         None, None, None) == swc.SWC_INVALID_INPUT
+    assert L.swc_factor(None, None, 0, 0, ctypes.byref(info)) == swc.SWC_INVALID_INPUT
+    assert L.swc_get_L(None, None, 0) == swc.SWC_INVALID_INPUT
+    assert L.swc_sizes(None, None) == swc.SWC_INVALID_INPUT
+    assert L.swc_set_stream(None, None) == swc.SWC_INVALID_INPUT
+    assert L.swc_profile(None, None, 0, ctypes.byref(info), None, None, None, None) == \
+        swc.SWC_INVALID_INPUT
+    assert L.swc_get_stream(None) is None
+    assert L.swc_device_L(None) is None
