@@ -84,6 +84,23 @@ int swc_factor(swc_handle_t handle, const double *values, int values_on_device, 
 /* Copies L (xsize doubles, reference layout) to host (to_device == 0) or device memory. */
 int swc_get_L(swc_handle_t handle, double *lValues, int to_device);
 
+/* x = (L L^T)^{-1} b with the handle's factor, in the factor's (permuted) ordering, for
+ * nrhs right-hand sides stored column by column (leading dimension n).  on_device != 0: b
+ * and x are device pointers on the handle's GPU.  Supernodal forward and backward solves,
+ * level by level; the forward solve is the reference's blockedLsolve
+ * (triangularSolve/Triangular_BCSC.h:14-48) in gather form; the backward solve has no
+ * reference counterpart. */
+int swc_solve(swc_handle_t handle, const double *b, double *x, int nrhs, int on_device);
+
+/* Solve with FP64 iterative refinement against A (the values of the last factor):
+ * x_{k+1} = x_k + (L L^T)^{-1} (b - A x_k) until the backward error
+ * ||b - A x||_inf / (||A||_inf ||x||_inf) <= tol for every right-hand side, at most maxit
+ * steps; when refinement stalls (two steps without halving the error) it falls back to
+ * conjugate gradients preconditioned with the factor.  berr (nrhs doubles), iterations and
+ * method (0 direct, 1 refinement, 2 CG) may be NULL.  No reference counterpart. */
+int swc_refine(swc_handle_t handle, const double *b, double *x, int nrhs, int on_device,
+               double tol, int maxit, double *berr, int *iterations, int *method);
+
 /* Device pointer to the handle's L (xsize doubles), valid until the next analyze. */
 const double *swc_device_L(swc_handle_t handle);
 
@@ -99,6 +116,16 @@ int swc_sizes(swc_handle_t handle, long long *sizes);
  * algorithmic flops and DRAM bytes of one factorization.  Any output may be NULL. */
 int swc_profile(swc_handle_t handle, const double *values, int values_on_device, int *info,
                 int *launches, double *ms, double *flops, double *bytes);
+
+/* Host-only: validates the structure (as swc_analyze does) and describes the execution
+ * plan without touching a GPU.  stats[0..19] = levels, kernel launches per factorization,
+ * small-class supernodes, tiled-class supernodes, update tiles, update (tile, descendant)
+ * pairs, TRSM tiles, SYRK tiles, then per kernel class (memset, small, assemble, update,
+ * panel, syrk) the algorithmic flops [8..13] and DRAM bytes [14..19] of one
+ * factorization.  No reference counterpart. */
+int swc_plan_stats(int n, const int *c, const int *r, const size_t *lC, const int *Ls,
+                   const size_t *Li_ptr, const int *blockSet, int supNo, const int *prunePtr,
+                   const int *pruneSet, double *stats);
 
 /* ---- host layout builder ---------------------------------------------------------
  * Builds the BCSC layout the reference's analyze_p2 produces for a given supernode

@@ -37,7 +37,8 @@ SWC_MODE_FP64 = 0
 EXPORTS = (
     "sw_cholesky_left_par_05", "swc_last_info", "swc_last_error", "swc_create", "swc_destroy",
     "swc_set_stream", "swc_get_stream", "swc_analyze", "swc_factor", "swc_get_L",
-    "swc_device_L", "swc_sizes", "swc_profile", "swc_layout_sizes", "swc_layout",
+    "swc_device_L", "swc_sizes", "swc_profile", "swc_plan_stats", "swc_layout_sizes",
+    "swc_layout", "swc_solve", "swc_refine",
 )
 KERNEL_CLASSES = ("memset", "small", "assemble", "update", "panel", "syrk")
 
@@ -76,6 +77,10 @@ def lib() -> ctypes.CDLL:
         L.swc_device_L.argtypes = [_VP]
         L.swc_sizes.argtypes = [_VP, _VP]
         L.swc_profile.argtypes = [_VP, _VP, _I, ctypes.POINTER(_I), _VP, _VP, _VP, _VP]
+        L.swc_solve.argtypes = [_VP, _VP, _VP, _I, _I]
+        L.swc_refine.argtypes = [_VP, _VP, _VP, _I, _I, ctypes.c_double, _I, _VP,
+                                 ctypes.POINTER(_I), ctypes.POINTER(_I)]
+        L.swc_plan_stats.argtypes = [_I] + [_VP] * 6 + [_I] + [_VP] * 3
         L.swc_layout_sizes.argtypes = [_I] + [_VP] * 3 + [_I, _VP]
         L.swc_layout.argtypes = [_I] + [_VP] * 3 + [_I] + [_VP] * 9
         _lib = L
@@ -145,6 +150,27 @@ def layout(n, c, r, blockSet):
         "lC", "Ls", "Li_ptr", "sparent", "prunePtr", "pruneSet", "levelPtr", "parPtr",
         "partition")]))
     out["xsize"] = xsize
+    return out
+
+
+PLAN_FIELDS = ("levels", "launches", "small", "tiled", "update_tiles", "update_pairs",
+               "trsm_tiles", "syrk_tiles")
+
+
+def plan_stats(n, c, r, lC, Ls, Li_ptr, blockSet, prunePtr, pruneSet):
+    """Execution plan of a structure, computed on the host (no GPU needed): counts and the
+    algorithmic flops / bytes per kernel class."""
+    st = np.zeros(8 + 2 * len(KERNEL_CLASSES))
+    args = [_c(c, np.int32), _c(r, np.int32), _c(lC, np.uint64), _c(Ls, np.int32),
+            _c(Li_ptr, np.uint64), _c(blockSet, np.int32), _c(prunePtr, np.int32),
+            _c(pruneSet, np.int32)]
+    _check(lib().swc_plan_stats(int(n), _p(args[0]), _p(args[1]), _p(args[2]), _p(args[3]),
+                                _p(args[4]), _p(args[5]), args[5].size - 1, _p(args[6]),
+                                _p(args[7]), _p(st)))
+    out = {k: int(st[i]) for i, k in enumerate(PLAN_FIELDS)}
+    k = len(KERNEL_CLASSES)
+    out["flops"] = {name: float(st[8 + i]) for i, name in enumerate(KERNEL_CLASSES)}
+    out["bytes"] = {name: float(st[8 + k + i]) for i, name in enumerate(KERNEL_CLASSES)}
     return out
 
 
@@ -231,6 +257,39 @@ class Handle:
             _check(rc)
         return {name: (int(la[i]), float(ms[i]), float(fl[i]), float(by[i]))
                 for i, name in enumerate(KERNEL_CLASSES)}
+
+    def solve(self, b, out=None):
+        """x = (L L^T)^{-1} b in the factor's ordering; b is (n,) or (n, nrhs) numpy, or a
+        CUDA tensor (column-major for several right-hand sides: shape (nrhs, n))."""
+        on_dev = hasattr(b, "data_ptr")
+        if on_dev:
+            nrhs = 1 if b.dim() == 1 else b.shape[0]
+            x = out if out is not None else b.clone()
+        else:
+            b = np.asarray(b, np.float64)
+            nrhs = 1 if b.ndim == 1 else b.shape[1]
+            b = np.asfortranarray(b)
+            x = np.zeros_like(b, order="F")
+        _check(self._lib.swc_solve(self._h, _p(b), _p(x), int(nrhs), 1 if on_dev else 0))
+        return x
+
+    def refine(self, b, tol: float = 1e-14, maxit: int = 30, out=None):
+        """Refined solve (see swc_refine).  Returns (x, berr per rhs, iterations, method)."""
+        on_dev = hasattr(b, "data_ptr")
+        if on_dev:
+            nrhs = 1 if b.dim() == 1 else b.shape[0]
+            x = out if out is not None else b.clone()
+        else:
+            b = np.asarray(b, np.float64)
+            nrhs = 1 if b.ndim == 1 else b.shape[1]
+            b = np.asfortranarray(b)
+            x = np.zeros_like(b, order="F")
+        berr = np.zeros(nrhs)
+        it, meth = ctypes.c_int(0), ctypes.c_int(0)
+        _check(self._lib.swc_refine(self._h, _p(b), _p(x), int(nrhs), 1 if on_dev else 0,
+                                    float(tol), int(maxit), _p(berr), ctypes.byref(it),
+                                    ctypes.byref(meth)))
+        return x, berr, int(it.value), int(meth.value)
 
     def get_L(self, out=None):
         """L in the reference layout: into ``out`` (numpy or CUDA tensor) or a new numpy array."""

@@ -38,6 +38,30 @@ std::vector<int64_t> to_i64(const size_t *p, int count) {
 
 }  // namespace
 
+namespace {
+// Runs fn on device copies of host right-hand sides (and copies x back) when needed.
+template <typename F>
+int with_device_vectors(swc_handle_t h, const double *b, double *x, int nrhs, int on_device, F fn) {
+  const size_t bytes = sizeof(double) * (size_t)h->eng->n() * nrhs;
+  if (on_device) return fn(b, x);
+  double *db = nullptr, *dx = nullptr;
+  cudaError_t e = cudaMalloc(&db, bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&dx, bytes);
+  if (e == cudaSuccess) e = cudaMemcpy(db, b, bytes, cudaMemcpyHostToDevice);
+  int rc = SWC_CUDA_ERROR;
+  if (e == cudaSuccess) {
+    rc = fn(db, dx);
+    if (rc == SWC_OK && cudaMemcpy(x, dx, bytes, cudaMemcpyDeviceToHost) != cudaSuccess)
+      rc = fail(SWC_CUDA_ERROR, "copy of the solution to the host failed");
+  } else {
+    rc = fail(SWC_CUDA_ERROR, std::string("solve buffers: ") + cudaGetErrorString(e));
+  }
+  if (db) cudaFree(db);
+  if (dx) cudaFree(dx);
+  return rc;
+}
+}  // namespace
+
 extern "C" {
 
 const char *swc_last_error(void) { return g_err.c_str(); }
@@ -111,7 +135,7 @@ int swc_factor(swc_handle_t h, const double *values, int values_on_device, int m
     h->factored = true;
     return SWC_OK;
   }
-  h->factored = (rc == 1);
+  h->factored = false;
   if (rc == 1) return fail(SWC_NOT_SPD, err);
   if (rc == -2) return fail(SWC_STRUCTURE_ERROR, err);
   return fail(SWC_CUDA_ERROR, err);
@@ -126,6 +150,34 @@ int swc_get_L(swc_handle_t h, double *lValues, int to_device) {
 }
 
 const double *swc_device_L(swc_handle_t h) { return h ? h->eng->device_L() : nullptr; }
+
+
+int swc_solve(swc_handle_t h, const double *b, double *x, int nrhs, int on_device) {
+  if (!h) return fail(SWC_INVALID_INPUT, "null handle");
+  if (!h->factored) return fail(SWC_NOT_READY, "solve before a successful factor");
+  if (!b || !x || nrhs <= 0) return fail(SWC_INVALID_INPUT, "bad solve arguments");
+  return with_device_vectors(h, b, x, nrhs, on_device, [&](const double *db, double *dx) {
+    std::string err;
+    if (!h->eng->solve(db, dx, nrhs, err)) return fail(SWC_CUDA_ERROR, err);
+    return SWC_OK;
+  });
+}
+
+int swc_refine(swc_handle_t h, const double *b, double *x, int nrhs, int on_device, double tol,
+               int maxit, double *berr, int *iterations, int *method) {
+  if (!h) return fail(SWC_INVALID_INPUT, "null handle");
+  if (!h->factored) return fail(SWC_NOT_READY, "refine before a successful factor");
+  if (!b || !x || nrhs <= 0 || maxit < 0) return fail(SWC_INVALID_INPUT, "bad refine arguments");
+  return with_device_vectors(h, b, x, nrhs, on_device, [&](const double *db, double *dx) {
+    std::string err;
+    swc::RefineInfo info;
+    if (!h->eng->refine(db, dx, nrhs, tol, maxit, info, err)) return fail(SWC_CUDA_ERROR, err);
+    if (berr) for (int k = 0; k < nrhs; ++k) berr[k] = info.berr[k];
+    if (iterations) *iterations = info.iterations;
+    if (method) *method = info.method;
+    return SWC_OK;
+  });
+}
 
 int swc_sizes(swc_handle_t h, long long *sizes) {
   if (!h || !sizes) return fail(SWC_INVALID_INPUT, "null argument");
@@ -186,6 +238,32 @@ int sw_cholesky_left_par_05(int n, int *c, int *r, double *values, size_t *lC, i
   if (rc != SWC_OK && rc != SWC_NOT_SPD) return 0;
   if (swc_get_L(g_default, lValues, 0) != SWC_OK) return 0;
   return rc == SWC_OK ? 1 : 0;
+}
+
+int swc_plan_stats(int n, const int *c, const int *r, const size_t *lC, const int *Ls,
+                   const size_t *Li_ptr, const int *blockSet, int supNo, const int *prunePtr,
+                   const int *pruneSet, double *stats) {
+  if (n <= 0 || !lC || !Li_ptr || !stats) return fail(SWC_INVALID_INPUT, "null or empty input");
+  std::vector<int64_t> lc = to_i64(lC, n + 1), lip = to_i64(Li_ptr, n + 1);
+  swc::HostSym H;
+  swc::Plan P;
+  std::string err;
+  if (!swc::build_plan(n, c, r, lc.data(), Ls, lip.data(), blockSet, supNo, prunePtr, pruneSet,
+                       H, P, err))
+    return fail(SWC_INVALID_INPUT, err);
+  stats[0] = (double)P.waves.size();
+  stats[1] = (double)P.launches;
+  stats[2] = (double)P.small_list.size();
+  stats[3] = (double)P.big_list.size();
+  stats[4] = (double)P.upd_tasks.size();
+  stats[5] = (double)P.upd_pairs.size();
+  stats[6] = (double)P.panel_tasks.size();
+  stats[7] = (double)P.syrk_tasks.size();
+  for (int k = 0; k < swc::K_NKINDS; ++k) {
+    stats[8 + k] = P.work.flops[k];
+    stats[8 + swc::K_NKINDS + k] = P.work.bytes[k];
+  }
+  return SWC_OK;
 }
 
 int swc_layout_sizes(int n, const int *c, const int *r, const int *blockSet, int supNo,

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cstdlib>
 #include <cstring>
 
 #include "swc_engine.h"
@@ -29,25 +30,107 @@ bool small_class(int w, int64_t m) {
   return w <= SMALL_MAX_W && m <= SMALL_MAX_M && (int64_t)w * m <= SMALL_MAX_ELEMS;
 }
 
+// One update tile of the tiled class with the descendants that touch it.
+struct TileWork {
+  int4 task;                 // (s, r0, c0, first pair -- filled when flattened)
+  std::vector<int4> pairs;   // (d, a0, b0, na | nb << 16)
+  double flops = 0, bytes = 0;
+};
+
+// Splits every update d -> s of the prune set into the 64x64 tiles of s it touches.  The
+// rows of d at or below s's first column map monotonically into s's row list, so each
+// tile receives one contiguous run of d's rows for its row range and one for its column
+// range.  Appends one TileWork per touched tile (row-major tile order).
+bool build_update_pairs(int s, int f, int w, int m, const std::vector<int> &super,
+                        const std::vector<int64_t> &rowptr, const int *Ls, const int *prunePtr,
+                        const int *pruneSet, std::vector<TileWork> &out, std::string &err) {
+  const int ntr = (m + TB - 1) / TB, ntc = (w + TB - 1) / TB;
+  std::vector<int> tile_of((size_t)ntr * ntc, -1);
+  std::vector<TileWork> tiles;
+  const int *rows_s = Ls + rowptr[s];
+  std::vector<int> pos;
+  struct Run { int tile, start, count; };
+  std::vector<Run> runs;
+  for (int q = prunePtr[s]; q < prunePtr[s + 1]; ++q) {
+    const int d = pruneSet[q];
+    const int *rd = Ls + rowptr[d];
+    const int md = (int)(rowptr[d + 1] - rowptr[d]);
+    const int wd = super[d + 1] - super[d];
+    const int lb = (int)(std::lower_bound(rd, rd + md, f) - rd);
+    pos.clear();
+    int k = 0;
+    for (int i = lb; i < md; ++i) {
+      while (k < m && rows_s[k] < rd[i]) ++k;
+      if (k == m || rows_s[k] != rd[i]) {
+        err = "row structure of a descendant is not contained in its ancestor's";
+        return false;
+      }
+      pos.push_back(k);
+    }
+    runs.clear();
+    for (int i = 0; i < (int)pos.size(); ++i) {
+      const int tl = pos[i] / TB;
+      if (runs.empty() || runs.back().tile != tl) runs.push_back({tl, lb + i, 1});
+      else runs.back().count++;
+    }
+    for (const Run &cr : runs) {
+      if ((int64_t)cr.tile * TB >= w) break;   // column runs: positions < w only
+      int nb = 0;
+      for (int i = cr.start - lb; i < cr.start - lb + cr.count; ++i) nb += pos[i] < w;
+      if (nb == 0) continue;
+      for (const Run &rr : runs) {
+        if (rr.tile < cr.tile) continue;
+        const int key = rr.tile * ntc + cr.tile;
+        if (tile_of[key] < 0) {
+          tile_of[key] = (int)tiles.size();
+          TileWork tw;
+          tw.task = make_int4(s, rr.tile * TB, cr.tile * TB, 0);
+          tiles.push_back(std::move(tw));
+        }
+        TileWork &tw = tiles[tile_of[key]];
+        tw.pairs.push_back(make_int4(d, rr.start, cr.start, rr.count | (nb << 16)));
+        tw.flops += 2.0 * rr.count * nb * wd;
+        tw.bytes += 8.0 * (rr.count + nb) * wd;
+      }
+    }
+  }
+  for (TileWork &tw : tiles) {
+    tw.bytes += 16.0 * TB * TB;
+    out.push_back(std::move(tw));
+  }
+  return true;
+}
+
 }  // namespace
 
 Engine::Engine(int device) : device_(device) {
   cudaSetDevice(device_);
+  const char *ng = getenv("SWC_NO_GRAPH");
+  use_graph_ = !(ng && ng[0] == '1');
   cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking);
   stream_ = own_stream_;
+  cudaStreamCreateWithFlags(&aux_stream_, cudaStreamNonBlocking);
+  cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming);
   cudaMallocHost(&h_status_, 2 * sizeof(int));
 }
 
 Engine::~Engine() {
   release();
   if (h_status_) cudaFreeHost(h_status_);
+  if (h_norms_) cudaFreeHost(h_norms_);
   if (own_stream_) cudaStreamDestroy(own_stream_);
+  if (aux_stream_) cudaStreamDestroy(aux_stream_);
+  if (ev_fork_) cudaEventDestroy(ev_fork_);
+  if (ev_join_) cudaEventDestroy(ev_join_);
 }
 
 void Engine::release() {
   void *ptrs[] = {d_super_, d_Ls_, d_Ap_, d_Ai_, d_rowptr_, d_xptr_, d_upd_ptr_, d_upd_,
                   d_Ax_, dL_, d_status_, d_small_, d_big_, d_asm_, d_panel_, d_upd_tasks_,
-                  d_syrk_};
+                  d_syrk_, d_pairs_, d_upd_end_, d_dinv_, d_dinv_off_, d_diag_,
+                  d_slist_, d_scontrib_, d_sgather_, d_csr_rp_, d_csr_ci_, d_csr_map_,
+                  d_csr_val_, d_contrib_, d_work_, d_norms_};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   d_super_ = d_Ls_ = d_Ap_ = d_Ai_ = nullptr;
@@ -56,14 +139,25 @@ void Engine::release() {
   d_Ax_ = dL_ = nullptr;
   d_status_ = d_small_ = d_big_ = nullptr;
   d_asm_ = d_panel_ = nullptr;
-  d_upd_tasks_ = d_syrk_ = nullptr;
+  d_upd_tasks_ = d_syrk_ = d_pairs_ = nullptr;
+  d_upd_end_ = nullptr;
+  d_dinv_ = nullptr;
+  d_dinv_off_ = nullptr;
+  d_diag_ = nullptr;
+  d_slist_ = nullptr;
+  d_scontrib_ = d_sgather_ = nullptr;
+  d_csr_rp_ = d_csr_ci_ = d_csr_map_ = nullptr;
+  d_csr_val_ = d_contrib_ = d_work_ = d_norms_ = nullptr;
+  work_nrhs_ = 0;
+  if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+  if (graph_) cudaGraphDestroy(graph_);
+  graph_exec_ = nullptr;
+  graph_ = nullptr;
 }
 
-bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const int *Ls,
-                     const int64_t *Li_ptr, const int *blockSet, int supNo,
-                     const int *prunePtr, const int *pruneSet, std::string &err) {
-  cudaSetDevice(device_);
-  if (!kernels_configure(err)) return false;
+bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int *Ls,
+                const int64_t *Li_ptr, const int *blockSet, int supNo, const int *prunePtr,
+                const int *pruneSet, HostSym &H, Plan &P, std::string &err) {
   // ---- host-side validation of the symbolic arrays (no device work on bad input) ----
   if (n <= 0 || supNo <= 0 || !c || !r || !lC || !Ls || !Li_ptr || !blockSet || !prunePtr ||
       !pruneSet) {
@@ -134,11 +228,12 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
       if (level[pruneSet[q]] >= level[s]) { err = "prune set is not consistent with the etree"; return false; }
 
   // ---- plan ----
-  Plan P;
+  P = Plan();
   P.waves.resize(nlev);
   std::vector<std::vector<int>> by_level(nlev);
   for (int s = 0; s < supNo; ++s) by_level[level[s]].push_back(s);
   int launches = 2;
+  std::vector<TileWork> wave_tiles;
   for (int lv = 0; lv < nlev; ++lv) {
     Wave &W = P.waves[lv];
     W.small_off = (int)P.small_list.size();
@@ -150,7 +245,8 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
       int64_t m = rowptr[s + 1] - rowptr[s];
       if (small_class(w, m)) {
         P.small_list.push_back(s);
-        W.small_smem = std::max<int>(W.small_smem, (int)(8 * m * w + 8 * m));
+        // panel + rows + relative indices (+ padding to 8 bytes) + pivot column
+        W.small_smem = std::max<int>(W.small_smem, (int)(8 * m * w + 8 * m + 8 + 8 * w));
       } else {
         big.push_back(s);
       }
@@ -164,18 +260,30 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
       int f = super[s], w = super[s + 1] - f;
       int m = (int)(rowptr[s + 1] - rowptr[s]);
       for (int j = f; j < f + w; ++j) P.asm_tasks.push_back(make_int2(s, j));
-      if (prunePtr[s + 1] > prunePtr[s]) {
-        for (int c0 = 0; c0 < w; c0 += TB)
-          for (int r0 = 0; r0 < m; r0 += TB)
-            if (r0 + TB - 1 >= c0) P.upd_tasks.push_back(make_int4(s, r0, c0, 0));
-      }
+      if (prunePtr[s + 1] > prunePtr[s] &&
+          !build_update_pairs(s, f, w, m, super, rowptr, Ls, prunePtr, pruneSet, wave_tiles,
+                              err))
+        return false;
       maxnb = std::max(maxnb, (w + TB - 1) / TB);
     }
     W.asm_cnt = (int)P.asm_tasks.size() - W.asm_off;
+    // heaviest tiles first (shorter tail); ties keep supernode / tile order
+    std::stable_sort(wave_tiles.begin(), wave_tiles.end(),
+                     [](const TileWork &a, const TileWork &b) { return a.flops > b.flops; });
+    for (TileWork &tw : wave_tiles) {
+      tw.task.w = (int)P.upd_pairs.size();
+      P.upd_pairs.insert(P.upd_pairs.end(), tw.pairs.begin(), tw.pairs.end());
+      P.upd_tasks.push_back(tw.task);
+      P.upd_end.push_back((int)P.upd_pairs.size());
+      P.work.flops[K_UPDATE] += tw.flops;
+      P.work.bytes[K_UPDATE] += tw.bytes;
+    }
+    wave_tiles.clear();
     W.upd_cnt = (int)P.upd_tasks.size() - W.upd_off;
     for (int j = 0; j < maxnb; ++j) {
       W.panel_off.push_back((int)P.panel_tasks.size());
       W.syrk_off.push_back((int)P.syrk_tasks.size());
+      W.diag_off.push_back((int)P.diag_list.size());
       for (int s : big) {
         int w = super[s + 1] - super[s];
         int m = (int)(rowptr[s + 1] - rowptr[s]);
@@ -184,37 +292,24 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
         int bw = std::min(TB, w - c0);
         for (int r0 = c0 + bw; r0 < m; r0 += TB) P.panel_tasks.push_back(make_int2(s, r0));
         for (int cc = c0 + TB; cc < w; cc += TB)
-          for (int r0 = cc; r0 < m; r0 += TB) P.syrk_tasks.push_back(make_int4(s, r0, cc, 0));
+          for (int r0 = cc; r0 < m; r0 += TB)
+            if (!(cc == c0 + TB && r0 == cc))   // next diagonal tile: k_diag_step
+              P.syrk_tasks.push_back(make_int4(s, r0, cc, 0));
+        if (c0 + TB < w) P.diag_list.push_back(s);
       }
       W.panel_cnt.push_back((int)P.panel_tasks.size() - W.panel_off.back());
       W.syrk_cnt.push_back((int)P.syrk_tasks.size() - W.syrk_off.back());
+      W.diag_cnt.push_back((int)P.diag_list.size() - W.diag_off.back());
     }
     launches += (W.small_cnt > 0) + (W.asm_cnt > 0) + (W.upd_cnt > 0) + (W.big_cnt > 0);
-    for (int j = 0; j < maxnb; ++j) launches += (W.panel_cnt[j] > 0) + (W.syrk_cnt[j] > 0);
+    for (int j = 0; j < maxnb; ++j)
+      launches += (W.panel_cnt[j] > 0) + (W.syrk_cnt[j] > 0) + (W.diag_cnt[j] > 0);
   }
   P.launches = launches;
 
   // ---- algorithmic work per kernel class (one factorization) ----
   {
     KernelStats &K = P.work;
-    auto upd_flops = [&](int s, int64_t lo_row, int64_t hi_row, int64_t lo_col, int64_t hi_col,
-                         double &bytes) {
-      // sum over the prune set of 2 * (rows of d in [lo_row,hi_row]) * (rows of d in
-      // [lo_col,hi_col]) * width(d)
-      double fl = 0;
-      for (int q = prunePtr[s]; q < prunePtr[s + 1]; ++q) {
-        int d = pruneSet[q];
-        const int *b = Ls + rowptr[d], *e = Ls + rowptr[d + 1];
-        int64_t na = std::lower_bound(b, e, (int)hi_row + 1) - std::lower_bound(b, e, (int)lo_row);
-        int64_t nb = std::lower_bound(b, e, (int)hi_col + 1) - std::lower_bound(b, e, (int)lo_col);
-        int wd = super[d + 1] - super[d];
-        if (na > 0 && nb > 0) {
-          fl += 2.0 * na * nb * wd;
-          bytes += 8.0 * (na + nb) * wd;
-        }
-      }
-      return fl;
-    };
     for (int s : P.small_list) {
       int f = super[s], w = super[s + 1] - f;
       int64_t m = rowptr[s + 1] - rowptr[s];
@@ -232,15 +327,6 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
       by += 16.0 * m * w + 12.0 * (c[f + w] - c[f]);
       K.flops[K_SMALL] += fl;
       K.bytes[K_SMALL] += by;
-    }
-    for (const int4 &t : P.upd_tasks) {
-      int s = t.x, f = super[s], w = super[s + 1] - f;
-      int64_t m = rowptr[s + 1] - rowptr[s];
-      int nrow = (int)std::min<int64_t>(TB, m - t.y), ncol = std::min(TB, w - t.z);
-      const int *rows = Ls + rowptr[s];
-      double by = 16.0 * nrow * ncol;
-      K.flops[K_UPDATE] += upd_flops(s, rows[t.y], rows[t.y + nrow - 1], f + t.z, f + t.z + ncol - 1, by);
-      K.bytes[K_UPDATE] += by;
     }
     for (const int4 &t : P.syrk_tasks) {
       int s = t.x, w = super[s + 1] - super[s];
@@ -263,6 +349,98 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
         K.bytes[K_ASSEMBLE] += 12.0 * (c[super[s + 1]] - c[super[s]]) + 8.0 * m * w;
       }
   }
+  H.dinv_off.assign(supNo, -1);
+  H.ndinv = 0;
+  for (int s : P.big_list) {
+    H.dinv_off[s] = (int)H.ndinv;
+    H.ndinv += (super[s + 1] - super[s] + TB - 1) / TB;
+  }
+  H.super = std::move(super);
+  H.rowptr = std::move(rowptr);
+  H.xptr = std::move(xptr);
+  H.nls = nls;
+  H.xsize = xsize;
+  H.nnz = nnz;
+  H.nprune = nprune;
+  return true;
+}
+
+bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const int *Ls,
+                     const int64_t *Li_ptr, const int *blockSet, int supNo,
+                     const int *prunePtr, const int *pruneSet, std::string &err) {
+  cudaSetDevice(device_);
+  if (!kernels_configure(err)) return false;
+  HostSym H;
+  Plan P;
+  if (!build_plan(n, c, r, lC, Ls, Li_ptr, blockSet, supNo, prunePtr, pruneSet, H, P, err))
+    return false;
+  const std::vector<int> &super = H.super;
+  const std::vector<int64_t> &rowptr = H.rowptr, &xptr = H.xptr;
+  const int64_t nls = H.nls, xsize = H.xsize, nnz = H.nnz;
+  const int nprune = H.nprune;
+
+  // ---- solve plan: levels of the supernodal etree, per-level task lists ----
+  SolvePlan SP;
+  {
+    std::vector<int> lev(supNo, 0);
+    int nl = 0;
+    std::vector<int> col2sup(n);
+    for (int s = 0; s < supNo; ++s)
+      for (int j = super[s]; j < super[s + 1]; ++j) col2sup[j] = s;
+    for (int s = 0; s < supNo; ++s) {
+      const int w = super[s + 1] - super[s];
+      const int64_t m = rowptr[s + 1] - rowptr[s];
+      nl = std::max(nl, lev[s] + 1);
+      if (m > w) {
+        const int p = col2sup[Ls[rowptr[s] + w]];
+        lev[p] = std::max(lev[p], lev[s] + 1);
+      }
+      SP.max_w = std::max(SP.max_w, w);
+    }
+    std::vector<std::vector<int>> bylev(nl);
+    for (int s = 0; s < supNo; ++s) bylev[lev[s]].push_back(s);
+    for (int l = 0; l < nl; ++l) {
+      SP.level_off.push_back((int)SP.list.size());
+      SP.contrib_off.push_back((int)SP.contrib_tasks.size());
+      SP.gather_off.push_back((int)SP.gather_tasks.size());
+      for (int s : bylev[l]) {
+        SP.list.push_back(s);
+        const int w = super[s + 1] - super[s];
+        const int m = (int)(rowptr[s + 1] - rowptr[s]);
+        for (int r0 = w; r0 < m; r0 += 256) SP.contrib_tasks.push_back(make_int2(s, r0));
+        if (m > w)
+          for (int j0 = 0; j0 < w; j0 += 32) SP.gather_tasks.push_back(make_int2(s, j0));
+      }
+    }
+    SP.level_off.push_back((int)SP.list.size());
+    SP.contrib_off.push_back((int)SP.contrib_tasks.size());
+    SP.gather_off.push_back((int)SP.gather_tasks.size());
+    SP.contrib_len = nls - n;
+  }
+  if (!solve_configure(SP.max_w, err)) return false;
+  // ---- full CSR of the symmetric matrix for residuals: entry -> index into A2 values ----
+  std::vector<int> csr_rp(n + 1, 0), csr_ci, csr_map;
+  {
+    for (int j = 0; j < n; ++j)
+      for (int p = c[j]; p < c[j + 1]; ++p) {
+        csr_rp[r[p] + 1]++;
+        if (r[p] != j) csr_rp[j + 1]++;
+      }
+    for (int i = 0; i < n; ++i) csr_rp[i + 1] += csr_rp[i];
+    csr_ci.resize(csr_rp[n]);
+    csr_map.resize(csr_rp[n]);
+    std::vector<int> fill(csr_rp.begin(), csr_rp.end() - 1);
+    for (int j = 0; j < n; ++j)
+      for (int p = c[j]; p < c[j + 1]; ++p) {
+        const int i = r[p];
+        csr_ci[fill[i]] = j;
+        csr_map[fill[i]++] = p;
+        if (i != j) {
+          csr_ci[fill[j]] = i;
+          csr_map[fill[j]++] = p;
+        }
+      }
+  }
 
   // ---- upload ----
   release();
@@ -278,14 +456,29 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
             upload(d_upd_, pruneSet, (size_t)nprune, st, err) &&
             upload(d_small_, P.small_list.data(), P.small_list.size(), st, err) &&
             upload(d_big_, P.big_list.data(), P.big_list.size(), st, err) &&
+            upload(d_diag_, P.diag_list.data(), P.diag_list.size(), st, err) &&
             upload(d_asm_, P.asm_tasks.data(), P.asm_tasks.size(), st, err) &&
             upload(d_upd_tasks_, P.upd_tasks.data(), P.upd_tasks.size(), st, err) &&
+            upload(d_upd_end_, P.upd_end.data(), P.upd_end.size(), st, err) &&
+            upload(d_pairs_, P.upd_pairs.data(), P.upd_pairs.size(), st, err) &&
             upload(d_panel_, P.panel_tasks.data(), P.panel_tasks.size(), st, err) &&
-            upload(d_syrk_, P.syrk_tasks.data(), P.syrk_tasks.size(), st, err);
+            upload(d_syrk_, P.syrk_tasks.data(), P.syrk_tasks.size(), st, err) &&
+            upload(d_dinv_off_, H.dinv_off.data(), H.dinv_off.size(), st, err) &&
+            upload(d_slist_, SP.list.data(), SP.list.size(), st, err) &&
+            upload(d_scontrib_, SP.contrib_tasks.data(), SP.contrib_tasks.size(), st, err) &&
+            upload(d_sgather_, SP.gather_tasks.data(), SP.gather_tasks.size(), st, err) &&
+            upload(d_csr_rp_, csr_rp.data(), csr_rp.size(), st, err) &&
+            upload(d_csr_ci_, csr_ci.data(), csr_ci.size(), st, err) &&
+            upload(d_csr_map_, csr_map.data(), csr_map.size(), st, err);
   if (!ok) return false;
   cudaError_t e = cudaMalloc(&d_Ax_, sizeof(double) * std::max<int64_t>(nnz, 1));
   if (e == cudaSuccess) e = cudaMalloc(&dL_, sizeof(double) * std::max<int64_t>(xsize, 1));
   if (e == cudaSuccess) e = cudaMalloc(&d_status_, 2 * sizeof(int));
+  if (e == cudaSuccess)
+    e = cudaMalloc(&d_dinv_, sizeof(double) * TB * TB * std::max<int64_t>(H.ndinv, 1));
+  if (e == cudaSuccess)
+    e = cudaMalloc(&d_csr_val_, sizeof(double) * std::max<size_t>(csr_ci.size(), 1));
+
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     err = std::string("device allocation: ") + cudaGetErrorString(e);
@@ -296,6 +489,8 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
   xsize_ = xsize;
   nnz_ = nnz;
   plan_ = std::move(P);
+  splan_ = std::move(SP);
+  csr_nnz_ = (int64_t)csr_ci.size();
   sym_.n = n;
   sym_.nsuper = supNo;
   sym_.super = d_super_;
@@ -309,6 +504,9 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
   sym_.upd = d_upd_;
   sym_.L = dL_;
   sym_.status = d_status_;
+  sym_.dinv = d_dinv_;
+  sym_.dinv_off = d_dinv_off_;
+
   return true;
 }
 
@@ -334,18 +532,35 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof) {
     launch_assemble(sym_, d_asm_ + W.asm_off, W.asm_cnt, st);
     mark(-1, W.asm_cnt);
     mark(K_UPDATE, W.upd_cnt);
-    launch_update_tiles(sym_, d_upd_tasks_ + W.upd_off, W.upd_cnt, st);
+    launch_update_tiles(sym_, d_upd_tasks_ + W.upd_off, d_upd_end_ + W.upd_off, d_pairs_,
+                        W.upd_cnt, st);
     mark(-1, W.upd_cnt);
     mark(K_PANEL, W.big_cnt);
-    launch_potrf_first(sym_, d_big_ + W.big_off, W.big_cnt, st);
+    launch_diag_step(sym_, d_big_ + W.big_off, W.big_cnt, 0, st);
     mark(-1, W.big_cnt);
     for (size_t j = 0; j < W.panel_off.size(); ++j) {
       mark(K_PANEL, W.panel_cnt[j]);
       launch_trsm_step(sym_, d_panel_ + W.panel_off[j], W.panel_cnt[j], (int)j, st);
       mark(-1, W.panel_cnt[j]);
-      mark(K_SYRK, W.syrk_cnt[j]);
-      launch_syrk_step(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
-      mark(-1, W.syrk_cnt[j]);
+      if (prof) {
+        // profiled runs keep one stream so every launch is bracketed by its own events
+        mark(K_PANEL, W.diag_cnt[j]);
+        launch_diag_step(sym_, d_diag_ + W.diag_off[j], W.diag_cnt[j], (int)j + 1, st);
+        mark(-1, W.diag_cnt[j]);
+        mark(K_SYRK, W.syrk_cnt[j]);
+        launch_syrk_step(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
+        mark(-1, W.syrk_cnt[j]);
+      } else if (W.diag_cnt[j] > 0) {
+        // fork: next diagonal block on the auxiliary stream, trailing update here; join
+        cudaEventRecord(ev_fork_, st);
+        cudaStreamWaitEvent(aux_stream_, ev_fork_, 0);
+        launch_diag_step(sym_, d_diag_ + W.diag_off[j], W.diag_cnt[j], (int)j + 1, aux_stream_);
+        cudaEventRecord(ev_join_, aux_stream_);
+        launch_syrk_step(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
+        cudaStreamWaitEvent(st, ev_join_, 0);
+      } else {
+        launch_syrk_step(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
+      }
     }
   }
 }
@@ -354,17 +569,28 @@ int Engine::factor(const double *values, bool values_on_device, int *info, std::
   if (!dL_) { err = "factor before analyze"; return -1; }
   cudaSetDevice(device_);
   cudaStream_t st = stream_;
-  cudaError_t e;
-  if (values_on_device) {
-    sym_.Ax = values;
-    e = cudaSuccess;
-  } else {
-    sym_.Ax = d_Ax_;
-    e = cudaMemcpyAsync(d_Ax_, values, sizeof(double) * nnz_, cudaMemcpyHostToDevice, st);
-  }
+  // values always reach the kernels through d_Ax_, so a captured graph stays valid
+  cudaError_t e = cudaMemcpyAsync(d_Ax_, values, sizeof(double) * nnz_,
+                                  values_on_device ? cudaMemcpyDeviceToDevice
+                                                   : cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) { err = std::string("values upload: ") + cudaGetErrorString(e); return -1; }
   h2d_bytes_ = values_on_device ? 0 : (int64_t)sizeof(double) * nnz_;
-  launch_all();
+  if (use_graph_) {
+    // The whole launch sequence is fixed by the structure: capture it once, replay it.
+    if (!graph_exec_) {
+      e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+      if (e == cudaSuccess) {
+        launch_all();
+        e = cudaStreamEndCapture(st, &graph_);
+      }
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&graph_exec_, graph_, 0);
+      if (e != cudaSuccess) { err = std::string("graph capture: ") + cudaGetErrorString(e); return -1; }
+    }
+    e = cudaGraphLaunch(graph_exec_, st);
+    if (e != cudaSuccess) { err = std::string("graph launch: ") + cudaGetErrorString(e); return -1; }
+  } else {
+    launch_all();
+  }
   return finish(info, err);
 }
 
@@ -373,13 +599,9 @@ int Engine::factor_profiled(const double *values, bool values_on_device, int *in
   if (!dL_) { err = "factor before analyze"; return -1; }
   cudaSetDevice(device_);
   cudaStream_t st = stream_;
-  cudaError_t e = cudaSuccess;
-  if (values_on_device) {
-    sym_.Ax = values;
-  } else {
-    sym_.Ax = d_Ax_;
-    e = cudaMemcpyAsync(d_Ax_, values, sizeof(double) * nnz_, cudaMemcpyHostToDevice, st);
-  }
+  cudaError_t e = cudaMemcpyAsync(d_Ax_, values, sizeof(double) * nnz_,
+                                  values_on_device ? cudaMemcpyDeviceToDevice
+                                                   : cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) { err = std::string("values upload: ") + cudaGetErrorString(e); return -1; }
   std::vector<std::pair<int, cudaEvent_t>> prof;
   launch_all(&prof);
@@ -399,6 +621,8 @@ int Engine::factor_profiled(const double *values, bool values_on_device, int *in
 
 int Engine::finish(int *info, std::string &err) {
   cudaStream_t st = stream_;
+  // full-CSR values of this matrix for residuals, and ||A||_inf
+  launch_gather_vals((int)csr_nnz_, d_csr_map_, d_Ax_, d_csr_val_, st);
   cudaError_t e = cudaMemcpyAsync(h_status_, d_status_, 2 * sizeof(int), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e == cudaSuccess) e = cudaGetLastError();
@@ -422,6 +646,165 @@ bool Engine::download(double *lValues, bool to_device, std::string &err) {
   d2h_bytes_ = to_device ? 0 : (int64_t)sizeof(double) * xsize_;
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
   if (e != cudaSuccess) { err = std::string("download: ") + cudaGetErrorString(e); return false; }
+  return true;
+}
+
+bool Engine::ensure_work(int nrhs, std::string &err) {
+  if (nrhs <= work_nrhs_) return true;
+  if (d_contrib_) cudaFree(d_contrib_);
+  if (d_work_) cudaFree(d_work_);
+  if (d_norms_) cudaFree(d_norms_);
+  if (h_norms_) cudaFreeHost(h_norms_);
+  d_contrib_ = d_work_ = d_norms_ = h_norms_ = nullptr;
+  cudaError_t e = cudaMalloc(&d_contrib_, sizeof(double) * std::max<int64_t>(splan_.contrib_len, 1) * nrhs);
+  // work: r, d, p, q vectors (4 * n * nrhs) + row sums
+  if (e == cudaSuccess) e = cudaMalloc(&d_work_, sizeof(double) * ((size_t)4 * n_ * nrhs + n_));
+  if (e == cudaSuccess) e = cudaMalloc(&d_norms_, sizeof(double) * 8 * (nrhs + 1));
+  if (e == cudaSuccess) e = cudaMallocHost(&h_norms_, sizeof(double) * 8 * (nrhs + 1));
+  if (e != cudaSuccess) {
+    err = std::string("solve workspace: ") + cudaGetErrorString(e);
+    work_nrhs_ = 0;
+    return false;
+  }
+  work_nrhs_ = nrhs;
+  return true;
+}
+
+void Engine::run_solve(double *x, int nrhs) {
+  cudaStream_t st = stream_;
+  const SolvePlan &SP = splan_;
+  const int nl = (int)SP.level_off.size() - 1;
+  const int smem = (int)sizeof(double) * std::max(SP.max_w, 1);
+  const int64_t cs = std::max<int64_t>(SP.contrib_len, 1);
+  for (int l = 0; l < nl; ++l) {
+    launch_fwd_diag(sym_, d_slist_ + SP.level_off[l], SP.level_off[l + 1] - SP.level_off[l], smem,
+                    x, d_contrib_, n_, nrhs, cs, st);
+    launch_fwd_contrib(sym_, d_scontrib_ + SP.contrib_off[l], SP.contrib_off[l + 1] - SP.contrib_off[l],
+                       x, d_contrib_, n_, nrhs, cs, st);
+  }
+  for (int l = nl - 1; l >= 0; --l) {
+    launch_bwd_gather(sym_, d_sgather_ + SP.gather_off[l], SP.gather_off[l + 1] - SP.gather_off[l],
+                      x, n_, nrhs, st);
+    launch_bwd_diag(sym_, d_slist_ + SP.level_off[l], SP.level_off[l + 1] - SP.level_off[l], smem,
+                    x, n_, nrhs, st);
+  }
+}
+
+bool Engine::solve(const double *b, double *x, int nrhs, std::string &err) {
+  if (!dL_) { err = "solve before factor"; return false; }
+  cudaSetDevice(device_);
+  if (!ensure_work(nrhs, err)) return false;
+  cudaError_t e = cudaSuccess;
+  if (x != b) e = cudaMemcpyAsync(x, b, sizeof(double) * n_ * nrhs, cudaMemcpyDeviceToDevice, stream_);
+  if (e != cudaSuccess) { err = std::string("solve: ") + cudaGetErrorString(e); return false; }
+  run_solve(x, nrhs);
+  e = cudaStreamSynchronize(stream_);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) { err = std::string("solve: ") + cudaGetErrorString(e); return false; }
+  return true;
+}
+
+bool Engine::refine(const double *b, double *x, int nrhs, double tol, int maxit, RefineInfo &info,
+                    std::string &err) {
+  if (!dL_) { err = "refine before factor"; return false; }
+  cudaSetDevice(device_);
+  if (!ensure_work(nrhs, err)) return false;
+  cudaStream_t st = stream_;
+  const size_t len = (size_t)n_ * nrhs;
+  double *r = d_work_, *dv = r + len, *pv = dv + len, *qv = pv + len, *rows = qv + len;
+  auto sync_norms = [&](int count) -> bool {
+    cudaError_t e = cudaMemcpyAsync(h_norms_, d_norms_, sizeof(double) * 2 * count,
+                                    cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) { err = std::string("refine: ") + cudaGetErrorString(e); return false; }
+    return true;
+  };
+  // ||A||_inf
+  launch_rowabs(n_, d_csr_rp_, d_csr_val_, rows, st);
+  launch_norms(n_, 1, rows, nullptr, d_norms_, st);
+  if (!sync_norms(1)) return false;
+  anorm_ = h_norms_[0];
+  // residual r = b - A x and backward errors; returns the max over right-hand sides
+  std::vector<double> berr(nrhs, 0.0);
+  auto residual = [&](const double *xx) -> bool {
+    launch_spmv(n_, d_csr_rp_, d_csr_ci_, d_csr_val_, xx, r, nrhs, st);
+    launch_residual(len, b, r, st);
+    launch_norms(n_, nrhs, r, nullptr, d_norms_, st);
+    launch_norms(n_, nrhs, xx, nullptr, d_norms_ + 2 * nrhs, st);
+    if (!sync_norms(2 * nrhs)) return false;
+    for (int k = 0; k < nrhs; ++k) {
+      const double rn = h_norms_[2 * k], xn = h_norms_[2 * (nrhs + k)];
+      berr[k] = (xn > 0 && anorm_ > 0) ? rn / (anorm_ * xn) : rn;
+    }
+    return true;
+  };
+  auto worst = [&]() { return *std::max_element(berr.begin(), berr.end()); };
+  // x0 = solve(b)
+  cudaMemcpyAsync(x, b, sizeof(double) * len, cudaMemcpyDeviceToDevice, st);
+  run_solve(x, nrhs);
+  if (!residual(x)) return false;
+  info.method = 0;
+  info.iterations = 0;
+  double prev = worst(), cur = prev;
+  int stall = 0;
+  while (cur > tol && info.iterations < maxit) {
+    cudaMemcpyAsync(dv, r, sizeof(double) * len, cudaMemcpyDeviceToDevice, st);
+    run_solve(dv, nrhs);
+    launch_axpy(len, 1.0, dv, x, st);
+    info.method = 1;
+    info.iterations++;
+    if (!residual(x)) return false;
+    cur = worst();
+    stall = (cur > 0.5 * prev) ? stall + 1 : 0;
+    prev = cur;
+    if (stall >= 2) break;
+  }
+  if (cur > tol && stall >= 2) {
+    // factor-preconditioned conjugate gradients, one right-hand side at a time
+    info.method = 2;
+    for (int k = 0; k < nrhs; ++k) {
+      double *xk = x + (size_t)k * n_, *rk = r + (size_t)k * n_;
+      double *zk = dv + (size_t)k * n_, *pk = pv + (size_t)k * n_, *qk = qv + (size_t)k * n_;
+      const double *bk = b + (size_t)k * n_;
+      auto norms1 = [&](const double *a, const double *bb) -> bool {
+        launch_norms(n_, 1, a, bb, d_norms_, st);
+        return sync_norms(1);
+      };
+      launch_spmv(n_, d_csr_rp_, d_csr_ci_, d_csr_val_, xk, rk, 1, st);
+      launch_residual((size_t)n_, bk, rk, st);
+      cudaMemcpyAsync(zk, rk, sizeof(double) * n_, cudaMemcpyDeviceToDevice, st);
+      run_solve(zk, 1);
+      cudaMemcpyAsync(pk, zk, sizeof(double) * n_, cudaMemcpyDeviceToDevice, st);
+      if (!norms1(rk, zk)) return false;
+      double rz = h_norms_[1];
+      for (int it = 0; it < maxit * 10; ++it) {
+        launch_spmv(n_, d_csr_rp_, d_csr_ci_, d_csr_val_, pk, qk, 1, st);
+        if (!norms1(pk, qk)) return false;
+        const double pq = h_norms_[1];
+        if (!(pq > 0)) break;
+        const double alpha = rz / pq;
+        launch_axpy((size_t)n_, alpha, pk, xk, st);
+        launch_axpy((size_t)n_, -alpha, qk, rk, st);
+        info.iterations++;
+        if (!norms1(rk, nullptr)) return false;
+        const double rn = h_norms_[0];
+        if (!norms1(xk, nullptr)) return false;
+        const double bk_err = rn / (anorm_ * h_norms_[0]);
+        if (bk_err <= tol) break;
+        cudaMemcpyAsync(zk, rk, sizeof(double) * n_, cudaMemcpyDeviceToDevice, st);
+        run_solve(zk, 1);
+        if (!norms1(rk, zk)) return false;
+        const double rz2 = h_norms_[1];
+        const double beta = rz2 / rz;
+        rz = rz2;
+        launch_xpby((size_t)n_, zk, beta, pk, st);   // p = z + beta p
+      }
+    }
+    if (!residual(x)) return false;
+  }
+  info.berr = berr;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) { err = std::string("refine: ") + cudaGetErrorString(e); return false; }
   return true;
 }
 

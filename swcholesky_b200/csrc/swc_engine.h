@@ -26,6 +26,8 @@ struct DevSym {
   double *L;              // supernodal values (the reference's lValues)
   int *status;            // [0] = smallest failing column + 1 (INT_MAX if none),
                           // [1] = structure error flag
+  double *dinv;           // scratch: inverses of the 64x64 diagonal blocks of the tiled class
+  const int *dinv_off;    // per supernode: first block of its inverses in dinv (-1: none)
 };
 
 // One level of the schedule (supernodes whose descendants all belong to earlier levels).
@@ -37,6 +39,7 @@ struct Wave {
   int big_off = 0, big_cnt = 0;    // tiled-class supernodes (block 0 POTRF)
   std::vector<int> panel_off, panel_cnt;  // per column block step: TRSM tiles
   std::vector<int> syrk_off, syrk_cnt;
+  std::vector<int> diag_off, diag_cnt;    // per step j: supernodes whose block j+1 exists
 };
 
 // Kernel classes, for per-kernel timing (profiled factorization) and flop accounting.
@@ -54,13 +57,69 @@ struct Plan {
   std::vector<int> small_list;
   std::vector<int> big_list;
   std::vector<int2> asm_tasks;
-  std::vector<int4> upd_tasks;
+  std::vector<int4> upd_tasks;     // (s, r0, c0, first pair)
+  std::vector<int> upd_end;        // one past the last pair of each task
+  std::vector<int4> upd_pairs;     // (d, a0, b0, na | nb << 16)
   std::vector<int2> panel_tasks;
   std::vector<int4> syrk_tasks;
+  std::vector<int> diag_list;
   int launches = 0;  // kernel launches per factorization
   KernelStats work;  // algorithmic flops/bytes per kernel class
 };
 
+
+// Triangular solves and refinement (swc_solve.cu)
+bool solve_configure(int max_w, std::string &err);
+void launch_fwd_diag(const DevSym &S, const int *list, int count, int smem, double *y,
+                     const double *contrib, int n, int nrhs, int64_t cstride, cudaStream_t st);
+void launch_fwd_contrib(const DevSym &S, const int2 *tasks, int count, const double *y,
+                        double *contrib, int n, int nrhs, int64_t cstride, cudaStream_t st);
+void launch_bwd_gather(const DevSym &S, const int2 *tasks, int count, double *x, int n, int nrhs,
+                       cudaStream_t st);
+void launch_bwd_diag(const DevSym &S, const int *list, int count, int smem, double *x, int n,
+                     int nrhs, cudaStream_t st);
+void launch_spmv(int n, const int *rp, const int *ci, const double *val, const double *x,
+                 double *y, int nrhs, cudaStream_t st);
+void launch_gather_vals(int nnz, const int *map, const double *ax, double *val, cudaStream_t st);
+void launch_residual(size_t len, const double *b, double *r, cudaStream_t st);
+void launch_axpy(size_t len, double a, const double *x, double *y, cudaStream_t st);
+void launch_xpby(size_t len, const double *z, double beta, double *p, cudaStream_t st);
+void launch_norms(int n, int nrhs, const double *x, const double *y, double *out, cudaStream_t st);
+void launch_rowabs(int n, const int *rp, const double *val, double *out, cudaStream_t st);
+
+// Per-level task lists of the solves.
+struct SolvePlan {
+  std::vector<int> level_off;       // supernodes of level l: list[level_off[l] .. level_off[l+1])
+  std::vector<int> list;
+  std::vector<int> contrib_off;     // (s, r0) tasks of level l
+  std::vector<int2> contrib_tasks;
+  std::vector<int> gather_off;      // (s, j0) tasks of level l
+  std::vector<int2> gather_tasks;
+  int max_w = 0;
+  int64_t contrib_len = 0;          // off-diagonal rows in total (one contribution each)
+};
+
+// Result of a refined solve, per right-hand side.
+struct RefineInfo {
+  std::vector<double> berr;         // final backward error ||b - A x|| / (||A|| ||x||), inf-norms
+  int iterations = 0;               // refinement steps (or CG iterations after the fallback)
+  int method = 0;                   // 0: direct solve sufficed, 1: refinement, 2: CG fallback
+};
+
+// Host copy of the per-supernode arrays the kernels index by.
+struct HostSym {
+  std::vector<int> super;
+  std::vector<int64_t> rowptr, xptr;
+  int64_t nls = 0, xsize = 0, nnz = 0;
+  int nprune = 0;
+  std::vector<int> dinv_off;   // per supernode: first diagonal-block inverse (-1: none)
+  int64_t ndinv = 0;           // diagonal-block inverses in total
+};
+
+// Validates the symbolic arrays and derives the execution plan (no device work).
+bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int *Ls,
+                const int64_t *Li_ptr, const int *blockSet, int supNo, const int *prunePtr,
+                const int *pruneSet, HostSym &H, Plan &P, std::string &err);
 
 class Engine {
  public:
@@ -76,6 +135,12 @@ class Engine {
   // launch counts and device milliseconds (no other difference).
   int factor_profiled(const double *values, bool values_on_device, int *info,
                       KernelStats &out, std::string &err);
+  // x = (L L^T)^{-1} b for nrhs right-hand sides (device pointers, leading dimension n).
+  bool solve(const double *b, double *x, int nrhs, std::string &err);
+  // FP64 iterative refinement with the factor (falls back to factor-preconditioned CG when
+  // refinement stalls); device pointers.
+  bool refine(const double *b, double *x, int nrhs, double tol, int maxit, RefineInfo &info,
+              std::string &err);
   int64_t h2d_bytes() const { return h2d_bytes_; }
   int64_t d2h_bytes() const { return d2h_bytes_; }
   bool download(double *lValues, bool to_device, std::string &err);
@@ -102,20 +167,40 @@ class Engine {
   int *d_super_ = nullptr, *d_Ls_ = nullptr, *d_Ap_ = nullptr, *d_Ai_ = nullptr;
   int64_t *d_rowptr_ = nullptr, *d_xptr_ = nullptr;
   int *d_upd_ptr_ = nullptr, *d_upd_ = nullptr;
-  double *d_Ax_ = nullptr, *dL_ = nullptr;
+  double *d_Ax_ = nullptr, *dL_ = nullptr, *d_dinv_ = nullptr;
+  int *d_dinv_off_ = nullptr;
   int *d_status_ = nullptr, *h_status_ = nullptr;
-  int *d_small_ = nullptr, *d_big_ = nullptr;
+  int *d_small_ = nullptr, *d_big_ = nullptr, *d_diag_ = nullptr;
+  cudaStream_t aux_stream_ = nullptr;          // second branch of each dense step
+  cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
   int2 *d_asm_ = nullptr, *d_panel_ = nullptr;
-  int4 *d_upd_tasks_ = nullptr, *d_syrk_ = nullptr;
+  int4 *d_upd_tasks_ = nullptr, *d_syrk_ = nullptr, *d_pairs_ = nullptr;
+  int *d_upd_end_ = nullptr;
+  cudaGraph_t graph_ = nullptr;
+  cudaGraphExec_t graph_exec_ = nullptr;
+  bool use_graph_ = true;
   Plan plan_;
   DevSym sym_{};
+  // solve data
+  SolvePlan splan_;
+  int *d_slist_ = nullptr;
+  int2 *d_scontrib_ = nullptr, *d_sgather_ = nullptr;
+  int *d_csr_rp_ = nullptr, *d_csr_ci_ = nullptr, *d_csr_map_ = nullptr;
+  double *d_csr_val_ = nullptr;
+  int64_t csr_nnz_ = 0;
+  double *d_contrib_ = nullptr, *d_work_ = nullptr, *d_norms_ = nullptr, *h_norms_ = nullptr;
+  int work_nrhs_ = 0;
+  double anorm_ = 0.0;
+  bool ensure_work(int nrhs, std::string &err);
+  void run_solve(double *x, int nrhs);
 };
 
 // kernel launch wrappers (swc_kernels.cu)
 void launch_factor_small(const DevSym &S, const int *list, int count, int smem, cudaStream_t st);
 void launch_assemble(const DevSym &S, const int2 *tasks, int count, cudaStream_t st);
-void launch_update_tiles(const DevSym &S, const int4 *tasks, int count, cudaStream_t st);
-void launch_potrf_first(const DevSym &S, const int *list, int count, cudaStream_t st);
+void launch_update_tiles(const DevSym &S, const int4 *tasks, const int *task_end,
+                         const int4 *pairs, int count, cudaStream_t st);
+void launch_diag_step(const DevSym &S, const int *list, int count, int step, cudaStream_t st);
 void launch_trsm_step(const DevSym &S, const int2 *tasks, int count, int step, cudaStream_t st);
 void launch_syrk_step(const DevSym &S, const int4 *tasks, int count, int step, cudaStream_t st);
 void launch_init_status(int *status, cudaStream_t st);

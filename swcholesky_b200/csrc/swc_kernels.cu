@@ -13,10 +13,11 @@
 //                    every descendant in the prune set (the SYRK/GEMM of .c:299-359 limited
 //                    to the tile, scattered through relative indices, .c:364-378); the tile
 //                    is written once.  Deterministic: no atomics, fixed update order.
-//   k_potrf_first,   blocked right-looking dense factorization of a wide supernode by
-//   k_trsm_step,     64-column blocks: POTRF of diagonal block 0, then per block the TRSM
-//   k_syrk_step      of the tiles below the diagonal block and the trailing SYRK/GEMM
-//                    update, whose diagonal-tile CTA also factors the next diagonal block.
+//   k_diag_step,     blocked right-looking dense factorization of a wide supernode by
+//   k_trsm_step,     64-column blocks: per block, POTRF of the diagonal block (and its
+//   k_syrk_step      inverse), the TRSM of the tiles below it as a DMMA product with that
+//                    inverse, and the trailing SYRK/GEMM update; the next diagonal block's
+//                    update and POTRF run concurrently with that trailing update.
 //
 // All arithmetic is FP64; tiles are 64x64 with 256 threads, each thread holding a 4x4
 // register micro-tile.
@@ -115,23 +116,26 @@ __global__ void __launch_bounds__(NT) k_factor_small(DevSym S, const int *list, 
     __syncthreads();
   }
 
-  // POTRF + TRSM on the tall panel: unblocked right-looking Cholesky of m x w
+  // POTRF + TRSM on the tall panel: unblocked right-looking Cholesky of m x w.  Rows are
+  // strided over the threads; the scaled pivot column's first w entries go through colv so
+  // a single barrier separates scaling from the trailing update.
+  double *colv = reinterpret_cast<double *>(rel + m);   // w doubles (8-byte aligned slot)
   for (int j = 0; j < w; ++j) {
-    const double djj = P[(size_t)j * m + j];
-    if (!(djj > 0.0) && tid == 0) atomicMin(&S.status[0], f + j + 1);
-    const double dsq = sqrt(djj);
     __syncthreads();
-    for (int i = j + tid; i < m; i += NT)
-      P[(size_t)j * m + i] = (i == j) ? dsq : P[(size_t)j * m + i] / dsq;
+    const double piv = P[(size_t)j * m + j];
+    const double dsq = sqrt(piv);
+    const double inv = 1.0 / dsq;
+    if (tid == 0 && !(piv > 0.0)) atomicMin(&S.status[0], f + j + 1);
+    for (int i = j + tid; i < w; i += NT) colv[i] = (i == j) ? dsq : P[(size_t)j * m + i] * inv;
     __syncthreads();
-    const int ncol = w - j - 1;
-    for (int idx = tid; idx < ncol * m; idx += NT) {
-      const int cc = j + 1 + idx / m;
-      const int i = idx - (cc - j - 1) * m;
-      if (i >= cc) P[(size_t)cc * m + i] -= P[(size_t)j * m + i] * P[(size_t)j * m + cc];
+    for (int i = j + tid; i < m; i += NT) {
+      const double lij = (i == j) ? dsq : P[(size_t)j * m + i] * inv;
+      P[(size_t)j * m + i] = lij;
+      const int cend = min(i, w - 1);
+      for (int c = j + 1; c <= cend; ++c) P[(size_t)c * m + i] = fma(-lij, colv[c], P[(size_t)c * m + i]);
     }
-    __syncthreads();
   }
+  __syncthreads();
   double *dst = S.L + S.xptr[s];
   for (int i = tid; i < m * w; i += NT) dst[i] = P[i];
 }
@@ -157,143 +161,415 @@ __global__ void k_assemble(DevSym S, const int2 *tasks, int count) {
 }
 
 // ---------------------------------------------------------------------------------------
-// Register-tiled 64x64 FP64 product of two row blocks over K columns:
-//   acc[i][j] += sum_k A[ty+16i, k] * B[tx+16j, k]
-// A rows come from a column-major panel (ld), starting at row a0, na valid rows; same for B.
-__device__ __forceinline__ void tile_product(const double *__restrict__ Pa, int lda, int na,
-                                             const double *__restrict__ Pb, int ldb, int nb,
-                                             int K, double (*As)[TB], double (*Bs)[TB],
-                                             double acc[4][4]) {
-  const int tid = threadIdx.x;
-  const int tx = tid & 15, ty = tid >> 4;
-  for (int k0 = 0; k0 < K; k0 += KC) {
-    __syncthreads();
-    for (int e = tid; e < KC * TB; e += NT) {
-      const int k = e / TB, i = e - k * TB;
-      const bool kin = (k0 + k) < K;
-      As[k][i] = (kin && i < na) ? Pa[(size_t)(k0 + k) * lda + i] : 0.0;
-      Bs[k][i] = (kin && i < nb) ? Pb[(size_t)(k0 + k) * ldb + i] : 0.0;
+// 64x64 FP64 tile product on the tensor cores (DMMA, mma.sync m8n8k4 .f64):
+//   C[i][j] = sum_k A[i][k] * B[j][k],  A = rows [0,na) of a column-major panel (lda),
+//                                       B = rows [0,nb) of a column-major panel (ldb).
+// 128 threads = 4 warps in a 2x2 grid, each warp a 32x32 sub-tile of 4x4 MMA tiles.
+// Operands stream through shared memory in k-chunks of KC columns with a two-stage
+// cp.async pipeline; rows beyond na / nb and columns beyond K are zero-filled.
+// Fragment layout of m8n8k4 .f64: A[lane/4][lane%4], B[k = lane%4][n = lane/4],
+// C[lane/4][2*(lane%4) + e].
+constexpr int MT = 128;               // threads of the tensor-core tile kernels
+constexpr int LDS = TB + 8;           // padded row of a staged k-slice (bank spread)
+constexpr int STAGE = 2 * KC * LDS;   // doubles per pipeline stage (A and B slices)
+
+__device__ __forceinline__ void cp_async8(double *smem, const double *gmem, bool pred) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  const int sz = pred ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(sz));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+__device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c[0]), "+d"(c[1])
+               : "d"(a), "d"(b));
+}
+
+struct TileAcc {
+  double v[4][4][2];
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) v[i][j][0] = v[i][j][1] = 0.0;
+  }
+};
+
+__device__ __forceinline__ void load_chunk(const double *__restrict__ Pa, int lda, int na,
+                                           const double *__restrict__ Pb, int ldb, int nb,
+                                           int K, int k0, double *st) {
+  double *As = st, *Bs = st + KC * LDS;
+  for (int e = threadIdx.x; e < KC * TB; e += MT) {
+    const int k = e / TB, i = e - k * TB;
+    const int kk = k0 + k;
+    const bool pa = kk < K && i < na, pb = kk < K && i < nb;
+    cp_async8(&As[k * LDS + i], pa ? Pa + (size_t)kk * lda + i : Pa, pa);
+    cp_async8(&Bs[k * LDS + i], pb ? Pb + (size_t)kk * ldb + i : Pb, pb);
+  }
+  cp_async_commit();
+}
+
+__device__ __forceinline__ void dmma_tile_product(const double *__restrict__ Pa, int lda, int na,
+                                                  const double *__restrict__ Pb, int ldb, int nb,
+                                                  int K, double *stages, TileAcc &acc) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
+  const int kq = lane & 3, g = lane >> 2;
+  const int nchunks = (K + KC - 1) / KC;
+  __syncthreads();   // stages free (previous users done)
+  load_chunk(Pa, lda, na, Pb, ldb, nb, K, 0, stages);
+  for (int c = 0; c < nchunks; ++c) {
+    if (c + 1 < nchunks) {
+      load_chunk(Pa, lda, na, Pb, ldb, nb, K, (c + 1) * KC, stages + ((c + 1) & 1) * STAGE);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
     }
     __syncthreads();
+    const double *As = stages + (c & 1) * STAGE, *Bs = As + KC * LDS;
 #pragma unroll
-    for (int k = 0; k < KC; ++k) {
+    for (int k4 = 0; k4 < KC; k4 += 4) {
       double a[4], b[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[k][ty + 16 * i];
+      for (int i = 0; i < 4; ++i) a[i] = As[(k4 + kq) * LDS + wr + 8 * i + g];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = Bs[k][tx + 16 * j];
+      for (int j = 0; j < 4; ++j) b[j] = Bs[(k4 + kq) * LDS + wc + 8 * j + g];
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        for (int j = 0; j < 4; ++j) dmma(acc.v[i][j], a[i], b[j]);
     }
+    __syncthreads();
   }
 }
 
-// Tile-owner update of the tiled class.  task = (s, r0, c0): the tile covers panel rows
-// [r0, r0+64) and columns [c0, c0+64) of supernode s.
-constexpr int UPD_SMEM = (2 * KC * TB + TB * (TB + 1)) * 8 + 3 * TB * 4;
+// Gathered variant: operand rows are picked through index maps, ia[i] / ib[j] = row of the
+// source panel that feeds tile row i / column j, or -1 for a zero row.  Lets one
+// accumulator collect the contributions of several descendants in the target's own
+// coordinates, with no scatter.
+__device__ __forceinline__ void load_chunk_gather(const double *__restrict__ Ld, int ld,
+                                                  const int *ia, const int *ib, int K, int k0,
+                                                  double *st) {
+  double *As = st, *Bs = st + KC * LDS;
+  for (int e = threadIdx.x; e < KC * TB; e += MT) {
+    const int k = e / TB, i = e - k * TB;
+    const int kk = k0 + k;
+    const int ra = ia[i], rb = ib[i];
+    const bool pa = kk < K && ra >= 0, pb = kk < K && rb >= 0;
+    cp_async8(&As[k * LDS + i], pa ? Ld + (size_t)kk * ld + ra : Ld, pa);
+    cp_async8(&Bs[k * LDS + i], pb ? Ld + (size_t)kk * ld + rb : Ld, pb);
+  }
+  cp_async_commit();
+}
 
-__global__ void __launch_bounds__(NT) k_update_tiles(DevSym S, const int4 *tasks, int count) {
+__device__ __forceinline__ void dmma_tile_product_gather(const double *__restrict__ Ld, int ld,
+                                                         const int *ia, const int *ib, int K,
+                                                         double *stages, TileAcc &acc) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
+  const int kq = lane & 3, g = lane >> 2;
+  const int nchunks = (K + KC - 1) / KC;
+  __syncthreads();
+  // 8x8 MMA tiles whose gathered rows (or columns) are all empty contribute nothing: skip
+  // them (warp-uniform masks over this warp's 4 row groups and 4 column groups)
+  unsigned rmask = 0, cmask = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    if (__any_sync(0xffffffffu, ia[wr + 8 * i + (lane & 7)] >= 0)) rmask |= 1u << i;
+    if (__any_sync(0xffffffffu, ib[wc + 8 * i + (lane & 7)] >= 0)) cmask |= 1u << i;
+  }
+  load_chunk_gather(Ld, ld, ia, ib, K, 0, stages);
+  for (int c = 0; c < nchunks; ++c) {
+    if (c + 1 < nchunks) {
+      load_chunk_gather(Ld, ld, ia, ib, K, (c + 1) * KC, stages + ((c + 1) & 1) * STAGE);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const double *As = stages + (c & 1) * STAGE, *Bs = As + KC * LDS;
+    if (rmask && cmask) {
+#pragma unroll
+      for (int k4 = 0; k4 < KC; k4 += 4) {
+        double a[4], b[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = As[(k4 + kq) * LDS + wr + 8 * i + g];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) b[j] = Bs[(k4 + kq) * LDS + wc + 8 * j + g];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            if (((rmask >> i) & (cmask >> j)) & 1u) dmma(acc.v[i][j], a[i], b[j]);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Sign flip through the integer pipe (FP64 arithmetic outside the tensor cores is slow).
+__device__ __forceinline__ double neg(double x) {
+  return __longlong_as_double(__double_as_longlong(x) ^ (long long)0x8000000000000000ULL);
+}
+
+// Position of accumulator element (i, j, e) of this thread inside the 64x64 tile.
+__device__ __forceinline__ int acc_row(int i) {
+  return ((threadIdx.x >> 5) >> 1) * 32 + 8 * i + ((threadIdx.x & 31) >> 2);
+}
+__device__ __forceinline__ int acc_col(int j, int e) {
+  return ((threadIdx.x >> 5) & 1) * 32 + 8 * j + 2 * (threadIdx.x & 3) + e;
+}
+
+// Tile-owner update of the tiled class.  task = (s, r0, c0, first pair); the tile covers
+// panel rows [r0, r0+64) and columns [c0, c0+64) of supernode s.  Its pair list holds
+// exactly the descendants that touch it: pair = (d, a0, b0, na | nb << 16) where rows
+// a0..a0+na-1 of d's row list fall in the tile's rows and b0..b0+nb-1 in its columns.
+// The accumulator starts as minus the tile, collects every pair's product in the tile's
+// own coordinates (rows gathered through index maps), and minus it is stored back:
+// tile - sum_d L_d L_d^T without any scalar FP64 operation.
+constexpr int UPD_SMEM = 2 * STAGE * 8 + 4 * TB * 4;
+
+__global__ void __launch_bounds__(MT, 4) k_update_tiles(DevSym S, const int4 *tasks,
+                                                     const int *task_end, const int4 *pairs,
+                                                     int count) {
   extern __shared__ double dyn[];
-  double(*As)[TB] = reinterpret_cast<double(*)[TB]>(dyn);
-  double(*Bs)[TB] = reinterpret_cast<double(*)[TB]>(dyn + KC * TB);
-  double(*Acc)[TB + 1] = reinterpret_cast<double(*)[TB + 1]>(dyn + 2 * KC * TB);  // [col][row]
-  int *trow = reinterpret_cast<int *>(dyn + 2 * KC * TB + TB * (TB + 1));
-  int *relr = trow + TB, *relc = relr + TB;
+  double *stages = dyn;
+  int *trow = reinterpret_cast<int *>(dyn + 2 * STAGE);
+  int *ia = trow + TB, *ib = ia + TB;
   const int4 t = tasks[blockIdx.x];
   const int s = t.x, r0 = t.y, c0 = t.z;
+  const int p_begin = t.w, p_end = task_end[blockIdx.x];
   const int tid = threadIdx.x;
-  const int tx = tid & 15, ty = tid >> 4;
   const int f = S.super[s];
   const int w = S.super[s + 1] - f;
   const int64_t rb = S.rowptr[s];
   const int m = (int)(S.rowptr[s + 1] - rb);
   const int nrow = min(TB, m - r0), ncol = min(TB, w - c0);
-  for (int i = tid; i < nrow; i += NT) trow[i] = S.Ls[rb + r0 + i];
-  for (int e = tid; e < TB * (TB + 1); e += NT) (&Acc[0][0])[e] = 0.0;
-  __syncthreads();
-  const int gr_lo = trow[0], gr_hi = trow[nrow - 1];
-  const int gc_lo = f + c0, gc_hi = f + c0 + ncol - 1;
-
-  for (int q = S.upd_ptr[s]; q < S.upd_ptr[s + 1]; ++q) {
-    const int d = S.upd[q];
+  const int gc_lo = f + c0;
+  double *P = S.L + S.xptr[s];
+  for (int i = tid; i < nrow; i += MT) trow[i] = S.Ls[rb + r0 + i];
+  TileAcc acc;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = acc_row(i);
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int c = acc_col(j, e);
+        acc.v[i][j][e] = (r < nrow && c < ncol && r0 + r >= c0 + c)
+                             ? neg(P[(size_t)(c0 + c) * m + r0 + r]) : 0.0;
+      }
+  }
+  for (int q = p_begin; q < p_end; ++q) {
+    const int4 pr = pairs[q];
+    const int d = pr.x, a0 = pr.y, b0 = pr.z;
+    const int na = pr.w & 0xffff, nb = pr.w >> 16;
     const int wd = S.super[d + 1] - S.super[d];
     const int64_t rbd = S.rowptr[d];
     const int md = (int)(S.rowptr[d + 1] - rbd);
     const int *Lsd = S.Ls + rbd;
-    const int a0 = lbound(Lsd, md, gr_lo), a1 = lbound(Lsd, md, gr_hi + 1);
-    const int b0 = lbound(Lsd, md, gc_lo), b1 = lbound(Lsd, md, gc_hi + 1);
-    if (a0 >= a1 || b0 >= b1) continue;   // uniform across the CTA
-    int na = a1 - a0, nb = b1 - b0;
-    if (na > TB || nb > TB) { flag_structure_error(S); continue; }
+    __syncthreads();   // trow ready; the previous pair is done with ia / ib
+    if (tid < TB) { ia[tid] = -1; ib[tid] = -1; }
+    __syncthreads();
     if (tid < na) {
       const int key = Lsd[a0 + tid];
-      int pos = lbound(trow, nrow, key);
-      if (pos >= nrow || trow[pos] != key) { flag_structure_error(S); pos = -1; }
-      relr[tid] = pos;
+      const int pos = lbound(trow, nrow, key);
+      if (pos < nrow && trow[pos] == key) ia[pos] = a0 + tid;
+      else flag_structure_error(S);
     } else if (tid >= TB && tid < TB + nb) {
-      relc[tid - TB] = Lsd[b0 + tid - TB] - gc_lo;
+      const int cc = Lsd[b0 + tid - TB] - gc_lo;
+      if (cc >= 0 && cc < ncol) ib[cc] = b0 + tid - TB;
+      else flag_structure_error(S);
     }
-    double acc[4][4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
     const double *Ld = S.L + S.xptr[d];
-    tile_product(Ld + a0, md, na, Ld + b0, md, nb, wd, As, Bs, acc);
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int r = ty + 16 * i;
-      if (r >= na) continue;
-      const int rr = relr[r];
-      if (rr < 0) continue;
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int c = tx + 16 * j;
-        if (c < nb) Acc[relc[c]][rr] += acc[i][j];
-      }
-    }
-    __syncthreads();
+    dmma_tile_product_gather(Ld, md, ia, ib, wd, stages, acc);
   }
-  double *P = S.L + S.xptr[s];
-  for (int e = tid; e < TB * TB; e += NT) {
-    const int c = e / TB, r = e - c * TB;
-    if (r < nrow && c < ncol && trow[r] >= gc_lo + c)
-      P[(size_t)(c0 + c) * m + r0 + r] -= Acc[c][r];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = acc_row(i);
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int c = acc_col(j, e);
+        if (r < nrow && c < ncol && r0 + r >= c0 + c)
+          P[(size_t)(c0 + c) * m + r0 + r] = neg(acc.v[i][j][e]);
+      }
   }
 }
 
 // ---------------------------------------------------------------------------------------
 // Dense factorization of a tiled-class panel, blocked by 64 columns (right-looking):
-//   step j:  TRSM of the tiles below diagonal block j against the factored block,
-//            then the trailing SYRK/GEMM update of the column blocks after j; the CTA that
-//            owns diagonal tile j+1 factors it (POTRF) right after its update, so every
+//   step j:  TRSM of the tiles below diagonal block j (k_trsm_step), then, concurrently,
+//            the trailing SYRK/GEMM update of the column blocks after j (k_syrk_step) and
+//            the update + POTRF + inverse of diagonal block j+1 (k_diag_step), so every
 //            diagonal block is factored before the next step's TRSM reads it.
-//   block 0 is factored by k_potrf_first.
+//   block 0 is factored by k_diag_step with step 0.
 
-// In-place lower Cholesky of the bw x bw block D (shared memory, [column][row]); the
-// first non-positive pivot's global column + 1 goes to status[0] when `report`.
-__device__ void potrf_smem(double (*D)[TB + 1], int bw, const DevSym &S, int gcol0, bool report) {
-  const int tid = threadIdx.x;
-  for (int j = 0; j < bw; ++j) {
-    const double djj = D[j][j];
-    const double dsq = sqrt(djj);
-    if (report && tid == 0 && !(djj > 0.0)) atomicMin(&S.status[0], gcol0 + j + 1);
+// ---- one 64x64 diagonal block: POTRF and its inverse, blocked by 8 ----------------------
+// Every 8x8 block product runs on the tensor cores (DMMA); scalar FP64 work is limited to
+// the 8x8 diagonal pieces, done by one warp with shuffles.  D and E are [column][row]
+// shared arrays with leading dimension DLD; 128 threads (4 warps).
+constexpr int DLD = TB + 1;
+
+// c += A_blk * B_blk^T for 8x8 blocks of [column][row] arrays: A_blk = rows ar0..ar0+7,
+// columns ak0..ak0+7 of Am; B_blk = rows bn0..bn0+7, columns bk0..bk0+7 of Bm.
+__device__ __forceinline__ void mma8_abt(double (&c)[2], const double *Am, int ar0, int ak0,
+                                         const double *Bm, int bn0, int bk0, bool negate_a) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, kq = lane & 3;
+#pragma unroll
+  for (int t = 0; t < 2; ++t) {
+    const double a = Am[(ak0 + 4 * t + kq) * DLD + ar0 + g];
+    const double b = Bm[(bk0 + 4 * t + kq) * DLD + bn0 + g];
+    dmma(c, negate_a ? neg(a) : a, b);
+  }
+}
+
+// c += A_blk * B_blk for 8x8 blocks: A_blk as above, B_blk = rows bk0..bk0+7 (the k index),
+// columns bn0..bn0+7 of Bm.
+__device__ __forceinline__ void mma8_ab(double (&c)[2], const double *Am, int ar0, int ak0,
+                                        const double *Bm, int bk0, int bn0) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, kq = lane & 3;
+#pragma unroll
+  for (int t = 0; t < 2; ++t) {
+    const double a = Am[(ak0 + 4 * t + kq) * DLD + ar0 + g];
+    const double b = Bm[(bn0 + g) * DLD + bk0 + 4 * t + kq];
+    dmma(c, a, b);
+  }
+}
+
+__device__ __forceinline__ void load8(double (&c)[2], const double *X, int r0, int c0) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, kq = lane & 3;
+  c[0] = X[(c0 + 2 * kq) * DLD + r0 + g];
+  c[1] = X[(c0 + 2 * kq + 1) * DLD + r0 + g];
+}
+__device__ __forceinline__ void store8(const double (&c)[2], double *X, int r0, int c0, bool lower_only) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, kq = lane & 3;
+#pragma unroll
+  for (int e = 0; e < 2; ++e)
+    if (!lower_only || g >= 2 * kq + e) X[(c0 + 2 * kq + e) * DLD + r0 + g] = c[e];
+}
+
+// Warp-level Cholesky of the 8x8 diagonal block kb of D and its inverse into E (same
+// position).  Lane r < 8 holds row r; each column is broadcast through `bc` (8 doubles of
+// shared scratch).  Pivot: the column is scaled by 1/sqrt(pivot), which is also kept for
+// the inverse's diagonal, so the inverse needs no division.
+__device__ void potrf8_inv8(double *D, double *E, double *bc, int kb, const DevSym &S,
+                            int gcol0, int bw, bool report) {
+  const int lane = threadIdx.x & 31, r = lane & 7, k0 = 8 * kb;
+  double x[8], rd[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) x[c] = (c <= r) ? D[(k0 + c) * DLD + k0 + r] : 0.0;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const double piv = __shfl_sync(0xffffffffu, x[c], c);
+    const double dsq = sqrt(piv), inv = 1.0 / dsq;
+    rd[c] = inv;
+    if (report && lane == 0 && k0 + c < bw && !(piv > 0.0))
+      atomicMin(&S.status[0], gcol0 + k0 + c + 1);
+    x[c] = (r == c) ? dsq : ((r > c) ? x[c] * inv : x[c]);
+    if (lane < 8) bc[r] = x[c];
+    __syncwarp();
+#pragma unroll
+    for (int c2 = c + 1; c2 < 8; ++c2)
+      if (r >= c2) x[c2] = fma(-x[c], bc[c2], x[c2]);
+    __syncwarp();
+  }
+  if (lane < 8) {
+#pragma unroll
+    for (int c = 0; c < 8; ++c)
+      if (c <= r) D[(k0 + c) * DLD + k0 + r] = x[c];
+  }
+  __syncwarp();
+  // lane j < 8: column j of the inverse by forward substitution, 1/L(i,i) = rd[i]
+  const int j = r;
+  double t[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < i; ++k)
+      if (k >= j) s = fma(D[(k0 + k) * DLD + k0 + i], t[k], s);
+    t[i] = (i < j) ? 0.0 : ((i == j) ? rd[i] : -s * rd[i]);
+  }
+  if (lane < 8) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) E[(k0 + j) * DLD + k0 + i] = t[i];
+  }
+  __syncwarp();
+}
+
+// D: bw x bw lower block padded to a multiple of 8 with identity.  Factors it in place
+// (right-looking over 8-column blocks) and leaves the inverses of its 8x8 diagonal blocks
+// in E.
+__device__ void potrf64_blocked(double *D, double *E, double *bc, int bw, const DevSym &S,
+                                int gcol0) {
+  const int warp = threadIdx.x >> 5;
+  const int nbk = (bw + 7) >> 3;
+  for (int kb = 0; kb < nbk; ++kb) {
+    if (warp == 0) potrf8_inv8(D, E, bc, kb, S, gcol0, bw, true);
     __syncthreads();
-    if (tid >= j && tid < bw) D[j][tid] = (tid == j) ? dsq : D[j][tid] / dsq;
-    __syncthreads();
-    const int nc = bw - j - 1;
-    for (int e = tid; e < nc * bw; e += NT) {
-      const int c = j + 1 + e / bw, r = e - (c - j - 1) * bw;
-      if (r >= c) D[c][r] -= D[j][r] * D[j][c];
+    // panel below: X_ib = B_ib * T_kk^T
+    for (int ib = kb + 1 + warp; ib < nbk; ib += 4) {
+      double c[2] = {0.0, 0.0};
+      mma8_abt(c, D, 8 * ib, 8 * kb, E, 8 * kb, 8 * kb, false);
+      __syncwarp();
+      store8(c, D, 8 * ib, 8 * kb, false);
     }
+    __syncthreads();
+    // trailing update: D_ib,jb -= X_ib X_jb^T for kb < jb <= ib
+    int q = 0;
+    for (int jb = kb + 1; jb < nbk; ++jb)
+      for (int ib = jb; ib < nbk; ++ib, ++q) {
+        if ((q & 3) != warp) continue;
+        double c[2];
+        load8(c, D, 8 * ib, 8 * jb);
+        mma8_abt(c, D, 8 * ib, 8 * kb, D, 8 * jb, 8 * kb, true);
+        store8(c, D, 8 * ib, 8 * jb, ib == jb);
+      }
     __syncthreads();
   }
 }
 
-// Factor diagonal block `c0/64` of supernode s in place (lower triangle only).
-__device__ void factor_diag_block(const DevSym &S, int s, int c0, double (*D)[TB + 1]) {
+// Inverse of the factored block: off-diagonal 8x8 blocks T_ik = -T_ii sum_{j=k}^{i-1}
+// L_ij T_jk, one column block per warp (E holds T_kk on entry; W: 64 doubles per warp).
+__device__ void trtri64_blocked(const double *D, double *E, double *W, int bw) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, kq = lane & 3;
+  const int nbk = (bw + 7) >> 3;
+  double *Ww = W + warp * 64;
+  for (int k = warp; k < nbk; k += 4) {
+    for (int i = k + 1; i < nbk; ++i) {
+      double sacc[2] = {0.0, 0.0};
+      for (int j = k; j < i; ++j) mma8_ab(sacc, D, 8 * i, 8 * j, E, 8 * j, 8 * k);
+      // S (C layout) -> W[col * 8 + row], read back as the B operand of T_ii * S
+      Ww[(2 * kq) * 8 + g] = sacc[0];
+      Ww[(2 * kq + 1) * 8 + g] = sacc[1];
+      __syncwarp();
+      double c[2] = {0.0, 0.0};
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        const double a = neg(E[(8 * i + 4 * t + kq) * DLD + 8 * i + g]);
+        const double b = Ww[g * 8 + 4 * t + kq];
+        dmma(c, a, b);
+      }
+      store8(c, E, 8 * i, 8 * k, false);
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+}
+
+// Factor diagonal block c0/64 of supernode s in place (lower triangle only) and, when rows
+// follow below it, store its inverse (T(r, c) at dinv[c * 64 + r]) for their TRSM.
+// 128 threads, DIAG_SMEM bytes of dynamic shared memory.
+constexpr int DIAG_SMEM = (2 * TB * DLD + 4 * 64) * 8;
+
+__device__ void factor_diag_block(const DevSym &S, int s, int c0, double *smem) {
+  double *D = smem, *E = smem + TB * DLD, *W = E + TB * DLD;
   const int tid = threadIdx.x;
   const int f = S.super[s];
   const int w = S.super[s + 1] - f;
@@ -301,34 +577,87 @@ __device__ void factor_diag_block(const DevSym &S, int s, int c0, double (*D)[TB
   double *P = S.L + S.xptr[s];
   const int bw = min(TB, w - c0);
   __syncthreads();
-  for (int e = tid; e < bw * bw; e += NT) {
-    const int c = e / bw, r = e - c * bw;
-    D[c][r] = (r >= c) ? P[(size_t)(c0 + c) * m + c0 + r] : 0.0;
+  for (int e = tid; e < TB * TB; e += blockDim.x) {
+    const int c = e >> 6, r = e & (TB - 1);
+    double v;
+    if (c < bw && r < bw) v = (r >= c) ? P[(size_t)(c0 + c) * m + c0 + r] : 0.0;
+    else v = (r == c) ? 1.0 : 0.0;
+    D[c * DLD + r] = v;
+    E[c * DLD + r] = 0.0;
   }
   __syncthreads();
-  potrf_smem(D, bw, S, f + c0, true);
-  for (int e = tid; e < bw * bw; e += NT) {
-    const int c = e / bw, r = e - c * bw;
-    if (r >= c) P[(size_t)(c0 + c) * m + c0 + r] = D[c][r];
+  potrf64_blocked(D, E, W, bw, S, f + c0);
+  for (int e = tid; e < TB * TB; e += blockDim.x) {
+    const int c = e >> 6, r = e & (TB - 1);
+    if (c < bw && r < bw && r >= c) P[(size_t)(c0 + c) * m + c0 + r] = D[c * DLD + r];
+  }
+  if (c0 + bw < m) {
+    trtri64_blocked(D, E, W, bw);
+    double *T = S.dinv + ((size_t)S.dinv_off[s] + c0 / TB) * (TB * TB);
+    for (int e = tid; e < TB * TB; e += blockDim.x) {
+      const int c = e >> 6, r = e & (TB - 1);
+      T[e] = (c < bw && r < bw && r >= c) ? E[c * DLD + r] : 0.0;
+    }
   }
 }
 
-constexpr int PANEL_SMEM = 2 * TB * (TB + 1) * 8;
-
-// One CTA per supernode of the list: factor diagonal block 0.
-__global__ void __launch_bounds__(NT) k_potrf_first(DevSym S, const int *list, int count) {
-  __shared__ double D[TB][TB + 1];
-  factor_diag_block(S, list[blockIdx.x], 0, D);
+// Trailing SYRK/GEMM update of one 64x64 tile of a tiled-class panel by column block
+// `kblk`: tile(r0, c0) -= L[r0:, kblk] L[c0:, kblk]^T.  The accumulator is seeded with
+// minus the tile, so the tensor cores produce -(C - A B^T); stored back negated.
+__device__ void syrk_tile(const DevSym &S, int s, int r0, int c0, int kblk, double *stages) {
+  const int f = S.super[s];
+  const int w = S.super[s + 1] - f;
+  const int m = (int)(S.rowptr[s + 1] - S.rowptr[s]);
+  double *P = S.L + S.xptr[s];
+  const int k0 = kblk * TB;
+  const int bk = min(TB, w - k0);
+  const int nrow = min(TB, m - r0), ncol = min(TB, w - c0);
+  TileAcc acc;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = acc_row(i);
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int c = acc_col(j, e);
+        acc.v[i][j][e] = (r < nrow && c < ncol && r0 + r >= c0 + c)
+                             ? neg(P[(size_t)(c0 + c) * m + r0 + r]) : 0.0;
+      }
+  }
+  dmma_tile_product(P + (size_t)k0 * m + r0, m, nrow, P + (size_t)k0 * m + c0, m, ncol, bk,
+                    stages, acc);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = acc_row(i);
+    if (r >= nrow) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int c = acc_col(j, e);
+        if (c < ncol && r0 + r >= c0 + c) P[(size_t)(c0 + c) * m + r0 + r] = neg(acc.v[i][j][e]);
+      }
+  }
 }
 
-// task = (s, r0): B = L[r0:r0+64, blk] := B * L_blk^{-T}, L_blk already factored.
-__global__ void __launch_bounds__(NT) k_trsm_step(DevSym S, const int2 *tasks, int count,
+// One CTA per supernode of the list: bring diagonal block `step` up to date (its update by
+// column block step-1, which the SYRK launch of that step leaves out) and factor it.
+__global__ void __launch_bounds__(MT) k_diag_step(DevSym S, const int *list, int count, int step) {
+  extern __shared__ double dyn[];
+  const int s = list[blockIdx.x];
+  const int c0 = step * TB;
+  if (step > 0) syrk_tile(S, s, c0, c0, step - 1, dyn);
+  factor_diag_block(S, s, c0, dyn);
+}
+
+// task = (s, r0): B = L[r0:r0+64, blk] := B * L_blk^{-T} = B * T^T with T = L_blk^{-1},
+// stored by the CTA that factored the block (T(r, c) at T[c * 64 + r]), as one DMMA tile
+// product.
+__global__ void __launch_bounds__(MT) k_trsm_step(DevSym S, const int2 *tasks, int count,
                                                   int step) {
   extern __shared__ double dyn[];
-  double(*D)[TB + 1] = reinterpret_cast<double(*)[TB + 1]>(dyn);   // [column][row]
-  double(*B)[TB + 1] = reinterpret_cast<double(*)[TB + 1]>(dyn + TB * (TB + 1));
   const int s = tasks[blockIdx.x].x, r0 = tasks[blockIdx.x].y;
-  const int tid = threadIdx.x;
   const int f = S.super[s];
   const int w = S.super[s + 1] - f;
   const int m = (int)(S.rowptr[s + 1] - S.rowptr[s]);
@@ -336,72 +665,34 @@ __global__ void __launch_bounds__(NT) k_trsm_step(DevSym S, const int2 *tasks, i
   const int c0 = step * TB;
   const int bw = min(TB, w - c0);
   const int nr = min(TB, m - r0);
-  for (int e = tid; e < bw * bw; e += NT) {
-    const int c = e / bw, r = e - c * bw;
-    D[c][r] = (r >= c) ? P[(size_t)(c0 + c) * m + c0 + r] : 0.0;
-  }
-  for (int e = tid; e < nr * bw; e += NT) {
-    const int c = e / nr, r = e - c * nr;
-    B[c][r] = P[(size_t)(c0 + c) * m + r0 + r];
-  }
-  __syncthreads();
-  // X D^T = B, column by column
-  for (int c = 0; c < bw; ++c) {
-    if (tid < nr) B[c][tid] = B[c][tid] / D[c][c];
-    __syncthreads();
-    const int nc = bw - c - 1;
-    for (int e = tid; e < nr * nc; e += NT) {
-      const int c2 = c + 1 + e / nr, r = e - (c2 - c - 1) * nr;
-      B[c2][r] -= B[c][r] * D[c][c2];
-    }
-    __syncthreads();
-  }
-  for (int e = tid; e < nr * bw; e += NT) {
-    const int c = e / nr, r = e - c * nr;
-    P[(size_t)(c0 + c) * m + r0 + r] = B[c][r];
+  const double *T = S.dinv + ((size_t)S.dinv_off[s] + step) * (TB * TB);
+  TileAcc acc;
+  acc.zero();
+  // X[r][c] = sum_k B[r][k] T(c, k); operand element (row c, column k) = T[k * 64 + c]
+  dmma_tile_product(P + (size_t)c0 * m + r0, m, nr, T, TB, bw, bw, dyn, acc);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = acc_row(i);
+    if (r >= nr) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int c = acc_col(j, e);
+        if (c < bw) P[(size_t)(c0 + c) * m + r0 + r] = acc.v[i][j][e];
+      }
   }
 }
 
-// Trailing update of step `step`: task = (s, r0, c0) with c0 >= (step+1)*64, r0 >= c0:
-// tile(r0, c0) -= L[r0:, blk] * L[c0:, blk]^T over the step's column block.  The CTA
-// holding tile (c0, c0) with c0 == (step+1)*64 then factors that diagonal block.
-__global__ void __launch_bounds__(NT) k_syrk_step(DevSym S, const int4 *tasks, int count,
+// Trailing update of step `step`: task = (s, r0, c0) with c0 >= (step+1)*64, r0 >= c0.
+// The diagonal tile of the next block is left to k_diag_step, which runs concurrently.
+constexpr int SYRK_SMEM = 2 * STAGE * 8;
+
+__global__ void __launch_bounds__(MT) k_syrk_step(DevSym S, const int4 *tasks, int count,
                                                   int step) {
-  __shared__ double buf[TB * (TB + 1)];
-  double(*As)[TB] = reinterpret_cast<double(*)[TB]>(buf);
-  double(*Bs)[TB] = reinterpret_cast<double(*)[TB]>(buf + KC * TB);
+  extern __shared__ double dyn[];
   const int4 t = tasks[blockIdx.x];
-  const int s = t.x, r0 = t.y, c0 = t.z;
-  const int tid = threadIdx.x;
-  const int tx = tid & 15, ty = tid >> 4;
-  const int f = S.super[s];
-  const int w = S.super[s + 1] - f;
-  const int m = (int)(S.rowptr[s + 1] - S.rowptr[s]);
-  double *P = S.L + S.xptr[s];
-  const int k0 = step * TB;
-  const int bk = min(TB, w - k0);
-  const int nrow = min(TB, m - r0), ncol = min(TB, w - c0);
-  double acc[4][4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-  tile_product(P + (size_t)k0 * m + r0, m, nrow, P + (size_t)k0 * m + c0, m, ncol, bk, As,
-               Bs, acc);
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int r = ty + 16 * i;
-    if (r >= nrow) continue;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int c = tx + 16 * j;
-      if (c < ncol && r0 + r >= c0 + c) P[(size_t)(c0 + c) * m + r0 + r] -= acc[i][j];
-    }
-  }
-  if (r0 == c0 && c0 == k0 + TB) {
-    // writes above are visible to the whole CTA after the barrier inside factor_diag_block
-    factor_diag_block(S, s, c0, reinterpret_cast<double(*)[TB + 1]>(buf));
-  }
+  syrk_tile(S, t.x, t.y, t.z, step, dyn);
 }
 
 __global__ void k_init_status(int *status) {
@@ -417,7 +708,11 @@ bool kernels_configure(std::string &err) {
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_update_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, UPD_SMEM);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_trsm_step, cudaFuncAttributeMaxDynamicSharedMemorySize, PANEL_SMEM);
+    e = cudaFuncSetAttribute(k_trsm_step, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * STAGE * 8);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_diag_step, cudaFuncAttributeMaxDynamicSharedMemorySize, DIAG_SMEM);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_syrk_step, cudaFuncAttributeMaxDynamicSharedMemorySize, SYRK_SMEM);
   if (e != cudaSuccess) {
     err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e);
     return false;
@@ -431,17 +726,18 @@ void launch_factor_small(const DevSym &S, const int *list, int count, int smem, 
 void launch_assemble(const DevSym &S, const int2 *tasks, int count, cudaStream_t st) {
   if (count > 0) k_assemble<<<(count * 32 + NT - 1) / NT, NT, 0, st>>>(S, tasks, count);
 }
-void launch_update_tiles(const DevSym &S, const int4 *tasks, int count, cudaStream_t st) {
-  if (count > 0) k_update_tiles<<<count, NT, UPD_SMEM, st>>>(S, tasks, count);
+void launch_update_tiles(const DevSym &S, const int4 *tasks, const int *task_end,
+                         const int4 *pairs, int count, cudaStream_t st) {
+  if (count > 0) k_update_tiles<<<count, MT, UPD_SMEM, st>>>(S, tasks, task_end, pairs, count);
 }
-void launch_potrf_first(const DevSym &S, const int *list, int count, cudaStream_t st) {
-  if (count > 0) k_potrf_first<<<count, NT, 0, st>>>(S, list, count);
+void launch_diag_step(const DevSym &S, const int *list, int count, int step, cudaStream_t st) {
+  if (count > 0) k_diag_step<<<count, MT, DIAG_SMEM, st>>>(S, list, count, step);
 }
 void launch_trsm_step(const DevSym &S, const int2 *tasks, int count, int step, cudaStream_t st) {
-  if (count > 0) k_trsm_step<<<count, NT, PANEL_SMEM, st>>>(S, tasks, count, step);
+  if (count > 0) k_trsm_step<<<count, MT, 2 * STAGE * 8, st>>>(S, tasks, count, step);
 }
 void launch_syrk_step(const DevSym &S, const int4 *tasks, int count, int step, cudaStream_t st) {
-  if (count > 0) k_syrk_step<<<count, NT, 0, st>>>(S, tasks, count, step);
+  if (count > 0) k_syrk_step<<<count, MT, SYRK_SMEM, st>>>(S, tasks, count, step);
 }
 void launch_init_status(int *status, cudaStream_t st) { k_init_status<<<1, 1, 0, st>>>(status); }
 

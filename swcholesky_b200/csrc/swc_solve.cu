@@ -1,0 +1,310 @@
+// Supernodal triangular solves, sparse matrix-vector product and vector kernels for
+// iterative refinement.  No reference counterpart for the backward solve; the forward
+// solve follows the reference's layout-compatible blockedLsolve
+// (triangularSolve/Triangular_BCSC.h:14-48) in gather (left-looking) form, so every
+// supernode of a level runs in parallel with no atomics and a fixed summation order.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "swc_engine.h"
+
+namespace swc {
+
+namespace {
+
+constexpr int ST = 256;   // threads of the solve kernels
+constexpr int SB = 32;    // column block of the dense triangular solves (one warp)
+
+__device__ __forceinline__ int lbound_s(const int *a, int len, int key) {
+  int lo = 0, hi = len;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (a[mid] < key) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+// Forward solve, level by level (leaves first), in two kernels per level:
+//   k_fwd_diag    y[cols of s] := L_ss^{-1} (y[cols of s] - sum over descendants d of
+//                 their contributions to those rows), one CTA per supernode; the
+//                 descendants' contributions were stored by k_fwd_contrib, so the gather
+//                 costs one subtraction per contributed row, in prune-set order.
+//   k_fwd_contrib c_s = L_s[rows below the diagonal block, :] y[cols of s], one CTA per
+//                 256-row slab: the off-diagonal GEMV of every supernode runs in parallel.
+// c_s lives at contrib + rowptr[s] - super[s] (one entry per off-diagonal row).
+__global__ void __launch_bounds__(ST) k_fwd_diag(DevSym S, const int *list, double *y,
+                                                 const double *contrib, int n, int nrhs,
+                                                 int64_t cstride) {
+  extern __shared__ double v[];
+  const int s = list[blockIdx.x];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int f = S.super[s], w = S.super[s + 1] - f;
+  const int m = (int)(S.rowptr[s + 1] - S.rowptr[s]);
+  const double *Ls_s = S.L + S.xptr[s];
+  for (int rhs = 0; rhs < nrhs; ++rhs) {
+    double *yr = y + (size_t)rhs * n;
+    const double *cr = contrib + (size_t)rhs * cstride;
+    __syncthreads();
+    for (int i = tid; i < w; i += ST) v[i] = yr[f + i];
+    __syncthreads();
+    for (int q = S.upd_ptr[s]; q < S.upd_ptr[s + 1]; ++q) {
+      const int d = S.upd[q];
+      const int fd = S.super[d], wd = S.super[d + 1] - fd;
+      const int64_t rbd = S.rowptr[d];
+      const int md = (int)(S.rowptr[d + 1] - rbd);
+      const int *Lsd = S.Ls + rbd;
+      const int lb = wd + lbound_s(Lsd + wd, md - wd, f);
+      const int ub = wd + lbound_s(Lsd + wd, md - wd, f + w);
+      const double *cd = cr + (rbd - fd) - wd;   // cd[a] for a >= wd
+      for (int a = lb + tid; a < ub; a += ST) v[Lsd[a] - f] -= cd[a];
+      __syncthreads();
+    }
+    // dense lower solve with the diagonal block, blocked by SB columns
+    for (int j0 = 0; j0 < w; j0 += SB) {
+      const int jb = min(SB, w - j0);
+      if (warp == 0) {
+        double x = (lane < jb) ? v[j0 + lane] : 0.0;
+        for (int j = 0; j < jb; ++j) {
+          const double xj = __shfl_sync(0xffffffffu, x, j) / Ls_s[(size_t)(j0 + j) * m + j0 + j];
+          if (lane == j) x = xj;
+          if (lane > j && lane < jb) x = fma(-Ls_s[(size_t)(j0 + j) * m + j0 + lane], xj, x);
+        }
+        if (lane < jb) v[j0 + lane] = x;
+      }
+      __syncthreads();
+      for (int i = j0 + jb + tid; i < w; i += ST) {
+        double acc = v[i];
+        for (int j = 0; j < jb; ++j) acc = fma(-Ls_s[(size_t)(j0 + j) * m + i], v[j0 + j], acc);
+        v[i] = acc;
+      }
+      __syncthreads();
+    }
+    for (int i = tid; i < w; i += ST) yr[f + i] = v[i];
+  }
+}
+
+// task = (s, r0): rows r0..r0+255 of supernode s's off-diagonal block (r0 >= w).
+__global__ void __launch_bounds__(ST) k_fwd_contrib(DevSym S, const int2 *tasks,
+                                                    const double *y, double *contrib, int n,
+                                                    int nrhs, int64_t cstride) {
+  const int s = tasks[blockIdx.x].x, r0 = tasks[blockIdx.x].y;
+  const int f = S.super[s], w = S.super[s + 1] - f;
+  const int64_t rb = S.rowptr[s];
+  const int m = (int)(S.rowptr[s + 1] - rb);
+  const double *Ls_s = S.L + S.xptr[s];
+  const int a = r0 + threadIdx.x;
+  if (a >= m) return;
+  for (int rhs = 0; rhs < nrhs; ++rhs) {
+    const double *yr = y + (size_t)rhs * n + f;
+    double acc0 = 0.0, acc1 = 0.0;
+    int k = 0;
+    for (; k + 1 < w; k += 2) {
+      acc0 = fma(Ls_s[(size_t)k * m + a], yr[k], acc0);
+      acc1 = fma(Ls_s[(size_t)(k + 1) * m + a], yr[k + 1], acc1);
+    }
+    if (k < w) acc0 = fma(Ls_s[(size_t)k * m + a], yr[k], acc0);
+    contrib[(size_t)rhs * cstride + (rb - f) + (a - w)] = acc0 + acc1;
+  }
+}
+
+// Backward solve, level by level (root first):
+//   k_bwd_gather  x[f + j] := x[f + j] - sum_{a >= w} L(a, j) x[rows[a]] for the columns
+//                 j0..j0+31 of s (one warp per column); the rows below are columns of
+//                 ancestors, already solved.
+//   k_bwd_diag    x[cols of s] := L_ss^{-T} x[cols of s], one CTA per supernode.
+__global__ void __launch_bounds__(ST) k_bwd_gather(DevSym S, const int2 *tasks, double *x,
+                                                   int n, int nrhs) {
+  const int s = tasks[blockIdx.x].x, j0 = tasks[blockIdx.x].y;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int f = S.super[s], w = S.super[s + 1] - f;
+  const int64_t rb = S.rowptr[s];
+  const int m = (int)(S.rowptr[s + 1] - rb);
+  const int *rows = S.Ls + rb;
+  const double *Ls_s = S.L + S.xptr[s];
+  for (int rhs = 0; rhs < nrhs; ++rhs) {
+    double *xr = x + (size_t)rhs * n;
+    for (int j = j0 + warp; j < min(w, j0 + SB); j += ST / 32) {
+      double acc = 0.0;
+      for (int a = w + lane; a < m; a += 32) acc = fma(Ls_s[(size_t)j * m + a], xr[rows[a]], acc);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if (lane == 0) xr[f + j] -= acc;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(ST) k_bwd_diag(DevSym S, const int *list, double *x, int n,
+                                                 int nrhs) {
+  extern __shared__ double v[];
+  const int s = list[blockIdx.x];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int f = S.super[s], w = S.super[s + 1] - f;
+  const int m = (int)(S.rowptr[s + 1] - S.rowptr[s]);
+  const double *Ls_s = S.L + S.xptr[s];
+  for (int rhs = 0; rhs < nrhs; ++rhs) {
+    double *xr = x + (size_t)rhs * n;
+    __syncthreads();
+    for (int i = tid; i < w; i += ST) v[i] = xr[f + i];
+    __syncthreads();
+    for (int j1 = w; j1 > 0; j1 -= SB) {
+      const int j0 = max(0, j1 - SB), jb = j1 - j0;
+      // v[j0..j1) -= sum_{i >= j1} L(i, j) v[i]
+      for (int j = j0 + warp; j < j1; j += ST / 32) {
+        double acc = 0.0;
+        for (int i = j1 + lane; i < w; i += 32) acc = fma(Ls_s[(size_t)j * m + i], v[i], acc);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) v[j] -= acc;
+      }
+      __syncthreads();
+      if (warp == 0) {
+        double xv = (lane < jb) ? v[j0 + lane] : 0.0;
+        for (int jj = jb - 1; jj >= 0; --jj) {
+          const double xj = __shfl_sync(0xffffffffu, xv, jj) /
+                            Ls_s[(size_t)(j0 + jj) * m + j0 + jj];
+          if (lane == jj) xv = xj;
+          if (lane < jj) xv = fma(-Ls_s[(size_t)(j0 + lane) * m + j0 + jj], xj, xv);
+        }
+        if (lane < jb) v[j0 + lane] = xv;
+      }
+      __syncthreads();
+    }
+    for (int i = tid; i < w; i += ST) xr[f + i] = v[i];
+  }
+}
+
+// y = A x for the symmetric matrix held as full CSR (both triangles), nrhs vectors.
+__global__ void k_spmv(int n, const int *rp, const int *ci, const double *val, const double *x,
+                       double *y, int nrhs) {
+  const int row = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  for (int r = 0; r < nrhs; ++r) {
+    const double *xr = x + (size_t)r * n;
+    double acc = 0.0;
+    for (int p = rp[row] + lane; p < rp[row + 1]; p += 32) acc = fma(val[p], xr[ci[p]], acc);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) y[(size_t)r * n + row] = acc;
+  }
+}
+
+// out[i] = sum_j |A(i, j)| (rows of the full CSR)
+__global__ void k_rowabs(int n, const int *rp, const double *val, double *out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double acc = 0.0;
+  for (int p = rp[i]; p < rp[i + 1]; ++p) acc += fabs(val[p]);
+  out[i] = acc;
+}
+
+// full-CSR values from the lower-CSC values through the precomputed map
+__global__ void k_gather_vals(int nnz, const int *map, const double *ax, double *val) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nnz) val[i] = ax[map[i]];
+}
+
+// r = b - r (r holds A x on entry)
+__global__ void k_residual(size_t len, const double *b, double *r) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < len) r[i] = b[i] - r[i];
+}
+
+// p = z + beta p
+__global__ void k_xpby(size_t len, const double *z, double beta, double *p) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < len) p[i] = fma(beta, p[i], z[i]);
+}
+
+__global__ void k_axpy(size_t len, double a, const double *x, double *y) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < len) y[i] = fma(a, x[i], y[i]);
+}
+
+// per-vector max |x| and sum x*y for nrhs vectors of length n (out[2*r], out[2*r+1]),
+// deterministic: one CTA per vector, fixed reduction tree.
+__global__ void k_norms(int n, const double *x, const double *y, double *out) {
+  __shared__ double smax[ST], sdot[ST];
+  const int r = blockIdx.x;
+  const double *xr = x + (size_t)r * n, *yr = y ? y + (size_t)r * n : nullptr;
+  double mx = 0.0, dt = 0.0;
+  for (int i = threadIdx.x; i < n; i += ST) {
+    mx = fmax(mx, fabs(xr[i]));
+    if (yr) dt = fma(xr[i], yr[i], dt);
+  }
+  smax[threadIdx.x] = mx;
+  sdot[threadIdx.x] = dt;
+  __syncthreads();
+  for (int o = ST / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      smax[threadIdx.x] = fmax(smax[threadIdx.x], smax[threadIdx.x + o]);
+      sdot[threadIdx.x] += sdot[threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[2 * r] = smax[0];
+    out[2 * r + 1] = sdot[0];
+  }
+}
+
+}  // namespace
+
+bool solve_configure(int max_w, std::string &err) {
+  size_t smem = sizeof(double) * (size_t)(max_w > 0 ? max_w : 1);
+  if (smem > 220 * 1024) {
+    err = "supernode too wide for the shared-memory triangular solve";
+    return false;
+  }
+  cudaError_t e = cudaFuncSetAttribute(k_fwd_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_bwd_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) {
+    err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e);
+    return false;
+  }
+  return true;
+}
+
+void launch_fwd_diag(const DevSym &S, const int *list, int count, int smem, double *y,
+                     const double *contrib, int n, int nrhs, int64_t cstride, cudaStream_t st) {
+  if (count > 0) k_fwd_diag<<<count, ST, smem, st>>>(S, list, y, contrib, n, nrhs, cstride);
+}
+void launch_fwd_contrib(const DevSym &S, const int2 *tasks, int count, const double *y,
+                        double *contrib, int n, int nrhs, int64_t cstride, cudaStream_t st) {
+  if (count > 0) k_fwd_contrib<<<count, ST, 0, st>>>(S, tasks, y, contrib, n, nrhs, cstride);
+}
+void launch_bwd_gather(const DevSym &S, const int2 *tasks, int count, double *x, int n, int nrhs,
+                       cudaStream_t st) {
+  if (count > 0) k_bwd_gather<<<count, ST, 0, st>>>(S, tasks, x, n, nrhs);
+}
+void launch_bwd_diag(const DevSym &S, const int *list, int count, int smem, double *x, int n,
+                     int nrhs, cudaStream_t st) {
+  if (count > 0) k_bwd_diag<<<count, ST, smem, st>>>(S, list, x, n, nrhs);
+}
+void launch_spmv(int n, const int *rp, const int *ci, const double *val, const double *x,
+                 double *y, int nrhs, cudaStream_t st) {
+  const int warps = 8;
+  k_spmv<<<(n + warps - 1) / warps, warps * 32, 0, st>>>(n, rp, ci, val, x, y, nrhs);
+}
+void launch_gather_vals(int nnz, const int *map, const double *ax, double *val, cudaStream_t st) {
+  if (nnz > 0) k_gather_vals<<<(nnz + 255) / 256, 256, 0, st>>>(nnz, map, ax, val);
+}
+void launch_rowabs(int n, const int *rp, const double *val, double *out, cudaStream_t st) {
+  k_rowabs<<<(n + 255) / 256, 256, 0, st>>>(n, rp, val, out);
+}
+void launch_residual(size_t len, const double *b, double *r, cudaStream_t st) {
+  if (len) k_residual<<<(unsigned)((len + 255) / 256), 256, 0, st>>>(len, b, r);
+}
+void launch_xpby(size_t len, const double *z, double beta, double *p, cudaStream_t st) {
+  if (len) k_xpby<<<(unsigned)((len + 255) / 256), 256, 0, st>>>(len, z, beta, p);
+}
+void launch_axpy(size_t len, double a, const double *x, double *y, cudaStream_t st) {
+  if (len) k_axpy<<<(unsigned)((len + 255) / 256), 256, 0, st>>>(len, a, x, y);
+}
+void launch_norms(int n, int nrhs, const double *x, const double *y, double *out, cudaStream_t st) {
+  k_norms<<<nrhs, ST, 0, st>>>(n, x, y, out);
+}
+
+}  // namespace swc
