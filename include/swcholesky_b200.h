@@ -101,6 +101,22 @@ int swc_solve(swc_handle_t handle, const double *b, double *x, int nrhs, int on_
 int swc_refine(swc_handle_t handle, const double *b, double *x, int nrhs, int on_device,
                double tol, int maxit, double *berr, int *iterations, int *method);
 
+/* Allocation-free variant of swc_solve, for callers that cannot allocate device memory
+ * when they solve (their device memory is owned by a pool that forbids further CUDA
+ * allocations, their host only allows allocation at start-up, or the implicit
+ * synchronisation of cudaMalloc is not acceptable in their loop).  No counterpart in the
+ * reference.  Same result as swc_solve with on_device = 1 (b and x are device pointers on
+ * the handle's GPU; the handle was analysed and factored before); its scratch is a fixed
+ * array of SWC_SOLVE_NOALLOC_MAX doubles (8 MiB) in the library's device image, held by
+ * every GPU that loads the library until the process exits.  It needs (number of
+ * off-diagonal rows of L) x nrhs doubles, i.e. (Li_ptr[n] - n) * nrhs <= SWC_SOLVE_NOALLOC_MAX,
+ * and returns SWC_INVALID_INPUT with a message otherwise.  The first call on a device looks
+ * up the scratch's device address; make that first call before any stream capture.  All
+ * calls on a GPU share the scratch: overlapping calls race and must be serialised by the
+ * caller.  Nothing in the scratch needs clearing between calls. */
+#define SWC_SOLVE_NOALLOC_MAX 1048576
+int swc_solve_noalloc(swc_handle_t handle, const double *b, double *x, int nrhs);
+
 /* Device pointer to the handle's L (xsize doubles), valid until the next analyze. */
 const double *swc_device_L(swc_handle_t handle);
 

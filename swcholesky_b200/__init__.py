@@ -38,7 +38,7 @@ EXPORTS = (
     "sw_cholesky_left_par_05", "swc_last_info", "swc_last_error", "swc_create", "swc_destroy",
     "swc_set_stream", "swc_get_stream", "swc_analyze", "swc_factor", "swc_get_L",
     "swc_device_L", "swc_sizes", "swc_profile", "swc_plan_stats", "swc_layout_sizes",
-    "swc_layout", "swc_solve", "swc_refine",
+    "swc_layout", "swc_solve", "swc_refine", "swc_solve_noalloc",
 )
 KERNEL_CLASSES = ("memset", "small", "assemble", "update", "panel", "syrk")
 
@@ -78,6 +78,7 @@ def lib() -> ctypes.CDLL:
         L.swc_sizes.argtypes = [_VP, _VP]
         L.swc_profile.argtypes = [_VP, _VP, _I, ctypes.POINTER(_I), _VP, _VP, _VP, _VP]
         L.swc_solve.argtypes = [_VP, _VP, _VP, _I, _I]
+        L.swc_solve_noalloc.argtypes = [_VP, _VP, _VP, _I]
         L.swc_refine.argtypes = [_VP, _VP, _VP, _I, _I, ctypes.c_double, _I, _VP,
                                  ctypes.POINTER(_I), ctypes.POINTER(_I)]
         L.swc_plan_stats.argtypes = [_I] + [_VP] * 6 + [_I] + [_VP] * 3

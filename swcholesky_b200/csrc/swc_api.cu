@@ -11,12 +11,7 @@
 #include "../../include/swcholesky_b200.h"
 #include "swc_engine.h"
 
-struct swc_handle {
-  std::unique_ptr<swc::Engine> eng;
-  int device = 0;
-  bool analyzed = false;
-  bool factored = false;
-};
+#include "swc_handle.h"
 
 namespace {
 
@@ -37,6 +32,10 @@ std::vector<int64_t> to_i64(const size_t *p, int count) {
 }
 
 }  // namespace
+
+namespace swc {
+void set_last_error(const std::string &msg) { g_err = msg; }
+}  // namespace swc
 
 namespace {
 // Runs fn on device copies of host right-hand sides (and copies x back) when needed.

@@ -808,4 +808,40 @@ bool Engine::refine(const double *b, double *x, int nrhs, double tol, int maxit,
   return true;
 }
 
+bool Engine::solve_in_scratch(const double *b, double *x, int nrhs, double *scratch,
+                              int64_t capacity, std::string &err) {
+  if (!dL_) { err = "solve before factor"; return false; }
+  const SolvePlan &SP = splan_;
+  const int64_t cs = std::max<int64_t>(SP.contrib_len, 1);
+  if (nrhs <= 0 || cs * nrhs > capacity) {
+    err = "solve needs " + std::to_string(cs * (nrhs > 0 ? nrhs : 1)) +
+          " doubles of scratch (off-diagonal rows of L times right-hand sides); the fixed "
+          "scratch holds " + std::to_string(capacity);
+    return false;
+  }
+  cudaSetDevice(device_);
+  cudaStream_t st = stream_;
+  cudaError_t e = cudaSuccess;
+  if (x != b) e = cudaMemcpyAsync(x, b, sizeof(double) * n_ * nrhs, cudaMemcpyDeviceToDevice, st);
+  if (e != cudaSuccess) { err = std::string("solve: ") + cudaGetErrorString(e); return false; }
+  const int nl = (int)SP.level_off.size() - 1;
+  const int smem = (int)sizeof(double) * std::max(SP.max_w, 1);
+  for (int l = 0; l < nl; ++l) {
+    launch_fwd_diag(sym_, d_slist_ + SP.level_off[l], SP.level_off[l + 1] - SP.level_off[l], smem,
+                    x, scratch, n_, nrhs, cs, st);
+    launch_fwd_contrib(sym_, d_scontrib_ + SP.contrib_off[l], SP.contrib_off[l + 1] - SP.contrib_off[l],
+                       x, scratch, n_, nrhs, cs, st);
+  }
+  for (int l = nl - 1; l >= 0; --l) {
+    launch_bwd_gather(sym_, d_sgather_ + SP.gather_off[l], SP.gather_off[l + 1] - SP.gather_off[l],
+                      x, n_, nrhs, st);
+    launch_bwd_diag(sym_, d_slist_ + SP.level_off[l], SP.level_off[l + 1] - SP.level_off[l], smem,
+                    x, n_, nrhs, st);
+  }
+  e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) { err = std::string("solve: ") + cudaGetErrorString(e); return false; }
+  return true;
+}
+
 }  // namespace swc

@@ -137,6 +137,10 @@ class Engine {
                       KernelStats &out, std::string &err);
   // x = (L L^T)^{-1} b for nrhs right-hand sides (device pointers, leading dimension n).
   bool solve(const double *b, double *x, int nrhs, std::string &err);
+  // The same solve with the contribution scratch supplied by the caller (capacity in
+  // doubles); allocates nothing.  Fails if the scratch is too small.
+  bool solve_in_scratch(const double *b, double *x, int nrhs, double *scratch,
+                        int64_t capacity, std::string &err);
   // FP64 iterative refinement with the factor (falls back to factor-preconditioned CG when
   // refinement stalls); device pointers.
   bool refine(const double *b, double *x, int nrhs, double tol, int maxit, RefineInfo &info,
