@@ -1,10 +1,12 @@
 """Benchmark of the supernodal numeric factorization (one JSON line on stdout, rank 0).
 
-A step is one numeric factorization of the workload matrix (default grid3d_60: the 3D
+A step is one mixed-precision numeric factorization of the workload matrix followed by a
+solve refined in FP64 to backward error <= 1e-12 (default workload grid3d_60: the 3D
 7-point Laplacian on 60^3 plus 1e-3 I, n = 216,000, ordered by geometric nested dissection
 and analysed by the reference's own symbolic phase; the supernode partition and final
 permutation come from tests/golden/sym_grid3d_60.npz).  The metric is the reference's flop
-measure fl = sum_j c_j^2 (exact column counts) divided by the factorization time.
+measure fl = sum_j c_j^2 (exact column counts) divided by the step time; the plain FP64
+factorization is timed alongside (--mode fp64 makes it the headline).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -29,7 +31,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "factorization GFLOP/s (fl = sum c_j^2), FP64 supernodal numeric factor"
+METRIC = ("factorization GFLOP/s (fl = sum c_j^2 / time) of the mixed-precision factor + "
+          "FP64-refined solve to backward error <= 1e-12 (FP64 factor timed alongside)")
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 
@@ -172,6 +175,32 @@ def run_reference(args, rank, world):
     print(json.dumps(line))
 
 
+def tf32_gemm_peak(torch, dev):
+    """Dense TF32 GEMM throughput measured with cuBLAS (torch.matmul on float32 with TF32
+    allowed, 8192^3), best of 5; a split-TF32 product costs three TF32 products, so its
+    peak is a third of this."""
+    n = 8192
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = True
+    a = torch.randn(n, n, dtype=torch.float32, device=dev)
+    b = torch.randn(n, n, dtype=torch.float32, device=dev)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        best = max(best, 2.0 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    torch.backends.cuda.matmul.allow_tf32 = prev
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -180,71 +209,121 @@ def run_ours(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     A, perm_in, meta, P, fl = load_problem(args.workload)
+    tol = 1e-12
 
     h = swc.Handle(local_rank)
     h.analyze(P.n, P.A2p, P.A2i, P.lC, P.Ls, P.Li_ptr, P.super, P.prunePtr, P.pruneSet,
               P.levelPtr, P.parPtr, P.partition)
+    plan = swc.plan_stats(P.n, P.A2p, P.A2i, P.lC, P.Ls, P.Li_ptr, P.super, P.prunePtr,
+                          P.pruneSet)
+    solve_launches = 4 * plan["levels"]
     vals = torch.from_numpy(P.A2x).to(dev)
+    b_host = np.random.default_rng(0).standard_normal(P.n)
+    b = torch.from_numpy(b_host).to(dev)
+    x = torch.zeros_like(b)
     stream = torch.cuda.ExternalStream(h.stream, device=dev)
+    mixed = args.mode == "mixed"
+    mode = swc.SWC_MODE_MIXED_TF32X3 if mixed else swc.SWC_MODE_FP64
 
     def barrier():
         if world > 1:
             dist.barrier()
 
-    for _ in range(args.warmup):
-        info = h.factor(vals)
+    def timed(fn, steps):
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms = e0.elapsed_time(e1) / steps
+        if world > 1:
+            t = torch.tensor([ms], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    last = {}
+
+    def step_headline():
+        info = h.factor(vals, mode)
         assert info == 0, f"not SPD at column {info - 1}"
+        _, berr, iters, meth = h.refine(b, tol=tol, maxit=30, out=x)
+        last.update(berr=float(berr.max()), iters=iters, method=meth)
+
+    def step_fp64():
+        info = h.factor(vals, swc.SWC_MODE_FP64)
+        assert info == 0, f"not SPD at column {info - 1}"
+
+    for _ in range(args.warmup):
+        step_fp64()
+        step_headline()
     torch.cuda.synchronize()
+    ms_fp64 = timed(step_fp64, args.steps)
+    ms_fact = timed(lambda: h.factor(vals, mode), args.steps)
     clocks = ClockSampler(local_rank)
     clocks.start()
-    barrier()
-    torch.cuda.synchronize()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for _ in range(args.steps):
-        h.factor(vals)
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    barrier()
+    ms = timed(step_headline, args.steps)
     clk = clocks.stop()
-    ms = ev0.elapsed_time(ev1) / args.steps
-    if world > 1:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    # FP64 factor followed by a refined solve, for the like-for-like comparison
+    last_fp64 = {}
+
+    def step_fp64_solve():
+        step_fp64()
+        _, berr, iters, meth = h.refine(b, tol=tol, maxit=30, out=x)
+        last_fp64.update(berr=float(berr.max()), iters=iters)
+    ms_fp64_solve = timed(step_fp64_solve, max(1, args.steps // 2))
     value = world * fl / (ms * 1e-3) / 1e9
 
-    # ---- per-kernel roofline (a separate profiled factorization, untimed) ----
-    prof = h.profile(vals)
+    # ---- per-kernel roofline (a separate profiled factorization in the headline mode) ----
+    prof64 = h.profile(vals, swc.SWC_MODE_FP64) if mixed else None
+    prof = h.profile(vals, mode)
     kinds = {k: v for k, v in prof.items() if k != "memset"}
     dom = max(kinds, key=lambda k: kinds[k][1])
     la, kms, kfl, kby = kinds[dom]
     peak64 = fp64_gemm_peak(torch, dev) if rank == 0 else None
+    peak32 = tf32_gemm_peak(torch, dev) if rank == 0 and mixed else None
+    if mixed and dom in ("update", "syrk"):
+        peak, psrc = peak32 / 3.0, ("cuBLAS TF32 GEMM 8192^3 measured in this run, divided by 3 "
+                                    "(a split-TF32 product costs three TF32 products)")
+    else:
+        peak, psrc = peak64, "FP64 cuBLAS DGEMM 8192^3 measured in this run"
 
-    # ---- end to end through the reference-facing C-ABI call, host buffers ----
+    # ---- end to end through the public API with host buffers ----
     e2e = None
     if rank == 0 and not args.no_e2e:
-        L_host = np.zeros(P.xsize, np.float64)
-        e2e_steps = max(1, min(3, args.steps))
+        x_host = np.zeros(P.n)
         t_e2e = []
-        for i in range(e2e_steps + 1):
+        for i in range(max(1, min(3, args.steps)) + 1):
+            t0 = time.perf_counter()
+            info = h.factor(P.A2x, mode)                              # values from host
+            xh, berr, iters, meth = h.refine(b_host, tol=tol, maxit=30)   # b / x on host
+            dt = time.perf_counter() - t0
+            assert info == 0 and berr.max() <= tol
+            if i > 0:
+                t_e2e.append(dt)
+        te = float(np.mean(t_e2e))
+        e2e = {"value": round(fl / te / 1e9, 3), "unit": "GFLOP/s",
+               "h2d_bytes_per_step": int(P.A2x.nbytes + b_host.nbytes),
+               "d2h_bytes_per_step": int(b_host.nbytes),
+               "ms_per_step": round(te * 1e3, 3),
+               "note": "swc_factor with host values + swc_refine with host b and x"}
+        # the reference-facing drop-in call (FP64 factor only, structure re-uploaded)
+        L_host = np.zeros(P.xsize, np.float64)
+        t_d = []
+        for i in range(2):
             t0 = time.perf_counter()
             ret = swc.sw_cholesky_left_par_05(
                 P.n, P.A2p, P.A2i, P.A2x, P.lC, P.Ls, P.Li_ptr, L_host, P.super, P.nsuper,
                 None, P.prunePtr, P.pruneSet, P.levelPtr.size - 1, P.levelPtr, None, 0,
                 P.parPtr, P.partition, 0, 1, 0, 0, None)
-            dt = time.perf_counter() - t0
             assert ret == 1
-            if i > 0:          # the first call also creates the library's default handle
-                t_e2e.append(dt)
-        h2d = (P.A2x.nbytes + P.A2p.nbytes + P.A2i.nbytes + P.Ls.nbytes + P.super.nbytes +
-               P.prunePtr.nbytes + P.pruneSet.nbytes + 8 * 2 * P.nsuper)
-        te = float(np.mean(t_e2e))
-        e2e = {"value": round(fl / te / 1e9, 3), "unit": "GFLOP/s",
-               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(8 * P.xsize),
-               "ms_per_step": round(te * 1e3, 3),
-               "note": "sw_cholesky_left_par_05 with host arrays: host validation + plan, "
-                       "upload of structure and values, factorization, download of L"}
+            if i > 0:
+                t_d.append(time.perf_counter() - t0)
+        e2e["dropin_fp64_ms"] = round(float(np.mean(t_d)) * 1e3, 3)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -254,7 +333,7 @@ def run_ours(args, rank, world, local_rank):
             tref, reps, _ = reference_time(A, perm_in, threads, budget_s=15.0, max_reps=5)
             cpu = {"value": round(fl / tref / 1e9, 3), "unit": "GFLOP/s", "cores": threads,
                    "kind": "reference",
-                   "sample": f"{reps} full {args.workload} factorizations, median "
+                   "sample": f"{reps} full {args.workload} FP64 factorizations, median "
                              f"(reference sw_cholesky_left_par_05_check + OpenBLAS)"}
         else:
             cpu = {"value": None, "unit": "GFLOP/s", "cores": 0, "kind": "reference",
@@ -262,28 +341,44 @@ def run_ours(args, rank, world, local_rank):
 
     if rank == 0:
         achieved = kfl / (kms * 1e-3) / 1e12
+        per_step = h.launches + (last.get("iters", 0) + 1) * (solve_launches + 5)
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64+tf32x3" if mixed else "f64",
             "data": "synthetic (seeded generator; reference symbolic phase via fixture)",
             "config": {"workload": args.workload, "n": P.n, "nnz_lower": int(P.A2p[-1]),
-                       "nsuper": P.nsuper, "xsize": P.xsize, "fl": fl,
+                       "nsuper": P.nsuper, "xsize": P.xsize, "fl": fl, "mode": args.mode,
+                       "backward_error_target": tol,
                        "parallelism": "replicas only" if world > 1 else "single GPU",
                        "l2": f"inputs larger than L2 (L = {P.xsize * 8 / 1e9:.2f} GB)"},
+            "headline": {"ms_factor_plus_refined_solve": round(ms, 4),
+                         "ms_factor": round(ms_fact, 4),
+                         "refine_iterations": last.get("iters"),
+                         "refine_method": last.get("method"),
+                         "backward_error": last.get("berr"),
+                         "fp64_ms_factor": round(ms_fp64, 4),
+                         "fp64_gflops": round(world * fl / (ms_fp64 * 1e-3) / 1e9, 3),
+                         "fp64_ms_factor_plus_refined_solve": round(ms_fp64_solve, 4),
+                         "fp64_backward_error": last_fp64.get("berr"),
+                         "speedup_vs_fp64_factor": round(ms_fp64 / ms, 3),
+                         "speedup_vs_fp64_factor_plus_solve": round(ms_fp64_solve / ms, 3)},
             "roofline": {"bound": "tensor", "kernel": dom, "achieved": round(achieved, 4),
-                         "peak": round(peak64, 3) if peak64 else None, "unit": "TFLOP/s",
-                         "frac": round(achieved / peak64, 4) if peak64 else None,
-                         "traffic": None,
-                         "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run",
+                         "peak": round(peak, 3) if peak else None, "unit": "TFLOP/s",
+                         "frac": round(achieved / peak, 4) if peak else None,
+                         "traffic": None, "peak_source": psrc,
+                         "fp64_peak": round(peak64, 3) if peak64 else None,
                          "launches": la, "kernel_ms": round(kms, 4),
                          "algorithmic_flops": kfl,
                          "classes": {k: {"launches": v[0], "ms": round(v[1], 4),
                                          "gflop": round(v[2] / 1e9, 4)}
-                                     for k, v in prof.items()}},
+                                     for k, v in prof.items()},
+                         "classes_fp64": ({k: {"ms": round(v[1], 4)} for k, v in prof64.items()}
+                                          if prof64 else None)},
             "cpu_baseline": cpu,
             "e2e": e2e,
-            "gpu_launches": int(h.launches * args.steps),
+            "gpu_launches": int(per_step * args.steps),
             "clocks": clk,
         }
         print(json.dumps(line))
@@ -299,6 +394,7 @@ def main():
     ap.add_argument("--workload", default="grid3d_60")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--mode", default="mixed", choices=["mixed", "fp64"])
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

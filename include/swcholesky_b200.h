@@ -29,6 +29,9 @@ extern "C" {
 
 /* factorization modes */
 #define SWC_MODE_FP64 0        /* every operation in FP64 */
+#define SWC_MODE_MIXED_TF32X3 1 /* Schur updates of the wide supernodes as split-TF32 tensor-core
+                                   products (FP32-class accuracy, FP32/FP64 accumulation); POTRF,
+                                   TRSM and small supernodes in FP64.  Pair with swc_refine. */
 
 typedef struct swc_handle *swc_handle_t;
 
@@ -130,8 +133,8 @@ int swc_sizes(swc_handle_t handle, long long *sizes);
 /* One factorization, as swc_factor, with a CUDA event pair around every kernel launch:
  * per kernel class the number of launches, the summed device milliseconds, and the
  * algorithmic flops and DRAM bytes of one factorization.  Any output may be NULL. */
-int swc_profile(swc_handle_t handle, const double *values, int values_on_device, int *info,
-                int *launches, double *ms, double *flops, double *bytes);
+int swc_profile(swc_handle_t handle, const double *values, int values_on_device, int mode,
+                int *info, int *launches, double *ms, double *flops, double *bytes);
 
 /* Host-only: validates the structure (as swc_analyze does) and describes the execution
  * plan without touching a GPU.  stats[0..19] = levels, kernel launches per factorization,

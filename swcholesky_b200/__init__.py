@@ -32,6 +32,7 @@ SWC_CUDA_ERROR = 3
 SWC_STRUCTURE_ERROR = 4
 SWC_NOT_READY = 5
 SWC_MODE_FP64 = 0
+SWC_MODE_MIXED_TF32X3 = 1
 
 # every symbol include/swcholesky_b200.h declares
 EXPORTS = (
@@ -76,7 +77,7 @@ def lib() -> ctypes.CDLL:
         L.swc_device_L.restype = _VP
         L.swc_device_L.argtypes = [_VP]
         L.swc_sizes.argtypes = [_VP, _VP]
-        L.swc_profile.argtypes = [_VP, _VP, _I, ctypes.POINTER(_I), _VP, _VP, _VP, _VP]
+        L.swc_profile.argtypes = [_VP, _VP, _I, _I, ctypes.POINTER(_I), _VP, _VP, _VP, _VP]
         L.swc_solve.argtypes = [_VP, _VP, _VP, _I, _I]
         L.swc_solve_noalloc.argtypes = [_VP, _VP, _VP, _I]
         L.swc_refine.argtypes = [_VP, _VP, _VP, _I, _I, ctypes.c_double, _I, _VP,
@@ -242,7 +243,7 @@ class Handle:
         _check(self._lib.swc_sizes(self._h, _p(sz)))
         return int(sz[4]), int(sz[5])
 
-    def profile(self, values):
+    def profile(self, values, mode: int = SWC_MODE_FP64):
         """One factorization with per-kernel-class event timing.  Returns a dict
         class -> (launches, ms, algorithmic flops, algorithmic bytes)."""
         on_dev = hasattr(values, "data_ptr")
@@ -252,8 +253,8 @@ class Handle:
         la = np.zeros(k, np.int32)
         ms, fl, by = np.zeros(k), np.zeros(k), np.zeros(k)
         info = ctypes.c_int(0)
-        rc = self._lib.swc_profile(self._h, _p(values), 1 if on_dev else 0, ctypes.byref(info),
-                                   _p(la), _p(ms), _p(fl), _p(by))
+        rc = self._lib.swc_profile(self._h, _p(values), 1 if on_dev else 0, int(mode),
+                                   ctypes.byref(info), _p(la), _p(ms), _p(fl), _p(by))
         if rc not in (SWC_OK, SWC_NOT_SPD):
             _check(rc)
         return {name: (int(la[i]), float(ms[i]), float(fl[i]), float(by[i]))

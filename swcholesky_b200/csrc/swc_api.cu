@@ -124,11 +124,12 @@ int swc_analyze(swc_handle_t h, int n, const int *c, const int *r, const size_t 
 int swc_factor(swc_handle_t h, const double *values, int values_on_device, int mode, int *info) {
   if (!h) return fail(SWC_INVALID_INPUT, "null handle");
   if (!h->analyzed) return fail(SWC_NOT_READY, "factor before analyze");
-  if (mode != SWC_MODE_FP64) return fail(SWC_INVALID_INPUT, "unknown factorization mode");
+  if (mode != SWC_MODE_FP64 && mode != SWC_MODE_MIXED_TF32X3)
+    return fail(SWC_INVALID_INPUT, "unknown factorization mode");
   if (!values) return fail(SWC_INVALID_INPUT, "null values");
   std::string err;
   int lin = 0;
-  int rc = h->eng->factor(values, values_on_device != 0, &lin, err);
+  int rc = h->eng->factor(values, values_on_device != 0, &lin, err, mode == SWC_MODE_MIXED_TF32X3);
   if (info) *info = lin;
   if (rc == 0) {
     h->factored = true;
@@ -189,7 +190,7 @@ int swc_sizes(swc_handle_t h, long long *sizes) {
   return SWC_OK;
 }
 
-int swc_profile(swc_handle_t h, const double *values, int values_on_device, int *info,
+int swc_profile(swc_handle_t h, const double *values, int values_on_device, int mode, int *info,
                 int *launches, double *ms, double *flops, double *bytes) {
   if (!h) return fail(SWC_INVALID_INPUT, "null handle");
   if (!h->analyzed) return fail(SWC_NOT_READY, "profile before analyze");
@@ -197,7 +198,9 @@ int swc_profile(swc_handle_t h, const double *values, int values_on_device, int 
   swc::KernelStats ks;
   std::string err;
   int lin = 0;
-  int rc = h->eng->factor_profiled(values, values_on_device != 0, &lin, ks, err);
+  int rc = h->eng->factor_profiled(values, values_on_device != 0, &lin, ks, err,
+                                   mode == SWC_MODE_MIXED_TF32X3);
+  h->factored = (rc == 0);
   if (info) *info = lin;
   for (int k = 0; k < swc::K_NKINDS; ++k) {
     if (launches) launches[k] = ks.launches[k];

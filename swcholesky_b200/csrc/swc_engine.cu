@@ -112,7 +112,7 @@ Engine::Engine(int device) : device_(device) {
   cudaStreamCreateWithFlags(&aux_stream_, cudaStreamNonBlocking);
   cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming);
   cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming);
-  cudaMallocHost(&h_status_, 2 * sizeof(int));
+  cudaMallocHost(&h_status_, 4 * sizeof(int));
 }
 
 Engine::~Engine() {
@@ -129,7 +129,8 @@ void Engine::release() {
   void *ptrs[] = {d_super_, d_Ls_, d_Ap_, d_Ai_, d_rowptr_, d_xptr_, d_upd_ptr_, d_upd_,
                   d_Ax_, dL_, d_status_, d_small_, d_big_, d_asm_, d_panel_, d_upd_tasks_,
                   d_syrk_, d_pairs_, d_upd_end_, d_dinv_, d_dinv_off_, d_diag_,
-                  d_slist_, d_scontrib_, d_sgather_, d_csr_rp_, d_csr_ci_, d_csr_map_,
+                  d_slist_, d_cptr_, d_cidx_, d_flags_, d_fchain_, d_bchain_, d_scontrib_, d_sgather_, d_csr_rp_, d_csr_ci_,
+                  d_csr_map_,
                   d_csr_val_, d_contrib_, d_work_, d_norms_};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -144,15 +145,20 @@ void Engine::release() {
   d_dinv_ = nullptr;
   d_dinv_off_ = nullptr;
   d_diag_ = nullptr;
-  d_slist_ = nullptr;
+  d_slist_ = d_cptr_ = d_cidx_ = d_flags_ = nullptr;
+  d_fchain_ = d_bchain_ = nullptr;
   d_scontrib_ = d_sgather_ = nullptr;
   d_csr_rp_ = d_csr_ci_ = d_csr_map_ = nullptr;
   d_csr_val_ = d_contrib_ = d_work_ = d_norms_ = nullptr;
   work_nrhs_ = 0;
   if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
   if (graph_) cudaGraphDestroy(graph_);
-  graph_exec_ = nullptr;
-  graph_ = nullptr;
+  if (graph_exec_mx_) cudaGraphExecDestroy(graph_exec_mx_);
+  if (graph_mx_) cudaGraphDestroy(graph_mx_);
+  graph_exec_ = graph_exec_mx_ = nullptr;
+  graph_ = graph_mx_ = nullptr;
+  if (d_Lf_) cudaFree(d_Lf_);
+  d_Lf_ = nullptr;
 }
 
 bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int *Ls,
@@ -369,7 +375,7 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
                      const int64_t *Li_ptr, const int *blockSet, int supNo,
                      const int *prunePtr, const int *pruneSet, std::string &err) {
   cudaSetDevice(device_);
-  if (!kernels_configure(err)) return false;
+  if (!kernels_configure(err) || !mixed_configure(err)) return false;
   HostSym H;
   Plan P;
   if (!build_plan(n, c, r, lC, Ls, Li_ptr, blockSet, supNo, prunePtr, pruneSet, H, P, err))
@@ -401,21 +407,44 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
     for (int s = 0; s < supNo; ++s) bylev[lev[s]].push_back(s);
     for (int l = 0; l < nl; ++l) {
       SP.level_off.push_back((int)SP.list.size());
+      SP.chain_off.push_back((int)SP.fchain.size());
       SP.contrib_off.push_back((int)SP.contrib_tasks.size());
       SP.gather_off.push_back((int)SP.gather_tasks.size());
       for (int s : bylev[l]) {
-        SP.list.push_back(s);
         const int w = super[s + 1] - super[s];
         const int m = (int)(rowptr[s + 1] - rowptr[s]);
+        if (H.dinv_off[s] >= 0) {   // tiled class: chained solves through the block inverses
+          const int nb = (w + TB - 1) / TB;
+          for (int k = 0; k < nb; ++k) SP.fchain.push_back(make_int2(s, k));
+          for (int k = nb - 1; k >= 0; --k) SP.bchain.push_back(make_int2(s, k));
+        } else {
+          SP.list.push_back(s);
+        }
         for (int r0 = w; r0 < m; r0 += 256) SP.contrib_tasks.push_back(make_int2(s, r0));
         if (m > w)
           for (int j0 = 0; j0 < w; j0 += 32) SP.gather_tasks.push_back(make_int2(s, j0));
       }
     }
     SP.level_off.push_back((int)SP.list.size());
+    SP.chain_off.push_back((int)SP.fchain.size());
     SP.contrib_off.push_back((int)SP.contrib_tasks.size());
     SP.gather_off.push_back((int)SP.gather_tasks.size());
     SP.contrib_len = nls - n;
+    // column contribution lists: off-diagonal row a of supernode d (a >= w_d) feeds column
+    // Ls[a] through contribution (rowptr[d] - super[d]) + (a - w_d)
+    SP.cptr.assign(n + 1, 0);
+    for (int d = 0; d < supNo; ++d) {
+      const int w = super[d + 1] - super[d];
+      for (int64_t q = rowptr[d] + w; q < rowptr[d + 1]; ++q) SP.cptr[Ls[q] + 1]++;
+    }
+    for (int j = 0; j < n; ++j) SP.cptr[j + 1] += SP.cptr[j];
+    SP.cidx.resize(SP.cptr[n]);
+    std::vector<int> fillc(SP.cptr.begin(), SP.cptr.end() - 1);
+    for (int d = 0; d < supNo; ++d) {
+      const int w = super[d + 1] - super[d];
+      for (int64_t q = rowptr[d] + w; q < rowptr[d + 1]; ++q)
+        SP.cidx[fillc[Ls[q]]++] = (int)((rowptr[d] - super[d]) + (q - rowptr[d] - w));
+    }
   }
   if (!solve_configure(SP.max_w, err)) return false;
   // ---- full CSR of the symmetric matrix for residuals: entry -> index into A2 values ----
@@ -465,6 +494,10 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
             upload(d_syrk_, P.syrk_tasks.data(), P.syrk_tasks.size(), st, err) &&
             upload(d_dinv_off_, H.dinv_off.data(), H.dinv_off.size(), st, err) &&
             upload(d_slist_, SP.list.data(), SP.list.size(), st, err) &&
+            upload(d_cptr_, SP.cptr.data(), SP.cptr.size(), st, err) &&
+            upload(d_cidx_, SP.cidx.data(), SP.cidx.size(), st, err) &&
+            upload(d_fchain_, SP.fchain.data(), SP.fchain.size(), st, err) &&
+            upload(d_bchain_, SP.bchain.data(), SP.bchain.size(), st, err) &&
             upload(d_scontrib_, SP.contrib_tasks.data(), SP.contrib_tasks.size(), st, err) &&
             upload(d_sgather_, SP.gather_tasks.data(), SP.gather_tasks.size(), st, err) &&
             upload(d_csr_rp_, csr_rp.data(), csr_rp.size(), st, err) &&
@@ -473,7 +506,9 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
   if (!ok) return false;
   cudaError_t e = cudaMalloc(&d_Ax_, sizeof(double) * std::max<int64_t>(nnz, 1));
   if (e == cudaSuccess) e = cudaMalloc(&dL_, sizeof(double) * std::max<int64_t>(xsize, 1));
-  if (e == cudaSuccess) e = cudaMalloc(&d_status_, 2 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&d_status_, 4 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&d_flags_, sizeof(int) * std::max<int64_t>(H.ndinv, 1));
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_flags_, 0, sizeof(int) * std::max<int64_t>(H.ndinv, 1), st);
   if (e == cudaSuccess)
     e = cudaMalloc(&d_dinv_, sizeof(double) * TB * TB * std::max<int64_t>(H.ndinv, 1));
   if (e == cudaSuccess)
@@ -490,6 +525,8 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
   nnz_ = nnz;
   plan_ = std::move(P);
   splan_ = std::move(SP);
+  solve_epoch_ = 0;
+  nflags_ = H.ndinv;
   csr_nnz_ = (int64_t)csr_ci.size();
   sym_.n = n;
   sym_.nsuper = supNo;
@@ -505,12 +542,13 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
   sym_.L = dL_;
   sym_.status = d_status_;
   sym_.dinv = d_dinv_;
+  sym_.Lf = nullptr;
   sym_.dinv_off = d_dinv_off_;
 
   return true;
 }
 
-void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof) {
+void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, bool mixed) {
   cudaStream_t st = stream_;
   // With profiling on, every launch is preceded by an event and followed by one.
   auto mark = [&](int kind, int count) {
@@ -532,8 +570,12 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof) {
     launch_assemble(sym_, d_asm_ + W.asm_off, W.asm_cnt, st);
     mark(-1, W.asm_cnt);
     mark(K_UPDATE, W.upd_cnt);
-    launch_update_tiles(sym_, d_upd_tasks_ + W.upd_off, d_upd_end_ + W.upd_off, d_pairs_,
-                        W.upd_cnt, st);
+    if (mixed)
+      launch_update_tiles_mx(sym_, d_upd_tasks_ + W.upd_off, d_upd_end_ + W.upd_off, d_pairs_,
+                             W.upd_cnt, st);
+    else
+      launch_update_tiles(sym_, d_upd_tasks_ + W.upd_off, d_upd_end_ + W.upd_off, d_pairs_,
+                          W.upd_cnt, st);
     mark(-1, W.upd_cnt);
     mark(K_PANEL, W.big_cnt);
     launch_diag_step(sym_, d_big_ + W.big_off, W.big_cnt, 0, st);
@@ -548,7 +590,8 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof) {
         launch_diag_step(sym_, d_diag_ + W.diag_off[j], W.diag_cnt[j], (int)j + 1, st);
         mark(-1, W.diag_cnt[j]);
         mark(K_SYRK, W.syrk_cnt[j]);
-        launch_syrk_step(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
+        if (mixed) launch_syrk_step_mx(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
+        else launch_syrk_step(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
         mark(-1, W.syrk_cnt[j]);
       } else if (W.diag_cnt[j] > 0) {
         // fork: next diagonal block on the auxiliary stream, trailing update here; join
@@ -556,18 +599,35 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof) {
         cudaStreamWaitEvent(aux_stream_, ev_fork_, 0);
         launch_diag_step(sym_, d_diag_ + W.diag_off[j], W.diag_cnt[j], (int)j + 1, aux_stream_);
         cudaEventRecord(ev_join_, aux_stream_);
-        launch_syrk_step(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
+        if (mixed) launch_syrk_step_mx(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
+        else launch_syrk_step(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
         cudaStreamWaitEvent(st, ev_join_, 0);
       } else {
-        launch_syrk_step(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
+        if (mixed) launch_syrk_step_mx(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
+        else launch_syrk_step(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
       }
     }
   }
 }
 
-int Engine::factor(const double *values, bool values_on_device, int *info, std::string &err) {
+bool Engine::set_mode(bool mixed, std::string &err) {
+  if (mixed && !d_Lf_) {
+    cudaError_t e = cudaMalloc(&d_Lf_, sizeof(float2) * std::max<int64_t>(xsize_, 1));
+    if (e != cudaSuccess) {
+      d_Lf_ = nullptr;
+      err = std::string("mirror allocation: ") + cudaGetErrorString(e);
+      return false;
+    }
+  }
+  sym_.Lf = mixed ? d_Lf_ : nullptr;
+  return true;
+}
+
+int Engine::factor(const double *values, bool values_on_device, int *info, std::string &err,
+                   bool mixed) {
   if (!dL_) { err = "factor before analyze"; return -1; }
   cudaSetDevice(device_);
+  if (!set_mode(mixed, err)) return -1;
   cudaStream_t st = stream_;
   // values always reach the kernels through d_Ax_, so a captured graph stays valid
   cudaError_t e = cudaMemcpyAsync(d_Ax_, values, sizeof(double) * nnz_,
@@ -576,35 +636,39 @@ int Engine::factor(const double *values, bool values_on_device, int *info, std::
   if (e != cudaSuccess) { err = std::string("values upload: ") + cudaGetErrorString(e); return -1; }
   h2d_bytes_ = values_on_device ? 0 : (int64_t)sizeof(double) * nnz_;
   if (use_graph_) {
-    // The whole launch sequence is fixed by the structure: capture it once, replay it.
-    if (!graph_exec_) {
+    // The whole launch sequence is fixed by the structure (and the mode): capture it once
+    // per mode, replay it.
+    cudaGraph_t &g = mixed ? graph_mx_ : graph_;
+    cudaGraphExec_t &ge = mixed ? graph_exec_mx_ : graph_exec_;
+    if (!ge) {
       e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
       if (e == cudaSuccess) {
-        launch_all();
-        e = cudaStreamEndCapture(st, &graph_);
+        launch_all(nullptr, mixed);
+        e = cudaStreamEndCapture(st, &g);
       }
-      if (e == cudaSuccess) e = cudaGraphInstantiate(&graph_exec_, graph_, 0);
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&ge, g, 0);
       if (e != cudaSuccess) { err = std::string("graph capture: ") + cudaGetErrorString(e); return -1; }
     }
-    e = cudaGraphLaunch(graph_exec_, st);
+    e = cudaGraphLaunch(ge, st);
     if (e != cudaSuccess) { err = std::string("graph launch: ") + cudaGetErrorString(e); return -1; }
   } else {
-    launch_all();
+    launch_all(nullptr, mixed);
   }
   return finish(info, err);
 }
 
 int Engine::factor_profiled(const double *values, bool values_on_device, int *info,
-                            KernelStats &out, std::string &err) {
+                            KernelStats &out, std::string &err, bool mixed) {
   if (!dL_) { err = "factor before analyze"; return -1; }
   cudaSetDevice(device_);
+  if (!set_mode(mixed, err)) return -1;
   cudaStream_t st = stream_;
   cudaError_t e = cudaMemcpyAsync(d_Ax_, values, sizeof(double) * nnz_,
                                   values_on_device ? cudaMemcpyDeviceToDevice
                                                    : cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) { err = std::string("values upload: ") + cudaGetErrorString(e); return -1; }
   std::vector<std::pair<int, cudaEvent_t>> prof;
-  launch_all(&prof);
+  launch_all(&prof, mixed);
   int rc = finish(info, err);
   out = plan_.work;
   for (int k = 0; k < K_NKINDS; ++k) { out.launches[k] = 0; out.ms[k] = 0; }
@@ -670,24 +734,46 @@ bool Engine::ensure_work(int nrhs, std::string &err) {
   return true;
 }
 
-void Engine::run_solve(double *x, int nrhs) {
+void Engine::run_solve(double *x, int nrhs) { run_solve_with(x, nrhs, d_contrib_); }
+
+// Forward then backward supernodal solve, level by level, with the contribution scratch
+// `contrib` (one double per off-diagonal row of L per right-hand side).
+void Engine::run_solve_with(double *x, int nrhs, double *contrib) {
   cudaStream_t st = stream_;
   const SolvePlan &SP = splan_;
   const int nl = (int)SP.level_off.size() - 1;
   const int smem = (int)sizeof(double) * std::max(SP.max_w, 1);
   const int64_t cs = std::max<int64_t>(SP.contrib_len, 1);
+  const int base = solve_epoch_;
+  solve_epoch_ += 2 * nrhs;
+  cudaMemsetAsync(d_status_ + 2, 0, sizeof(int), st);
   for (int l = 0; l < nl; ++l) {
     launch_fwd_diag(sym_, d_slist_ + SP.level_off[l], SP.level_off[l + 1] - SP.level_off[l], smem,
-                    x, d_contrib_, n_, nrhs, cs, st);
+                    x, contrib, d_cptr_, d_cidx_, n_, nrhs, cs, st);
+    for (int r = 0; r < nrhs; ++r)
+      launch_fwd_chain(sym_, d_fchain_ + SP.chain_off[l], SP.chain_off[l + 1] - SP.chain_off[l],
+                       x + (size_t)r * n_, contrib + (size_t)r * cs, d_cptr_, d_cidx_, d_flags_,
+                       base + 2 * r + 1, n_, cs, st);
     launch_fwd_contrib(sym_, d_scontrib_ + SP.contrib_off[l], SP.contrib_off[l + 1] - SP.contrib_off[l],
-                       x, d_contrib_, n_, nrhs, cs, st);
+                       x, contrib, n_, nrhs, cs, st);
   }
   for (int l = nl - 1; l >= 0; --l) {
     launch_bwd_gather(sym_, d_sgather_ + SP.gather_off[l], SP.gather_off[l + 1] - SP.gather_off[l],
                       x, n_, nrhs, st);
     launch_bwd_diag(sym_, d_slist_ + SP.level_off[l], SP.level_off[l + 1] - SP.level_off[l], smem,
                     x, n_, nrhs, st);
+    for (int r = 0; r < nrhs; ++r)
+      launch_bwd_chain(sym_, d_bchain_ + SP.chain_off[l], SP.chain_off[l + 1] - SP.chain_off[l],
+                       x + (size_t)r * n_, d_flags_, base + 2 * r + 2, st);
   }
+}
+
+// After a synchronised solve: did a chained block wait time out?
+bool Engine::solve_status_ok(std::string &err) {
+  cudaError_t e = cudaMemcpy(h_status_ + 2, d_status_ + 2, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) { err = std::string("solve status: ") + cudaGetErrorString(e); return false; }
+  if (h_status_[2]) { err = "triangular solve: a block waited too long for its predecessor"; return false; }
+  return true;
 }
 
 bool Engine::solve(const double *b, double *x, int nrhs, std::string &err) {
@@ -701,7 +787,7 @@ bool Engine::solve(const double *b, double *x, int nrhs, std::string &err) {
   e = cudaStreamSynchronize(stream_);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) { err = std::string("solve: ") + cudaGetErrorString(e); return false; }
-  return true;
+  return solve_status_ok(err);
 }
 
 bool Engine::refine(const double *b, double *x, int nrhs, double tol, int maxit, RefineInfo &info,
@@ -805,7 +891,7 @@ bool Engine::refine(const double *b, double *x, int nrhs, double tol, int maxit,
   info.berr = berr;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) { err = std::string("refine: ") + cudaGetErrorString(e); return false; }
-  return true;
+  return solve_status_ok(err);
 }
 
 bool Engine::solve_in_scratch(const double *b, double *x, int nrhs, double *scratch,
@@ -824,24 +910,11 @@ bool Engine::solve_in_scratch(const double *b, double *x, int nrhs, double *scra
   cudaError_t e = cudaSuccess;
   if (x != b) e = cudaMemcpyAsync(x, b, sizeof(double) * n_ * nrhs, cudaMemcpyDeviceToDevice, st);
   if (e != cudaSuccess) { err = std::string("solve: ") + cudaGetErrorString(e); return false; }
-  const int nl = (int)SP.level_off.size() - 1;
-  const int smem = (int)sizeof(double) * std::max(SP.max_w, 1);
-  for (int l = 0; l < nl; ++l) {
-    launch_fwd_diag(sym_, d_slist_ + SP.level_off[l], SP.level_off[l + 1] - SP.level_off[l], smem,
-                    x, scratch, n_, nrhs, cs, st);
-    launch_fwd_contrib(sym_, d_scontrib_ + SP.contrib_off[l], SP.contrib_off[l + 1] - SP.contrib_off[l],
-                       x, scratch, n_, nrhs, cs, st);
-  }
-  for (int l = nl - 1; l >= 0; --l) {
-    launch_bwd_gather(sym_, d_sgather_ + SP.gather_off[l], SP.gather_off[l + 1] - SP.gather_off[l],
-                      x, n_, nrhs, st);
-    launch_bwd_diag(sym_, d_slist_ + SP.level_off[l], SP.level_off[l + 1] - SP.level_off[l], smem,
-                    x, n_, nrhs, st);
-  }
+  run_solve_with(x, nrhs, scratch);
   e = cudaStreamSynchronize(st);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) { err = std::string("solve: ") + cudaGetErrorString(e); return false; }
-  return true;
+  return solve_status_ok(err);
 }
 
 }  // namespace swc

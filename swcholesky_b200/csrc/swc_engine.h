@@ -26,6 +26,7 @@ struct DevSym {
   double *L;              // supernodal values (the reference's lValues)
   int *status;            // [0] = smallest failing column + 1 (INT_MAX if none),
                           // [1] = structure error flag
+  float2 *Lf;             // split-TF32 mirror {hi, lo} of L (mixed-precision only, else null)
   double *dinv;           // scratch: inverses of the 64x64 diagonal blocks of the tiled class
   const int *dinv_off;    // per supernode: first block of its inverses in dinv (-1: none)
 };
@@ -71,13 +72,19 @@ struct Plan {
 // Triangular solves and refinement (swc_solve.cu)
 bool solve_configure(int max_w, std::string &err);
 void launch_fwd_diag(const DevSym &S, const int *list, int count, int smem, double *y,
-                     const double *contrib, int n, int nrhs, int64_t cstride, cudaStream_t st);
+                     const double *contrib, const int *cptr, const int *cidx, int n, int nrhs,
+                     int64_t cstride, cudaStream_t st);
 void launch_fwd_contrib(const DevSym &S, const int2 *tasks, int count, const double *y,
                         double *contrib, int n, int nrhs, int64_t cstride, cudaStream_t st);
 void launch_bwd_gather(const DevSym &S, const int2 *tasks, int count, double *x, int n, int nrhs,
                        cudaStream_t st);
 void launch_bwd_diag(const DevSym &S, const int *list, int count, int smem, double *x, int n,
                      int nrhs, cudaStream_t st);
+void launch_fwd_chain(const DevSym &S, const int2 *tasks, int count, double *y,
+                      const double *contrib, const int *cptr, const int *cidx, int *flags,
+                      int epoch, int n, int64_t cstride, cudaStream_t st);
+void launch_bwd_chain(const DevSym &S, const int2 *tasks, int count, double *x, int *flags,
+                      int epoch, cudaStream_t st);
 void launch_spmv(int n, const int *rp, const int *ci, const double *val, const double *x,
                  double *y, int nrhs, cudaStream_t st);
 void launch_gather_vals(int nnz, const int *map, const double *ax, double *val, cudaStream_t st);
@@ -89,14 +96,17 @@ void launch_rowabs(int n, const int *rp, const double *val, double *out, cudaStr
 
 // Per-level task lists of the solves.
 struct SolvePlan {
-  std::vector<int> level_off;       // supernodes of level l: list[level_off[l] .. level_off[l+1])
-  std::vector<int> list;
+  std::vector<int> level_off;       // small-class supernodes of level l:
+  std::vector<int> list;            //   list[level_off[l] .. level_off[l+1])
+  std::vector<int> chain_off;       // (s, block) tasks of the tiled class in level l:
+  std::vector<int2> fchain, bchain; //   forward (increasing block) / backward (decreasing)
   std::vector<int> contrib_off;     // (s, r0) tasks of level l
   std::vector<int2> contrib_tasks;
   std::vector<int> gather_off;      // (s, j0) tasks of level l
   std::vector<int2> gather_tasks;
   int max_w = 0;
   int64_t contrib_len = 0;          // off-diagonal rows in total (one contribution each)
+  std::vector<int> cptr, cidx;      // per column: contributions it receives (CSR)
 };
 
 // Result of a refined solve, per right-hand side.
@@ -130,11 +140,13 @@ class Engine {
                const int *pruneSet, std::string &err);
   // values: the A2 values (host or device).  Returns 0 on success, 1 if not SPD
   // (*info = failing column + 1), <0 on errors.
-  int factor(const double *values, bool values_on_device, int *info, std::string &err);
+  // mixed: Schur updates of the tiled class as split-TF32 tensor-core products.
+  int factor(const double *values, bool values_on_device, int *info, std::string &err,
+             bool mixed = false);
   // The same factorization with a CUDA event pair around every launch; fills per-class
   // launch counts and device milliseconds (no other difference).
   int factor_profiled(const double *values, bool values_on_device, int *info,
-                      KernelStats &out, std::string &err);
+                      KernelStats &out, std::string &err, bool mixed = false);
   // x = (L L^T)^{-1} b for nrhs right-hand sides (device pointers, leading dimension n).
   bool solve(const double *b, double *x, int nrhs, std::string &err);
   // The same solve with the contribution scratch supplied by the caller (capacity in
@@ -159,7 +171,8 @@ class Engine {
 
  private:
   void release();
-  void launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof = nullptr);
+  void launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof = nullptr, bool mixed = false);
+  bool set_mode(bool mixed, std::string &err);
   int finish(int *info, std::string &err);
   int64_t h2d_bytes_ = 0, d2h_bytes_ = 0;
   int device_ = 0;
@@ -180,14 +193,18 @@ class Engine {
   int2 *d_asm_ = nullptr, *d_panel_ = nullptr;
   int4 *d_upd_tasks_ = nullptr, *d_syrk_ = nullptr, *d_pairs_ = nullptr;
   int *d_upd_end_ = nullptr;
-  cudaGraph_t graph_ = nullptr;
-  cudaGraphExec_t graph_exec_ = nullptr;
+  cudaGraph_t graph_ = nullptr, graph_mx_ = nullptr;
+  cudaGraphExec_t graph_exec_ = nullptr, graph_exec_mx_ = nullptr;
+  float2 *d_Lf_ = nullptr;
   bool use_graph_ = true;
   Plan plan_;
   DevSym sym_{};
   // solve data
   SolvePlan splan_;
-  int *d_slist_ = nullptr;
+  int *d_slist_ = nullptr, *d_cptr_ = nullptr, *d_cidx_ = nullptr, *d_flags_ = nullptr;
+  int2 *d_fchain_ = nullptr, *d_bchain_ = nullptr;
+  int solve_epoch_ = 0;
+  int64_t nflags_ = 0;
   int2 *d_scontrib_ = nullptr, *d_sgather_ = nullptr;
   int *d_csr_rp_ = nullptr, *d_csr_ci_ = nullptr, *d_csr_map_ = nullptr;
   double *d_csr_val_ = nullptr;
@@ -197,6 +214,8 @@ class Engine {
   double anorm_ = 0.0;
   bool ensure_work(int nrhs, std::string &err);
   void run_solve(double *x, int nrhs);
+  void run_solve_with(double *x, int nrhs, double *contrib);
+  bool solve_status_ok(std::string &err);
 };
 
 // kernel launch wrappers (swc_kernels.cu)
@@ -209,5 +228,10 @@ void launch_trsm_step(const DevSym &S, const int2 *tasks, int count, int step, c
 void launch_syrk_step(const DevSym &S, const int4 *tasks, int count, int step, cudaStream_t st);
 void launch_init_status(int *status, cudaStream_t st);
 bool kernels_configure(std::string &err);
+// mixed-precision Schur updates (swc_mixed.cu)
+bool mixed_configure(std::string &err);
+void launch_update_tiles_mx(const DevSym &S, const int4 *tasks, const int *task_end,
+                            const int4 *pairs, int count, cudaStream_t st);
+void launch_syrk_step_mx(const DevSym &S, const int4 *tasks, int count, int step, cudaStream_t st);
 
 }  // namespace swc

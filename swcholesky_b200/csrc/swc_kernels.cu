@@ -44,6 +44,15 @@ __device__ __forceinline__ int lbound(const int *a, int len, int key) {
   return lo;
 }
 
+// {hi, lo} split of x for the tensor-core mirror: hi = tf32(x), lo = tf32(x - hi).
+__device__ __forceinline__ float2 split_tf32(double x) {
+  const float xf = (float)x;
+  unsigned hi, lo;
+  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(hi) : "f"(xf));
+  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(lo) : "f"(xf - __uint_as_float(hi)));
+  return make_float2(__uint_as_float(hi), __uint_as_float(lo));
+}
+
 __device__ __forceinline__ void flag_structure_error(const DevSym &S) {
   atomicExch(&S.status[1], 1);
 }
@@ -138,6 +147,10 @@ __global__ void __launch_bounds__(NT) k_factor_small(DevSym S, const int *list, 
   __syncthreads();
   double *dst = S.L + S.xptr[s];
   for (int i = tid; i < m * w; i += NT) dst[i] = P[i];
+  if (S.Lf) {   // mixed-precision factorization: split mirror for the Schur updates
+    float2 *dstf = S.Lf + S.xptr[s];
+    for (int i = tid; i < m * w; i += NT) dstf[i] = split_tf32(P[i]);
+  }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -170,8 +183,9 @@ __global__ void k_assemble(DevSym S, const int2 *tasks, int count) {
 // Fragment layout of m8n8k4 .f64: A[lane/4][lane%4], B[k = lane%4][n = lane/4],
 // C[lane/4][2*(lane%4) + e].
 constexpr int MT = 128;               // threads of the tensor-core tile kernels
-constexpr int LDS = TB + 8;           // padded row of a staged k-slice (bank spread)
+constexpr int LDS = TB + 4;           // padded row of a staged k-slice: 64-bit fragment loads conflict-free
 constexpr int STAGE = 2 * KC * LDS;   // doubles per pipeline stage (A and B slices)
+static_assert(MT == 2 * TB, "staging pattern: two threads per tile row");
 
 __device__ __forceinline__ void cp_async8(double *smem, const double *gmem, bool pred) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
@@ -198,16 +212,22 @@ struct TileAcc {
   }
 };
 
+// Thread t copies tile row t % 64 at chunk offsets t / 64, t / 64 + 2, ... (one pointer
+// step per copy).
 __device__ __forceinline__ void load_chunk(const double *__restrict__ Pa, int lda, int na,
                                            const double *__restrict__ Pb, int ldb, int nb,
                                            int K, int k0, double *st) {
-  double *As = st, *Bs = st + KC * LDS;
-  for (int e = threadIdx.x; e < KC * TB; e += MT) {
-    const int k = e / TB, i = e - k * TB;
-    const int kk = k0 + k;
-    const bool pa = kk < K && i < na, pb = kk < K && i < nb;
-    cp_async8(&As[k * LDS + i], pa ? Pa + (size_t)kk * lda + i : Pa, pa);
-    cp_async8(&Bs[k * LDS + i], pb ? Pb + (size_t)kk * ldb + i : Pb, pb);
+  const int i = threadIdx.x & (TB - 1), kq = threadIdx.x >> 6;
+  double *As = st + kq * LDS + i, *Bs = st + KC * LDS + kq * LDS + i;
+  const double *pa = Pa + (size_t)(k0 + kq) * lda + i, *pb = Pb + (size_t)(k0 + kq) * ldb + i;
+  const bool ina = i < na, inb = i < nb;
+#pragma unroll
+  for (int it = 0; it < KC / 2; ++it) {
+    const bool kin = k0 + kq + 2 * it < K;
+    cp_async8(As + 2 * it * LDS, kin && ina ? pa : Pa, kin && ina);
+    cp_async8(Bs + 2 * it * LDS, kin && inb ? pb : Pb, kin && inb);
+    pa += (size_t)2 * lda;
+    pb += (size_t)2 * ldb;
   }
   cp_async_commit();
 }
@@ -250,17 +270,19 @@ __device__ __forceinline__ void dmma_tile_product(const double *__restrict__ Pa,
 // source panel that feeds tile row i / column j, or -1 for a zero row.  Lets one
 // accumulator collect the contributions of several descendants in the target's own
 // coordinates, with no scatter.
-__device__ __forceinline__ void load_chunk_gather(const double *__restrict__ Ld, int ld,
-                                                  const int *ia, const int *ib, int K, int k0,
-                                                  double *st) {
-  double *As = st, *Bs = st + KC * LDS;
-  for (int e = threadIdx.x; e < KC * TB; e += MT) {
-    const int k = e / TB, i = e - k * TB;
-    const int kk = k0 + k;
-    const int ra = ia[i], rb = ib[i];
-    const bool pa = kk < K && ra >= 0, pb = kk < K && rb >= 0;
-    cp_async8(&As[k * LDS + i], pa ? Ld + (size_t)kk * ld + ra : Ld, pa);
-    cp_async8(&Bs[k * LDS + i], pb ? Ld + (size_t)kk * ld + rb : Ld, pb);
+__device__ __forceinline__ void load_chunk_gather(const double *__restrict__ Ld, int ld, int ra,
+                                                  int rb, int K, int k0, double *st) {
+  const int i = threadIdx.x & (TB - 1), kq = threadIdx.x >> 6;
+  double *As = st + kq * LDS + i, *Bs = st + KC * LDS + kq * LDS + i;
+  const double *pa = Ld + (size_t)(k0 + kq) * ld + (ra >= 0 ? ra : 0);
+  const double *pb = Ld + (size_t)(k0 + kq) * ld + (rb >= 0 ? rb : 0);
+#pragma unroll
+  for (int it = 0; it < KC / 2; ++it) {
+    const bool kin = k0 + kq + 2 * it < K;
+    cp_async8(As + 2 * it * LDS, kin && ra >= 0 ? pa : Ld, kin && ra >= 0);
+    cp_async8(Bs + 2 * it * LDS, kin && rb >= 0 ? pb : Ld, kin && rb >= 0);
+    pa += (size_t)2 * ld;
+    pb += (size_t)2 * ld;
   }
   cp_async_commit();
 }
@@ -281,10 +303,11 @@ __device__ __forceinline__ void dmma_tile_product_gather(const double *__restric
     if (__any_sync(0xffffffffu, ia[wr + 8 * i + (lane & 7)] >= 0)) rmask |= 1u << i;
     if (__any_sync(0xffffffffu, ib[wc + 8 * i + (lane & 7)] >= 0)) cmask |= 1u << i;
   }
-  load_chunk_gather(Ld, ld, ia, ib, K, 0, stages);
+  const int ra = ia[threadIdx.x & (TB - 1)], rb = ib[threadIdx.x & (TB - 1)];
+  load_chunk_gather(Ld, ld, ra, rb, K, 0, stages);
   for (int c = 0; c < nchunks; ++c) {
     if (c + 1 < nchunks) {
-      load_chunk_gather(Ld, ld, ia, ib, K, (c + 1) * KC, stages + ((c + 1) & 1) * STAGE);
+      load_chunk_gather(Ld, ld, ra, rb, K, (c + 1) * KC, stages + ((c + 1) & 1) * STAGE);
       cp_async_wait<1>();
     } else {
       cp_async_wait<0>();
@@ -563,8 +586,9 @@ __device__ void trtri64_blocked(const double *D, double *E, double *W, int bw) {
   __syncthreads();
 }
 
-// Factor diagonal block c0/64 of supernode s in place (lower triangle only) and, when rows
-// follow below it, store its inverse (T(r, c) at dinv[c * 64 + r]) for their TRSM.
+// Factor diagonal block c0/64 of supernode s in place (lower triangle only) and store its
+// inverse (T(r, c) at dinv[c * 64 + r]) for the TRSM of the rows below it and for the
+// chained triangular solves.
 // 128 threads, DIAG_SMEM bytes of dynamic shared memory.
 constexpr int DIAG_SMEM = (2 * TB * DLD + 4 * 64) * 8;
 
@@ -591,7 +615,7 @@ __device__ void factor_diag_block(const DevSym &S, int s, int c0, double *smem) 
     const int c = e >> 6, r = e & (TB - 1);
     if (c < bw && r < bw && r >= c) P[(size_t)(c0 + c) * m + c0 + r] = D[c * DLD + r];
   }
-  if (c0 + bw < m) {
+  {   // the inverse serves the TRSM of the rows below and the chained triangular solves
     trtri64_blocked(D, E, W, bw);
     double *T = S.dinv + ((size_t)S.dinv_off[s] + c0 / TB) * (TB * TB);
     for (int e = tid; e < TB * TB; e += blockDim.x) {
@@ -679,7 +703,10 @@ __global__ void __launch_bounds__(MT) k_trsm_step(DevSym S, const int2 *tasks, i
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         const int c = acc_col(j, e);
-        if (c < bw) P[(size_t)(c0 + c) * m + r0 + r] = acc.v[i][j][e];
+        if (c < bw) {
+          P[(size_t)(c0 + c) * m + r0 + r] = acc.v[i][j][e];
+          if (S.Lf) S.Lf[S.xptr[s] + (size_t)(c0 + c) * m + r0 + r] = split_tf32(acc.v[i][j][e]);
+        }
       }
   }
 }

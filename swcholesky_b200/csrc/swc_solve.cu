@@ -16,25 +16,18 @@ namespace {
 constexpr int ST = 256;   // threads of the solve kernels
 constexpr int SB = 32;    // column block of the dense triangular solves (one warp)
 
-__device__ __forceinline__ int lbound_s(const int *a, int len, int key) {
-  int lo = 0, hi = len;
-  while (lo < hi) {
-    int mid = (lo + hi) >> 1;
-    if (a[mid] < key) lo = mid + 1; else hi = mid;
-  }
-  return lo;
-}
-
 // Forward solve, level by level (leaves first), in two kernels per level:
-//   k_fwd_diag    y[cols of s] := L_ss^{-1} (y[cols of s] - sum over descendants d of
-//                 their contributions to those rows), one CTA per supernode; the
-//                 descendants' contributions were stored by k_fwd_contrib, so the gather
-//                 costs one subtraction per contributed row, in prune-set order.
+//   k_fwd_diag    y[cols of s] := L_ss^{-1} (y[cols of s] - sum of the contributions the
+//                 descendants stored for those columns), one CTA per supernode; column j's
+//                 contributions are listed in cidx[cptr[j] .. cptr[j+1]) (one entry per
+//                 off-diagonal row of L equal to j, in increasing supernode order), so
+//                 every column sums its own list with no barrier.
 //   k_fwd_contrib c_s = L_s[rows below the diagonal block, :] y[cols of s], one CTA per
 //                 256-row slab: the off-diagonal GEMV of every supernode runs in parallel.
 // c_s lives at contrib + rowptr[s] - super[s] (one entry per off-diagonal row).
 __global__ void __launch_bounds__(ST) k_fwd_diag(DevSym S, const int *list, double *y,
-                                                 const double *contrib, int n, int nrhs,
+                                                 const double *contrib, const int *cptr,
+                                                 const int *cidx, int n, int nrhs,
                                                  int64_t cstride) {
   extern __shared__ double v[];
   const int s = list[blockIdx.x];
@@ -46,20 +39,13 @@ __global__ void __launch_bounds__(ST) k_fwd_diag(DevSym S, const int *list, doub
     double *yr = y + (size_t)rhs * n;
     const double *cr = contrib + (size_t)rhs * cstride;
     __syncthreads();
-    for (int i = tid; i < w; i += ST) v[i] = yr[f + i];
-    __syncthreads();
-    for (int q = S.upd_ptr[s]; q < S.upd_ptr[s + 1]; ++q) {
-      const int d = S.upd[q];
-      const int fd = S.super[d], wd = S.super[d + 1] - fd;
-      const int64_t rbd = S.rowptr[d];
-      const int md = (int)(S.rowptr[d + 1] - rbd);
-      const int *Lsd = S.Ls + rbd;
-      const int lb = wd + lbound_s(Lsd + wd, md - wd, f);
-      const int ub = wd + lbound_s(Lsd + wd, md - wd, f + w);
-      const double *cd = cr + (rbd - fd) - wd;   // cd[a] for a >= wd
-      for (int a = lb + tid; a < ub; a += ST) v[Lsd[a] - f] -= cd[a];
-      __syncthreads();
+    // column j of s receives the contributions listed for it (descendant order)
+    for (int i = tid; i < w; i += ST) {
+      double acc = yr[f + i];
+      for (int q = cptr[f + i]; q < cptr[f + i + 1]; ++q) acc -= cr[cidx[q]];
+      v[i] = acc;
     }
+    __syncthreads();
     // dense lower solve with the diagonal block, blocked by SB columns
     for (int j0 = 0; j0 < w; j0 += SB) {
       const int jb = min(SB, w - j0);
@@ -174,6 +160,138 @@ __global__ void __launch_bounds__(ST) k_bwd_diag(DevSym S, const int *list, doub
   }
 }
 
+// ---- chained dense solves with the diagonal block of a tiled-class supernode -----------
+// One CTA per 64-row block k of the diagonal block; block k consumes the solved blocks
+// c < k (forward) or c > k (backward) as they are published through per-block flags
+// (flag == epoch), and applies its own block through the stored inverse of the 64x64
+// diagonal block (DMMA-free GEMVs: the work per block is small and latency-bound).  All
+// CTAs of a chain are resident together (a few hundred at most) and only wait on CTAs with
+// a lower blockIdx, which the hardware dispatches first.  Waits are bounded: after
+// SPIN_LIMIT polls the CTA records a timeout in status[2] and stops waiting.
+constexpr long long SPIN_LIMIT = 1LL << 24;
+
+__device__ __forceinline__ int ld_acquire(const int *p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ void st_release(int *p, int v) {
+  asm volatile("st.release.gpu.global.s32 [%0], %1;\n" ::"l"(p), "r"(v));
+}
+
+// thread 0 polls, everyone waits at the barrier; returns false after a timeout
+__device__ bool wait_flag(const int *flag, int val, int *status) {
+  __shared__ int ok;
+  if (threadIdx.x == 0) {
+    long long it = 0;
+    ok = 1;
+    while (ld_acquire(flag) != val) {
+      if (++it > SPIN_LIMIT) {
+        atomicExch(&status[2], 1);
+        ok = 0;
+        break;
+      }
+      __nanosleep(100);
+    }
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+// task = (s, k); forward: y[f + 64k ..] := T_k (y[...] - contributions - sum_{c<k} L_kc x_c)
+__global__ void __launch_bounds__(ST) k_fwd_chain(DevSym S, const int2 *tasks, double *y,
+                                                  const double *contrib, const int *cptr,
+                                                  const int *cidx, int *flags, int epoch,
+                                                  int n, int64_t cstride) {
+  __shared__ double v[TB], part[4][TB], xc[TB];
+  const int s = tasks[blockIdx.x].x, k = tasks[blockIdx.x].y;
+  const int tid = threadIdx.x, r = tid & (TB - 1), q = tid >> 6;
+  const int f = S.super[s], w = S.super[s + 1] - f;
+  const int m = (int)(S.rowptr[s + 1] - S.rowptr[s]);
+  const double *P = S.L + S.xptr[s];
+  const int r0 = k * TB, bw = min(TB, w - r0);
+  const int base = S.dinv_off[s];
+  const double *T = S.dinv + ((size_t)base + k) * (TB * TB);
+  // right-hand side of the block minus the descendants' contributions
+  if (tid < TB) {
+    double acc = 0.0;
+    if (tid < bw) {
+      const int j = f + r0 + tid;
+      acc = y[j];
+      for (int qq = cptr[j]; qq < cptr[j + 1]; ++qq) acc -= contrib[cidx[qq]];
+    }
+    v[tid] = acc;
+  }
+  __syncthreads();
+  for (int c = 0; c < k; ++c) {
+    if (!wait_flag(&flags[base + c], epoch, S.status)) break;
+    if (tid < TB) xc[tid] = __ldcg(&y[f + c * TB + tid]);
+    __syncthreads();
+    double acc = 0.0;
+    if (r < bw)
+      for (int jj = q * 16; jj < q * 16 + 16; ++jj)
+        acc = fma(P[(size_t)(c * TB + jj) * m + r0 + r], xc[jj], acc);
+    part[q][r] = acc;
+    __syncthreads();
+    if (tid < TB) v[tid] -= (part[0][tid] + part[1][tid]) + (part[2][tid] + part[3][tid]);
+    __syncthreads();
+  }
+  // x_k = T_k v
+  double acc = 0.0;
+  if (r < bw)
+    for (int jj = q * 16; jj < q * 16 + 16; ++jj) acc = fma(T[(size_t)jj * TB + r], v[jj], acc);
+  part[q][r] = acc;
+  __syncthreads();
+  if (tid < bw) y[f + r0 + tid] = (part[0][tid] + part[1][tid]) + (part[2][tid] + part[3][tid]);
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) st_release(&flags[base + k], epoch);
+}
+
+// task = (s, k) in decreasing k; backward: x[f + 64k ..] := T_k^T (x[...] - sum_{c>k} L_ck^T x_c)
+__global__ void __launch_bounds__(ST) k_bwd_chain(DevSym S, const int2 *tasks, double *x,
+                                                  int *flags, int epoch) {
+  __shared__ double v[TB], xc[TB];
+  const int s = tasks[blockIdx.x].x, k = tasks[blockIdx.x].y;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int f = S.super[s], w = S.super[s + 1] - f;
+  const int m = (int)(S.rowptr[s + 1] - S.rowptr[s]);
+  const double *P = S.L + S.xptr[s];
+  const int r0 = k * TB, bw = min(TB, w - r0);
+  const int nb = (w + TB - 1) / TB;
+  const int base = S.dinv_off[s];
+  const double *T = S.dinv + ((size_t)base + k) * (TB * TB);
+  if (tid < TB) v[tid] = (tid < bw) ? x[f + r0 + tid] : 0.0;
+  __syncthreads();
+  for (int c = nb - 1; c > k; --c) {
+    if (!wait_flag(&flags[base + c], epoch, S.status)) break;
+    const int cw = min(TB, w - c * TB);
+    if (tid < TB) xc[tid] = (tid < cw) ? __ldcg(&x[f + c * TB + tid]) : 0.0;
+    __syncthreads();
+    // v[i] -= sum_r L(64c + r, 64k + i) x_c[r]: one warp per i, lanes over r
+    for (int i = warp; i < bw; i += ST / 32) {
+      const double *col = P + (size_t)(r0 + i) * m + c * TB;
+      double acc = 0.0;
+      for (int rr = lane; rr < cw; rr += 32) acc = fma(col[rr], xc[rr], acc);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if (lane == 0) v[i] -= acc;
+    }
+    __syncthreads();
+  }
+  // x_k[i] = sum_{r >= i} T(r, i) v[r]: column i of T is contiguous
+  for (int i = warp; i < bw; i += ST / 32) {
+    double acc = 0.0;
+    for (int rr = lane; rr < bw; rr += 32) acc = fma(T[(size_t)i * TB + rr], v[rr], acc);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) x[f + r0 + i] = acc;
+  }
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) st_release(&flags[base + k], epoch);
+}
+
 // y = A x for the symmetric matrix held as full CSR (both triangles), nrhs vectors.
 __global__ void k_spmv(int n, const int *rp, const int *ci, const double *val, const double *x,
                        double *y, int nrhs) {
@@ -268,8 +386,10 @@ bool solve_configure(int max_w, std::string &err) {
 }
 
 void launch_fwd_diag(const DevSym &S, const int *list, int count, int smem, double *y,
-                     const double *contrib, int n, int nrhs, int64_t cstride, cudaStream_t st) {
-  if (count > 0) k_fwd_diag<<<count, ST, smem, st>>>(S, list, y, contrib, n, nrhs, cstride);
+                     const double *contrib, const int *cptr, const int *cidx, int n, int nrhs,
+                     int64_t cstride, cudaStream_t st) {
+  if (count > 0)
+    k_fwd_diag<<<count, ST, smem, st>>>(S, list, y, contrib, cptr, cidx, n, nrhs, cstride);
 }
 void launch_fwd_contrib(const DevSym &S, const int2 *tasks, int count, const double *y,
                         double *contrib, int n, int nrhs, int64_t cstride, cudaStream_t st) {
@@ -282,6 +402,16 @@ void launch_bwd_gather(const DevSym &S, const int2 *tasks, int count, double *x,
 void launch_bwd_diag(const DevSym &S, const int *list, int count, int smem, double *x, int n,
                      int nrhs, cudaStream_t st) {
   if (count > 0) k_bwd_diag<<<count, ST, smem, st>>>(S, list, x, n, nrhs);
+}
+void launch_fwd_chain(const DevSym &S, const int2 *tasks, int count, double *y,
+                      const double *contrib, const int *cptr, const int *cidx, int *flags,
+                      int epoch, int n, int64_t cstride, cudaStream_t st) {
+  if (count > 0)
+    k_fwd_chain<<<count, ST, 0, st>>>(S, tasks, y, contrib, cptr, cidx, flags, epoch, n, cstride);
+}
+void launch_bwd_chain(const DevSym &S, const int2 *tasks, int count, double *x, int *flags,
+                      int epoch, cudaStream_t st) {
+  if (count > 0) k_bwd_chain<<<count, ST, 0, st>>>(S, tasks, x, flags, epoch);
 }
 void launch_spmv(int n, const int *rp, const int *ci, const double *val, const double *x,
                  double *y, int nrhs, cudaStream_t st) {

@@ -48,7 +48,7 @@ def test_null_handle_calls_fail_cleanly():
     assert L.swc_get_L(None, None, 0) == swc.SWC_INVALID_INPUT
     assert L.swc_sizes(None, None) == swc.SWC_INVALID_INPUT
     assert L.swc_set_stream(None, None) == swc.SWC_INVALID_INPUT
-    assert L.swc_profile(None, None, 0, ctypes.byref(info), None, None, None, None) == \
+    assert L.swc_profile(None, None, 0, 0, ctypes.byref(info), None, None, None, None) == \
         swc.SWC_INVALID_INPUT
     assert L.swc_get_stream(None) is None
     assert L.swc_device_L(None) is None

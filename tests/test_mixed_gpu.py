@@ -1,0 +1,43 @@
+"""Mixed-precision factorization (split-TF32 Schur updates) followed by FP64 refinement.
+
+The mixed factor differs from the FP64 one by FP32-class rounding amplified by the
+conditioning (checked: relative difference of L above 1e-12, below 1e-5 for the Laplacian
+and below 1e-2 for the cond ~1e6 stencil), and refinement against the FP64 matrix reaches
+the FP64 backward error (<= 1e-14)."""
+import numpy as np
+import pytest
+
+from conftest import load_sym
+import swcholesky_b200 as swc
+from swcholesky_b200 import workloads as W
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name,lbound", [("grid3d_24", 1e-5), ("stencil27_12", 1e-2)])
+def test_mixed_factor_then_refine(cuda_ok, name, lbound):
+    gs = load_sym(name)
+    A, _, _ = W.build(name)
+    P = W.assemble(A, gs["perm"], gs["super"])
+    h = swc.Handle(0)
+    h.analyze(P.n, P.A2p, P.A2i, P.lC, P.Ls, P.Li_ptr, P.super, P.prunePtr, P.pruneSet)
+    assert h.factor(P.A2x, swc.SWC_MODE_FP64) == 0
+    L64 = h.get_L()
+    assert h.factor(P.A2x, swc.SWC_MODE_MIXED_TF32X3) == 0
+    Lmx = h.get_L()
+    rel = np.abs(Lmx - L64).max() / np.abs(L64).max()
+    assert 1e-12 < rel < lbound, rel
+    # deterministic
+    assert h.factor(P.A2x, swc.SWC_MODE_MIXED_TF32X3) == 0
+    assert np.array_equal(h.get_L(), Lmx)
+    rng = np.random.default_rng(0)
+    b = rng.standard_normal((P.n, 2))
+    x, berr, iters, method = h.refine(b, tol=1e-14, maxit=30)
+    assert method in (1, 2) and iters >= 1
+    assert berr.max() <= 1e-14
+    Afull = A.to_scipy_full()
+    anorm = abs(Afull).sum(axis=1).max()
+    for k in range(2):
+        r = O.oracle_symv(P.n, P.A2p, P.A2i, P.A2x, x[:, k]) - b[:, k]
+        assert np.abs(r).max() / (anorm * np.abs(x[:, k]).max()) <= 1e-14
