@@ -120,6 +120,23 @@ int swc_refine(swc_handle_t handle, const double *b, double *x, int nrhs, int on
 #define SWC_SOLVE_NOALLOC_MAX 1048576
 int swc_solve_noalloc(swc_handle_t handle, const double *b, double *x, int nrhs);
 
+/* ---- adjoint (no reference counterpart: the reference computes no derivatives) -----
+ * All three work on the handle's current factor (any mode) and on the stored nonzeros of
+ * A2 = P A P^T (lower triangle, the `values` of swc_factor; a stored off-diagonal value
+ * stands for both A_ij and A_ji).  Vectors are in the factor's ordering.
+ *
+ * swc_logdet: log det A = 2 sum_j log L_jj.
+ * swc_logdet_grad: grad[p] = d log det A / d values[p] = (A^{-1})_ij (2 - delta_ij), from
+ *   the selected inverse of A on the pattern of L (reverse sweep over the elimination
+ *   tree).  grad has c[n] doubles.
+ * swc_solve_grad: for a scalar f(x) with x = A^{-1} b and lam = A^{-1} df/dx (one more
+ *   solve), grad[p] = df / d values[p] = -(lam_i x_j + lam_j x_i), or -lam_i x_i on the
+ *   diagonal.  x and lam have n doubles, grad c[n]; df/db is lam itself. */
+int swc_logdet(swc_handle_t handle, double *logdet);
+int swc_logdet_grad(swc_handle_t handle, double *grad, int on_device);
+int swc_solve_grad(swc_handle_t handle, const double *x, const double *lam, double *grad,
+                   int on_device);
+
 /* Device pointer to the handle's L (xsize doubles), valid until the next analyze. */
 const double *swc_device_L(swc_handle_t handle);
 
@@ -157,6 +174,15 @@ int swc_layout_sizes(int n, const int *c, const int *r, const int *blockSet, int
 int swc_layout(int n, const int *c, const int *r, const int *blockSet, int supNo,
                size_t *lC, int *Ls, size_t *Li_ptr, int *sparent, int *prunePtr,
                int *pruneSet, int *levelPtr, int *parPtr, int *partition);
+
+/* Host-only supernode partition of an ordered matrix, for matrices the reference's
+ * analyze_p2 has not seen (the batched path): elimination tree, exact column counts, and
+ * relaxed chains with the reference's relaxation parameters (nrelax = {4, 16, 48},
+ * zrelax = {0.8, 0.1, 0.05} when NULL) and supernodes at most max_width wide.  blockSet
+ * needs room for n + 1 entries; *supNo receives the number of supernodes.  Pair with
+ * swc_layout.  No reference counterpart as a function (it is part of analyze_p2). */
+int swc_supernodes(int n, const int *c, const int *r, const int *nrelax, const double *zrelax,
+                   int max_width, int *blockSet, int *supNo);
 
 #ifdef __cplusplus
 }

@@ -39,7 +39,8 @@ EXPORTS = (
     "sw_cholesky_left_par_05", "swc_last_info", "swc_last_error", "swc_create", "swc_destroy",
     "swc_set_stream", "swc_get_stream", "swc_analyze", "swc_factor", "swc_get_L",
     "swc_device_L", "swc_sizes", "swc_profile", "swc_plan_stats", "swc_layout_sizes",
-    "swc_layout", "swc_solve", "swc_refine", "swc_solve_noalloc",
+    "swc_layout", "swc_solve", "swc_refine", "swc_solve_noalloc", "swc_logdet",
+    "swc_logdet_grad", "swc_solve_grad", "swc_supernodes",
 )
 KERNEL_CLASSES = ("memset", "small", "assemble", "update", "panel", "syrk")
 
@@ -85,6 +86,10 @@ def lib() -> ctypes.CDLL:
         L.swc_plan_stats.argtypes = [_I] + [_VP] * 6 + [_I] + [_VP] * 3
         L.swc_layout_sizes.argtypes = [_I] + [_VP] * 3 + [_I, _VP]
         L.swc_layout.argtypes = [_I] + [_VP] * 3 + [_I] + [_VP] * 9
+        L.swc_logdet.argtypes = [_VP, ctypes.POINTER(ctypes.c_double)]
+        L.swc_logdet_grad.argtypes = [_VP, _VP, _I]
+        L.swc_solve_grad.argtypes = [_VP, _VP, _VP, _VP, _I]
+        L.swc_supernodes.argtypes = [_I, _VP, _VP, _VP, _VP, _I, _VP, ctypes.POINTER(_I)]
         _lib = L
     return _lib
 
@@ -155,6 +160,20 @@ def layout(n, c, r, blockSet):
     return out
 
 
+def supernodes(n, c, r, max_width: int = 1 << 30, nrelax=None, zrelax=None):
+    """Supernode partition (blockSet) of an ordered lower CSC pattern: elimination tree,
+    column counts and relaxed chains (the reference's nrelax / zrelax by default)."""
+    c = _c(c, np.int32)
+    r = _c(r, np.int32)
+    nr = None if nrelax is None else _c(nrelax, np.int32)
+    zr = None if zrelax is None else _c(zrelax, np.float64)
+    bs = np.zeros(int(n) + 1, np.int32)
+    ns = ctypes.c_int(0)
+    _check(lib().swc_supernodes(int(n), _p(c), _p(r), _p(nr), _p(zr), int(max_width), _p(bs),
+                                ctypes.byref(ns)))
+    return bs[: ns.value + 1].copy()
+
+
 PLAN_FIELDS = ("levels", "launches", "small", "tiled", "update_tiles", "update_pairs",
                "trsm_tiles", "syrk_tiles")
 
@@ -219,6 +238,7 @@ class Handle:
         _check(self._lib.swc_analyze(self._h, int(n), _p(c), _p(r), _p(lC), _p(Ls), _p(Li_ptr),
                                      _p(bs), bs.size - 1, _p(pp), _p(ps), nlev, _p(sched[0]),
                                      _p(sched[1]), _p(sched[2])))
+        self.nnz = int(c[int(n)])
         self._keep = None
         sz = np.zeros(6, np.int64)
         _check(self._lib.swc_sizes(self._h, _p(sz)))
@@ -292,6 +312,33 @@ class Handle:
                                     float(tol), int(maxit), _p(berr), ctypes.byref(it),
                                     ctypes.byref(meth)))
         return x, berr, int(it.value), int(meth.value)
+
+    def logdet(self) -> float:
+        """log det A of the current factor."""
+        v = ctypes.c_double(0.0)
+        _check(self._lib.swc_logdet(self._h, ctypes.byref(v)))
+        return float(v.value)
+
+    def logdet_grad(self, out=None):
+        """d log det A / d values (one entry per stored nonzero of A2)."""
+        if out is None:
+            out = np.zeros(self.nnz, np.float64)
+        _check(self._lib.swc_logdet_grad(self._h, _p(out), 1 if hasattr(out, "data_ptr") else 0))
+        return out
+
+    def solve_grad(self, x, lam, out=None):
+        """d f / d values for f(x), x = A^{-1} b, given lam = A^{-1} df/dx."""
+        on_dev = hasattr(x, "data_ptr")
+        if not on_dev:
+            x, lam = _c(x, np.float64), _c(lam, np.float64)
+        if out is None:
+            if on_dev:
+                import torch
+                out = torch.empty(self.nnz, dtype=torch.float64, device=x.device)
+            else:
+                out = np.zeros(self.nnz, np.float64)
+        _check(self._lib.swc_solve_grad(self._h, _p(x), _p(lam), _p(out), 1 if on_dev else 0))
+        return out
 
     def get_L(self, out=None):
         """L in the reference layout: into ``out`` (numpy or CUDA tensor) or a new numpy array."""

@@ -1,6 +1,7 @@
 // C ABI of libswchol_b200 (declared in include/swcholesky_b200.h).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
 #include <memory>
@@ -177,6 +178,73 @@ int swc_refine(swc_handle_t h, const double *b, double *x, int nrhs, int on_devi
     if (method) *method = info.method;
     return SWC_OK;
   });
+}
+
+int swc_logdet(swc_handle_t h, double *logdet) {
+  if (!h || !logdet) return fail(SWC_INVALID_INPUT, "null argument");
+  if (!h->factored) return fail(SWC_NOT_READY, "logdet before a successful factor");
+  std::string err;
+  if (!h->eng->logdet(logdet, err)) return fail(SWC_CUDA_ERROR, err);
+  return SWC_OK;
+}
+
+int swc_logdet_grad(swc_handle_t h, double *grad, int on_device) {
+  if (!h || !grad) return fail(SWC_INVALID_INPUT, "null argument");
+  if (!h->factored) return fail(SWC_NOT_READY, "logdet gradient before a successful factor");
+  std::string err;
+  const size_t bytes = sizeof(double) * (size_t)h->eng->nnz();
+  double *dg = grad;
+  if (!on_device && cudaMalloc(&dg, std::max<size_t>(bytes, 8)) != cudaSuccess)
+    return fail(SWC_CUDA_ERROR, "gradient buffer");
+  int rc = SWC_OK;
+  if (!h->eng->logdet_grad(dg, err)) rc = fail(SWC_CUDA_ERROR, err);
+  else if (!on_device && cudaMemcpy(grad, dg, bytes, cudaMemcpyDeviceToHost) != cudaSuccess)
+    rc = fail(SWC_CUDA_ERROR, "copy of the gradient to the host failed");
+  if (!on_device) cudaFree(dg);
+  return rc;
+}
+
+int swc_solve_grad(swc_handle_t h, const double *x, const double *lam, double *grad,
+                   int on_device) {
+  if (!h || !x || !lam || !grad) return fail(SWC_INVALID_INPUT, "null argument");
+  if (!h->analyzed) return fail(SWC_NOT_READY, "solve gradient before analyze");
+  std::string err;
+  const size_t gbytes = sizeof(double) * (size_t)h->eng->nnz();
+  const size_t vbytes = sizeof(double) * (size_t)h->eng->n();
+  if (on_device) {
+    if (!h->eng->solve_grad(x, lam, grad, err)) return fail(SWC_CUDA_ERROR, err);
+    return SWC_OK;
+  }
+  double *dx = nullptr, *dl = nullptr, *dg = nullptr;
+  cudaError_t e = cudaMalloc(&dx, vbytes);
+  if (e == cudaSuccess) e = cudaMalloc(&dl, vbytes);
+  if (e == cudaSuccess) e = cudaMalloc(&dg, std::max<size_t>(gbytes, 8));
+  if (e == cudaSuccess) e = cudaMemcpy(dx, x, vbytes, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dl, lam, vbytes, cudaMemcpyHostToDevice);
+  int rc = SWC_OK;
+  if (e != cudaSuccess) rc = fail(SWC_CUDA_ERROR, std::string("solve gradient buffers: ") + cudaGetErrorString(e));
+  else if (!h->eng->solve_grad(dx, dl, dg, err)) rc = fail(SWC_CUDA_ERROR, err);
+  else if (cudaMemcpy(grad, dg, gbytes, cudaMemcpyDeviceToHost) != cudaSuccess)
+    rc = fail(SWC_CUDA_ERROR, "copy of the gradient to the host failed");
+  if (dx) cudaFree(dx);
+  if (dl) cudaFree(dl);
+  if (dg) cudaFree(dg);
+  return rc;
+}
+
+int swc_supernodes(int n, const int *c, const int *r, const int *nrelax, const double *zrelax,
+                   int max_width, int *blockSet, int *supNo) {
+  if (!c || !r || !blockSet || !supNo) return fail(SWC_INVALID_INPUT, "null argument");
+  static const int kNrelax[3] = {4, 16, 48};
+  static const double kZrelax[3] = {0.8, 0.1, 0.05};
+  std::vector<int> super;
+  std::string err;
+  if (!swc::supernode_partition(n, c, r, nrelax ? nrelax : kNrelax, zrelax ? zrelax : kZrelax,
+                                max_width, super, err))
+    return fail(SWC_INVALID_INPUT, err);
+  std::copy(super.begin(), super.end(), blockSet);
+  *supNo = (int)super.size() - 1;
+  return SWC_OK;
 }
 
 int swc_sizes(swc_handle_t h, long long *sizes) {

@@ -134,6 +134,7 @@ void Engine::release() {
                   d_csr_val_, d_contrib_, d_work_, d_norms_};
   for (void *p : ptrs)
     if (p) cudaFree(p);
+  release_adjoint();
   d_super_ = d_Ls_ = d_Ap_ = d_Ai_ = nullptr;
   d_rowptr_ = d_xptr_ = nullptr;
   d_upd_ptr_ = d_upd_ = nullptr;
@@ -544,6 +545,8 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
   sym_.dinv = d_dinv_;
   sym_.Lf = nullptr;
   sym_.dinv_off = d_dinv_off_;
+  hsym_ = H;
+  h_Ls_.assign(Ls, Ls + nls);
 
   return true;
 }
@@ -590,7 +593,7 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, bool mix
         launch_diag_step(sym_, d_diag_ + W.diag_off[j], W.diag_cnt[j], (int)j + 1, st);
         mark(-1, W.diag_cnt[j]);
         mark(K_SYRK, W.syrk_cnt[j]);
-        if (mixed) launch_syrk_step_mx(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
+        if (mixed && mx_syrk_) launch_syrk_step_mx(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
         else launch_syrk_step(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
         mark(-1, W.syrk_cnt[j]);
       } else if (W.diag_cnt[j] > 0) {
@@ -599,11 +602,11 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, bool mix
         cudaStreamWaitEvent(aux_stream_, ev_fork_, 0);
         launch_diag_step(sym_, d_diag_ + W.diag_off[j], W.diag_cnt[j], (int)j + 1, aux_stream_);
         cudaEventRecord(ev_join_, aux_stream_);
-        if (mixed) launch_syrk_step_mx(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
+        if (mixed && mx_syrk_) launch_syrk_step_mx(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
         else launch_syrk_step(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
         cudaStreamWaitEvent(st, ev_join_, 0);
       } else {
-        if (mixed) launch_syrk_step_mx(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
+        if (mixed && mx_syrk_) launch_syrk_step_mx(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
         else launch_syrk_step(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
       }
     }

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -131,6 +132,8 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
                 const int64_t *Li_ptr, const int *blockSet, int supNo, const int *prunePtr,
                 const int *pruneSet, HostSym &H, Plan &P, std::string &err);
 
+struct AdjointPlan;   // reverse-sweep schedule of the adjoint (swc_adjoint.cu)
+
 class Engine {
  public:
   explicit Engine(int device);
@@ -164,12 +167,35 @@ class Engine {
   void set_stream(cudaStream_t s) { stream_ = s ? s : own_stream_; }
   int64_t xsize() const { return xsize_; }
   int n() const { return n_; }
+  int64_t nnz() const { return nnz_; }
   int nsuper() const { return nsuper_; }
   const Plan &plan() const { return plan_; }
   double *device_L() const { return dL_; }
   int launches_per_factor() const { return plan_.launches; }
 
+  // Adjoint (swc_adjoint.cu), on the current factor; device pointers, grad has one entry
+  // per stored nonzero of A.
+  bool logdet(double *out, std::string &err);
+  bool selected_inverse(std::string &err);   // Z = A^{-1} on the pattern of L
+  const double *selected_inverse_ptr() const { return d_adj_Z_; }
+  bool logdet_grad(double *grad, std::string &err);
+  bool solve_grad(const double *x, const double *lam, double *grad, std::string &err);
+
  private:
+  bool prepare_adjoint(std::string &err);
+  void release_adjoint();
+  std::shared_ptr<AdjointPlan> adj_;
+  HostSym hsym_;
+  std::vector<int> h_Ls_;
+  int4 *d_adj_units_ = nullptr;
+  int64_t *d_adj_tinv_off_ = nullptr, *d_adj_seg_tbl_ = nullptr;
+  int2 *d_adj_tasks_ = nullptr;
+  int *d_adj_wave_units_ = nullptr, *d_adj_ut_begin_ = nullptr, *d_adj_ut_end_ = nullptr;
+  int *d_adj_rowseg_ = nullptr, *d_adj_seg_t_ = nullptr, *d_adj_seg_S_ = nullptr;
+  int *d_adj_tbl_ = nullptr;
+  double *d_adj_Z_ = nullptr, *d_adj_U_ = nullptr, *d_adj_tinv_ = nullptr, *d_adj_P_ = nullptr;
+  double *d_adj_partial_ = nullptr;
+
   void release();
   void launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof = nullptr, bool mixed = false);
   bool set_mode(bool mixed, std::string &err);
@@ -197,6 +223,10 @@ class Engine {
   cudaGraphExec_t graph_exec_ = nullptr, graph_exec_mx_ = nullptr;
   float2 *d_Lf_ = nullptr;
   bool use_graph_ = true;
+  // Trailing SYRK of the dense steps in split-TF32 too (mixed mode).  Off: on B200 the
+  // FP64 DMMA kernel is the faster one for these 64x64x64 tiles (measured 6.9 ms vs 13.4 ms
+  // per factorization of the 60^3 Laplacian).
+  bool mx_syrk_ = false;
   Plan plan_;
   DevSym sym_{};
   // solve data

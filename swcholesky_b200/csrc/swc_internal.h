@@ -22,6 +22,12 @@ struct Layout {
 bool build_layout(int n, const int *c, const int *r, const int *blockSet, int supNo,
                   Layout &out, std::string &err);
 
+// Supernode partition of an ordered lower CSC pattern (elimination tree, column counts,
+// relaxed chains); super receives nsuper + 1 entries.
+bool supernode_partition(int n, const int *c, const int *r, const int nrelax[3],
+                         const double zrelax[3], int max_width, std::vector<int> &super,
+                         std::string &err);
+
 // Tile edge used by every tiled kernel.
 constexpr int TB = 64;
 

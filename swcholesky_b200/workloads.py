@@ -25,7 +25,7 @@ import numpy as np
 
 from . import matrices as M
 
-__all__ = ["build", "assemble", "Problem", "cond_shift"]
+__all__ = ["build", "assemble", "assemble_own", "Problem", "cond_shift"]
 
 
 def cond_shift(L: M.LowerCSC, cond: float) -> float:
@@ -97,3 +97,15 @@ def assemble(A: M.LowerCSC, perm, super_) -> Problem:
                    Li_ptr=lay["Li_ptr"], sparent=lay["sparent"], prunePtr=lay["prunePtr"],
                    pruneSet=lay["pruneSet"], levelPtr=lay["levelPtr"], parPtr=lay["parPtr"],
                    partition=lay["partition"], xsize=int(lay["xsize"]), perm=perm)
+
+
+def assemble_own(A: M.LowerCSC, perm, max_width: int = 1 << 30, nrelax=None,
+                 zrelax=None) -> Problem:
+    """As ``assemble``, with the library's own supernode partition (elimination tree,
+    column counts, relaxed chains) instead of one from the reference's symbolic phase."""
+    from . import supernodes
+    perm = np.asarray(perm)
+    A2 = M.permute_lower(A, perm)
+    super_ = supernodes(A2.n, A2.indptr, A2.indices, max_width=max_width, nrelax=nrelax,
+                        zrelax=zrelax)
+    return assemble(A, perm, super_)
