@@ -175,6 +175,25 @@ int swc_layout(int n, const int *c, const int *r, const int *blockSet, int supNo
                size_t *lC, int *Ls, size_t *Li_ptr, int *sparent, int *prunePtr,
                int *pruneSet, int *levelPtr, int *parPtr, int *partition);
 
+/* ---- batched factorization (no reference counterpart) ------------------------------
+ * nmat independent SPD matrices, each already ordered (P_k A_k P_k^T, lower CSC): n[k]
+ * columns, column pointers c (n[k] + 1 entries per matrix, each starting at 0, the
+ * matrices' arrays concatenated) and row indices r (local to the matrix, concatenated).
+ * The handle then holds them as ONE block-diagonal matrix of N = sum n[k] columns with
+ * the library's own supernode partition: swc_factor takes the matrices' values
+ * concatenated in the same order, swc_solve / swc_refine the right-hand sides
+ * concatenated, and the whole batch is factored by one CUDA graph replay.
+ * swc_batch_autotune times the factorization of the batch for each supernode grouping and
+ * plan candidate and keeps the fastest (choice[0] = partition, choice[1] = plan,
+ * *best_ms = its time); cache_path (may be NULL) is a text file of earlier results keyed
+ * by structure and mode.  swc_batch_berr gives every matrix's backward error
+ * ||b - A x||_inf / (||A||_inf ||x||_inf) for concatenated b and x (nmat doubles). */
+int swc_batch_analyze(swc_handle_t handle, int nmat, const int *n, const int *c, const int *r);
+int swc_batch_autotune(swc_handle_t handle, const double *values, int values_on_device,
+                       int mode, const char *cache_path, int *choice, double *best_ms);
+int swc_batch_berr(swc_handle_t handle, const double *b, const double *x, int on_device,
+                   double *berr);
+
 /* Host-only supernode partition of an ordered matrix, for matrices the reference's
  * analyze_p2 has not seen (the batched path): elimination tree, exact column counts, and
  * relaxed chains with the reference's relaxation parameters (nrelax = {4, 16, 48},

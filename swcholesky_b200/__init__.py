@@ -40,7 +40,8 @@ EXPORTS = (
     "swc_set_stream", "swc_get_stream", "swc_analyze", "swc_factor", "swc_get_L",
     "swc_device_L", "swc_sizes", "swc_profile", "swc_plan_stats", "swc_layout_sizes",
     "swc_layout", "swc_solve", "swc_refine", "swc_solve_noalloc", "swc_logdet",
-    "swc_logdet_grad", "swc_solve_grad", "swc_supernodes",
+    "swc_logdet_grad", "swc_solve_grad", "swc_supernodes", "swc_batch_analyze",
+    "swc_batch_autotune", "swc_batch_berr",
 )
 KERNEL_CLASSES = ("memset", "small", "assemble", "update", "panel", "syrk")
 
@@ -90,6 +91,9 @@ def lib() -> ctypes.CDLL:
         L.swc_logdet_grad.argtypes = [_VP, _VP, _I]
         L.swc_solve_grad.argtypes = [_VP, _VP, _VP, _VP, _I]
         L.swc_supernodes.argtypes = [_I, _VP, _VP, _VP, _VP, _I, _VP, ctypes.POINTER(_I)]
+        L.swc_batch_analyze.argtypes = [_VP, _I, _VP, _VP, _VP]
+        L.swc_batch_autotune.argtypes = [_VP, _VP, _I, _I, ctypes.c_char_p, _VP, _VP]
+        L.swc_batch_berr.argtypes = [_VP, _VP, _VP, _I, _VP]
         _lib = L
     return _lib
 
@@ -312,6 +316,49 @@ class Handle:
                                     float(tol), int(maxit), _p(berr), ctypes.byref(it),
                                     ctypes.byref(meth)))
         return x, berr, int(it.value), int(meth.value)
+
+    def batch_analyze(self, mats):
+        """Analyse independent ordered matrices (objects with n, indptr, indices: lower CSC
+        of P A P^T) as one block-diagonal batch.  Afterwards factor / solve / refine take
+        the matrices' values and vectors concatenated in this order."""
+        nn = np.array([int(m.n) for m in mats], np.int32)
+        c = np.concatenate([np.asarray(m.indptr, np.int32) for m in mats])
+        r = np.concatenate([np.asarray(m.indices, np.int32) for m in mats])
+        _check(self._lib.swc_batch_analyze(self._h, int(nn.size), _p(nn), _p(c), _p(r)))
+        self.nnz = int(sum(int(m.indptr[-1]) for m in mats))
+        self.batch_n = nn
+        self.batch_offsets = np.concatenate([[0], np.cumsum(nn.astype(np.int64))])
+        sz = np.zeros(6, np.int64)
+        _check(self._lib.swc_sizes(self._h, _p(sz)))
+        self.n, self.nsuper, self.xsize, self.launches = (int(v) for v in sz[:4])
+
+    def batch_autotune(self, values, mode: int = SWC_MODE_FP64, cache_path: str | None = None):
+        """Times the supernode-grouping and plan candidates on these values and keeps the
+        fastest.  Returns ((partition, plan), best milliseconds per batch factorization)."""
+        on_dev = hasattr(values, "data_ptr")
+        if not on_dev:
+            values = _c(values, np.float64)
+        choice = np.zeros(2, np.int32)
+        best = np.zeros(1)
+        _check(self._lib.swc_batch_autotune(self._h, _p(values), 1 if on_dev else 0, int(mode),
+                                            cache_path.encode() if cache_path else None,
+                                            _p(choice), _p(best)))
+        self._refresh_sizes()
+        return (int(choice[0]), int(choice[1])), float(best[0])
+
+    def _refresh_sizes(self):
+        sz = np.zeros(6, np.int64)
+        _check(self._lib.swc_sizes(self._h, _p(sz)))
+        self.n, self.nsuper, self.xsize, self.launches = (int(v) for v in sz[:4])
+
+    def batch_berr(self, b, x):
+        """Backward error of every matrix of the batch for concatenated b and x."""
+        on_dev = hasattr(b, "data_ptr")
+        if not on_dev:
+            b, x = _c(b, np.float64), _c(x, np.float64)
+        out = np.zeros(self.batch_n.size)
+        _check(self._lib.swc_batch_berr(self._h, _p(b), _p(x), 1 if on_dev else 0, _p(out)))
+        return out
 
     def logdet(self) -> float:
         """log det A of the current factor."""

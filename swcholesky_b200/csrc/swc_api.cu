@@ -116,6 +116,8 @@ int swc_analyze(swc_handle_t h, int n, const int *c, const int *r, const size_t 
   std::string err;
   h->analyzed = false;
   h->factored = false;
+  h->batch.reset();
+  h->eng->set_tuning(swc::Tuning());
   if (!h->eng->analyze(n, c, r, lc.data(), Ls, lip.data(), blockSet, supNo, prunePtr, pruneSet, err))
     return fail(err.rfind("device", 0) == 0 ? SWC_CUDA_ERROR : SWC_INVALID_INPUT, err);
   h->analyzed = true;
@@ -230,6 +232,78 @@ int swc_solve_grad(swc_handle_t h, const double *x, const double *lam, double *g
   if (dl) cudaFree(dl);
   if (dg) cudaFree(dg);
   return rc;
+}
+
+int swc_batch_analyze(swc_handle_t h, int nmat, const int *n, const int *c, const int *r) {
+  if (!h) return fail(SWC_INVALID_INPUT, "null handle");
+  std::string err;
+  h->analyzed = false;
+  h->factored = false;
+  std::unique_ptr<swc::BatchState> b(new swc::BatchState);
+  if (!b->set(nmat, n, c, r, err)) return fail(SWC_INVALID_INPUT, err);
+  if (!b->analyze(*h->eng, 0, swc::plan_candidate(0), err))
+    return fail(err.rfind("device", 0) == 0 ? SWC_CUDA_ERROR : SWC_INVALID_INPUT, err);
+  h->batch = std::move(b);
+  h->analyzed = true;
+  return SWC_OK;
+}
+
+int swc_batch_autotune(swc_handle_t h, const double *values, int values_on_device, int mode,
+                       const char *cache_path, int *choice, double *best_ms) {
+  if (!h) return fail(SWC_INVALID_INPUT, "null handle");
+  if (!h->batch || !h->analyzed) return fail(SWC_NOT_READY, "autotune before swc_batch_analyze");
+  if (mode != SWC_MODE_FP64 && mode != SWC_MODE_MIXED_TF32X3)
+    return fail(SWC_INVALID_INPUT, "unknown factorization mode");
+  if (!values) return fail(SWC_INVALID_INPUT, "null values");
+  const size_t bytes = sizeof(double) * h->batch->cp[h->batch->N];
+  const double *dv = values;
+  double *tmp = nullptr;
+  if (!values_on_device) {
+    if (cudaMalloc(&tmp, std::max<size_t>(bytes, 8)) != cudaSuccess ||
+        cudaMemcpy(tmp, values, bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+      if (tmp) cudaFree(tmp);
+      return fail(SWC_CUDA_ERROR, "autotune: values upload failed");
+    }
+    dv = tmp;
+  }
+  std::string err;
+  h->factored = false;
+  const bool ok = h->batch->autotune(*h->eng, dv, mode == SWC_MODE_MIXED_TF32X3, cache_path, 3,
+                                     choice, best_ms, err);
+  if (tmp) cudaFree(tmp);
+  if (!ok) {
+    h->analyzed = false;
+    return fail(err.find("not positive definite") != std::string::npos ? SWC_NOT_SPD : SWC_CUDA_ERROR, err);
+  }
+  h->analyzed = true;
+  return SWC_OK;
+}
+
+int swc_batch_berr(swc_handle_t h, const double *b, const double *x, int on_device, double *berr) {
+  if (!h || !b || !x || !berr) return fail(SWC_INVALID_INPUT, "null argument");
+  if (!h->batch) return fail(SWC_NOT_READY, "swc_batch_berr without swc_batch_analyze");
+  if (!h->factored) return fail(SWC_NOT_READY, "swc_batch_berr before a successful factor");
+  std::string err;
+  const size_t bytes = sizeof(double) * (size_t)h->batch->N;
+  const double *db = b, *dx = x;
+  double *tb = nullptr, *tx = nullptr;
+  if (!on_device) {
+    cudaError_t e = cudaMalloc(&tb, bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&tx, bytes);
+    if (e == cudaSuccess) e = cudaMemcpy(tb, b, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(tx, x, bytes, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      if (tb) cudaFree(tb);
+      if (tx) cudaFree(tx);
+      return fail(SWC_CUDA_ERROR, std::string("batch berr buffers: ") + cudaGetErrorString(e));
+    }
+    db = tb;
+    dx = tx;
+  }
+  const bool ok = h->eng->segment_berr(h->batch->d_seg, h->batch->nmat, db, dx, berr, err);
+  if (tb) cudaFree(tb);
+  if (tx) cudaFree(tx);
+  return ok ? SWC_OK : fail(SWC_CUDA_ERROR, err);
 }
 
 int swc_supernodes(int n, const int *c, const int *r, const int *nrelax, const double *zrelax,

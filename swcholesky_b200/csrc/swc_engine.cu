@@ -26,9 +26,14 @@ bool upload(T *&dst, const T *src, size_t count, cudaStream_t st, std::string &e
   return true;
 }
 
-bool small_class(int w, int64_t m) {
-  return w <= SMALL_MAX_W && m <= SMALL_MAX_M && (int64_t)w * m <= SMALL_MAX_ELEMS;
+bool small_class(int w, int64_t m, const Tuning &T) {
+  return w <= std::min(T.small_max_w, SMALL_MAX_W) && m <= std::min(T.small_max_m, SMALL_MAX_M) &&
+         (int64_t)w * m <= std::min(T.small_max_elems, SMALL_MAX_ELEMS);
 }
+
+// shared memory of the small-class kernel for an m x w panel: panel, rows, relative
+// indices (+ padding to 8 bytes), pivot column
+int64_t small_smem(int w, int64_t m) { return 8 * m * w + 8 * m + 8 + 8 * (int64_t)w; }
 
 // One update tile of the tiled class with the descendants that touch it.
 struct TileWork {
@@ -131,7 +136,7 @@ void Engine::release() {
                   d_syrk_, d_pairs_, d_upd_end_, d_dinv_, d_dinv_off_, d_diag_,
                   d_slist_, d_cptr_, d_cidx_, d_flags_, d_fchain_, d_bchain_, d_scontrib_, d_sgather_, d_csr_rp_, d_csr_ci_,
                   d_csr_map_,
-                  d_csr_val_, d_contrib_, d_work_, d_norms_};
+                  d_csr_val_, d_contrib_, d_work_, d_norms_, d_persist_, d_qctr_};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   release_adjoint();
@@ -151,6 +156,8 @@ void Engine::release() {
   d_scontrib_ = d_sgather_ = nullptr;
   d_csr_rp_ = d_csr_ci_ = d_csr_map_ = nullptr;
   d_csr_val_ = d_contrib_ = d_work_ = d_norms_ = nullptr;
+  d_persist_ = d_qctr_ = nullptr;
+  persist_ctas_ = 0;
   work_nrhs_ = 0;
   if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
   if (graph_) cudaGraphDestroy(graph_);
@@ -164,7 +171,7 @@ void Engine::release() {
 
 bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int *Ls,
                 const int64_t *Li_ptr, const int *blockSet, int supNo, const int *prunePtr,
-                const int *pruneSet, HostSym &H, Plan &P, std::string &err) {
+                const int *pruneSet, HostSym &H, Plan &P, std::string &err, const Tuning &T) {
   // ---- host-side validation of the symbolic arrays (no device work on bad input) ----
   if (n <= 0 || supNo <= 0 || !c || !r || !lC || !Ls || !Li_ptr || !blockSet || !prunePtr ||
       !pruneSet) {
@@ -226,6 +233,7 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
     nlev = std::max(nlev, level[s] + 1);
     if (m > w) {
       int p = col2sup[Ls[rowptr[s] + w]];
+      if (p <= s) { err = "supernodes are not numbered children before parents"; return false; }
       level[p] = std::max(level[p], level[s] + 1);
     }
   }
@@ -233,6 +241,18 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
   for (int s = 0; s < supNo; ++s)
     for (int q = prunePtr[s]; q < prunePtr[s + 1]; ++q)
       if (level[pruneSet[q]] >= level[s]) { err = "prune set is not consistent with the etree"; return false; }
+
+  // ---- persistent bottom set: small supernodes whose whole subtree is small ----
+  std::vector<char> in_persist(supNo, 0);
+  if (T.persist) {
+    std::vector<char> kids_ok(supNo, 1);
+    for (int s = 0; s < supNo; ++s) {
+      const int w = super[s + 1] - super[s];
+      const int64_t m = rowptr[s + 1] - rowptr[s];
+      in_persist[s] = kids_ok[s] && small_class(w, m, T) && small_smem(w, m) <= T.persist_max_smem;
+      if (!in_persist[s] && m > w) kids_ok[col2sup[Ls[rowptr[s] + w]]] = 0;
+    }
+  }
 
   // ---- plan ----
   P = Plan();
@@ -250,10 +270,12 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
     for (int s : by_level[lv]) {
       int w = super[s + 1] - super[s];
       int64_t m = rowptr[s + 1] - rowptr[s];
-      if (small_class(w, m)) {
+      if (in_persist[s]) {
+        P.persist_list.push_back(s);
+        P.persist_smem = std::max<int>(P.persist_smem, (int)small_smem(w, m));
+      } else if (small_class(w, m, T)) {
         P.small_list.push_back(s);
-        // panel + rows + relative indices (+ padding to 8 bytes) + pivot column
-        W.small_smem = std::max<int>(W.small_smem, (int)(8 * m * w + 8 * m + 8 + 8 * w));
+        W.small_smem = std::max<int>(W.small_smem, (int)small_smem(w, m));
       } else {
         big.push_back(s);
       }
@@ -312,12 +334,15 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
     for (int j = 0; j < maxnb; ++j)
       launches += (W.panel_cnt[j] > 0) + (W.syrk_cnt[j] > 0) + (W.diag_cnt[j] > 0);
   }
+  if (!P.persist_list.empty()) launches += 1;
   P.launches = launches;
 
   // ---- algorithmic work per kernel class (one factorization) ----
   {
     KernelStats &K = P.work;
-    for (int s : P.small_list) {
+    std::vector<int> all_small(P.small_list);
+    all_small.insert(all_small.end(), P.persist_list.begin(), P.persist_list.end());
+    for (int s : all_small) {
       int f = super[s], w = super[s + 1] - f;
       int64_t m = rowptr[s + 1] - rowptr[s];
       double fl = 0, by = 0;
@@ -347,7 +372,7 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
       for (int s : by_level[lv]) {
         int w = super[s + 1] - super[s];
         int64_t m = rowptr[s + 1] - rowptr[s];
-        if (small_class(w, m)) continue;
+        if (small_class(w, m, T)) continue;
         for (int c0 = 0; c0 < w; c0 += TB) {
           int bw = std::min(TB, w - c0);
           K.flops[K_PANEL] += (double)bw * bw * bw / 3.0 + (double)(m - c0 - bw) * bw * bw;
@@ -379,7 +404,8 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
   if (!kernels_configure(err) || !mixed_configure(err)) return false;
   HostSym H;
   Plan P;
-  if (!build_plan(n, c, r, lC, Ls, Li_ptr, blockSet, supNo, prunePtr, pruneSet, H, P, err))
+  if (!build_plan(n, c, r, lC, Ls, Li_ptr, blockSet, supNo, prunePtr, pruneSet, H, P, err,
+                  tuning_))
     return false;
   const std::vector<int> &super = H.super;
   const std::vector<int64_t> &rowptr = H.rowptr, &xptr = H.xptr;
@@ -485,6 +511,7 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
             upload(d_upd_ptr_, prunePtr, (size_t)supNo + 1, st, err) &&
             upload(d_upd_, pruneSet, (size_t)nprune, st, err) &&
             upload(d_small_, P.small_list.data(), P.small_list.size(), st, err) &&
+            upload(d_persist_, P.persist_list.data(), P.persist_list.size(), st, err) &&
             upload(d_big_, P.big_list.data(), P.big_list.size(), st, err) &&
             upload(d_diag_, P.diag_list.data(), P.diag_list.size(), st, err) &&
             upload(d_asm_, P.asm_tasks.data(), P.asm_tasks.size(), st, err) &&
@@ -514,6 +541,9 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
     e = cudaMalloc(&d_dinv_, sizeof(double) * TB * TB * std::max<int64_t>(H.ndinv, 1));
   if (e == cudaSuccess)
     e = cudaMalloc(&d_csr_val_, sizeof(double) * std::max<size_t>(csr_ci.size(), 1));
+  if (e == cudaSuccess) e = cudaMalloc(&d_qctr_, sizeof(int) * ((size_t)supNo + 1));
+  if (e == cudaSuccess && !P.persist_list.empty())
+    persist_ctas_ = persist_ctas(P.persist_smem, (int)P.persist_list.size());
 
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
@@ -565,6 +595,13 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, bool mix
   cudaMemsetAsync(dL_, 0, sizeof(double) * xsize_, st);
   launch_init_status(d_status_, st);
   mark(-1, 1);
+  if (!plan_.persist_list.empty()) {
+    mark(K_SMALL, 1);
+    cudaMemsetAsync(d_qctr_, 0, sizeof(int) * (nsuper_ + 1), st);
+    launch_factor_small_persist(sym_, d_persist_, (int)plan_.persist_list.size(),
+                                plan_.persist_smem, persist_ctas_, d_qctr_, st);
+    mark(-1, 1);
+  }
   for (const Wave &W : plan_.waves) {
     mark(K_SMALL, W.small_cnt);
     launch_factor_small(sym_, d_small_ + W.small_off, W.small_cnt, W.small_smem, st);
@@ -690,11 +727,12 @@ int Engine::finish(int *info, std::string &err) {
   cudaStream_t st = stream_;
   // full-CSR values of this matrix for residuals, and ||A||_inf
   launch_gather_vals((int)csr_nnz_, d_csr_map_, d_Ax_, d_csr_val_, st);
-  cudaError_t e = cudaMemcpyAsync(h_status_, d_status_, 2 * sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaError_t e = cudaMemcpyAsync(h_status_, d_status_, 4 * sizeof(int), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) { err = std::string("factor: ") + cudaGetErrorString(e); return -1; }
   if (h_status_[1]) { err = "symbolic structure inconsistent with the matrix pattern"; return -2; }
+  if (h_status_[3]) { err = "factorization: a supernode waited too long for its descendants"; return -1; }
   if (h_status_[0] != INT_MAX) {
     if (info) *info = h_status_[0];
     err = "matrix is not positive definite";

@@ -26,7 +26,8 @@ struct DevSym {
   const int *upd;
   double *L;              // supernodal values (the reference's lValues)
   int *status;            // [0] = smallest failing column + 1 (INT_MAX if none),
-                          // [1] = structure error flag
+                          // [1] = structure error flag, [2] = solve wait timeout,
+                          // [3] = factorization wait timeout (persistent walk)
   float2 *Lf;             // split-TF32 mirror {hi, lo} of L (mixed-precision only, else null)
   double *dinv;           // scratch: inverses of the 64x64 diagonal blocks of the tiled class
   const int *dinv_off;    // per supernode: first block of its inverses in dinv (-1: none)
@@ -65,6 +66,8 @@ struct Plan {
   std::vector<int2> panel_tasks;
   std::vector<int4> syrk_tasks;
   std::vector<int> diag_list;
+  std::vector<int> persist_list;   // small supernodes of the persistent walk, in level order
+  int persist_smem = 0;
   int launches = 0;  // kernel launches per factorization
   KernelStats work;  // algorithmic flops/bytes per kernel class
 };
@@ -130,7 +133,8 @@ struct HostSym {
 // Validates the symbolic arrays and derives the execution plan (no device work).
 bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int *Ls,
                 const int64_t *Li_ptr, const int *blockSet, int supNo, const int *prunePtr,
-                const int *pruneSet, HostSym &H, Plan &P, std::string &err);
+                const int *pruneSet, HostSym &H, Plan &P, std::string &err,
+                const Tuning &T = Tuning());
 
 struct AdjointPlan;   // reverse-sweep schedule of the adjoint (swc_adjoint.cu)
 
@@ -165,6 +169,9 @@ class Engine {
   bool download(double *lValues, bool to_device, std::string &err);
   cudaStream_t stream() const { return stream_; }
   void set_stream(cudaStream_t s) { stream_ = s ? s : own_stream_; }
+  // Plan parameters used by the next analyze.
+  void set_tuning(const Tuning &t) { tuning_ = t; }
+  const Tuning &tuning() const { return tuning_; }
   int64_t xsize() const { return xsize_; }
   int n() const { return n_; }
   int64_t nnz() const { return nnz_; }
@@ -180,6 +187,11 @@ class Engine {
   const double *selected_inverse_ptr() const { return d_adj_Z_; }
   bool logdet_grad(double *grad, std::string &err);
   bool solve_grad(const double *x, const double *lam, double *grad, std::string &err);
+
+  // Backward error ||b - A x||_inf / (||A||_inf ||x||_inf) of every diagonal block of A
+  // (rows d_seg[k] .. d_seg[k+1]; a batch's matrices); device b, x; berr on the host.
+  bool segment_berr(const int64_t *d_seg, int nseg, const double *b, const double *x,
+                    double *berr, std::string &err);
 
  private:
   bool prepare_adjoint(std::string &err);
@@ -223,6 +235,9 @@ class Engine {
   cudaGraphExec_t graph_exec_ = nullptr, graph_exec_mx_ = nullptr;
   float2 *d_Lf_ = nullptr;
   bool use_graph_ = true;
+  Tuning tuning_;
+  int *d_persist_ = nullptr, *d_qctr_ = nullptr;
+  int persist_ctas_ = 0;
   // Trailing SYRK of the dense steps in split-TF32 too (mixed mode).  Off: on B200 the
   // FP64 DMMA kernel is the faster one for these 64x64x64 tiles (measured 6.9 ms vs 13.4 ms
   // per factorization of the 60^3 Laplacian).
@@ -250,6 +265,10 @@ class Engine {
 
 // kernel launch wrappers (swc_kernels.cu)
 void launch_factor_small(const DevSym &S, const int *list, int count, int smem, cudaStream_t st);
+// persistent small-class walk: CTAs to launch (occupancy x SMs, at most count) and the launch
+int persist_ctas(int smem, int count);
+void launch_factor_small_persist(const DevSym &S, const int *order, int count, int smem,
+                                 int ctas, int *qctr, cudaStream_t st);
 void launch_assemble(const DevSym &S, const int2 *tasks, int count, cudaStream_t st);
 void launch_update_tiles(const DevSym &S, const int4 *tasks, const int *task_end,
                          const int4 *pairs, int count, cudaStream_t st);

@@ -3,6 +3,7 @@
 #include <memory>
 #include <string>
 
+#include "swc_batch.h"
 #include "swc_engine.h"
 
 namespace swc {
@@ -15,4 +16,5 @@ struct swc_handle {
   int device = 0;
   bool analyzed = false;
   bool factored = false;
+  std::unique_ptr<swc::BatchState> batch;   // set by swc_batch_analyze
 };

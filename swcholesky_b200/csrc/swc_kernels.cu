@@ -23,6 +23,7 @@
 // register micro-tile.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <climits>
 #include <cstdint>
 
@@ -58,10 +59,8 @@ __device__ __forceinline__ void flag_structure_error(const DevSym &S) {
 }
 
 // ---------------------------------------------------------------------------------------
-// One CTA per small supernode.
-__global__ void __launch_bounds__(NT) k_factor_small(DevSym S, const int *list, int count) {
-  extern __shared__ double smem[];
-  const int s = list[blockIdx.x];
+// Whole factorization of one small supernode s by the calling CTA (all NT threads).
+__device__ __noinline__ void factor_small_body(const DevSym &S, int s, double *smem) {
   const int tid = threadIdx.x;
   const int f = S.super[s];
   const int w = S.super[s + 1] - f;
@@ -150,6 +149,68 @@ __global__ void __launch_bounds__(NT) k_factor_small(DevSym S, const int *list, 
   if (S.Lf) {   // mixed-precision factorization: split mirror for the Schur updates
     float2 *dstf = S.Lf + S.xptr[s];
     for (int i = tid; i < m * w; i += NT) dstf[i] = split_tf32(P[i]);
+  }
+}
+
+// One CTA per small supernode of a level.
+__global__ void __launch_bounds__(NT) k_factor_small(DevSym S, const int *list, int count) {
+  extern __shared__ double smem[];
+  factor_small_body(S, list[blockIdx.x], smem);
+}
+
+// The small supernodes of the bottom of the tree (a set closed under descendants) in ONE
+// persistent launch: CTAs take supernodes from a device work queue in level order
+// (order[0 .. count)), wait until every descendant in the supernode's update list is
+// finished (acquire on its done flag), factor it and publish its own flag (release).  A
+// CTA only waits for supernodes taken from the queue before its own, which were taken by
+// CTAs already running and waiting on even earlier ones, so the walk always progresses,
+// whatever the number of resident CTAs.  qctr[0] is the queue head, qctr[1 + s] the done
+// flag of supernode s; both are zeroed before every launch.  A wait gives up after
+// PERSIST_SPIN polls and records the timeout in status[3].
+constexpr long long PERSIST_SPIN = 1LL << 24;
+
+__device__ __forceinline__ int ld_acquire_k(const int *p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ void st_release_k(int *p, int v) {
+  asm volatile("st.release.gpu.global.s32 [%0], %1;\n" ::"l"(p), "r"(v));
+}
+
+__global__ void __launch_bounds__(NT) k_factor_small_persist(DevSym S, const int *order, int count,
+                                                              int *qctr) {
+  extern __shared__ double smem[];
+  __shared__ int item;
+  int *done = qctr + 1;
+  for (;;) {
+    if (threadIdx.x == 0) item = atomicAdd(qctr, 1);
+    __syncthreads();
+    const int idx = item;
+    if (idx >= count) break;
+    const int s = order[idx];
+    if (threadIdx.x < 32) {   // warp 0 waits for the update sources, one lane per source
+      bool timed_out = false;
+      for (int q = S.upd_ptr[s] + threadIdx.x; q < S.upd_ptr[s + 1] && !timed_out; q += 32) {
+        const int *flag = done + S.upd[q];
+        long long it = 0;
+        while (ld_acquire_k(flag) == 0) {
+          if (++it > PERSIST_SPIN) {
+            atomicExch(&S.status[3], 1);
+            timed_out = true;
+            break;
+          }
+          __nanosleep(64);
+        }
+      }
+    }
+    __syncthreads();
+    factor_small_body(S, s, smem);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      st_release_k(done + s, 1);
+    }
   }
 }
 
@@ -725,6 +786,7 @@ __global__ void __launch_bounds__(MT) k_syrk_step(DevSym S, const int4 *tasks, i
 __global__ void k_init_status(int *status) {
   status[0] = INT_MAX;
   status[1] = 0;
+  status[3] = 0;
 }
 
 }  // namespace
@@ -732,6 +794,9 @@ __global__ void k_init_status(int *status) {
 bool kernels_configure(std::string &err) {
   cudaError_t e = cudaFuncSetAttribute(k_factor_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        200 * 1024);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_factor_small_persist, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             200 * 1024);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_update_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, UPD_SMEM);
   if (e == cudaSuccess)
@@ -749,6 +814,19 @@ bool kernels_configure(std::string &err) {
 
 void launch_factor_small(const DevSym &S, const int *list, int count, int smem, cudaStream_t st) {
   if (count > 0) k_factor_small<<<count, NT, smem, st>>>(S, list, count);
+}
+int persist_ctas(int smem, int count) {
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_factor_small_persist, NT, smem) !=
+          cudaSuccess || per < 1)
+    per = 1;
+  return std::max(1, std::min(count, sms * per));
+}
+void launch_factor_small_persist(const DevSym &S, const int *order, int count, int smem,
+                                 int ctas, int *qctr, cudaStream_t st) {
+  if (count > 0) k_factor_small_persist<<<ctas, NT, smem, st>>>(S, order, count, qctr);
 }
 void launch_assemble(const DevSym &S, const int2 *tasks, int count, cudaStream_t st) {
   if (count > 0) k_assemble<<<(count * 32 + NT - 1) / NT, NT, 0, st>>>(S, tasks, count);

@@ -60,3 +60,22 @@ def test_bad_input_rejected():
     S = lib_or_skip()
     with pytest.raises(S.SWCError):
         S.supernodes(3, np.array([0, 1, 2, 3]), np.array([0, 7, 2]))
+
+
+def test_forest_partition_is_per_matrix_partition():
+    """The batched path analyses a block-diagonal matrix: its partition is the matrices'
+    own partitions side by side (no supernode crosses a matrix)."""
+    S = lib_or_skip()
+    from swcholesky_b200 import workloads as W
+    mats, _ = W.batch_matrices(count=6, seed=2, lo=5, hi=25)
+    parts, off, nzo = [], 0, 0
+    cs, rs = [], []
+    for m in mats:
+        parts.append(S.supernodes(m.n, m.indptr, m.indices)[:-1] + off)
+        cs.append(np.asarray(m.indptr[:-1]) + nzo)
+        rs.append(np.asarray(m.indices) + off)
+        off += m.n
+        nzo += int(m.indptr[-1])
+    cs.append([nzo])
+    forest = S.supernodes(off, np.concatenate(cs), np.concatenate(rs))
+    np.testing.assert_array_equal(forest, np.concatenate(parts + [[off]]))
