@@ -1,0 +1,79 @@
+"""Runs the numeric factorization of a named workload a given number of times.
+
+    python -m swcholesky_b200.run --workload grid3d_60 --mode fp64 --reps 1 [--solve]
+    python -m swcholesky_b200.run --workload batch256 --mode mixed --reps 1
+
+The single-matrix workloads use the supernode partition stored in tests/golden (the
+reference's symbolic phase) when present, else the library's own partition; ``batch256``
+is the batched workload.  Prints one line with the sizes and the device milliseconds of
+the last factorization.  Meant as the command under a profiler: no warm-up, no extra
+kernels besides the factorization (and the solve with ``--solve``).
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import time
+
+import numpy as np
+
+from . import SWC_MODE_FP64, SWC_MODE_MIXED_TF32X3, Handle
+from . import matrices as M
+from . import workloads as W
+
+GOLDEN = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tests",
+                      "golden")
+
+
+def load(name: str):
+    """(problem or list of matrices, values)."""
+    if name == "batch256":
+        src, _ = W.batch_sources()
+        mats = [M.permute_lower(A, p) for A, p in src]
+        return mats, np.concatenate([m.data for m in mats])
+    A, perm, _ = W.build(name)
+    fx = os.path.join(GOLDEN, f"sym_{name}.npz")
+    if os.path.exists(fx):
+        g = dict(np.load(fx))
+        P = W.assemble(A, g["perm"], g["super"])
+    else:
+        P = W.assemble_own(A, perm)
+    return P, P.A2x
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="grid3d_60")
+    ap.add_argument("--mode", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--reps", type=int, default=1)
+    ap.add_argument("--solve", action="store_true")
+    args = ap.parse_args()
+    mode = SWC_MODE_MIXED_TF32X3 if args.mode == "mixed" else SWC_MODE_FP64
+    prob, vals = load(args.workload)
+    h = Handle(0)
+    if isinstance(prob, list):
+        h.batch_analyze(prob)
+    else:
+        P = prob
+        h.analyze(P.n, P.A2p, P.A2i, P.lC, P.Ls, P.Li_ptr, P.super, P.prunePtr, P.pruneSet)
+    import torch
+    v = torch.from_numpy(vals).cuda()
+    b = torch.from_numpy(np.random.default_rng(0).standard_normal(h.n)).cuda()
+    ms = 0.0
+    for _ in range(args.reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        info = h.factor(v, mode)
+        torch.cuda.synchronize()
+        ms = (time.perf_counter() - t0) * 1e3
+        if info:
+            raise SystemExit(f"not positive definite at column {info - 1}")
+        if args.solve:
+            h.refine(b, tol=1e-12)
+    print(f"workload {args.workload} n {h.n} nsuper {h.nsuper} xsize {h.xsize} "
+          f"launches {h.launches} last factor {ms:.3f} ms (host clock)")
+    h.close()
+
+
+if __name__ == "__main__":
+    main()
