@@ -539,46 +539,50 @@ __device__ __forceinline__ void store8(const double (&c)[2], double *X, int r0, 
 }
 
 // Warp-level Cholesky of the 8x8 diagonal block kb of D and its inverse into E (same
-// position).  Lane r < 8 holds row r; each column is broadcast through `bc` (8 doubles of
-// shared scratch).  Pivot: the column is scaled by 1/sqrt(pivot), which is also kept for
-// the inverse's diagonal, so the inverse needs no division.
-__device__ void potrf8_inv8(double *D, double *E, double *bc, int kb, const DevSym &S,
-                            int gcol0, int bw, bool report) {
-  const int lane = threadIdx.x & 31, r = lane & 7, k0 = 8 * kb;
-  double x[8], rd[8];
-#pragma unroll
-  for (int c = 0; c < 8; ++c) x[c] = (c <= r) ? D[(k0 + c) * DLD + k0 + r] : 0.0;
+// position).  Lane 4r + q holds row r, columns 2q and 2q+1; the scaled pivot column reaches
+// the other lanes by shuffles (no shared-memory round trip).
+__device__ void potrf8_inv8(double *D, double *E, int kb, const DevSym &S, int gcol0, int bw,
+                            bool report) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31, r = lane >> 2, q = lane & 3, k0 = 8 * kb;
+  double x0 = (2 * q <= r) ? D[(k0 + 2 * q) * DLD + k0 + r] : 0.0;
+  double x1 = (2 * q + 1 <= r) ? D[(k0 + 2 * q + 1) * DLD + k0 + r] : 0.0;
+  double rd_row = 0.0;   // 1 / L(r, r)
 #pragma unroll
   for (int c = 0; c < 8; ++c) {
-    const double piv = __shfl_sync(0xffffffffu, x[c], c);
+    const int qc = c >> 1;
+    const bool odd = c & 1;
+    const double piv = __shfl_sync(FULL, odd ? x1 : x0, 4 * c + qc);
     const double dsq = sqrt(piv), inv = 1.0 / dsq;
-    rd[c] = inv;
     if (report && lane == 0 && k0 + c < bw && !(piv > 0.0))
       atomicMin(&S.status[0], gcol0 + k0 + c + 1);
-    x[c] = (r == c) ? dsq : ((r > c) ? x[c] * inv : x[c]);
-    if (lane < 8) bc[r] = x[c];
-    __syncwarp();
-#pragma unroll
-    for (int c2 = c + 1; c2 < 8; ++c2)
-      if (r >= c2) x[c2] = fma(-x[c], bc[c2], x[c2]);
-    __syncwarp();
+    if (q == qc && r >= c) {
+      const double v = (r == c) ? dsq : (odd ? x1 : x0) * inv;
+      if (odd) x1 = v; else x0 = v;
+    }
+    if (r == c) rd_row = inv;
+    const double lrc = __shfl_sync(FULL, odd ? x1 : x0, 4 * r + qc);
+    const double l0 = __shfl_sync(FULL, odd ? x1 : x0, 8 * q + qc);
+    const double l1 = __shfl_sync(FULL, odd ? x1 : x0, 8 * q + 4 + qc);
+    if (2 * q > c && 2 * q <= r) x0 = fma(-lrc, l0, x0);
+    if (2 * q + 1 > c && 2 * q + 1 <= r) x1 = fma(-lrc, l1, x1);
   }
-  if (lane < 8) {
+  if (2 * q <= r) D[(k0 + 2 * q) * DLD + k0 + r] = x0;
+  if (2 * q + 1 <= r) D[(k0 + 2 * q + 1) * DLD + k0 + r] = x1;
+  double rd[8];
 #pragma unroll
-    for (int c = 0; c < 8; ++c)
-      if (c <= r) D[(k0 + c) * DLD + k0 + r] = x[c];
-  }
+  for (int i = 0; i < 8; ++i) rd[i] = __shfl_sync(FULL, rd_row, 4 * i);
   __syncwarp();
   // lane j < 8: column j of the inverse by forward substitution, 1/L(i,i) = rd[i]
-  const int j = r;
+  const int j = lane & 7;
   double t[8];
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
-    double s = 0.0;
+    double sacc = 0.0;
 #pragma unroll
     for (int k = 0; k < i; ++k)
-      if (k >= j) s = fma(D[(k0 + k) * DLD + k0 + i], t[k], s);
-    t[i] = (i < j) ? 0.0 : ((i == j) ? rd[i] : -s * rd[i]);
+      if (k >= j) sacc = fma(D[(k0 + k) * DLD + k0 + i], t[k], sacc);
+    t[i] = (i < j) ? 0.0 : ((i == j) ? rd[i] : -sacc * rd[i]);
   }
   if (lane < 8) {
 #pragma unroll
@@ -589,15 +593,16 @@ __device__ void potrf8_inv8(double *D, double *E, double *bc, int kb, const DevS
 
 // D: bw x bw lower block padded to a multiple of 8 with identity.  Factors it in place
 // (right-looking over 8-column blocks) and leaves the inverses of its 8x8 diagonal blocks
-// in E.
-__device__ void potrf64_blocked(double *D, double *E, double *bc, int bw, const DevSym &S,
-                                int gcol0) {
+// in E.  Look-ahead: in the trailing update of step kb, warp 0 updates diagonal block kb+1
+// first and factors it while warps 1-3 update the other blocks, so each step costs one
+// panel phase and one trailing phase (two barriers).
+__device__ void potrf64_blocked(double *D, double *E, int bw, const DevSym &S, int gcol0) {
   const int warp = threadIdx.x >> 5;
   const int nbk = (bw + 7) >> 3;
+  if (warp == 0) potrf8_inv8(D, E, 0, S, gcol0, bw, true);
+  __syncthreads();
   for (int kb = 0; kb < nbk; ++kb) {
-    if (warp == 0) potrf8_inv8(D, E, bc, kb, S, gcol0, bw, true);
-    __syncthreads();
-    // panel below: X_ib = B_ib * T_kk^T
+    // panel below: X_ib = B_ib * T_kk^T (warp 0 gets ib = kb + 1)
     for (int ib = kb + 1 + warp; ib < nbk; ib += 4) {
       double c[2] = {0.0, 0.0};
       mma8_abt(c, D, 8 * ib, 8 * kb, E, 8 * kb, 8 * kb, false);
@@ -605,16 +610,28 @@ __device__ void potrf64_blocked(double *D, double *E, double *bc, int bw, const 
       store8(c, D, 8 * ib, 8 * kb, false);
     }
     __syncthreads();
-    // trailing update: D_ib,jb -= X_ib X_jb^T for kb < jb <= ib
-    int q = 0;
-    for (int jb = kb + 1; jb < nbk; ++jb)
-      for (int ib = jb; ib < nbk; ++ib, ++q) {
-        if ((q & 3) != warp) continue;
-        double c[2];
-        load8(c, D, 8 * ib, 8 * jb);
-        mma8_abt(c, D, 8 * ib, 8 * kb, D, 8 * jb, 8 * kb, true);
-        store8(c, D, 8 * ib, 8 * jb, ib == jb);
-      }
+    if (kb + 1 >= nbk) break;
+    // trailing update D_ib,jb -= X_ib X_jb^T for kb < jb <= ib
+    if (warp == 0) {
+      const int nb = kb + 1;
+      double c[2];
+      load8(c, D, 8 * nb, 8 * nb);
+      mma8_abt(c, D, 8 * nb, 8 * kb, D, 8 * nb, 8 * kb, true);
+      store8(c, D, 8 * nb, 8 * nb, true);
+      __syncwarp();
+      potrf8_inv8(D, E, nb, S, gcol0, bw, true);
+    } else {
+      int q = 0;
+      for (int jb = kb + 1; jb < nbk; ++jb)
+        for (int ib = jb; ib < nbk; ++ib) {
+          if (ib == kb + 1) continue;   // (kb+1, kb+1) belongs to warp 0
+          if ((q++ % 3) != warp - 1) continue;
+          double c[2];
+          load8(c, D, 8 * ib, 8 * jb);
+          mma8_abt(c, D, 8 * ib, 8 * kb, D, 8 * jb, 8 * kb, true);
+          store8(c, D, 8 * ib, 8 * jb, ib == jb);
+        }
+    }
     __syncthreads();
   }
 }
@@ -649,11 +666,15 @@ __device__ void trtri64_blocked(const double *D, double *E, double *W, int bw) {
 
 // Factor diagonal block c0/64 of supernode s in place (lower triangle only) and store its
 // inverse (T(r, c) at dinv[c * 64 + r]) for the TRSM of the rows below it and for the
-// chained triangular solves.
+// chained triangular solves.  upd (optional): the diagonal tile's value, negated, as left in
+// a tile accumulator by syrk_tile_acc (its update by the previous column block), so the
+// updated block never leaves the chip before its factorization; when the block is narrower
+// than 64 the tile's remaining rows are panel rows below it and go to L.
 // 128 threads, DIAG_SMEM bytes of dynamic shared memory.
 constexpr int DIAG_SMEM = (2 * TB * DLD + 4 * 64) * 8;
 
-__device__ void factor_diag_block(const DevSym &S, int s, int c0, double *smem) {
+__device__ void factor_diag_block(const DevSym &S, int s, int c0, double *smem,
+                                  const TileAcc *upd) {
   double *D = smem, *E = smem + TB * DLD, *W = E + TB * DLD;
   const int tid = threadIdx.x;
   const int f = S.super[s];
@@ -665,13 +686,29 @@ __device__ void factor_diag_block(const DevSym &S, int s, int c0, double *smem) 
   for (int e = tid; e < TB * TB; e += blockDim.x) {
     const int c = e >> 6, r = e & (TB - 1);
     double v;
-    if (c < bw && r < bw) v = (r >= c) ? P[(size_t)(c0 + c) * m + c0 + r] : 0.0;
+    if (c < bw && r < bw) v = (!upd && r >= c) ? P[(size_t)(c0 + c) * m + c0 + r] : 0.0;
     else v = (r == c) ? 1.0 : 0.0;
     D[c * DLD + r] = v;
     E[c * DLD + r] = 0.0;
   }
+  if (upd) {
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int r = acc_row(i);
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int c = acc_col(j, e);
+          if (r < bw && c < bw && r >= c) D[c * DLD + r] = neg(upd->v[i][j][e]);
+          // a partial last block: the tile's rows below the block are panel rows
+          else if (r >= bw && c < bw && c0 + r < m) P[(size_t)(c0 + c) * m + c0 + r] = neg(upd->v[i][j][e]);
+        }
+    }
+  }
   __syncthreads();
-  potrf64_blocked(D, E, W, bw, S, f + c0);
+  potrf64_blocked(D, E, bw, S, f + c0);
   for (int e = tid; e < TB * TB; e += blockDim.x) {
     const int c = e >> 6, r = e & (TB - 1);
     if (c < bw && r < bw && r >= c) P[(size_t)(c0 + c) * m + c0 + r] = D[c * DLD + r];
@@ -688,16 +725,16 @@ __device__ void factor_diag_block(const DevSym &S, int s, int c0, double *smem) 
 
 // Trailing SYRK/GEMM update of one 64x64 tile of a tiled-class panel by column block
 // `kblk`: tile(r0, c0) -= L[r0:, kblk] L[c0:, kblk]^T.  The accumulator is seeded with
-// minus the tile, so the tensor cores produce -(C - A B^T); stored back negated.
-__device__ void syrk_tile(const DevSym &S, int s, int r0, int c0, int kblk, double *stages) {
+// minus the tile, so the tensor cores produce -(C - A B^T).
+__device__ void syrk_tile_acc(const DevSym &S, int s, int r0, int c0, int kblk, double *stages,
+                              TileAcc &acc) {
   const int f = S.super[s];
   const int w = S.super[s + 1] - f;
   const int m = (int)(S.rowptr[s + 1] - S.rowptr[s]);
-  double *P = S.L + S.xptr[s];
+  const double *P = S.L + S.xptr[s];
   const int k0 = kblk * TB;
   const int bk = min(TB, w - k0);
   const int nrow = min(TB, m - r0), ncol = min(TB, w - c0);
-  TileAcc acc;
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const int r = acc_row(i);
@@ -712,6 +749,17 @@ __device__ void syrk_tile(const DevSym &S, int s, int r0, int c0, int kblk, doub
   }
   dmma_tile_product(P + (size_t)k0 * m + r0, m, nrow, P + (size_t)k0 * m + c0, m, ncol, bk,
                     stages, acc);
+}
+
+// ... stored back negated.
+__device__ void syrk_tile(const DevSym &S, int s, int r0, int c0, int kblk, double *stages) {
+  const int f = S.super[s];
+  const int w = S.super[s + 1] - f;
+  const int m = (int)(S.rowptr[s + 1] - S.rowptr[s]);
+  double *P = S.L + S.xptr[s];
+  const int nrow = min(TB, m - r0), ncol = min(TB, w - c0);
+  TileAcc acc;
+  syrk_tile_acc(S, s, r0, c0, kblk, stages, acc);
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const int r = acc_row(i);
@@ -732,8 +780,13 @@ __global__ void __launch_bounds__(MT) k_diag_step(DevSym S, const int *list, int
   extern __shared__ double dyn[];
   const int s = list[blockIdx.x];
   const int c0 = step * TB;
-  if (step > 0) syrk_tile(S, s, c0, c0, step - 1, dyn);
-  factor_diag_block(S, s, c0, dyn);
+  if (step > 0) {
+    TileAcc acc;
+    syrk_tile_acc(S, s, c0, c0, step - 1, dyn, acc);
+    factor_diag_block(S, s, c0, dyn, &acc);
+  } else {
+    factor_diag_block(S, s, c0, dyn, nullptr);
+  }
 }
 
 // task = (s, r0): B = L[r0:r0+64, blk] := B * L_blk^{-T} = B * T^T with T = L_blk^{-1},
