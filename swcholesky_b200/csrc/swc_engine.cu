@@ -136,7 +136,7 @@ void Engine::release() {
                   d_syrk_, d_pairs_, d_upd_end_, d_dinv_, d_dinv_off_, d_diag_,
                   d_slist_, d_cptr_, d_cidx_, d_flags_, d_fchain_, d_bchain_, d_scontrib_, d_sgather_, d_csr_rp_, d_csr_ci_,
                   d_csr_map_,
-                  d_csr_val_, d_contrib_, d_work_, d_norms_, d_persist_, d_qctr_};
+                  d_csr_val_, d_contrib_, d_work_, d_norms_, d_persist_, d_qctr_, d_npart_};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   release_adjoint();
@@ -157,6 +157,7 @@ void Engine::release() {
   d_csr_rp_ = d_csr_ci_ = d_csr_map_ = nullptr;
   d_csr_val_ = d_contrib_ = d_work_ = d_norms_ = nullptr;
   d_persist_ = d_qctr_ = nullptr;
+  d_npart_ = nullptr;
   persist_ctas_ = 0;
   work_nrhs_ = 0;
   if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
@@ -447,7 +448,7 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
         } else {
           SP.list.push_back(s);
         }
-        for (int r0 = w; r0 < m; r0 += 256) SP.contrib_tasks.push_back(make_int2(s, r0));
+        for (int r0 = w; r0 < m; r0 += TB) SP.contrib_tasks.push_back(make_int2(s, r0));
         if (m > w)
           for (int j0 = 0; j0 < w; j0 += 32) SP.gather_tasks.push_back(make_int2(s, j0));
       }
@@ -760,12 +761,14 @@ bool Engine::ensure_work(int nrhs, std::string &err) {
   if (d_work_) cudaFree(d_work_);
   if (d_norms_) cudaFree(d_norms_);
   if (h_norms_) cudaFreeHost(h_norms_);
-  d_contrib_ = d_work_ = d_norms_ = h_norms_ = nullptr;
+  if (d_npart_) cudaFree(d_npart_);
+  d_contrib_ = d_work_ = d_norms_ = h_norms_ = d_npart_ = nullptr;
   cudaError_t e = cudaMalloc(&d_contrib_, sizeof(double) * std::max<int64_t>(splan_.contrib_len, 1) * nrhs);
   // work: r, d, p, q vectors (4 * n * nrhs) + row sums
   if (e == cudaSuccess) e = cudaMalloc(&d_work_, sizeof(double) * ((size_t)4 * n_ * nrhs + n_));
   if (e == cudaSuccess) e = cudaMalloc(&d_norms_, sizeof(double) * 8 * (nrhs + 1));
   if (e == cudaSuccess) e = cudaMallocHost(&h_norms_, sizeof(double) * 8 * (nrhs + 1));
+  if (e == cudaSuccess) e = cudaMalloc(&d_npart_, sizeof(double) * norm_scratch_doubles(nrhs));
   if (e != cudaSuccess) {
     err = std::string("solve workspace: ") + cudaGetErrorString(e);
     work_nrhs_ = 0;
@@ -848,7 +851,7 @@ bool Engine::refine(const double *b, double *x, int nrhs, double tol, int maxit,
   };
   // ||A||_inf
   launch_rowabs(n_, d_csr_rp_, d_csr_val_, rows, st);
-  launch_norms(n_, 1, rows, nullptr, d_norms_, st);
+  launch_norms(n_, 1, rows, nullptr, d_norms_, d_npart_, st);
   if (!sync_norms(1)) return false;
   anorm_ = h_norms_[0];
   // residual r = b - A x and backward errors; returns the max over right-hand sides
@@ -856,8 +859,8 @@ bool Engine::refine(const double *b, double *x, int nrhs, double tol, int maxit,
   auto residual = [&](const double *xx) -> bool {
     launch_spmv(n_, d_csr_rp_, d_csr_ci_, d_csr_val_, xx, r, nrhs, st);
     launch_residual(len, b, r, st);
-    launch_norms(n_, nrhs, r, nullptr, d_norms_, st);
-    launch_norms(n_, nrhs, xx, nullptr, d_norms_ + 2 * nrhs, st);
+    launch_norms(n_, nrhs, r, nullptr, d_norms_, d_npart_, st);
+    launch_norms(n_, nrhs, xx, nullptr, d_norms_ + 2 * nrhs, d_npart_, st);
     if (!sync_norms(2 * nrhs)) return false;
     for (int k = 0; k < nrhs; ++k) {
       const double rn = h_norms_[2 * k], xn = h_norms_[2 * (nrhs + k)];
@@ -894,7 +897,7 @@ bool Engine::refine(const double *b, double *x, int nrhs, double tol, int maxit,
       double *zk = dv + (size_t)k * n_, *pk = pv + (size_t)k * n_, *qk = qv + (size_t)k * n_;
       const double *bk = b + (size_t)k * n_;
       auto norms1 = [&](const double *a, const double *bb) -> bool {
-        launch_norms(n_, 1, a, bb, d_norms_, st);
+        launch_norms(n_, 1, a, bb, d_norms_, d_npart_, st);
         return sync_norms(1);
       };
       launch_spmv(n_, d_csr_rp_, d_csr_ci_, d_csr_val_, xk, rk, 1, st);

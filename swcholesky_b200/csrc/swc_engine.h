@@ -95,7 +95,9 @@ void launch_gather_vals(int nnz, const int *map, const double *ax, double *val, 
 void launch_residual(size_t len, const double *b, double *r, cudaStream_t st);
 void launch_axpy(size_t len, double a, const double *x, double *y, cudaStream_t st);
 void launch_xpby(size_t len, const double *z, double beta, double *p, cudaStream_t st);
-void launch_norms(int n, int nrhs, const double *x, const double *y, double *out, cudaStream_t st);
+void launch_norms(int n, int nrhs, const double *x, const double *y, double *out, double *part,
+                  cudaStream_t st);
+int norm_scratch_doubles(int nrhs);
 void launch_rowabs(int n, const int *rp, const double *val, double *out, cudaStream_t st);
 
 // Per-level task lists of the solves.
@@ -255,6 +257,7 @@ class Engine {
   double *d_csr_val_ = nullptr;
   int64_t csr_nnz_ = 0;
   double *d_contrib_ = nullptr, *d_work_ = nullptr, *d_norms_ = nullptr, *h_norms_ = nullptr;
+  double *d_npart_ = nullptr;   // slices of the norm reductions
   int work_nrhs_ = 0;
   double anorm_ = 0.0;
   bool ensure_work(int nrhs, std::string &err);

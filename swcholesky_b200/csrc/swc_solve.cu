@@ -70,27 +70,38 @@ __global__ void __launch_bounds__(ST) k_fwd_diag(DevSym S, const int *list, doub
   }
 }
 
-// task = (s, r0): rows r0..r0+255 of supernode s's off-diagonal block (r0 >= w).
+// task = (s, r0): rows r0..r0+63 of supernode s's off-diagonal block (r0 >= w); thread
+// (row r, group q) sums the columns k = q (mod 4), and the four partial sums meet in shared
+// memory in a fixed order.
 __global__ void __launch_bounds__(ST) k_fwd_contrib(DevSym S, const int2 *tasks,
                                                     const double *y, double *contrib, int n,
                                                     int nrhs, int64_t cstride) {
+  __shared__ double part[4][TB];
   const int s = tasks[blockIdx.x].x, r0 = tasks[blockIdx.x].y;
   const int f = S.super[s], w = S.super[s + 1] - f;
   const int64_t rb = S.rowptr[s];
   const int m = (int)(S.rowptr[s + 1] - rb);
   const double *Ls_s = S.L + S.xptr[s];
-  const int a = r0 + threadIdx.x;
-  if (a >= m) return;
+  const int r = threadIdx.x & (TB - 1), q = threadIdx.x >> 6;
+  const int a = r0 + r;
   for (int rhs = 0; rhs < nrhs; ++rhs) {
     const double *yr = y + (size_t)rhs * n + f;
     double acc0 = 0.0, acc1 = 0.0;
-    int k = 0;
-    for (; k + 1 < w; k += 2) {
-      acc0 = fma(Ls_s[(size_t)k * m + a], yr[k], acc0);
-      acc1 = fma(Ls_s[(size_t)(k + 1) * m + a], yr[k + 1], acc1);
+    if (a < m) {
+      const double *col = Ls_s + a;
+      int k = q;
+      for (; k + 4 < w; k += 8) {
+        acc0 = fma(col[(size_t)k * m], yr[k], acc0);
+        acc1 = fma(col[(size_t)(k + 4) * m], yr[k + 4], acc1);
+      }
+      if (k < w) acc0 = fma(col[(size_t)k * m], yr[k], acc0);
     }
-    if (k < w) acc0 = fma(Ls_s[(size_t)k * m + a], yr[k], acc0);
-    contrib[(size_t)rhs * cstride + (rb - f) + (a - w)] = acc0 + acc1;
+    part[q][r] = acc0 + acc1;
+    __syncthreads();
+    if (q == 0 && a < m)
+      contrib[(size_t)rhs * cstride + (rb - f) + (a - w)] =
+          (part[0][r] + part[1][r]) + (part[2][r] + part[3][r]);
+    __syncthreads();
   }
 }
 
@@ -198,11 +209,34 @@ __device__ bool wait_flag(const int *flag, int val, int *status) {
   return ok != 0;
 }
 
+// Shared staging of one 64x64 block of a panel (column-major source, leading dimension m):
+// dst[col * 65 + row] (padded), rows >= nr and columns >= nc zero-filled; 8-byte cp.async.
+constexpr int BLD = TB + 1;
+__device__ __forceinline__ void stage_block(double *dst, const double *src, int m, int nr, int nc) {
+  for (int e = threadIdx.x; e < TB * TB; e += ST) {
+    const int c = e >> 6, r = e & (TB - 1);
+    const bool in = r < nr && c < nc;
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst + c * BLD + r);
+    const double *g = in ? src + (size_t)c * m + r : src;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(g), "r"(in ? 8 : 0));
+  }
+  asm volatile("cp.async.commit_group;\n" ::);
+}
+template <int N>
+__device__ __forceinline__ void stage_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// Chain blocks stage the inverse of their diagonal block and the panel block of each
+// predecessor in shared memory before the predecessor's flag arrives (double buffer), so
+// the step that waits on the flag only reads x_c and multiplies from shared memory.
+constexpr int CHAIN_SMEM = 3 * TB * BLD * 8;
+
 // task = (s, k); forward: y[f + 64k ..] := T_k (y[...] - contributions - sum_{c<k} L_kc x_c)
 __global__ void __launch_bounds__(ST) k_fwd_chain(DevSym S, const int2 *tasks, double *y,
                                                   const double *contrib, const int *cptr,
                                                   const int *cidx, int *flags, int epoch,
                                                   int n, int64_t cstride) {
+  extern __shared__ double csm[];
+  double *Ts = csm, *Lb0 = csm + TB * BLD;   // Lb0 and Lb0 + TB * BLD: double buffer
   __shared__ double v[TB], part[4][TB], xc[TB];
   const int s = tasks[blockIdx.x].x, k = tasks[blockIdx.x].y;
   const int tid = threadIdx.x, r = tid & (TB - 1), q = tid >> 6;
@@ -212,6 +246,8 @@ __global__ void __launch_bounds__(ST) k_fwd_chain(DevSym S, const int2 *tasks, d
   const int r0 = k * TB, bw = min(TB, w - r0);
   const int base = S.dinv_off[s];
   const double *T = S.dinv + ((size_t)base + k) * (TB * TB);
+  stage_block(Ts, T, TB, TB, TB);                 // T(r, c) at Ts[c * BLD + r]
+  if (k > 0) stage_block(Lb0, P + r0, m, bw, TB); // L_k0(r, jj) at Lb0[jj * BLD + r]
   // right-hand side of the block minus the descendants' contributions
   if (tid < TB) {
     double acc = 0.0;
@@ -222,24 +258,30 @@ __global__ void __launch_bounds__(ST) k_fwd_chain(DevSym S, const int2 *tasks, d
     }
     v[tid] = acc;
   }
-  __syncthreads();
   for (int c = 0; c < k; ++c) {
-    if (!wait_flag(&flags[base + c], epoch, S.status)) break;
+    const double *Lc = Lb0 + (c & 1) * (TB * BLD);
+    if (c + 1 < k) {
+      stage_block(Lb0 + ((c + 1) & 1) * (TB * BLD), P + (size_t)(c + 1) * TB * m + r0, m, bw, TB);
+      stage_wait<1>();
+    } else {
+      stage_wait<0>();
+    }
+    if (!wait_flag(&flags[base + c], epoch, S.status)) break;   // ends with a barrier
     if (tid < TB) xc[tid] = __ldcg(&y[f + c * TB + tid]);
     __syncthreads();
     double acc = 0.0;
-    if (r < bw)
-      for (int jj = q * 16; jj < q * 16 + 16; ++jj)
-        acc = fma(P[(size_t)(c * TB + jj) * m + r0 + r], xc[jj], acc);
+#pragma unroll
+    for (int jj = q * 16; jj < q * 16 + 16; ++jj) acc = fma(Lc[jj * BLD + r], xc[jj], acc);
     part[q][r] = acc;
     __syncthreads();
     if (tid < TB) v[tid] -= (part[0][tid] + part[1][tid]) + (part[2][tid] + part[3][tid]);
-    __syncthreads();
   }
+  stage_wait<0>();
+  __syncthreads();
   // x_k = T_k v
   double acc = 0.0;
-  if (r < bw)
-    for (int jj = q * 16; jj < q * 16 + 16; ++jj) acc = fma(T[(size_t)jj * TB + r], v[jj], acc);
+#pragma unroll
+  for (int jj = q * 16; jj < q * 16 + 16; ++jj) acc = fma(Ts[jj * BLD + r], v[jj], acc);
   part[q][r] = acc;
   __syncthreads();
   if (tid < bw) y[f + r0 + tid] = (part[0][tid] + part[1][tid]) + (part[2][tid] + part[3][tid]);
@@ -251,9 +293,11 @@ __global__ void __launch_bounds__(ST) k_fwd_chain(DevSym S, const int2 *tasks, d
 // task = (s, k) in decreasing k; backward: x[f + 64k ..] := T_k^T (x[...] - sum_{c>k} L_ck^T x_c)
 __global__ void __launch_bounds__(ST) k_bwd_chain(DevSym S, const int2 *tasks, double *x,
                                                   int *flags, int epoch) {
-  __shared__ double v[TB], xc[TB];
+  extern __shared__ double csm[];
+  double *Ts = csm, *Lb0 = csm + TB * BLD;
+  __shared__ double v[TB], part[4][TB], xc[TB];
   const int s = tasks[blockIdx.x].x, k = tasks[blockIdx.x].y;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x, i = tid & (TB - 1), q = tid >> 6;
   const int f = S.super[s], w = S.super[s + 1] - f;
   const int m = (int)(S.rowptr[s + 1] - S.rowptr[s]);
   const double *P = S.L + S.xptr[s];
@@ -261,32 +305,42 @@ __global__ void __launch_bounds__(ST) k_bwd_chain(DevSym S, const int2 *tasks, d
   const int nb = (w + TB - 1) / TB;
   const int base = S.dinv_off[s];
   const double *T = S.dinv + ((size_t)base + k) * (TB * TB);
+  // panel block (c, k): rows 64c + rr, columns r0 + i, staged as Lc[i * BLD + rr]
+  stage_block(Ts, T, TB, TB, TB);   // T(rr, i) at Ts[i * BLD + rr]
+  if (k + 1 < nb)
+    stage_block(Lb0, P + (size_t)r0 * m + (nb - 1) * TB, m, min(TB, w - (nb - 1) * TB), bw);
   if (tid < TB) v[tid] = (tid < bw) ? x[f + r0 + tid] : 0.0;
-  __syncthreads();
-  for (int c = nb - 1; c > k; --c) {
+  int buf = 0;
+  for (int c = nb - 1; c > k; --c, buf ^= 1) {
+    const double *Lc = Lb0 + buf * (TB * BLD);
+    if (c - 1 > k) {
+      stage_block(Lb0 + (buf ^ 1) * (TB * BLD), P + (size_t)r0 * m + (c - 1) * TB, m,
+                  min(TB, w - (c - 1) * TB), bw);
+      stage_wait<1>();
+    } else {
+      stage_wait<0>();
+    }
     if (!wait_flag(&flags[base + c], epoch, S.status)) break;
     const int cw = min(TB, w - c * TB);
     if (tid < TB) xc[tid] = (tid < cw) ? __ldcg(&x[f + c * TB + tid]) : 0.0;
     __syncthreads();
-    // v[i] -= sum_r L(64c + r, 64k + i) x_c[r]: one warp per i, lanes over r
-    for (int i = warp; i < bw; i += ST / 32) {
-      const double *col = P + (size_t)(r0 + i) * m + c * TB;
-      double acc = 0.0;
-      for (int rr = lane; rr < cw; rr += 32) acc = fma(col[rr], xc[rr], acc);
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-      if (lane == 0) v[i] -= acc;
-    }
-    __syncthreads();
-  }
-  // x_k[i] = sum_{r >= i} T(r, i) v[r]: column i of T is contiguous
-  for (int i = warp; i < bw; i += ST / 32) {
+    // v[i] -= sum_rr L(64c + rr, r0 + i) x_c[rr]
     double acc = 0.0;
-    for (int rr = lane; rr < bw; rr += 32) acc = fma(T[(size_t)i * TB + rr], v[rr], acc);
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) x[f + r0 + i] = acc;
+    for (int rr = q * 16; rr < q * 16 + 16; ++rr) acc = fma(Lc[i * BLD + rr], xc[rr], acc);
+    part[q][i] = acc;
+    __syncthreads();
+    if (tid < TB) v[tid] -= (part[0][tid] + part[1][tid]) + (part[2][tid] + part[3][tid]);
   }
+  stage_wait<0>();
+  __syncthreads();
+  // x_k[i] = sum_{rr >= i} T(rr, i) v[rr]
+  double acc = 0.0;
+#pragma unroll
+  for (int rr = q * 16; rr < q * 16 + 16; ++rr) acc = fma(Ts[i * BLD + rr], v[rr], acc);
+  part[q][i] = acc;
+  __syncthreads();
+  if (tid < bw) x[f + r0 + tid] = (part[0][tid] + part[1][tid]) + (part[2][tid] + part[3][tid]);
   __threadfence();
   __syncthreads();
   if (tid == 0) st_release(&flags[base + k], epoch);
@@ -341,13 +395,17 @@ __global__ void k_axpy(size_t len, double a, const double *x, double *y) {
 }
 
 // per-vector max |x| and sum x*y for nrhs vectors of length n (out[2*r], out[2*r+1]),
-// deterministic: one CTA per vector, fixed reduction tree.
-__global__ void k_norms(int n, const double *x, const double *y, double *out) {
+// deterministic: NORM_BLOCKS fixed slices per vector, then one CTA per vector sums the
+// slices in order.
+constexpr int NORM_BLOCKS = 128;
+__global__ void k_norms_part(int n, const double *x, const double *y, double *part) {
   __shared__ double smax[ST], sdot[ST];
-  const int r = blockIdx.x;
+  const int r = blockIdx.y, b = blockIdx.x;
   const double *xr = x + (size_t)r * n, *yr = y ? y + (size_t)r * n : nullptr;
+  const int per = (n + NORM_BLOCKS - 1) / NORM_BLOCKS;
+  const int lo = b * per, hi = min(n, lo + per);
   double mx = 0.0, dt = 0.0;
-  for (int i = threadIdx.x; i < n; i += ST) {
+  for (int i = lo + threadIdx.x; i < hi; i += ST) {
     mx = fmax(mx, fabs(xr[i]));
     if (yr) dt = fma(xr[i], yr[i], dt);
   }
@@ -362,6 +420,24 @@ __global__ void k_norms(int n, const double *x, const double *y, double *out) {
     __syncthreads();
   }
   if (threadIdx.x == 0) {
+    part[2 * ((size_t)r * NORM_BLOCKS + b)] = smax[0];
+    part[2 * ((size_t)r * NORM_BLOCKS + b) + 1] = sdot[0];
+  }
+}
+__global__ void k_norms_final(const double *part, double *out) {
+  __shared__ double smax[NORM_BLOCKS], sdot[NORM_BLOCKS];
+  const int r = blockIdx.x, t = threadIdx.x;
+  smax[t] = part[2 * ((size_t)r * NORM_BLOCKS + t)];
+  sdot[t] = part[2 * ((size_t)r * NORM_BLOCKS + t) + 1];
+  __syncthreads();
+  for (int o = NORM_BLOCKS / 2; o > 0; o >>= 1) {
+    if (t < o) {
+      smax[t] = fmax(smax[t], smax[t + o]);
+      sdot[t] += sdot[t + o];
+    }
+    __syncthreads();
+  }
+  if (t == 0) {
     out[2 * r] = smax[0];
     out[2 * r + 1] = sdot[0];
   }
@@ -376,6 +452,10 @@ bool solve_configure(int max_w, std::string &err) {
     return false;
   }
   cudaError_t e = cudaFuncSetAttribute(k_fwd_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_fwd_chain, cudaFuncAttributeMaxDynamicSharedMemorySize, CHAIN_SMEM);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_bwd_chain, cudaFuncAttributeMaxDynamicSharedMemorySize, CHAIN_SMEM);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_bwd_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) {
@@ -407,11 +487,12 @@ void launch_fwd_chain(const DevSym &S, const int2 *tasks, int count, double *y,
                       const double *contrib, const int *cptr, const int *cidx, int *flags,
                       int epoch, int n, int64_t cstride, cudaStream_t st) {
   if (count > 0)
-    k_fwd_chain<<<count, ST, 0, st>>>(S, tasks, y, contrib, cptr, cidx, flags, epoch, n, cstride);
+    k_fwd_chain<<<count, ST, CHAIN_SMEM, st>>>(S, tasks, y, contrib, cptr, cidx, flags, epoch, n,
+                                               cstride);
 }
 void launch_bwd_chain(const DevSym &S, const int2 *tasks, int count, double *x, int *flags,
                       int epoch, cudaStream_t st) {
-  if (count > 0) k_bwd_chain<<<count, ST, 0, st>>>(S, tasks, x, flags, epoch);
+  if (count > 0) k_bwd_chain<<<count, ST, CHAIN_SMEM, st>>>(S, tasks, x, flags, epoch);
 }
 void launch_spmv(int n, const int *rp, const int *ci, const double *val, const double *x,
                  double *y, int nrhs, cudaStream_t st) {
@@ -433,8 +514,11 @@ void launch_xpby(size_t len, const double *z, double beta, double *p, cudaStream
 void launch_axpy(size_t len, double a, const double *x, double *y, cudaStream_t st) {
   if (len) k_axpy<<<(unsigned)((len + 255) / 256), 256, 0, st>>>(len, a, x, y);
 }
-void launch_norms(int n, int nrhs, const double *x, const double *y, double *out, cudaStream_t st) {
-  k_norms<<<nrhs, ST, 0, st>>>(n, x, y, out);
+void launch_norms(int n, int nrhs, const double *x, const double *y, double *out, double *part,
+                  cudaStream_t st) {
+  k_norms_part<<<dim3(NORM_BLOCKS, nrhs), ST, 0, st>>>(n, x, y, part);
+  k_norms_final<<<nrhs, NORM_BLOCKS, 0, st>>>(part, out);
 }
+int norm_scratch_doubles(int nrhs) { return 2 * NORM_BLOCKS * nrhs; }
 
 }  // namespace swc
