@@ -46,7 +46,7 @@ __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0
 
 
 __device__ __forceinline__ void mma_tf32(float (&c)[4], const unsigned (&a)[4], const unsigned (&b)[2]) {
-  asm volatile(
+  asm(
       "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
       "{%0,%1,%2,%3};\n"
       : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
@@ -142,15 +142,23 @@ __device__ __forceinline__ void tf32x3_product(const float2 *__restrict__ Lf, in
           bh[j][0] = __float_as_uint(y0.x); bl[j][0] = __float_as_uint(y0.y);
           bh[j][1] = __float_as_uint(y1.x); bl[j][1] = __float_as_uint(y1.y);
         }
+        // the three partial products of one tile depend on each other through the
+        // accumulator: issue each over all tiles before the next (8 independent MMAs apart)
 #pragma unroll
         for (int i = 0; i < 2; ++i)
 #pragma unroll
           for (int j = 0; j < 4; ++j)
-            if (((rmask >> i) & (cmask >> j)) & 1u) {
-              mma_tf32(acc.v[i][j], al[i], bh[j]);
-              mma_tf32(acc.v[i][j], ah[i], bl[j]);
-              mma_tf32(acc.v[i][j], ah[i], bh[j]);
-            }
+            if (((rmask >> i) & (cmask >> j)) & 1u) mma_tf32(acc.v[i][j], al[i], bh[j]);
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            if (((rmask >> i) & (cmask >> j)) & 1u) mma_tf32(acc.v[i][j], ah[i], bl[j]);
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            if (((rmask >> i) & (cmask >> j)) & 1u) mma_tf32(acc.v[i][j], ah[i], bh[j]);
       }
     }
     __syncthreads();
