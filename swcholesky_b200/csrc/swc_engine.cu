@@ -136,7 +136,8 @@ void Engine::release() {
                   d_syrk_, d_pairs_, d_upd_end_, d_dinv_, d_dinv_off_, d_diag_,
                   d_slist_, d_cptr_, d_cidx_, d_flags_, d_fchain_, d_bchain_, d_scontrib_, d_sgather_, d_csr_rp_, d_csr_ci_,
                   d_csr_map_,
-                  d_csr_val_, d_contrib_, d_work_, d_norms_, d_persist_, d_qctr_, d_npart_};
+                  d_csr_val_, d_contrib_, d_work_, d_norms_, d_persist_, d_qctr_, d_npart_,
+                  d_tiny_};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   release_adjoint();
@@ -156,7 +157,8 @@ void Engine::release() {
   d_scontrib_ = d_sgather_ = nullptr;
   d_csr_rp_ = d_csr_ci_ = d_csr_map_ = nullptr;
   d_csr_val_ = d_contrib_ = d_work_ = d_norms_ = nullptr;
-  d_persist_ = d_qctr_ = nullptr;
+  d_persist_ = d_qctr_ = d_tiny_ = nullptr;
+  tiny_ctas_ = 0;
   d_npart_ = nullptr;
   persist_ctas_ = 0;
   work_nrhs_ = 0;
@@ -243,15 +245,23 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
     for (int q = prunePtr[s]; q < prunePtr[s + 1]; ++q)
       if (level[pruneSet[q]] >= level[s]) { err = "prune set is not consistent with the etree"; return false; }
 
-  // ---- persistent bottom set: small supernodes whose whole subtree is small ----
-  std::vector<char> in_persist(supNo, 0);
-  if (T.persist) {
-    std::vector<char> kids_ok(supNo, 1);
+  // ---- persistent bottom sets: tiny supernodes whose whole subtree is tiny (one warp
+  // each), then small supernodes whose whole subtree is tiny or small (one CTA each) ----
+  std::vector<char> in_tiny(supNo, 0), in_persist(supNo, 0);
+  {
+    std::vector<char> kids_tiny(supNo, 1), kids_ok(supNo, 1);
     for (int s = 0; s < supNo; ++s) {
       const int w = super[s + 1] - super[s];
       const int64_t m = rowptr[s + 1] - rowptr[s];
-      in_persist[s] = kids_ok[s] && small_class(w, m, T) && small_smem(w, m) <= T.persist_max_smem;
-      if (!in_persist[s] && m > w) kids_ok[col2sup[Ls[rowptr[s] + w]]] = 0;
+      in_tiny[s] = T.tiny && kids_tiny[s] && m <= TINY_M && (int64_t)w * m <= TINY_ELEMS;
+      if (!in_tiny[s])
+        in_persist[s] = T.persist && kids_ok[s] && small_class(w, m, T) &&
+                        small_smem(w, m) <= T.persist_max_smem;
+      if (m > w) {
+        const int p = col2sup[Ls[rowptr[s] + w]];
+        if (!in_tiny[s]) kids_tiny[p] = 0;
+        if (!in_tiny[s] && !in_persist[s]) kids_ok[p] = 0;
+      }
     }
   }
 
@@ -271,7 +281,9 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
     for (int s : by_level[lv]) {
       int w = super[s + 1] - super[s];
       int64_t m = rowptr[s + 1] - rowptr[s];
-      if (in_persist[s]) {
+      if (in_tiny[s]) {
+        P.tiny_list.push_back(s);
+      } else if (in_persist[s]) {
         P.persist_list.push_back(s);
         P.persist_smem = std::max<int>(P.persist_smem, (int)small_smem(w, m));
       } else if (small_class(w, m, T)) {
@@ -336,6 +348,7 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
       launches += (W.panel_cnt[j] > 0) + (W.syrk_cnt[j] > 0) + (W.diag_cnt[j] > 0);
   }
   if (!P.persist_list.empty()) launches += 1;
+  if (!P.tiny_list.empty()) launches += 1;
   P.launches = launches;
 
   // ---- algorithmic work per kernel class (one factorization) ----
@@ -343,6 +356,7 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
     KernelStats &K = P.work;
     std::vector<int> all_small(P.small_list);
     all_small.insert(all_small.end(), P.persist_list.begin(), P.persist_list.end());
+    all_small.insert(all_small.end(), P.tiny_list.begin(), P.tiny_list.end());
     for (int s : all_small) {
       int f = super[s], w = super[s + 1] - f;
       int64_t m = rowptr[s + 1] - rowptr[s];
@@ -513,6 +527,7 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
             upload(d_upd_, pruneSet, (size_t)nprune, st, err) &&
             upload(d_small_, P.small_list.data(), P.small_list.size(), st, err) &&
             upload(d_persist_, P.persist_list.data(), P.persist_list.size(), st, err) &&
+            upload(d_tiny_, P.tiny_list.data(), P.tiny_list.size(), st, err) &&
             upload(d_big_, P.big_list.data(), P.big_list.size(), st, err) &&
             upload(d_diag_, P.diag_list.data(), P.diag_list.size(), st, err) &&
             upload(d_asm_, P.asm_tasks.data(), P.asm_tasks.size(), st, err) &&
@@ -542,7 +557,9 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
     e = cudaMalloc(&d_dinv_, sizeof(double) * TB * TB * std::max<int64_t>(H.ndinv, 1));
   if (e == cudaSuccess)
     e = cudaMalloc(&d_csr_val_, sizeof(double) * std::max<size_t>(csr_ci.size(), 1));
-  if (e == cudaSuccess) e = cudaMalloc(&d_qctr_, sizeof(int) * ((size_t)supNo + 1));
+  // queue head of the CTA walk, done flags, queue head of the warp walk
+  if (e == cudaSuccess) e = cudaMalloc(&d_qctr_, sizeof(int) * ((size_t)supNo + 2));
+  if (e == cudaSuccess && !P.tiny_list.empty()) tiny_ctas_ = tiny_ctas((int)P.tiny_list.size());
   if (e == cudaSuccess && !P.persist_list.empty())
     persist_ctas_ = persist_ctas(P.persist_smem, (int)P.persist_list.size());
 
@@ -596,9 +613,16 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, bool mix
   cudaMemsetAsync(dL_, 0, sizeof(double) * xsize_, st);
   launch_init_status(d_status_, st);
   mark(-1, 1);
+  if (!plan_.tiny_list.empty() || !plan_.persist_list.empty())
+    cudaMemsetAsync(d_qctr_, 0, sizeof(int) * (nsuper_ + 2), st);
+  if (!plan_.tiny_list.empty()) {
+    mark(K_SMALL, 1);
+    launch_factor_tiny_persist(sym_, d_tiny_, (int)plan_.tiny_list.size(), tiny_ctas_, d_qctr_,
+                               d_qctr_ + 1 + nsuper_, st);
+    mark(-1, 1);
+  }
   if (!plan_.persist_list.empty()) {
     mark(K_SMALL, 1);
-    cudaMemsetAsync(d_qctr_, 0, sizeof(int) * (nsuper_ + 1), st);
     launch_factor_small_persist(sym_, d_persist_, (int)plan_.persist_list.size(),
                                 plan_.persist_smem, persist_ctas_, d_qctr_, st);
     mark(-1, 1);

@@ -66,6 +66,7 @@ struct Plan {
   std::vector<int2> panel_tasks;
   std::vector<int4> syrk_tasks;
   std::vector<int> diag_list;
+  std::vector<int> tiny_list;      // tiny supernodes of the warp walk, in level order
   std::vector<int> persist_list;   // small supernodes of the persistent walk, in level order
   int persist_smem = 0;
   int launches = 0;  // kernel launches per factorization
@@ -238,8 +239,8 @@ class Engine {
   float2 *d_Lf_ = nullptr;
   bool use_graph_ = true;
   Tuning tuning_;
-  int *d_persist_ = nullptr, *d_qctr_ = nullptr;
-  int persist_ctas_ = 0;
+  int *d_persist_ = nullptr, *d_qctr_ = nullptr, *d_tiny_ = nullptr;
+  int persist_ctas_ = 0, tiny_ctas_ = 0;
   // Trailing SYRK of the dense steps in split-TF32 too (mixed mode).  Off: on B200 the
   // FP64 DMMA kernel is the faster one for these 64x64x64 tiles (measured 6.9 ms vs 13.4 ms
   // per factorization of the 60^3 Laplacian).
@@ -270,6 +271,9 @@ class Engine {
 void launch_factor_small(const DevSym &S, const int *list, int count, int smem, cudaStream_t st);
 // persistent small-class walk: CTAs to launch (occupancy x SMs, at most count) and the launch
 int persist_ctas(int smem, int count);
+int tiny_ctas(int count);
+void launch_factor_tiny_persist(const DevSym &S, const int *order, int count, int ctas,
+                                int *qctr, int *qhead, cudaStream_t st);
 void launch_factor_small_persist(const DevSym &S, const int *order, int count, int smem,
                                  int ctas, int *qctr, cudaStream_t st);
 void launch_assemble(const DevSym &S, const int2 *tasks, int count, cudaStream_t st);

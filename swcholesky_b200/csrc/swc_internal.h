@@ -39,11 +39,16 @@ constexpr int SMALL_MAX_W = 64;
 constexpr int SMALL_MAX_ELEMS = 12288;  // panel doubles held in shared memory (96 KB)
 constexpr int SMALL_MAX_M = 2048;
 
+// Tiny supernodes: one warp each (panel and row lists in a per-warp shared-memory slice).
+constexpr int TINY_ELEMS = 1024;
+constexpr int TINY_M = 256;
+
 // Execution-plan parameters (defaults above; the batched path's autotuner varies them).
 struct Tuning {
   int small_max_w = SMALL_MAX_W;         // size-class limits, at most the constants above
   int small_max_m = SMALL_MAX_M;
   int small_max_elems = SMALL_MAX_ELEMS;
+  int tiny = 1;                          // bottom tiny supernodes: one warp each, one launch
   int persist = 1;                       // bottom small supernodes in one persistent launch
   int persist_max_smem = 48 * 1024;      // shared-memory cap of a persistent supernode (bytes)
 };

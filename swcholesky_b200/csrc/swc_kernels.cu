@@ -842,6 +842,133 @@ __global__ void k_init_status(int *status) {
   status[3] = 0;
 }
 
+
+// ---------------------------------------------------------------------------------------
+// Tiny supernodes (panel at most TINY_ELEMS doubles, at most TINY_M rows): one WARP per
+// supernode, TW warps per CTA, each with its own shared-memory slice.  The bottom of the
+// tree (a set closed under descendants) is walked in ONE persistent launch: warps take
+// supernodes from their own device queue in level order, wait for the descendants in the
+// update list, factor with warp-synchronous code (no block barriers) and publish their done
+// flag, as the CTA walk below does at CTA granularity.
+constexpr int TW = 4;
+constexpr int TINY_SLICE = (TINY_ELEMS * 8 + 2 * TINY_M * 4 + 15) / 16 * 16;   // bytes per warp
+constexpr int TINY_SMEM = TW * TINY_SLICE;
+
+__device__ void factor_tiny_body(const DevSym &S, int s, double *P, int *rows, int *rel) {
+  const int lane = threadIdx.x & 31;
+  const int f = S.super[s];
+  const int w = S.super[s + 1] - f;
+  const int64_t rb = S.rowptr[s];
+  const int m = (int)(S.rowptr[s + 1] - rb);
+  for (int i = lane; i < m; i += 32) rows[i] = S.Ls[rb + i];
+  for (int i = lane; i < m * w; i += 32) P[i] = 0.0;
+  __syncwarp();
+  // assembly of A's columns
+  for (int j = 0; j < w; ++j)
+    for (int p = S.Ap[f + j] + lane; p < S.Ap[f + j + 1]; p += 32) {
+      const int i = S.Ai[p];
+      const int pos = lbound(rows, m, i);
+      if (pos < m && rows[pos] == i) P[(size_t)j * m + pos] = S.Ax[p];
+      else flag_structure_error(S);
+    }
+  __syncwarp();
+  // updates from the descendants of the update list, in order
+  for (int q = S.upd_ptr[s]; q < S.upd_ptr[s + 1]; ++q) {
+    const int d = S.upd[q];
+    const int wd = S.super[d + 1] - S.super[d];
+    const int64_t rbd = S.rowptr[d];
+    const int md = (int)(S.rowptr[d + 1] - rbd);
+    const int *Lsd = S.Ls + rbd;
+    const int lb = wd + lbound(Lsd + wd, md - wd, f);
+    const int ub = wd + lbound(Lsd + wd, md - wd, f + w);
+    const int nr = md - lb, n1 = ub - lb;
+    if (n1 <= 0 || nr > m) {
+      if (nr > m && lane == 0) flag_structure_error(S);
+      continue;
+    }
+    for (int i = lane; i < nr; i += 32) {
+      const int key = Lsd[lb + i];
+      int pos = lbound(rows, m, key);
+      if (pos >= m || rows[pos] != key) { flag_structure_error(S); pos = -1; }
+      rel[i] = pos;
+    }
+    __syncwarp();
+    const double *Ld = S.L + S.xptr[d] + lb;
+    // output (a, b), a < n1, b >= a: lanes run along b (contiguous rows of d's panel)
+    for (int a = 0; a < n1; ++a) {
+      const int ra = rel[a];
+      for (int b = a + lane; b < nr; b += 32) {
+        const int rbi = rel[b];
+        double acc = 0.0;
+        for (int k = 0; k < wd; ++k) acc = fma(Ld[(size_t)k * md + b], Ld[(size_t)k * md + a], acc);
+        if (ra >= 0 && rbi >= 0) P[(size_t)ra * m + rbi] -= acc;
+      }
+    }
+    __syncwarp();
+  }
+  // right-looking POTRF + TRSM of the m x w panel, lanes along the rows
+  for (int j = 0; j < w; ++j) {
+    const double piv = P[(size_t)j * m + j];
+    const double dsq = sqrt(piv), inv = 1.0 / dsq;
+    if (lane == 0 && !(piv > 0.0)) atomicMin(&S.status[0], f + j + 1);
+    __syncwarp();
+    for (int i = j + lane; i < m; i += 32) P[(size_t)j * m + i] = (i == j) ? dsq : P[(size_t)j * m + i] * inv;
+    __syncwarp();
+    for (int c = j + 1; c < w; ++c) {
+      const double lcj = P[(size_t)j * m + c];
+      for (int i = c + lane; i < m; i += 32)
+        P[(size_t)c * m + i] = fma(-P[(size_t)j * m + i], lcj, P[(size_t)c * m + i]);
+    }
+    __syncwarp();
+  }
+  double *dst = S.L + S.xptr[s];
+  for (int i = lane; i < m * w; i += 32) dst[i] = P[i];
+  if (S.Lf) {
+    float2 *dstf = S.Lf + S.xptr[s];
+    for (int i = lane; i < m * w; i += 32) dstf[i] = split_tf32(P[i]);
+  }
+}
+
+// qctr[1 + s]: done flags (shared with the CTA walk); qhead: this walk's queue head.
+__global__ void __launch_bounds__(TW * 32) k_factor_tiny_persist(DevSym S, const int *order,
+                                                                 int count, int *qctr,
+                                                                 int *qhead) {
+  extern __shared__ double smem_t[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  unsigned char *slice = reinterpret_cast<unsigned char *>(smem_t) + (size_t)warp * TINY_SLICE;
+  double *P = reinterpret_cast<double *>(slice);
+  int *rows = reinterpret_cast<int *>(slice + TINY_ELEMS * 8);
+  int *rel = rows + TINY_M;
+  int *done = qctr + 1;
+  for (;;) {
+    int idx = 0;
+    if (lane == 0) idx = atomicAdd(qhead, 1);
+    idx = __shfl_sync(0xffffffffu, idx, 0);
+    if (idx >= count) break;
+    const int s = order[idx];
+    bool timed_out = false;
+    for (int q = S.upd_ptr[s] + lane; q < S.upd_ptr[s + 1] && !timed_out; q += 32) {
+      const int *flag = done + S.upd[q];
+      long long it = 0;
+      while (ld_acquire_k(flag) == 0) {
+        if (++it > PERSIST_SPIN) {
+          atomicExch(&S.status[3], 1);
+          timed_out = true;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __syncwarp();
+    factor_tiny_body(S, s, P, rows, rel);
+    __syncwarp();
+    if (lane == 0) {
+      __threadfence();
+      st_release_k(done + s, 1);
+    }
+  }
+}
+
 }  // namespace
 
 bool kernels_configure(std::string &err) {
@@ -850,6 +977,9 @@ bool kernels_configure(std::string &err) {
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_factor_small_persist, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              200 * 1024);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_factor_tiny_persist, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             TINY_SMEM);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_update_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, UPD_SMEM);
   if (e == cudaSuccess)
@@ -876,6 +1006,19 @@ int persist_ctas(int smem, int count) {
           cudaSuccess || per < 1)
     per = 1;
   return std::max(1, std::min(count, sms * per));
+}
+int tiny_ctas(int count) {
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_factor_tiny_persist, TW * 32,
+                                                    TINY_SMEM) != cudaSuccess || per < 1)
+    per = 1;
+  return std::max(1, std::min((count + TW - 1) / TW, sms * per));
+}
+void launch_factor_tiny_persist(const DevSym &S, const int *order, int count, int ctas,
+                                int *qctr, int *qhead, cudaStream_t st) {
+  if (count > 0) k_factor_tiny_persist<<<ctas, TW * 32, TINY_SMEM, st>>>(S, order, count, qctr, qhead);
 }
 void launch_factor_small_persist(const DevSym &S, const int *order, int count, int smem,
                                  int ctas, int *qctr, cudaStream_t st) {
