@@ -32,8 +32,10 @@ bool small_class(int w, int64_t m, const Tuning &T) {
 }
 
 // shared memory of the small-class kernel for an m x w panel: panel, rows, relative
-// indices (+ padding to 8 bytes), pivot column
-int64_t small_smem(int w, int64_t m) { return 8 * m * w + 8 * m + 8 + 8 * (int64_t)w; }
+// indices (+ padding to 8 bytes), pivot column, staging slab
+int64_t small_smem(int w, int64_t m) {
+  return 8 * m * w + 8 * m + 8 + 8 * (int64_t)w + 8 * (int64_t)SMALL_SLAB;
+}
 
 // One update tile of the tiled class with the descendants that touch it.
 struct TileWork {

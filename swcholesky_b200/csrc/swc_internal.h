@@ -38,10 +38,15 @@ constexpr int TB = 64;
 constexpr int SMALL_MAX_W = 64;
 constexpr int SMALL_MAX_ELEMS = 12288;  // panel doubles held in shared memory (96 KB)
 constexpr int SMALL_MAX_M = 2048;
+// Shared-memory slab (doubles) through which a small supernode stages a descendant's rows,
+// a column chunk at a time, before forming its update.
+constexpr int SMALL_SLAB = 2048;   // >= SMALL_MAX_M: one full column always fits
 
 // Tiny supernodes: one warp each (panel and row lists in a per-warp shared-memory slice).
 constexpr int TINY_ELEMS = 1024;
 constexpr int TINY_M = 256;
+constexpr int TINY_SLAB = 512;     // >= TINY_M
+static_assert(SMALL_SLAB >= SMALL_MAX_M && TINY_SLAB >= TINY_M, "a slab holds one full column");
 
 // Execution-plan parameters (defaults above; the batched path's autotuner varies them).
 struct Tuning {

@@ -58,6 +58,38 @@ __device__ __forceinline__ void flag_structure_error(const DevSym &S) {
   atomicExch(&S.status[1], 1);
 }
 
+// Update of a small panel P (m rows, column-major) by descendant d: rows lb.. of d's panel
+// (Ld points at row lb; md = d's rows, wd = its width, nr rows from lb, the first n1 of them
+// inside the target's columns).  The rows are staged in the shared slab (capacity slab_cap
+// doubles) a column chunk at a time with independent loads from all threads, then
+// P[rel[a]][rel[b]] -= sum_k X[b][k] X[a][k] for a < n1, b >= a, from shared memory.
+// Threads t, t + nt, ...; `sync` is the barrier of the thread group (block or warp).
+template <bool WARP>
+__device__ __forceinline__ void small_update(const double *Ld, int md, int wd, int n1, int nr,
+                                             const int *rel, double *P, int m, double *slab,
+                                             int slab_cap, int t, int nt) {
+  const int kch = max(1, min(wd, slab_cap / nr));
+  for (int k0 = 0; k0 < wd; k0 += kch) {
+    const int kc = min(kch, wd - k0);
+    for (int e = t; e < nr * kc; e += nt) {
+      const int kk = e / nr, i = e - kk * nr;
+      slab[e] = Ld[(size_t)(k0 + kk) * md + i];
+    }
+    if (WARP) __syncwarp(); else __syncthreads();
+    const int total = n1 * nr;
+    for (int idx = t; idx < total; idx += nt) {
+      const int a = idx / nr, b = idx - a * nr;
+      if (b < a) continue;
+      const int ra = rel[a], rbi = rel[b];
+      if (ra < 0 || rbi < 0) continue;
+      double acc = 0.0;
+      for (int kk = 0; kk < kc; ++kk) acc = fma(slab[kk * nr + b], slab[kk * nr + a], acc);
+      P[(size_t)ra * m + rbi] -= acc;
+    }
+    if (WARP) __syncwarp(); else __syncthreads();
+  }
+}
+
 // ---------------------------------------------------------------------------------------
 // Whole factorization of one small supernode s by the calling CTA (all NT threads).
 __device__ __noinline__ void factor_small_body(const DevSym &S, int s, double *smem) {
@@ -109,19 +141,8 @@ __device__ __noinline__ void factor_small_body(const DevSym &S, int s, double *s
       rel[i] = pos;
     }
     __syncthreads();
-    const double *Ld = S.L + S.xptr[d];
-    const int total = n1 * nr;
-    for (int idx = tid; idx < total; idx += NT) {
-      const int a = idx / nr, b = idx - a * nr;
-      if (b < a) continue;
-      const int ra = rel[a], rbi = rel[b];
-      if (ra < 0 || rbi < 0) continue;
-      double acc = 0.0;
-      const double *pa = Ld + lb + a, *pb = Ld + lb + b;
-      for (int k = 0; k < wd; ++k) acc += pb[(size_t)k * md] * pa[(size_t)k * md];
-      P[(size_t)ra * m + rbi] -= acc;
-    }
-    __syncthreads();
+    small_update<false>(S.L + S.xptr[d] + lb, md, wd, n1, nr, rel, P, m,
+                        reinterpret_cast<double *>(rel + m) + w, SMALL_SLAB, tid, NT);
   }
 
   // POTRF + TRSM on the tall panel: unblocked right-looking Cholesky of m x w.  Rows are
@@ -851,10 +872,11 @@ __global__ void k_init_status(int *status) {
 // update list, factor with warp-synchronous code (no block barriers) and publish their done
 // flag, as the CTA walk below does at CTA granularity.
 constexpr int TW = 4;
-constexpr int TINY_SLICE = (TINY_ELEMS * 8 + 2 * TINY_M * 4 + 15) / 16 * 16;   // bytes per warp
+constexpr int TINY_SLICE = (TINY_ELEMS * 8 + TINY_SLAB * 8 + 2 * TINY_M * 4 + 15) / 16 * 16;   // bytes per warp
 constexpr int TINY_SMEM = TW * TINY_SLICE;
 
-__device__ void factor_tiny_body(const DevSym &S, int s, double *P, int *rows, int *rel) {
+__device__ void factor_tiny_body(const DevSym &S, int s, double *P, int *rows, int *rel,
+                                 double *slab) {
   const int lane = threadIdx.x & 31;
   const int f = S.super[s];
   const int w = S.super[s + 1] - f;
@@ -893,18 +915,7 @@ __device__ void factor_tiny_body(const DevSym &S, int s, double *P, int *rows, i
       rel[i] = pos;
     }
     __syncwarp();
-    const double *Ld = S.L + S.xptr[d] + lb;
-    // output (a, b), a < n1, b >= a: lanes run along b (contiguous rows of d's panel)
-    for (int a = 0; a < n1; ++a) {
-      const int ra = rel[a];
-      for (int b = a + lane; b < nr; b += 32) {
-        const int rbi = rel[b];
-        double acc = 0.0;
-        for (int k = 0; k < wd; ++k) acc = fma(Ld[(size_t)k * md + b], Ld[(size_t)k * md + a], acc);
-        if (ra >= 0 && rbi >= 0) P[(size_t)ra * m + rbi] -= acc;
-      }
-    }
-    __syncwarp();
+    small_update<true>(S.L + S.xptr[d] + lb, md, wd, n1, nr, rel, P, m, slab, TINY_SLAB, lane, 32);
   }
   // right-looking POTRF + TRSM of the m x w panel, lanes along the rows
   for (int j = 0; j < w; ++j) {
@@ -937,7 +948,8 @@ __global__ void __launch_bounds__(TW * 32) k_factor_tiny_persist(DevSym S, const
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   unsigned char *slice = reinterpret_cast<unsigned char *>(smem_t) + (size_t)warp * TINY_SLICE;
   double *P = reinterpret_cast<double *>(slice);
-  int *rows = reinterpret_cast<int *>(slice + TINY_ELEMS * 8);
+  double *slab = reinterpret_cast<double *>(slice + TINY_ELEMS * 8);
+  int *rows = reinterpret_cast<int *>(slice + (TINY_ELEMS + TINY_SLAB) * 8);
   int *rel = rows + TINY_M;
   int *done = qctr + 1;
   for (;;) {
@@ -960,7 +972,7 @@ __global__ void __launch_bounds__(TW * 32) k_factor_tiny_persist(DevSym S, const
       }
     }
     __syncwarp();
-    factor_tiny_body(S, s, P, rows, rel);
+    factor_tiny_body(S, s, P, rows, rel, slab);
     __syncwarp();
     if (lane == 0) {
       __threadfence();

@@ -1,7 +1,7 @@
 """Runs the numeric factorization of a named workload a given number of times.
 
     python -m swcholesky_b200.run --workload grid3d_60 --mode fp64 --reps 1 [--solve]
-    python -m swcholesky_b200.run --workload batch256 --mode mixed --reps 1
+    python -m swcholesky_b200.run --workload batch256 --mode mixed --reps 1 [--batch-count 64]
 
 The single-matrix workloads use the supernode partition stored in tests/golden (the
 reference's symbolic phase) when present, else the library's own partition; ``batch256``
@@ -25,10 +25,10 @@ GOLDEN = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))
                       "golden")
 
 
-def load(name: str):
+def load(name: str, batch_count: int = 256):
     """(problem or list of matrices, values)."""
     if name == "batch256":
-        src, _ = W.batch_sources()
+        src, _ = W.batch_sources(count=batch_count)
         mats = [M.permute_lower(A, p) for A, p in src]
         return mats, np.concatenate([m.data for m in mats])
     A, perm, _ = W.build(name)
@@ -47,9 +47,11 @@ def main():
     ap.add_argument("--mode", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--reps", type=int, default=1)
     ap.add_argument("--solve", action="store_true")
+    ap.add_argument("--batch-count", type=int, default=256,
+                    help="matrices of the batched workload (a smaller batch for profiling)")
     args = ap.parse_args()
     mode = SWC_MODE_MIXED_TF32X3 if args.mode == "mixed" else SWC_MODE_FP64
-    prob, vals = load(args.workload)
+    prob, vals = load(args.workload, args.batch_count)
     h = Handle(0)
     if isinstance(prob, list):
         h.batch_analyze(prob)
