@@ -137,6 +137,20 @@ def reference_time(A, perm_in, threads, budget_s, max_reps, min_reps=1):
     return float(np.median(times)), len(times), sym
 
 
+def profile_traffic(kernel: str, workload: str):
+    """DRAM bytes per launch of `kernel` on `workload` from the committed ncu summary
+    (profiles/<kernel>_<workload>.md, line 'traffic_bytes_per_launch: N'), else None."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.md")
+    try:
+        with open(path) as fh:
+            for line in fh:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return int(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -341,6 +355,10 @@ def run_ours(args, rank, world, local_rank):
 
     if rank == 0:
         achieved = kfl / (kms * 1e-3) / 1e12
+        kname = {"update": "k_update_tiles_mx" if mixed else "k_update_tiles"}.get(dom)
+        traffic = profile_traffic(kname, args.workload) if kname else None
+        tsrc = (f"dram__bytes_read.sum + dram__bytes_write.sum per launch, ncu capture summarised "
+                f"in profiles/{kname}_{args.workload}.md" if traffic else None)
         per_step = h.launches + (last.get("iters", 0) + 1) * (solve_launches + 5)
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world,
@@ -367,7 +385,7 @@ def run_ours(args, rank, world, local_rank):
             "roofline": {"bound": "tensor", "kernel": dom, "achieved": round(achieved, 4),
                          "peak": round(peak, 3) if peak else None, "unit": "TFLOP/s",
                          "frac": round(achieved / peak, 4) if peak else None,
-                         "traffic": None, "peak_source": psrc,
+                         "traffic": traffic, "traffic_source": tsrc, "peak_source": psrc,
                          "fp64_peak": round(peak64, 3) if peak64 else None,
                          "launches": la, "kernel_ms": round(kms, 4),
                          "algorithmic_flops": kfl,
