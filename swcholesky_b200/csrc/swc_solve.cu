@@ -30,6 +30,7 @@ __global__ void __launch_bounds__(ST) k_fwd_diag(DevSym S, const int *list, doub
                                                  const int *cidx, int n, int nrhs,
                                                  int64_t cstride) {
   extern __shared__ double v[];
+  __shared__ double blk[SB * (SB + 1)];
   const int s = list[blockIdx.x];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int f = S.super[s], w = S.super[s + 1] - f;
@@ -46,15 +47,23 @@ __global__ void __launch_bounds__(ST) k_fwd_diag(DevSym S, const int *list, doub
       v[i] = acc;
     }
     __syncthreads();
-    // dense lower solve with the diagonal block, blocked by SB columns
+    // dense lower solve with the diagonal block, blocked by SB columns; each SB x SB block
+    // and the reciprocals of its diagonal are staged first, so the serial chain of warp 0
+    // reads only shared memory
     for (int j0 = 0; j0 < w; j0 += SB) {
       const int jb = min(SB, w - j0);
+      for (int e = tid; e < jb * jb; e += ST) {
+        const int j = e / jb, i = e - j * jb;
+        blk[j * (SB + 1) + i] = Ls_s[(size_t)(j0 + j) * m + j0 + i];
+      }
+      __syncthreads();
       if (warp == 0) {
+        const double rdl = (lane < jb) ? 1.0 / blk[lane * (SB + 1) + lane] : 0.0;
         double x = (lane < jb) ? v[j0 + lane] : 0.0;
         for (int j = 0; j < jb; ++j) {
-          const double xj = __shfl_sync(0xffffffffu, x, j) / Ls_s[(size_t)(j0 + j) * m + j0 + j];
-          if (lane == j) x = xj;
-          if (lane > j && lane < jb) x = fma(-Ls_s[(size_t)(j0 + j) * m + j0 + lane], xj, x);
+          if (lane == j) x *= rdl;
+          const double xj = __shfl_sync(0xffffffffu, x, j);
+          if (lane > j && lane < jb) x = fma(-blk[j * (SB + 1) + lane], xj, x);
         }
         if (lane < jb) v[j0 + lane] = x;
       }
@@ -86,17 +95,19 @@ __global__ void __launch_bounds__(ST) k_fwd_contrib(DevSym S, const int2 *tasks,
   const int a = r0 + r;
   for (int rhs = 0; rhs < nrhs; ++rhs) {
     const double *yr = y + (size_t)rhs * n + f;
-    double acc0 = 0.0, acc1 = 0.0;
+    double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
     if (a < m) {
       const double *col = Ls_s + a;
       int k = q;
-      for (; k + 4 < w; k += 8) {
+      for (; k + 12 < w; k += 16) {   // four independent loads in flight per thread
         acc0 = fma(col[(size_t)k * m], yr[k], acc0);
         acc1 = fma(col[(size_t)(k + 4) * m], yr[k + 4], acc1);
+        acc2 = fma(col[(size_t)(k + 8) * m], yr[k + 8], acc2);
+        acc3 = fma(col[(size_t)(k + 12) * m], yr[k + 12], acc3);
       }
-      if (k < w) acc0 = fma(col[(size_t)k * m], yr[k], acc0);
+      for (; k < w; k += 4) acc0 = fma(col[(size_t)k * m], yr[k], acc0);
     }
-    part[q][r] = acc0 + acc1;
+    part[q][r] = (acc0 + acc1) + (acc2 + acc3);
     __syncthreads();
     if (q == 0 && a < m)
       contrib[(size_t)rhs * cstride + (rb - f) + (a - w)] =
@@ -110,8 +121,10 @@ __global__ void __launch_bounds__(ST) k_fwd_contrib(DevSym S, const int2 *tasks,
 //                 j0..j0+31 of s (one warp per column); the rows below are columns of
 //                 ancestors, already solved.
 //   k_bwd_diag    x[cols of s] := L_ss^{-T} x[cols of s], one CTA per supernode.
+constexpr int GCH = 1024;   // gathered rows staged per chunk
 __global__ void __launch_bounds__(ST) k_bwd_gather(DevSym S, const int2 *tasks, double *x,
                                                    int n, int nrhs) {
+  __shared__ double xg[GCH];
   const int s = tasks[blockIdx.x].x, j0 = tasks[blockIdx.x].y;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int f = S.super[s], w = S.super[s + 1] - f;
@@ -119,21 +132,51 @@ __global__ void __launch_bounds__(ST) k_bwd_gather(DevSym S, const int2 *tasks, 
   const int m = (int)(S.rowptr[s + 1] - rb);
   const int *rows = S.Ls + rb;
   const double *Ls_s = S.L + S.xptr[s];
+  // every column of this CTA reads the same x[rows[a]]: gather them once per chunk
   for (int rhs = 0; rhs < nrhs; ++rhs) {
     double *xr = x + (size_t)rhs * n;
-    for (int j = j0 + warp; j < min(w, j0 + SB); j += ST / 32) {
-      double acc = 0.0;
-      for (int a = w + lane; a < m; a += 32) acc = fma(Ls_s[(size_t)j * m + a], xr[rows[a]], acc);
+    const int j = j0 + warp;   // ST / 32 == 8 columns per CTA pass; SB == 32 columns per task
+    double acc[SB / (ST / 32)][4];
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-      if (lane == 0) xr[f + j] -= acc;
+    for (int u = 0; u < SB / (ST / 32); ++u)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[u][e] = 0.0;
+    for (int a0 = w; a0 < m; a0 += GCH) {
+      const int len = min(GCH, m - a0);
+      __syncthreads();
+      for (int i = threadIdx.x; i < len; i += ST) xg[i] = xr[rows[a0 + i]];
+      __syncthreads();
+#pragma unroll
+      for (int u = 0; u < SB / (ST / 32); ++u) {
+        const int jj = j + u * (ST / 32);
+        if (jj >= min(w, j0 + SB)) continue;
+        const double *col = Ls_s + (size_t)jj * m + a0;
+        int i = lane;
+        for (; i + 96 < len; i += 128) {
+          acc[u][0] = fma(col[i], xg[i], acc[u][0]);
+          acc[u][1] = fma(col[i + 32], xg[i + 32], acc[u][1]);
+          acc[u][2] = fma(col[i + 64], xg[i + 64], acc[u][2]);
+          acc[u][3] = fma(col[i + 96], xg[i + 96], acc[u][3]);
+        }
+        for (; i < len; i += 32) acc[u][0] = fma(col[i], xg[i], acc[u][0]);
+      }
     }
+#pragma unroll
+    for (int u = 0; u < SB / (ST / 32); ++u) {
+      const int jj = j + u * (ST / 32);
+      double t = (acc[u][0] + acc[u][1]) + (acc[u][2] + acc[u][3]);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+      if (lane == 0 && jj < min(w, j0 + SB)) xr[f + jj] -= t;
+    }
+    __syncthreads();   // xr of these columns written before the next right-hand side gathers
   }
 }
 
 __global__ void __launch_bounds__(ST) k_bwd_diag(DevSym S, const int *list, double *x, int n,
                                                  int nrhs) {
   extern __shared__ double v[];
+  __shared__ double blk[SB * (SB + 1)];
   const int s = list[blockIdx.x];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int f = S.super[s], w = S.super[s + 1] - f;
@@ -154,14 +197,18 @@ __global__ void __launch_bounds__(ST) k_bwd_diag(DevSym S, const int *list, doub
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
         if (lane == 0) v[j] -= acc;
       }
+      for (int e = tid; e < jb * jb; e += ST) {
+        const int j = e / jb, i = e - j * jb;
+        blk[j * (SB + 1) + i] = Ls_s[(size_t)(j0 + j) * m + j0 + i];
+      }
       __syncthreads();
       if (warp == 0) {
+        const double rdl = (lane < jb) ? 1.0 / blk[lane * (SB + 1) + lane] : 0.0;
         double xv = (lane < jb) ? v[j0 + lane] : 0.0;
         for (int jj = jb - 1; jj >= 0; --jj) {
-          const double xj = __shfl_sync(0xffffffffu, xv, jj) /
-                            Ls_s[(size_t)(j0 + jj) * m + j0 + jj];
-          if (lane == jj) xv = xj;
-          if (lane < jj) xv = fma(-Ls_s[(size_t)(j0 + lane) * m + j0 + jj], xj, xv);
+          if (lane == jj) xv *= rdl;
+          const double xj = __shfl_sync(0xffffffffu, xv, jj);
+          if (lane < jj) xv = fma(-blk[lane * (SB + 1) + jj], xj, xv);
         }
         if (lane < jb) v[j0 + lane] = xv;
       }
