@@ -309,7 +309,7 @@ class Handle:
             b = np.asarray(b, np.float64)
             nrhs = 1 if b.ndim == 1 else b.shape[1]
             b = np.asfortranarray(b)
-            x = np.zeros_like(b, order="F")
+            x = out if out is not None else np.zeros_like(b, order="F")
         berr = np.zeros(nrhs)
         it, meth = ctypes.c_int(0), ctypes.c_int(0)
         _check(self._lib.swc_refine(self._h, _p(b), _p(x), int(nrhs), 1 if on_dev else 0,

@@ -39,25 +39,24 @@ void set_last_error(const std::string &msg) { g_err = msg; }
 }  // namespace swc
 
 namespace {
-// Runs fn on device copies of host right-hand sides (and copies x back) when needed.
+// Runs fn on device copies of host right-hand sides (and copies x back) when needed; the
+// copies go through the handle's staging buffer (allocated once, grown on demand).
 template <typename F>
 int with_device_vectors(swc_handle_t h, const double *b, double *x, int nrhs, int on_device, F fn) {
-  const size_t bytes = sizeof(double) * (size_t)h->eng->n() * nrhs;
   if (on_device) return fn(b, x);
-  double *db = nullptr, *dx = nullptr;
-  cudaError_t e = cudaMalloc(&db, bytes);
-  if (e == cudaSuccess) e = cudaMalloc(&dx, bytes);
-  if (e == cudaSuccess) e = cudaMemcpy(db, b, bytes, cudaMemcpyHostToDevice);
-  int rc = SWC_CUDA_ERROR;
-  if (e == cudaSuccess) {
-    rc = fn(db, dx);
-    if (rc == SWC_OK && cudaMemcpy(x, dx, bytes, cudaMemcpyDeviceToHost) != cudaSuccess)
-      rc = fail(SWC_CUDA_ERROR, "copy of the solution to the host failed");
-  } else {
-    rc = fail(SWC_CUDA_ERROR, std::string("solve buffers: ") + cudaGetErrorString(e));
-  }
-  if (db) cudaFree(db);
-  if (dx) cudaFree(dx);
+  const size_t len = (size_t)h->eng->n() * nrhs;
+  std::string err;
+  double *stage = h->eng->staging(2 * len, err);
+  if (!stage) return fail(SWC_CUDA_ERROR, err);
+  double *db = stage, *dx = stage + len;
+  cudaStream_t st = h->eng->stream();
+  if (cudaMemcpyAsync(db, b, sizeof(double) * len, cudaMemcpyHostToDevice, st) != cudaSuccess)
+    return fail(SWC_CUDA_ERROR, "copy of the right-hand sides to the device failed");
+  int rc = fn(db, dx);
+  if (rc == SWC_OK &&
+      (cudaMemcpyAsync(x, dx, sizeof(double) * len, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+       cudaStreamSynchronize(st) != cudaSuccess))
+    rc = fail(SWC_CUDA_ERROR, "copy of the solution to the host failed");
   return rc;
 }
 }  // namespace

@@ -124,6 +124,7 @@ Engine::Engine(int device) : device_(device) {
 
 Engine::~Engine() {
   release();
+  if (d_stage_) cudaFree(d_stage_);
   if (h_status_) cudaFreeHost(h_status_);
   if (h_norms_) cudaFreeHost(h_norms_);
   if (own_stream_) cudaStreamDestroy(own_stream_);
@@ -779,6 +780,23 @@ bool Engine::download(double *lValues, bool to_device, std::string &err) {
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
   if (e != cudaSuccess) { err = std::string("download: ") + cudaGetErrorString(e); return false; }
   return true;
+}
+
+double *Engine::staging(size_t doubles, std::string &err) {
+  cudaSetDevice(device_);
+  if (doubles > stage_len_) {
+    if (d_stage_) cudaFree(d_stage_);
+    d_stage_ = nullptr;
+    stage_len_ = 0;
+    cudaError_t e = cudaMalloc(&d_stage_, sizeof(double) * doubles);
+    if (e != cudaSuccess) {
+      d_stage_ = nullptr;
+      err = std::string("staging buffer: ") + cudaGetErrorString(e);
+      return nullptr;
+    }
+    stage_len_ = doubles;
+  }
+  return d_stage_;
 }
 
 bool Engine::ensure_work(int nrhs, std::string &err) {

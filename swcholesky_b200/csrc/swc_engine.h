@@ -167,6 +167,9 @@ class Engine {
   // refinement stalls); device pointers.
   bool refine(const double *b, double *x, int nrhs, double tol, int maxit, RefineInfo &info,
               std::string &err);
+  // Device staging buffer of at least `doubles` entries (host-vector calls of the C ABI);
+  // allocated on first use and grown when needed, freed with the engine.  nullptr on error.
+  double *staging(size_t doubles, std::string &err);
   int64_t h2d_bytes() const { return h2d_bytes_; }
   int64_t d2h_bytes() const { return d2h_bytes_; }
   bool download(double *lValues, bool to_device, std::string &err);
@@ -259,6 +262,8 @@ class Engine {
   int64_t csr_nnz_ = 0;
   double *d_contrib_ = nullptr, *d_work_ = nullptr, *d_norms_ = nullptr, *h_norms_ = nullptr;
   double *d_npart_ = nullptr;   // slices of the norm reductions
+  double *d_stage_ = nullptr;
+  size_t stage_len_ = 0;
   int work_nrhs_ = 0;
   double anorm_ = 0.0;
   bool ensure_work(int nrhs, std::string &err);
