@@ -80,12 +80,14 @@ __global__ void __launch_bounds__(ST) k_fwd_diag(DevSym S, const int *list, doub
 }
 
 // task = (s, r0): rows r0..r0+63 of supernode s's off-diagonal block (r0 >= w); thread
-// (row r, group q) sums the columns k = q (mod 4), and the four partial sums meet in shared
-// memory in a fixed order.
-__global__ void __launch_bounds__(ST) k_fwd_contrib(DevSym S, const int2 *tasks,
+// (row r, group q) sums the columns k = q (mod CQ), and the CQ partial sums meet in shared
+// memory in a fixed order.  CT = 1024 threads keep enough loads in flight to stream the
+// panel from HBM when a level holds only a few wide supernodes.
+constexpr int CT = 1024, CQ = CT / TB;
+__global__ void __launch_bounds__(CT) k_fwd_contrib(DevSym S, const int2 *tasks,
                                                     const double *y, double *contrib, int n,
                                                     int nrhs, int64_t cstride) {
-  __shared__ double part[4][TB];
+  __shared__ double part[CQ][TB];
   const int s = tasks[blockIdx.x].x, r0 = tasks[blockIdx.x].y;
   const int f = S.super[s], w = S.super[s + 1] - f;
   const int64_t rb = S.rowptr[s];
@@ -95,23 +97,24 @@ __global__ void __launch_bounds__(ST) k_fwd_contrib(DevSym S, const int2 *tasks,
   const int a = r0 + r;
   for (int rhs = 0; rhs < nrhs; ++rhs) {
     const double *yr = y + (size_t)rhs * n + f;
-    double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
+    double acc0 = 0.0, acc1 = 0.0;
     if (a < m) {
       const double *col = Ls_s + a;
       int k = q;
-      for (; k + 12 < w; k += 16) {   // four independent loads in flight per thread
+      for (; k + CQ < w; k += 2 * CQ) {
         acc0 = fma(col[(size_t)k * m], yr[k], acc0);
-        acc1 = fma(col[(size_t)(k + 4) * m], yr[k + 4], acc1);
-        acc2 = fma(col[(size_t)(k + 8) * m], yr[k + 8], acc2);
-        acc3 = fma(col[(size_t)(k + 12) * m], yr[k + 12], acc3);
+        acc1 = fma(col[(size_t)(k + CQ) * m], yr[k + CQ], acc1);
       }
-      for (; k < w; k += 4) acc0 = fma(col[(size_t)k * m], yr[k], acc0);
+      if (k < w) acc0 = fma(col[(size_t)k * m], yr[k], acc0);
     }
-    part[q][r] = (acc0 + acc1) + (acc2 + acc3);
+    part[q][r] = acc0 + acc1;
     __syncthreads();
-    if (q == 0 && a < m)
-      contrib[(size_t)rhs * cstride + (rb - f) + (a - w)] =
-          (part[0][r] + part[1][r]) + (part[2][r] + part[3][r]);
+    if (q == 0 && a < m) {
+      double t = 0.0;
+#pragma unroll
+      for (int g = 0; g < CQ; ++g) t += part[g][r];
+      contrib[(size_t)rhs * cstride + (rb - f) + (a - w)] = t;
+    }
     __syncthreads();
   }
 }
@@ -121,8 +124,9 @@ __global__ void __launch_bounds__(ST) k_fwd_contrib(DevSym S, const int2 *tasks,
 //                 j0..j0+31 of s (one warp per column); the rows below are columns of
 //                 ancestors, already solved.
 //   k_bwd_diag    x[cols of s] := L_ss^{-T} x[cols of s], one CTA per supernode.
-constexpr int GCH = 1024;   // gathered rows staged per chunk
-__global__ void __launch_bounds__(ST) k_bwd_gather(DevSym S, const int2 *tasks, double *x,
+constexpr int GCH = 2048;       // gathered rows staged per chunk
+constexpr int GT = 32 * SB;     // one warp per column of the task
+__global__ void __launch_bounds__(GT) k_bwd_gather(DevSym S, const int2 *tasks, double *x,
                                                    int n, int nrhs) {
   __shared__ double xg[GCH];
   const int s = tasks[blockIdx.x].x, j0 = tasks[blockIdx.x].y;
@@ -132,44 +136,34 @@ __global__ void __launch_bounds__(ST) k_bwd_gather(DevSym S, const int2 *tasks, 
   const int m = (int)(S.rowptr[s + 1] - rb);
   const int *rows = S.Ls + rb;
   const double *Ls_s = S.L + S.xptr[s];
+  const int j = j0 + warp;
+  const bool own = j < w;
   // every column of this CTA reads the same x[rows[a]]: gather them once per chunk
   for (int rhs = 0; rhs < nrhs; ++rhs) {
     double *xr = x + (size_t)rhs * n;
-    const int j = j0 + warp;   // ST / 32 == 8 columns per CTA pass; SB == 32 columns per task
-    double acc[SB / (ST / 32)][4];
-#pragma unroll
-    for (int u = 0; u < SB / (ST / 32); ++u)
-#pragma unroll
-      for (int e = 0; e < 4; ++e) acc[u][e] = 0.0;
+    double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
     for (int a0 = w; a0 < m; a0 += GCH) {
       const int len = min(GCH, m - a0);
       __syncthreads();
-      for (int i = threadIdx.x; i < len; i += ST) xg[i] = xr[rows[a0 + i]];
+      for (int i = threadIdx.x; i < len; i += GT) xg[i] = xr[rows[a0 + i]];
       __syncthreads();
-#pragma unroll
-      for (int u = 0; u < SB / (ST / 32); ++u) {
-        const int jj = j + u * (ST / 32);
-        if (jj >= min(w, j0 + SB)) continue;
-        const double *col = Ls_s + (size_t)jj * m + a0;
+      if (own) {
+        const double *col = Ls_s + (size_t)j * m + a0;
         int i = lane;
         for (; i + 96 < len; i += 128) {
-          acc[u][0] = fma(col[i], xg[i], acc[u][0]);
-          acc[u][1] = fma(col[i + 32], xg[i + 32], acc[u][1]);
-          acc[u][2] = fma(col[i + 64], xg[i + 64], acc[u][2]);
-          acc[u][3] = fma(col[i + 96], xg[i + 96], acc[u][3]);
+          acc0 = fma(col[i], xg[i], acc0);
+          acc1 = fma(col[i + 32], xg[i + 32], acc1);
+          acc2 = fma(col[i + 64], xg[i + 64], acc2);
+          acc3 = fma(col[i + 96], xg[i + 96], acc3);
         }
-        for (; i < len; i += 32) acc[u][0] = fma(col[i], xg[i], acc[u][0]);
+        for (; i < len; i += 32) acc0 = fma(col[i], xg[i], acc0);
       }
     }
+    double t = (acc0 + acc1) + (acc2 + acc3);
 #pragma unroll
-    for (int u = 0; u < SB / (ST / 32); ++u) {
-      const int jj = j + u * (ST / 32);
-      double t = (acc[u][0] + acc[u][1]) + (acc[u][2] + acc[u][3]);
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-      if (lane == 0 && jj < min(w, j0 + SB)) xr[f + jj] -= t;
-    }
-    __syncthreads();   // xr of these columns written before the next right-hand side gathers
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (lane == 0 && own) xr[f + j] -= t;
+    __syncthreads();   // these columns are written before the next right-hand side gathers
   }
 }
 
@@ -520,11 +514,11 @@ void launch_fwd_diag(const DevSym &S, const int *list, int count, int smem, doub
 }
 void launch_fwd_contrib(const DevSym &S, const int2 *tasks, int count, const double *y,
                         double *contrib, int n, int nrhs, int64_t cstride, cudaStream_t st) {
-  if (count > 0) k_fwd_contrib<<<count, ST, 0, st>>>(S, tasks, y, contrib, n, nrhs, cstride);
+  if (count > 0) k_fwd_contrib<<<count, CT, 0, st>>>(S, tasks, y, contrib, n, nrhs, cstride);
 }
 void launch_bwd_gather(const DevSym &S, const int2 *tasks, int count, double *x, int n, int nrhs,
                        cudaStream_t st) {
-  if (count > 0) k_bwd_gather<<<count, ST, 0, st>>>(S, tasks, x, n, nrhs);
+  if (count > 0) k_bwd_gather<<<count, GT, 0, st>>>(S, tasks, x, n, nrhs);
 }
 void launch_bwd_diag(const DevSym &S, const int *list, int count, int smem, double *x, int n,
                      int nrhs, cudaStream_t st) {
