@@ -137,6 +137,24 @@ def reference_time(A, perm_in, threads, budget_s, max_reps, min_reps=1):
     return float(np.median(times)), len(times), sym
 
 
+def max_over_ranks(value: float, world: int, device) -> float:
+    """The largest `value` over all ranks (every rank gets it); the job's time is its
+    slowest rank's time."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def batch_seed(rank: int) -> int:
+    """Seed of a rank's own batch in the batched workload (weak scaling: every rank
+    factors a different batch of the same size and size distribution)."""
+    return rank
+
+
 def profile_traffic(kernel: str, workload: str):
     """DRAM bytes per launch of `kernel` on `workload` from the committed ncu summary
     (profiles/<kernel>_<workload>.md, line 'traffic_bytes_per_launch: N'), else None."""
@@ -254,11 +272,7 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
         barrier()
         ms = e0.elapsed_time(e1) / steps
-        if world > 1:
-            t = torch.tensor([ms], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return max_over_ranks(ms, world, dev)
 
     last = {}
 
@@ -426,7 +440,7 @@ def run_batch(args, rank, world, local_rank):
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
-    src, sides = W.batch_sources(seed=rank)
+    src, sides = W.batch_sources(seed=batch_seed(rank))
     mats = [M.permute_lower(A, p) for A, p in src]
     nmat = len(mats)
     vals_host = np.concatenate([m.data for m in mats])
@@ -455,11 +469,7 @@ def run_batch(args, rank, world, local_rank):
         torch.cuda.synchronize()
         barrier()
         ms = e0.elapsed_time(e1) / steps
-        if world > 1:
-            t = torch.tensor([ms], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return max_over_ranks(ms, world, dev)
 
     res = {}
     for name, mode in (("fp64", swc.SWC_MODE_FP64), ("mixed", swc.SWC_MODE_MIXED_TF32X3)):
