@@ -32,7 +32,7 @@ def load(name: str, batch_count: int = 256):
         mats = [M.permute_lower(A, p) for A, p in src]
         return mats, np.concatenate([m.data for m in mats])
     A, perm, _ = W.build(name)
-    fx = os.path.join(GOLDEN, f"sym_{name}.npz")
+    fx = os.path.join(GOLDEN, f"sym_{name[:-3] if name.endswith('c10') else name}.npz")
     if os.path.exists(fx):
         g = dict(np.load(fx))
         P = W.assemble(A, g["perm"], g["super"])

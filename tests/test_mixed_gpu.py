@@ -41,3 +41,27 @@ def test_mixed_factor_then_refine(cuda_ok, name, lbound):
     for k in range(2):
         r = O.oracle_symv(P.n, P.A2p, P.A2i, P.A2x, x[:, k]) - b[:, k]
         assert np.abs(r).max() / (anorm * np.abs(x[:, k]).max()) <= 1e-14
+
+
+@pytest.mark.parametrize("name", ["stencil27_40", "stencil27_40c10"])
+def test_stencil27_40_eight_rhs(cuda_ok, name):
+    """The 3-dof 27-point stencil on 40^3 (n = 192,000) at cond ~1e6 and ~1e10: split-TF32
+    factor, FP64 refinement (CG with the factor as preconditioner when refinement stalls)
+    of 8 right-hand sides to backward error <= 1e-12 each; per right-hand side the forward
+    difference from the FP64 factor's refined solution stays within cond * 1e-13."""
+    import torch
+    gs = load_sym("stencil27_40")          # the c10 variant shares the structure
+    A, _, meta = W.build(name)
+    P = W.assemble(A, gs["perm"], gs["super"])
+    h = swc.Handle(0)
+    h.analyze(P.n, P.A2p, P.A2i, P.lC, P.Ls, P.Li_ptr, P.super, P.prunePtr, P.pruneSet)
+    v = torch.tensor(P.A2x, dtype=torch.float64, device="cuda")
+    rng = np.random.default_rng(8)
+    b = torch.tensor(rng.standard_normal((8, P.n)), dtype=torch.float64, device="cuda")
+    assert h.factor(v, swc.SWC_MODE_FP64) == 0
+    x64, berr64, _, _ = h.refine(b, tol=1e-14, maxit=30)
+    assert h.factor(v, swc.SWC_MODE_MIXED_TF32X3) == 0
+    xmx, berr, iters, method = h.refine(b, tol=1e-12, maxit=60)
+    assert berr.shape == (8,) and berr.max() <= 1e-12, (berr, iters, method)
+    fwd = ((xmx - x64).abs().amax(dim=1) / x64.abs().amax(dim=1)).cpu().numpy()
+    assert fwd.max() <= meta["cond"] * 1e-13, fwd
