@@ -209,15 +209,16 @@ def run_reference(args, rank, world):
     print(json.dumps(line))
 
 
-def tf32_gemm_peak(torch, dev):
-    """Dense TF32 GEMM throughput measured with cuBLAS (torch.matmul on float32 with TF32
-    allowed, 8192^3), best of 5; a split-TF32 product costs three TF32 products, so its
-    peak is a third of this."""
+def tf32_gemm_peak(torch, dev, bf16: bool = False):
+    """Dense TF32 (or BF16) GEMM throughput measured with cuBLAS (torch.matmul, 8192^3),
+    best of 5; a split-TF32 product costs three TF32 products and a BF16x3 product six BF16
+    products, so their peaks are a third / a sixth of this."""
     n = 8192
     prev = torch.backends.cuda.matmul.allow_tf32
     torch.backends.cuda.matmul.allow_tf32 = True
-    a = torch.randn(n, n, dtype=torch.float32, device=dev)
-    b = torch.randn(n, n, dtype=torch.float32, device=dev)
+    dt = torch.bfloat16 if bf16 else torch.float32
+    a = torch.randn(n, n, dtype=dt, device=dev)
+    b = torch.randn(n, n, dtype=dt, device=dev)
     for _ in range(2):
         torch.matmul(a, b)
     torch.cuda.synchronize()
@@ -258,8 +259,9 @@ def run_ours(args, rank, world, local_rank):
     b = torch.from_numpy(b_host).to(dev)
     x = torch.zeros_like(b)
     stream = torch.cuda.ExternalStream(h.stream, device=dev)
-    mixed = args.mode == "mixed"
-    mode = swc.SWC_MODE_MIXED_TF32X3 if mixed else swc.SWC_MODE_FP64
+    mode = {"fp64": swc.SWC_MODE_FP64, "mixed": swc.SWC_MODE_MIXED_TF32X3,
+            "bf16": swc.SWC_MODE_MIXED_BF16X3}[args.mode]
+    mixed = mode != swc.SWC_MODE_FP64
 
     def barrier():
         if world > 1:
@@ -317,10 +319,15 @@ def run_ours(args, rank, world, local_rank):
     dom = max(kinds, key=lambda k: kinds[k][1])
     la, kms, kfl, kby = kinds[dom]
     peak64 = fp64_gemm_peak(torch, dev) if rank == 0 else None
-    peak32 = tf32_gemm_peak(torch, dev) if rank == 0 and mixed else None
-    if mixed and dom in ("update", "syrk"):
-        peak, psrc = peak32 / 3.0, ("cuBLAS TF32 GEMM 8192^3 measured in this run, divided by 3 "
-                                    "(a split-TF32 product costs three TF32 products)")
+    bf16 = mode == swc.SWC_MODE_MIXED_BF16X3
+    peak32 = tf32_gemm_peak(torch, dev, bf16) if rank == 0 and mixed else None
+    if mixed and dom == "update":
+        if bf16:
+            peak, psrc = peak32 / 6.0, ("cuBLAS BF16 GEMM 8192^3 measured in this run, divided by 6 "
+                                        "(a BF16x3 product costs six BF16 products)")
+        else:
+            peak, psrc = peak32 / 3.0, ("cuBLAS TF32 GEMM 8192^3 measured in this run, divided by 3 "
+                                        "(a split-TF32 product costs three TF32 products)")
     else:
         peak, psrc = peak64, "FP64 cuBLAS DGEMM 8192^3 measured in this run"
 
@@ -395,7 +402,7 @@ def run_ours(args, rank, world, local_rank):
             "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64+tf32x3" if mixed else "f64",
+            "dtype": {"fp64": "f64", "mixed": "f64+tf32x3", "bf16": "f64+bf16x3"}[args.mode],
             "data": "synthetic (seeded generator; reference symbolic phase via fixture)",
             "config": {"workload": args.workload, "n": P.n, "nnz_lower": int(P.A2p[-1]),
                        "nsuper": P.nsuper, "xsize": P.xsize, "fl": fl, "mode": args.mode,
@@ -574,7 +581,8 @@ def main():
     ap.add_argument("--workload", default="grid3d_60")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--mode", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--mode", default="mixed", choices=["mixed", "bf16", "fp64"],
+                    help="mixed: split-TF32 Schur updates; bf16: BF16x3; fp64")
     ap.add_argument("--nrhs", type=int, default=1, help="right-hand sides per refined solve")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

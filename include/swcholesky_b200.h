@@ -32,6 +32,9 @@ extern "C" {
 #define SWC_MODE_MIXED_TF32X3 1 /* Schur updates of the wide supernodes as split-TF32 tensor-core
                                    products (FP32-class accuracy, FP32/FP64 accumulation); POTRF,
                                    TRSM and small supernodes in FP64.  Pair with swc_refine. */
+#define SWC_MODE_MIXED_BF16X3 2 /* the same Schur updates as BF16x3 split products: each value as
+                                   three bfloat16 pieces, the six piece products down to the
+                                   third order, FP32 accumulation (about FP32 accuracy) */
 
 typedef struct swc_handle *swc_handle_t;
 

@@ -33,6 +33,7 @@ SWC_STRUCTURE_ERROR = 4
 SWC_NOT_READY = 5
 SWC_MODE_FP64 = 0
 SWC_MODE_MIXED_TF32X3 = 1
+SWC_MODE_MIXED_BF16X3 = 2
 
 # every symbol include/swcholesky_b200.h declares
 EXPORTS = (

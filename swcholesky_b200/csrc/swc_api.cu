@@ -126,12 +126,12 @@ int swc_analyze(swc_handle_t h, int n, const int *c, const int *r, const size_t 
 int swc_factor(swc_handle_t h, const double *values, int values_on_device, int mode, int *info) {
   if (!h) return fail(SWC_INVALID_INPUT, "null handle");
   if (!h->analyzed) return fail(SWC_NOT_READY, "factor before analyze");
-  if (mode != SWC_MODE_FP64 && mode != SWC_MODE_MIXED_TF32X3)
+  if (mode != SWC_MODE_FP64 && mode != SWC_MODE_MIXED_TF32X3 && mode != SWC_MODE_MIXED_BF16X3)
     return fail(SWC_INVALID_INPUT, "unknown factorization mode");
   if (!values) return fail(SWC_INVALID_INPUT, "null values");
   std::string err;
   int lin = 0;
-  int rc = h->eng->factor(values, values_on_device != 0, &lin, err, mode == SWC_MODE_MIXED_TF32X3);
+  int rc = h->eng->factor(values, values_on_device != 0, &lin, err, mode);
   if (info) *info = lin;
   if (rc == 0) {
     h->factored = true;
@@ -251,7 +251,7 @@ int swc_batch_autotune(swc_handle_t h, const double *values, int values_on_devic
                        const char *cache_path, int *choice, double *best_ms) {
   if (!h) return fail(SWC_INVALID_INPUT, "null handle");
   if (!h->batch || !h->analyzed) return fail(SWC_NOT_READY, "autotune before swc_batch_analyze");
-  if (mode != SWC_MODE_FP64 && mode != SWC_MODE_MIXED_TF32X3)
+  if (mode != SWC_MODE_FP64 && mode != SWC_MODE_MIXED_TF32X3 && mode != SWC_MODE_MIXED_BF16X3)
     return fail(SWC_INVALID_INPUT, "unknown factorization mode");
   if (!values) return fail(SWC_INVALID_INPUT, "null values");
   const size_t bytes = sizeof(double) * h->batch->cp[h->batch->N];
@@ -267,7 +267,7 @@ int swc_batch_autotune(swc_handle_t h, const double *values, int values_on_devic
   }
   std::string err;
   h->factored = false;
-  const bool ok = h->batch->autotune(*h->eng, dv, mode == SWC_MODE_MIXED_TF32X3, cache_path, 3,
+  const bool ok = h->batch->autotune(*h->eng, dv, mode, cache_path, 3,
                                      choice, best_ms, err);
   if (tmp) cudaFree(tmp);
   if (!ok) {
@@ -340,7 +340,7 @@ int swc_profile(swc_handle_t h, const double *values, int values_on_device, int 
   std::string err;
   int lin = 0;
   int rc = h->eng->factor_profiled(values, values_on_device != 0, &lin, ks, err,
-                                   mode == SWC_MODE_MIXED_TF32X3);
+                                   mode);
   h->factored = (rc == 0);
   if (info) *info = lin;
   for (int k = 0; k < swc::K_NKINDS; ++k) {

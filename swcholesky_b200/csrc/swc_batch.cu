@@ -241,9 +241,9 @@ void cache_store(const std::string &path, uint64_t key, int mode, int part, int 
 
 }  // namespace
 
-bool BatchState::autotune(Engine &eng, const double *d_values, bool mixed, const char *cache_path,
+bool BatchState::autotune(Engine &eng, const double *d_values, int mixed, const char *cache_path,
                           int reps, int *choice, double *best_ms, std::string &err) {
-  const int mode = mixed ? 1 : 0;
+  const int mode = mixed;
   int bp = 0, bl = 0;
   double best = DBL_MAX;
   if (cache_path && cache_lookup(cache_path, key, mode, bp, bl, best)) {

@@ -28,7 +28,7 @@ struct BatchState {
   bool analyze(Engine &eng, int partition, const Tuning &t, std::string &err);
   // Times every candidate on the device values (factor of the whole batch, mean of reps
   // runs after one warm-up) and leaves the engine analysed with the best one.
-  bool autotune(Engine &eng, const double *d_values, bool mixed, const char *cache_path, int reps,
+  bool autotune(Engine &eng, const double *d_values, int mode, const char *cache_path, int reps,
                 int *choice, double *best_ms, std::string &err);
 };
 

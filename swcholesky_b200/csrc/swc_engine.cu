@@ -165,12 +165,12 @@ void Engine::release() {
   d_npart_ = nullptr;
   persist_ctas_ = 0;
   work_nrhs_ = 0;
-  if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
-  if (graph_) cudaGraphDestroy(graph_);
-  if (graph_exec_mx_) cudaGraphExecDestroy(graph_exec_mx_);
-  if (graph_mx_) cudaGraphDestroy(graph_mx_);
-  graph_exec_ = graph_exec_mx_ = nullptr;
-  graph_ = graph_mx_ = nullptr;
+  for (int k = 0; k < 3; ++k) {
+    if (graph_exec_[k]) cudaGraphExecDestroy(graph_exec_[k]);
+    if (graph_[k]) cudaGraphDestroy(graph_[k]);
+    graph_exec_[k] = nullptr;
+    graph_[k] = nullptr;
+  }
   if (d_Lf_) cudaFree(d_Lf_);
   d_Lf_ = nullptr;
 }
@@ -602,7 +602,8 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
   return true;
 }
 
-void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, bool mixed) {
+void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec) {
+  const bool mixed = prec != 0;
   cudaStream_t st = stream_;
   // With profiling on, every launch is preceded by an event and followed by one.
   auto mark = [&](int kind, int count) {
@@ -658,7 +659,7 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, bool mix
         launch_diag_step(sym_, d_diag_ + W.diag_off[j], W.diag_cnt[j], (int)j + 1, st);
         mark(-1, W.diag_cnt[j]);
         mark(K_SYRK, W.syrk_cnt[j]);
-        if (mixed && mx_syrk_) launch_syrk_step_mx(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
+        if (prec == 1 && mx_syrk_) launch_syrk_step_mx(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
         else launch_syrk_step(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
         mark(-1, W.syrk_cnt[j]);
       } else if (W.diag_cnt[j] > 0) {
@@ -667,18 +668,19 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, bool mix
         cudaStreamWaitEvent(aux_stream_, ev_fork_, 0);
         launch_diag_step(sym_, d_diag_ + W.diag_off[j], W.diag_cnt[j], (int)j + 1, aux_stream_);
         cudaEventRecord(ev_join_, aux_stream_);
-        if (mixed && mx_syrk_) launch_syrk_step_mx(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
+        if (prec == 1 && mx_syrk_) launch_syrk_step_mx(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
         else launch_syrk_step(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
         cudaStreamWaitEvent(st, ev_join_, 0);
       } else {
-        if (mixed && mx_syrk_) launch_syrk_step_mx(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
+        if (prec == 1 && mx_syrk_) launch_syrk_step_mx(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
         else launch_syrk_step(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
       }
     }
   }
 }
 
-bool Engine::set_mode(bool mixed, std::string &err) {
+bool Engine::set_mode(int prec, std::string &err) {
+  const bool mixed = prec != 0;
   if (mixed && !d_Lf_) {
     cudaError_t e = cudaMalloc(&d_Lf_, sizeof(float2) * std::max<int64_t>(xsize_, 1));
     if (e != cudaSuccess) {
@@ -688,14 +690,16 @@ bool Engine::set_mode(bool mixed, std::string &err) {
     }
   }
   sym_.Lf = mixed ? d_Lf_ : nullptr;
+  sym_.mirror_kind = prec == 2 ? MIRROR_BF16X3 : MIRROR_TF32X2;
   return true;
 }
 
 int Engine::factor(const double *values, bool values_on_device, int *info, std::string &err,
-                   bool mixed) {
+                   int prec) {
+  if (prec < 0 || prec > 2) { err = "unknown precision mode"; return -1; }
   if (!dL_) { err = "factor before analyze"; return -1; }
   cudaSetDevice(device_);
-  if (!set_mode(mixed, err)) return -1;
+  if (!set_mode(prec, err)) return -1;
   cudaStream_t st = stream_;
   // values always reach the kernels through d_Ax_, so a captured graph stays valid
   cudaError_t e = cudaMemcpyAsync(d_Ax_, values, sizeof(double) * nnz_,
@@ -706,12 +710,12 @@ int Engine::factor(const double *values, bool values_on_device, int *info, std::
   if (use_graph_) {
     // The whole launch sequence is fixed by the structure (and the mode): capture it once
     // per mode, replay it.
-    cudaGraph_t &g = mixed ? graph_mx_ : graph_;
-    cudaGraphExec_t &ge = mixed ? graph_exec_mx_ : graph_exec_;
+    cudaGraph_t &g = graph_[prec];
+    cudaGraphExec_t &ge = graph_exec_[prec];
     if (!ge) {
       e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
       if (e == cudaSuccess) {
-        launch_all(nullptr, mixed);
+        launch_all(nullptr, prec);
         e = cudaStreamEndCapture(st, &g);
       }
       if (e == cudaSuccess) e = cudaGraphInstantiate(&ge, g, 0);
@@ -720,23 +724,24 @@ int Engine::factor(const double *values, bool values_on_device, int *info, std::
     e = cudaGraphLaunch(ge, st);
     if (e != cudaSuccess) { err = std::string("graph launch: ") + cudaGetErrorString(e); return -1; }
   } else {
-    launch_all(nullptr, mixed);
+    launch_all(nullptr, prec);
   }
   return finish(info, err);
 }
 
 int Engine::factor_profiled(const double *values, bool values_on_device, int *info,
-                            KernelStats &out, std::string &err, bool mixed) {
+                            KernelStats &out, std::string &err, int prec) {
+  if (prec < 0 || prec > 2) { err = "unknown precision mode"; return -1; }
   if (!dL_) { err = "factor before analyze"; return -1; }
   cudaSetDevice(device_);
-  if (!set_mode(mixed, err)) return -1;
+  if (!set_mode(prec, err)) return -1;
   cudaStream_t st = stream_;
   cudaError_t e = cudaMemcpyAsync(d_Ax_, values, sizeof(double) * nnz_,
                                   values_on_device ? cudaMemcpyDeviceToDevice
                                                    : cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) { err = std::string("values upload: ") + cudaGetErrorString(e); return -1; }
   std::vector<std::pair<int, cudaEvent_t>> prof;
-  launch_all(&prof, mixed);
+  launch_all(&prof, prec);
   int rc = finish(info, err);
   out = plan_.work;
   for (int k = 0; k < K_NKINDS; ++k) { out.launches[k] = 0; out.ms[k] = 0; }

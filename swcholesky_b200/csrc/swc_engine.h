@@ -28,10 +28,16 @@ struct DevSym {
   int *status;            // [0] = smallest failing column + 1 (INT_MAX if none),
                           // [1] = structure error flag, [2] = solve wait timeout,
                           // [3] = factorization wait timeout (persistent walk)
-  float2 *Lf;             // split-TF32 mirror {hi, lo} of L (mixed-precision only, else null)
+  float2 *Lf;             // split mirror of L (mixed-precision only, else null): per value
+                          // {hi, lo} TF32 pair, or three bfloat16 pieces (mirror_kind)
+  int mirror_kind;        // MIRROR_TF32X2 or MIRROR_BF16X3
   double *dinv;           // scratch: inverses of the 64x64 diagonal blocks of the tiled class
   const int *dinv_off;    // per supernode: first block of its inverses in dinv (-1: none)
 };
+
+// Formats of the split mirror (8 bytes per value).
+constexpr int MIRROR_TF32X2 = 0;   // {hi, lo} floats holding TF32 values
+constexpr int MIRROR_BF16X3 = 1;   // bits: x = hi | mid << 16, y = lo (bfloat16 pieces)
 
 // One level of the schedule (supernodes whose descendants all belong to earlier levels).
 struct Wave {
@@ -150,13 +156,14 @@ class Engine {
                const int *pruneSet, std::string &err);
   // values: the A2 values (host or device).  Returns 0 on success, 1 if not SPD
   // (*info = failing column + 1), <0 on errors.
-  // mixed: Schur updates of the tiled class as split-TF32 tensor-core products.
+  // prec: 0 FP64; 1 / 2: Schur updates of the tiled class as split-TF32 / BF16x3
+  // tensor-core products (the C ABI's mode numbers).
   int factor(const double *values, bool values_on_device, int *info, std::string &err,
-             bool mixed = false);
+             int prec = 0);
   // The same factorization with a CUDA event pair around every launch; fills per-class
   // launch counts and device milliseconds (no other difference).
   int factor_profiled(const double *values, bool values_on_device, int *info,
-                      KernelStats &out, std::string &err, bool mixed = false);
+                      KernelStats &out, std::string &err, int prec = 0);
   // x = (L L^T)^{-1} b for nrhs right-hand sides (device pointers, leading dimension n).
   bool solve(const double *b, double *x, int nrhs, std::string &err);
   // The same solve with the contribution scratch supplied by the caller (capacity in
@@ -215,8 +222,8 @@ class Engine {
   double *d_adj_partial_ = nullptr;
 
   void release();
-  void launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof = nullptr, bool mixed = false);
-  bool set_mode(bool mixed, std::string &err);
+  void launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof = nullptr, int prec = 0);
+  bool set_mode(int prec, std::string &err);
   int finish(int *info, std::string &err);
   int64_t h2d_bytes_ = 0, d2h_bytes_ = 0;
   int device_ = 0;
@@ -237,8 +244,8 @@ class Engine {
   int2 *d_asm_ = nullptr, *d_panel_ = nullptr;
   int4 *d_upd_tasks_ = nullptr, *d_syrk_ = nullptr, *d_pairs_ = nullptr;
   int *d_upd_end_ = nullptr;
-  cudaGraph_t graph_ = nullptr, graph_mx_ = nullptr;
-  cudaGraphExec_t graph_exec_ = nullptr, graph_exec_mx_ = nullptr;
+  cudaGraph_t graph_[3] = {nullptr, nullptr, nullptr};          // one per precision mode
+  cudaGraphExec_t graph_exec_[3] = {nullptr, nullptr, nullptr};
   float2 *d_Lf_ = nullptr;
   bool use_graph_ = true;
   Tuning tuning_;

@@ -21,6 +21,7 @@
 //
 // All arithmetic is FP64; tiles are 64x64 with 256 threads, each thread holding a 4x4
 // register micro-tile.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -52,6 +53,24 @@ __device__ __forceinline__ float2 split_tf32(double x) {
   asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(hi) : "f"(xf));
   asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(lo) : "f"(xf - __uint_as_float(hi)));
   return make_float2(__uint_as_float(hi), __uint_as_float(lo));
+}
+
+// Three bfloat16 pieces of x: hi = bf16(x), mid = bf16(x - hi), lo = bf16(x - hi - mid)
+// (the remainders are exact in FP64), packed as x = hi | mid << 16, y = lo.
+__device__ __forceinline__ float2 split_bf16x3(double x) {
+  const __nv_bfloat16 hi = __float2bfloat16_rn((float)x);
+  const double r1 = x - (double)__bfloat162float(hi);
+  const __nv_bfloat16 mid = __float2bfloat16_rn((float)r1);
+  const double r2 = r1 - (double)__bfloat162float(mid);
+  const __nv_bfloat16 lo = __float2bfloat16_rn((float)r2);
+  const unsigned bx = (unsigned)__bfloat16_as_ushort(hi) | ((unsigned)__bfloat16_as_ushort(mid) << 16);
+  const unsigned by = (unsigned)__bfloat16_as_ushort(lo);
+  return make_float2(__uint_as_float(bx), __uint_as_float(by));
+}
+
+// The mirror entry of value x in the format of this factorization.
+__device__ __forceinline__ float2 mirror_value(const DevSym &S, double x) {
+  return S.mirror_kind == MIRROR_BF16X3 ? split_bf16x3(x) : split_tf32(x);
 }
 
 __device__ __forceinline__ void flag_structure_error(const DevSym &S) {
@@ -169,7 +188,7 @@ __device__ __noinline__ void factor_small_body(const DevSym &S, int s, double *s
   for (int i = tid; i < m * w; i += NT) dst[i] = P[i];
   if (S.Lf) {   // mixed-precision factorization: split mirror for the Schur updates
     float2 *dstf = S.Lf + S.xptr[s];
-    for (int i = tid; i < m * w; i += NT) dstf[i] = split_tf32(P[i]);
+    for (int i = tid; i < m * w; i += NT) dstf[i] = mirror_value(S, P[i]);
   }
 }
 
@@ -840,7 +859,7 @@ __global__ void __launch_bounds__(MT) k_trsm_step(DevSym S, const int2 *tasks, i
         const int c = acc_col(j, e);
         if (c < bw) {
           P[(size_t)(c0 + c) * m + r0 + r] = acc.v[i][j][e];
-          if (S.Lf) S.Lf[S.xptr[s] + (size_t)(c0 + c) * m + r0 + r] = split_tf32(acc.v[i][j][e]);
+          if (S.Lf) S.Lf[S.xptr[s] + (size_t)(c0 + c) * m + r0 + r] = mirror_value(S, acc.v[i][j][e]);
         }
       }
   }
@@ -936,7 +955,7 @@ __device__ void factor_tiny_body(const DevSym &S, int s, double *P, int *rows, i
   for (int i = lane; i < m * w; i += 32) dst[i] = P[i];
   if (S.Lf) {
     float2 *dstf = S.Lf + S.xptr[s];
-    for (int i = lane; i < m * w; i += 32) dstf[i] = split_tf32(P[i]);
+    for (int i = lane; i < m * w; i += 32) dstf[i] = mirror_value(S, P[i]);
   }
 }
 

@@ -94,10 +94,123 @@ __device__ __forceinline__ void load_chunk_f(const float2 *__restrict__ Lf, int 
   cp_commit();
 }
 
-// acc += A B^T over K columns, split-TF32, with A / B rows gathered through ia / ib.
-// rmask / cmask: this warp's non-empty 16-row and 8-column groups.
-__device__ __forceinline__ void tf32x3_product(const float2 *__restrict__ Lf, int ld, const int *ia,
-                                               const int *ib, int K, float2 *stages, Acc32 &acc) {
+__device__ __forceinline__ void mma_bf16(float (&c)[4], const unsigned (&a)[4], const unsigned (&b)[2]) {
+  asm("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// One staged k-chunk, split-TF32: elements are {hi, lo} float pairs; per k8 step the three
+// partial products lo*hi', hi*lo', hi*hi' (each issued over all tiles before the next: the
+// products of one tile depend on each other through the accumulator).
+__device__ __forceinline__ void chunk_tf32(const float2 *As, const float2 *Bs, int wr, int wc,
+                                           int g, int t, unsigned rmask, unsigned cmask,
+                                           Acc32 &acc) {
+#pragma unroll
+  for (int k8 = 0; k8 < KF; k8 += 8) {
+    unsigned ah[2][4], al[2][4], bh[4][2], bl[4][2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int r = wr + 16 * i + g;
+      const float2 x0 = As[(k8 + t) * LDF + r], x1 = As[(k8 + t) * LDF + r + 8];
+      const float2 x2 = As[(k8 + t + 4) * LDF + r], x3 = As[(k8 + t + 4) * LDF + r + 8];
+      ah[i][0] = __float_as_uint(x0.x); al[i][0] = __float_as_uint(x0.y);
+      ah[i][1] = __float_as_uint(x1.x); al[i][1] = __float_as_uint(x1.y);
+      ah[i][2] = __float_as_uint(x2.x); al[i][2] = __float_as_uint(x2.y);
+      ah[i][3] = __float_as_uint(x3.x); al[i][3] = __float_as_uint(x3.y);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int n = wc + 8 * j + g;
+      const float2 y0 = Bs[(k8 + t) * LDF + n], y1 = Bs[(k8 + t + 4) * LDF + n];
+      bh[j][0] = __float_as_uint(y0.x); bl[j][0] = __float_as_uint(y0.y);
+      bh[j][1] = __float_as_uint(y1.x); bl[j][1] = __float_as_uint(y1.y);
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (((rmask >> i) & (cmask >> j)) & 1u) mma_tf32(acc.v[i][j], al[i], bh[j]);
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (((rmask >> i) & (cmask >> j)) & 1u) mma_tf32(acc.v[i][j], ah[i], bl[j]);
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (((rmask >> i) & (cmask >> j)) & 1u) mma_tf32(acc.v[i][j], ah[i], bh[j]);
+  }
+}
+
+// Two BF16x3 elements (bits: x = hi | mid << 16, y = lo) -> one register of component p for
+// the MMA, the element with the lower k index in the low half.
+__device__ __forceinline__ unsigned pack_bf16(uint2 e0, uint2 e1, int p) {
+  return p == 0 ? ((e0.x & 0xffffu) | (e1.x << 16))
+       : p == 1 ? ((e0.x >> 16) | (e1.x & 0xffff0000u))
+                : ((e0.y & 0xffffu) | (e1.y << 16));
+}
+
+// One staged k-chunk, BF16x3: elements are three bfloat16 pieces {hi, mid, lo} (x = hi + mid
+// + lo to about 24 bits); per k16 step the six partial products whose order is at most
+// two pieces below the leading one (lo*hi', mid*mid', hi*lo', mid*hi', hi*mid', hi*hi',
+// small terms first), FP32 accumulation.  Fragment layout of m16n8k16 .bf16: A regs
+// {(g, 2t..2t+1), (g+8, 2t..), (g, 2t+8..), (g+8, 2t+8..)}, B regs {(2t..2t+1, g),
+// (2t+8..2t+9, g)}, g = lane/4, t = lane%4.
+__device__ __forceinline__ void chunk_bf16(const float2 *Asf, const float2 *Bsf, int wr, int wc,
+                                           int g, int t, unsigned rmask, unsigned cmask,
+                                           Acc32 &acc) {
+  const uint2 *As = reinterpret_cast<const uint2 *>(Asf), *Bs = reinterpret_cast<const uint2 *>(Bsf);
+#pragma unroll
+  for (int k16 = 0; k16 < KF; k16 += 16) {
+    unsigned a[3][2][4], b[3][4][2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int r = wr + 16 * i + g;
+      const int k0 = k16 + 2 * t;
+      const uint2 e00 = As[k0 * LDF + r], e01 = As[(k0 + 1) * LDF + r];
+      const uint2 e10 = As[k0 * LDF + r + 8], e11 = As[(k0 + 1) * LDF + r + 8];
+      const uint2 e20 = As[(k0 + 8) * LDF + r], e21 = As[(k0 + 9) * LDF + r];
+      const uint2 e30 = As[(k0 + 8) * LDF + r + 8], e31 = As[(k0 + 9) * LDF + r + 8];
+#pragma unroll
+      for (int p = 0; p < 3; ++p) {
+        a[p][i][0] = pack_bf16(e00, e01, p);
+        a[p][i][1] = pack_bf16(e10, e11, p);
+        a[p][i][2] = pack_bf16(e20, e21, p);
+        a[p][i][3] = pack_bf16(e30, e31, p);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int n = wc + 8 * j + g;
+      const int k0 = k16 + 2 * t;
+      const uint2 f00 = Bs[k0 * LDF + n], f01 = Bs[(k0 + 1) * LDF + n];
+      const uint2 f10 = Bs[(k0 + 8) * LDF + n], f11 = Bs[(k0 + 9) * LDF + n];
+#pragma unroll
+      for (int p = 0; p < 3; ++p) {
+        b[p][j][0] = pack_bf16(f00, f01, p);
+        b[p][j][1] = pack_bf16(f10, f11, p);
+      }
+    }
+    constexpr int PA[6] = {2, 1, 0, 1, 0, 0}, PB[6] = {0, 1, 2, 0, 1, 0};
+#pragma unroll
+    for (int q = 0; q < 6; ++q)
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (((rmask >> i) & (cmask >> j)) & 1u) mma_bf16(acc.v[i][j], a[PA[q]][i], b[PB[q]][j]);
+  }
+}
+
+// acc += A B^T over K columns from the mirror (split-TF32 or BF16x3 by KIND), with A / B
+// rows gathered through ia / ib.  rmask / cmask: this warp's non-empty 16-row and 8-column
+// groups.
+template <int KIND>
+__device__ __forceinline__ void split_product(const float2 *__restrict__ Lf, int ld, const int *ia,
+                                              const int *ib, int K, float2 *stages, Acc32 &acc) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
   const int g = lane >> 2, t = lane & 3;
@@ -122,44 +235,8 @@ __device__ __forceinline__ void tf32x3_product(const float2 *__restrict__ Lf, in
     __syncthreads();
     const float2 *As = stages + (c & 1) * STAGEF, *Bs = As + KF * LDF;
     if (rmask && cmask) {
-#pragma unroll
-      for (int k8 = 0; k8 < KF; k8 += 8) {
-        unsigned ah[2][4], al[2][4], bh[4][2], bl[4][2];
-#pragma unroll
-        for (int i = 0; i < 2; ++i) {
-          const int r = wr + 16 * i + g;
-          const float2 x0 = As[(k8 + t) * LDF + r], x1 = As[(k8 + t) * LDF + r + 8];
-          const float2 x2 = As[(k8 + t + 4) * LDF + r], x3 = As[(k8 + t + 4) * LDF + r + 8];
-          ah[i][0] = __float_as_uint(x0.x); al[i][0] = __float_as_uint(x0.y);
-          ah[i][1] = __float_as_uint(x1.x); al[i][1] = __float_as_uint(x1.y);
-          ah[i][2] = __float_as_uint(x2.x); al[i][2] = __float_as_uint(x2.y);
-          ah[i][3] = __float_as_uint(x3.x); al[i][3] = __float_as_uint(x3.y);
-        }
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const int n = wc + 8 * j + g;
-          const float2 y0 = Bs[(k8 + t) * LDF + n], y1 = Bs[(k8 + t + 4) * LDF + n];
-          bh[j][0] = __float_as_uint(y0.x); bl[j][0] = __float_as_uint(y0.y);
-          bh[j][1] = __float_as_uint(y1.x); bl[j][1] = __float_as_uint(y1.y);
-        }
-        // the three partial products of one tile depend on each other through the
-        // accumulator: issue each over all tiles before the next (8 independent MMAs apart)
-#pragma unroll
-        for (int i = 0; i < 2; ++i)
-#pragma unroll
-          for (int j = 0; j < 4; ++j)
-            if (((rmask >> i) & (cmask >> j)) & 1u) mma_tf32(acc.v[i][j], al[i], bh[j]);
-#pragma unroll
-        for (int i = 0; i < 2; ++i)
-#pragma unroll
-          for (int j = 0; j < 4; ++j)
-            if (((rmask >> i) & (cmask >> j)) & 1u) mma_tf32(acc.v[i][j], ah[i], bl[j]);
-#pragma unroll
-        for (int i = 0; i < 2; ++i)
-#pragma unroll
-          for (int j = 0; j < 4; ++j)
-            if (((rmask >> i) & (cmask >> j)) & 1u) mma_tf32(acc.v[i][j], ah[i], bh[j]);
-      }
+      if (KIND == MIRROR_BF16X3) chunk_bf16(As, Bs, wr, wc, g, t, rmask, cmask, acc);
+      else chunk_tf32(As, Bs, wr, wc, g, t, rmask, cmask, acc);
     }
     __syncthreads();
   }
@@ -168,6 +245,7 @@ __device__ __forceinline__ void tf32x3_product(const float2 *__restrict__ Lf, in
 // Mixed-precision tile-owner update (same tasks and pair lists as the FP64 kernel).
 constexpr int UPDM_SMEM = 2 * STAGEF * 8 + 3 * TB * 4;
 
+template <int KIND>
 __global__ void __launch_bounds__(MXT, 3) k_update_tiles_mx(DevSym S, const int4 *tasks,
                                                            const int *task_end,
                                                            const int4 *pairs, int count) {
@@ -216,7 +294,7 @@ __global__ void __launch_bounds__(MXT, 3) k_update_tiles_mx(DevSym S, const int4
     }
     Acc32 acc;
     acc.zero();
-    tf32x3_product(S.Lf + S.xptr[d], md, ia, ib, wd, stages, acc);
+    split_product<KIND>(S.Lf + S.xptr[d], md, ia, ib, wd, stages, acc);
 #pragma unroll
     for (int i = 0; i < 2; ++i)
 #pragma unroll
@@ -260,7 +338,7 @@ __global__ void __launch_bounds__(MXT, 3) k_syrk_step_mx(DevSym S, const int4 *t
   }
   Acc32 acc;
   acc.zero();
-  tf32x3_product(S.Lf + S.xptr[s] + (size_t)k0 * m, m, ia, ib, bk, stages, acc);
+  split_product<MIRROR_TF32X2>(S.Lf + S.xptr[s] + (size_t)k0 * m, m, ia, ib, bk, stages, acc);
   double *P = S.L + S.xptr[s];
 #pragma unroll
   for (int i = 0; i < 2; ++i)
@@ -277,8 +355,11 @@ __global__ void __launch_bounds__(MXT, 3) k_syrk_step_mx(DevSym S, const int4 *t
 }  // namespace
 
 bool mixed_configure(std::string &err) {
-  cudaError_t e = cudaFuncSetAttribute(k_update_tiles_mx, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       UPDM_SMEM);
+  cudaError_t e = cudaFuncSetAttribute(k_update_tiles_mx<MIRROR_TF32X2>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, UPDM_SMEM);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_update_tiles_mx<MIRROR_BF16X3>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, UPDM_SMEM);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_syrk_step_mx, cudaFuncAttributeMaxDynamicSharedMemorySize, SYRKM_SMEM);
   if (e != cudaSuccess) {
@@ -290,7 +371,11 @@ bool mixed_configure(std::string &err) {
 
 void launch_update_tiles_mx(const DevSym &S, const int4 *tasks, const int *task_end,
                             const int4 *pairs, int count, cudaStream_t st) {
-  if (count > 0) k_update_tiles_mx<<<count, MXT, UPDM_SMEM, st>>>(S, tasks, task_end, pairs, count);
+  if (count <= 0) return;
+  if (S.mirror_kind == MIRROR_BF16X3)
+    k_update_tiles_mx<MIRROR_BF16X3><<<count, MXT, UPDM_SMEM, st>>>(S, tasks, task_end, pairs, count);
+  else
+    k_update_tiles_mx<MIRROR_TF32X2><<<count, MXT, UPDM_SMEM, st>>>(S, tasks, task_end, pairs, count);
 }
 void launch_syrk_step_mx(const DevSym &S, const int4 *tasks, int count, int step, cudaStream_t st) {
   if (count > 0) k_syrk_step_mx<<<count, MXT, SYRKM_SMEM, st>>>(S, tasks, count, step);

@@ -1,4 +1,5 @@
-"""Mixed-precision factorization (split-TF32 Schur updates) followed by FP64 refinement.
+"""Mixed-precision factorization (split-TF32 or BF16x3 Schur updates) followed by FP64
+refinement.
 
 The mixed factor differs from the FP64 one by FP32-class rounding amplified by the
 conditioning (checked: relative difference of L above 1e-12, below 1e-5 for the Laplacian
@@ -15,8 +16,12 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 
+MODES = [swc.SWC_MODE_MIXED_TF32X3, swc.SWC_MODE_MIXED_BF16X3]
+
+
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("name,lbound", [("grid3d_24", 1e-5), ("stencil27_12", 1e-2)])
-def test_mixed_factor_then_refine(cuda_ok, name, lbound):
+def test_mixed_factor_then_refine(cuda_ok, name, lbound, mode):
     gs = load_sym(name)
     A, _, _ = W.build(name)
     P = W.assemble(A, gs["perm"], gs["super"])
@@ -24,12 +29,12 @@ def test_mixed_factor_then_refine(cuda_ok, name, lbound):
     h.analyze(P.n, P.A2p, P.A2i, P.lC, P.Ls, P.Li_ptr, P.super, P.prunePtr, P.pruneSet)
     assert h.factor(P.A2x, swc.SWC_MODE_FP64) == 0
     L64 = h.get_L()
-    assert h.factor(P.A2x, swc.SWC_MODE_MIXED_TF32X3) == 0
+    assert h.factor(P.A2x, mode) == 0
     Lmx = h.get_L()
     rel = np.abs(Lmx - L64).max() / np.abs(L64).max()
     assert 1e-12 < rel < lbound, rel
     # deterministic
-    assert h.factor(P.A2x, swc.SWC_MODE_MIXED_TF32X3) == 0
+    assert h.factor(P.A2x, mode) == 0
     assert np.array_equal(h.get_L(), Lmx)
     rng = np.random.default_rng(0)
     b = rng.standard_normal((P.n, 2))
@@ -43,10 +48,13 @@ def test_mixed_factor_then_refine(cuda_ok, name, lbound):
         assert np.abs(r).max() / (anorm * np.abs(x[:, k]).max()) <= 1e-14
 
 
-@pytest.mark.parametrize("name", ["stencil27_40", "stencil27_40c10"])
-def test_stencil27_40_eight_rhs(cuda_ok, name):
+@pytest.mark.parametrize("name,mode", [("stencil27_40", swc.SWC_MODE_MIXED_TF32X3),
+                                       ("stencil27_40", swc.SWC_MODE_MIXED_BF16X3),
+                                       ("stencil27_40c10", swc.SWC_MODE_MIXED_TF32X3),
+                                       ("stencil27_40c10", swc.SWC_MODE_MIXED_BF16X3)])
+def test_stencil27_40_eight_rhs(cuda_ok, name, mode):
     """The 3-dof 27-point stencil on 40^3 (n = 192,000) at cond ~1e6 and ~1e10: split-TF32
-    factor, FP64 refinement (CG with the factor as preconditioner when refinement stalls)
+    or BF16x3 factor, FP64 refinement (CG with the factor as preconditioner when refinement stalls)
     of 8 right-hand sides to backward error <= 1e-12 each; per right-hand side the forward
     difference from the FP64 factor's refined solution stays within cond * 1e-13."""
     import torch
@@ -60,7 +68,7 @@ def test_stencil27_40_eight_rhs(cuda_ok, name):
     b = torch.tensor(rng.standard_normal((8, P.n)), dtype=torch.float64, device="cuda")
     assert h.factor(v, swc.SWC_MODE_FP64) == 0
     x64, berr64, _, _ = h.refine(b, tol=1e-14, maxit=30)
-    assert h.factor(v, swc.SWC_MODE_MIXED_TF32X3) == 0
+    assert h.factor(v, mode) == 0
     xmx, berr, iters, method = h.refine(b, tol=1e-12, maxit=60)
     assert berr.shape == (8,) and berr.max() <= 1e-12, (berr, iters, method)
     fwd = ((xmx - x64).abs().amax(dim=1) / x64.abs().amax(dim=1)).cpu().numpy()
