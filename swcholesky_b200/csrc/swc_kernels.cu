@@ -171,8 +171,8 @@ __device__ __noinline__ void factor_small_body(const DevSym &S, int s, double *s
   for (int j = 0; j < w; ++j) {
     __syncthreads();
     const double piv = P[(size_t)j * m + j];
-    const double dsq = sqrt(piv);
-    const double inv = 1.0 / dsq;
+    const double inv = rsqrt(piv);
+    const double dsq = piv * inv;
     if (tid == 0 && !(piv > 0.0)) atomicMin(&S.status[0], f + j + 1);
     for (int i = j + tid; i < w; i += NT) colv[i] = (i == j) ? dsq : P[(size_t)j * m + i] * inv;
     __syncthreads();
@@ -593,7 +593,7 @@ __device__ void potrf8_inv8(double *D, double *E, int kb, const DevSym &S, int g
     const int qc = c >> 1;
     const bool odd = c & 1;
     const double piv = __shfl_sync(FULL, odd ? x1 : x0, 4 * c + qc);
-    const double dsq = sqrt(piv), inv = 1.0 / dsq;
+    const double inv = rsqrt(piv), dsq = piv * inv;
     if (report && lane == 0 && k0 + c < bw && !(piv > 0.0))
       atomicMin(&S.status[0], gcol0 + k0 + c + 1);
     if (q == qc && r >= c) {
@@ -939,7 +939,7 @@ __device__ void factor_tiny_body(const DevSym &S, int s, double *P, int *rows, i
   // right-looking POTRF + TRSM of the m x w panel, lanes along the rows
   for (int j = 0; j < w; ++j) {
     const double piv = P[(size_t)j * m + j];
-    const double dsq = sqrt(piv), inv = 1.0 / dsq;
+    const double inv = rsqrt(piv), dsq = piv * inv;
     if (lane == 0 && !(piv > 0.0)) atomicMin(&S.status[0], f + j + 1);
     __syncwarp();
     for (int i = j + lane; i < m; i += 32) P[(size_t)j * m + i] = (i == j) ? dsq : P[(size_t)j * m + i] * inv;
