@@ -659,8 +659,7 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec
         launch_diag_step(sym_, d_diag_ + W.diag_off[j], W.diag_cnt[j], (int)j + 1, st);
         mark(-1, W.diag_cnt[j]);
         mark(K_SYRK, W.syrk_cnt[j]);
-        if (prec == 1 && mx_syrk_) launch_syrk_step_mx(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
-        else launch_syrk_step(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
+        launch_syrk_step(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
         mark(-1, W.syrk_cnt[j]);
       } else if (W.diag_cnt[j] > 0) {
         // fork: next diagonal block on the auxiliary stream, trailing update here; join
@@ -668,12 +667,10 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec
         cudaStreamWaitEvent(aux_stream_, ev_fork_, 0);
         launch_diag_step(sym_, d_diag_ + W.diag_off[j], W.diag_cnt[j], (int)j + 1, aux_stream_);
         cudaEventRecord(ev_join_, aux_stream_);
-        if (prec == 1 && mx_syrk_) launch_syrk_step_mx(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
-        else launch_syrk_step(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
+        launch_syrk_step(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
         cudaStreamWaitEvent(st, ev_join_, 0);
       } else {
-        if (prec == 1 && mx_syrk_) launch_syrk_step_mx(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
-        else launch_syrk_step(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
+        launch_syrk_step(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
       }
     }
   }

@@ -251,10 +251,6 @@ class Engine {
   Tuning tuning_;
   int *d_persist_ = nullptr, *d_qctr_ = nullptr, *d_tiny_ = nullptr;
   int persist_ctas_ = 0, tiny_ctas_ = 0;
-  // Trailing SYRK of the dense steps in split-TF32 too (mixed mode).  Off: on B200 the
-  // FP64 DMMA kernel is the faster one for these 64x64x64 tiles (measured 6.9 ms vs 13.4 ms
-  // per factorization of the 60^3 Laplacian).
-  bool mx_syrk_ = false;
   Plan plan_;
   DevSym sym_{};
   // solve data
@@ -300,6 +296,5 @@ bool kernels_configure(std::string &err);
 bool mixed_configure(std::string &err);
 void launch_update_tiles_mx(const DevSym &S, const int4 *tasks, const int *task_end,
                             const int4 *pairs, int count, cudaStream_t st);
-void launch_syrk_step_mx(const DevSym &S, const int4 *tasks, int count, int step, cudaStream_t st);
 
 }  // namespace swc

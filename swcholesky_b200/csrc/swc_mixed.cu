@@ -315,43 +315,6 @@ __global__ void __launch_bounds__(MXT, 3) k_update_tiles_mx(DevSym S, const int4
       }
 }
 
-// Mixed-precision trailing update of the dense factorization: tile(r0, c0) -= L[r0:, blk]
-// L[c0:, blk]^T with both operands from the mirror of column block `step`.
-constexpr int SYRKM_SMEM = 2 * STAGEF * 8 + 2 * TB * 4;
-
-__global__ void __launch_bounds__(MXT, 3) k_syrk_step_mx(DevSym S, const int4 *tasks, int count,
-                                                        int step) {
-  extern __shared__ float2 dynf[];
-  float2 *stages = dynf;
-  int *ia = reinterpret_cast<int *>(dynf + 2 * STAGEF), *ib = ia + TB;
-  const int4 tk = tasks[blockIdx.x];
-  const int s = tk.x, r0 = tk.y, c0 = tk.z;
-  const int f = S.super[s];
-  const int w = S.super[s + 1] - f;
-  const int m = (int)(S.rowptr[s + 1] - S.rowptr[s]);
-  const int k0 = step * TB;
-  const int bk = min(TB, w - k0);
-  const int nrow = min(TB, m - r0), ncol = min(TB, w - c0);
-  if (threadIdx.x < TB) {
-    ia[threadIdx.x] = (int)threadIdx.x < nrow ? r0 + (int)threadIdx.x : -1;
-    ib[threadIdx.x] = (int)threadIdx.x < ncol ? c0 + (int)threadIdx.x : -1;
-  }
-  Acc32 acc;
-  acc.zero();
-  split_product<MIRROR_TF32X2>(S.Lf + S.xptr[s] + (size_t)k0 * m, m, ia, ib, bk, stages, acc);
-  double *P = S.L + S.xptr[s];
-#pragma unroll
-  for (int i = 0; i < 2; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int r = mx_row(i, e), c = mx_col(j, e);
-        if (r < nrow && c < ncol && r0 + r >= c0 + c)
-          P[(size_t)(c0 + c) * m + r0 + r] -= (double)acc.v[i][j][e];
-      }
-}
-
 }  // namespace
 
 bool mixed_configure(std::string &err) {
@@ -360,8 +323,6 @@ bool mixed_configure(std::string &err) {
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_update_tiles_mx<MIRROR_BF16X3>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, UPDM_SMEM);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_syrk_step_mx, cudaFuncAttributeMaxDynamicSharedMemorySize, SYRKM_SMEM);
   if (e != cudaSuccess) {
     err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e);
     return false;
@@ -376,9 +337,6 @@ void launch_update_tiles_mx(const DevSym &S, const int4 *tasks, const int *task_
     k_update_tiles_mx<MIRROR_BF16X3><<<count, MXT, UPDM_SMEM, st>>>(S, tasks, task_end, pairs, count);
   else
     k_update_tiles_mx<MIRROR_TF32X2><<<count, MXT, UPDM_SMEM, st>>>(S, tasks, task_end, pairs, count);
-}
-void launch_syrk_step_mx(const DevSym &S, const int4 *tasks, int count, int step, cudaStream_t st) {
-  if (count > 0) k_syrk_step_mx<<<count, MXT, SYRKM_SMEM, st>>>(S, tasks, count, step);
 }
 
 }  // namespace swc
