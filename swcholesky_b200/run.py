@@ -47,6 +47,8 @@ def main():
     ap.add_argument("--mode", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--reps", type=int, default=1)
     ap.add_argument("--solve", action="store_true")
+    ap.add_argument("--tune-cache", default=None,
+                    help="batched workload: autotune (or reuse the cached choice in this file)")
     ap.add_argument("--batch-count", type=int, default=256,
                     help="matrices of the batched workload (a smaller batch for profiling)")
     args = ap.parse_args()
@@ -55,6 +57,9 @@ def main():
     h = Handle(0)
     if isinstance(prob, list):
         h.batch_analyze(prob)
+        if args.tune_cache:
+            choice, best = h.batch_autotune(vals, mode, args.tune_cache)
+            print(f"autotune: partition {choice[0]} plan {choice[1]} ({best:.3f} ms)")
     else:
         P = prob
         h.analyze(P.n, P.A2p, P.A2i, P.lC, P.Ls, P.Li_ptr, P.super, P.prunePtr, P.pruneSet)
