@@ -134,7 +134,7 @@ Engine::~Engine() {
 }
 
 void Engine::release() {
-  void *ptrs[] = {d_super_, d_Ls_, d_Ap_, d_Ai_, d_rowptr_, d_xptr_, d_upd_ptr_, d_upd_,
+  void *ptrs[] = {d_super_, d_Ls_, d_Ap_, d_Ai_, d_rowptr_, d_xptr_, d_upd_ptr_, d_upd_, d_upd_lbub_,
                   d_Ax_, dL_, d_status_, d_small_, d_big_, d_asm_, d_panel_, d_upd_tasks_,
                   d_syrk_, d_pairs_, d_upd_end_, d_dinv_, d_dinv_off_, d_diag_,
                   d_slist_, d_cptr_, d_cidx_, d_flags_, d_fchain_, d_bchain_, d_scontrib_, d_sgather_, d_csr_rp_, d_csr_ci_,
@@ -147,6 +147,7 @@ void Engine::release() {
   d_super_ = d_Ls_ = d_Ap_ = d_Ai_ = nullptr;
   d_rowptr_ = d_xptr_ = nullptr;
   d_upd_ptr_ = d_upd_ = nullptr;
+  d_upd_lbub_ = nullptr;
   d_Ax_ = dL_ = nullptr;
   d_status_ = d_small_ = d_big_ = nullptr;
   d_asm_ = d_panel_ = nullptr;
@@ -412,6 +413,15 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
   H.xsize = xsize;
   H.nnz = nnz;
   H.nprune = nprune;
+  H.upd_lbub.resize(nprune);
+  for (int t = 0; t < supNo; ++t)
+    for (int q = prunePtr[t]; q < prunePtr[t + 1]; ++q) {
+      const int d = pruneSet[q], wd = H.super[d + 1] - H.super[d];
+      const int *b = Ls + H.rowptr[d] + wd, *e = Ls + H.rowptr[d + 1];
+      const int lb = (int)(std::lower_bound(b, e, H.super[t]) - b) + wd;
+      const int ub = (int)(std::lower_bound(b, e, H.super[t + 1]) - b) + wd;
+      H.upd_lbub[q] = make_int2(lb, ub);
+    }
   return true;
 }
 
@@ -528,6 +538,7 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
             upload(d_Ai_, r, (size_t)nnz, st, err) &&
             upload(d_upd_ptr_, prunePtr, (size_t)supNo + 1, st, err) &&
             upload(d_upd_, pruneSet, (size_t)nprune, st, err) &&
+            upload(d_upd_lbub_, H.upd_lbub.data(), H.upd_lbub.size(), st, err) &&
             upload(d_small_, P.small_list.data(), P.small_list.size(), st, err) &&
             upload(d_persist_, P.persist_list.data(), P.persist_list.size(), st, err) &&
             upload(d_tiny_, P.tiny_list.data(), P.tiny_list.size(), st, err) &&
@@ -621,19 +632,20 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec
     cudaMemsetAsync(d_qctr_, 0, sizeof(int) * (nsuper_ + 2), st);
   if (!plan_.tiny_list.empty()) {
     mark(K_SMALL, 1);
-    launch_factor_tiny_persist(sym_, d_tiny_, (int)plan_.tiny_list.size(), tiny_ctas_, d_qctr_,
+    launch_factor_tiny_persist(sym_, d_upd_lbub_, d_tiny_, (int)plan_.tiny_list.size(), tiny_ctas_,
+                               d_qctr_,
                                d_qctr_ + 1 + nsuper_, st);
     mark(-1, 1);
   }
   if (!plan_.persist_list.empty()) {
     mark(K_SMALL, 1);
-    launch_factor_small_persist(sym_, d_persist_, (int)plan_.persist_list.size(),
+    launch_factor_small_persist(sym_, d_upd_lbub_, d_persist_, (int)plan_.persist_list.size(),
                                 plan_.persist_smem, persist_ctas_, d_qctr_, st);
     mark(-1, 1);
   }
   for (const Wave &W : plan_.waves) {
     mark(K_SMALL, W.small_cnt);
-    launch_factor_small(sym_, d_small_ + W.small_off, W.small_cnt, W.small_smem, st);
+    launch_factor_small(sym_, d_upd_lbub_, d_small_ + W.small_off, W.small_cnt, W.small_smem, st);
     mark(-1, W.small_cnt);
     mark(K_ASSEMBLE, W.asm_cnt);
     launch_assemble(sym_, d_asm_ + W.asm_off, W.asm_cnt, st);

@@ -136,6 +136,7 @@ struct HostSym {
   int64_t nls = 0, xsize = 0, nnz = 0;
   int nprune = 0;
   std::vector<int> dinv_off;   // per supernode: first diagonal-block inverse (-1: none)
+  std::vector<int2> upd_lbub;  // per update-list entry: the descendant's row range in the target
   int64_t ndinv = 0;           // diagonal-block inverses in total
 };
 
@@ -235,6 +236,7 @@ class Engine {
   int *d_super_ = nullptr, *d_Ls_ = nullptr, *d_Ap_ = nullptr, *d_Ai_ = nullptr;
   int64_t *d_rowptr_ = nullptr, *d_xptr_ = nullptr;
   int *d_upd_ptr_ = nullptr, *d_upd_ = nullptr;
+  int2 *d_upd_lbub_ = nullptr;
   double *d_Ax_ = nullptr, *dL_ = nullptr, *d_dinv_ = nullptr;
   int *d_dinv_off_ = nullptr;
   int *d_status_ = nullptr, *h_status_ = nullptr;
@@ -276,14 +278,17 @@ class Engine {
 };
 
 // kernel launch wrappers (swc_kernels.cu)
-void launch_factor_small(const DevSym &S, const int *list, int count, int smem, cudaStream_t st);
+// lbub: per update-list entry (s, d), the first row of d's row list at or below s's first
+// column and the first below its last column (computed on the host)
+void launch_factor_small(const DevSym &S, const int2 *lbub, const int *list, int count, int smem,
+                         cudaStream_t st);
 // persistent small-class walk: CTAs to launch (occupancy x SMs, at most count) and the launch
 int persist_ctas(int smem, int count);
 int tiny_ctas(int count);
-void launch_factor_tiny_persist(const DevSym &S, const int *order, int count, int ctas,
-                                int *qctr, int *qhead, cudaStream_t st);
-void launch_factor_small_persist(const DevSym &S, const int *order, int count, int smem,
-                                 int ctas, int *qctr, cudaStream_t st);
+void launch_factor_tiny_persist(const DevSym &S, const int2 *lbub, const int *order, int count,
+                                int ctas, int *qctr, int *qhead, cudaStream_t st);
+void launch_factor_small_persist(const DevSym &S, const int2 *lbub, const int *order, int count,
+                                 int smem, int ctas, int *qctr, cudaStream_t st);
 void launch_assemble(const DevSym &S, const int2 *tasks, int count, cudaStream_t st);
 void launch_update_tiles(const DevSym &S, const int4 *tasks, const int *task_end,
                          const int4 *pairs, int count, cudaStream_t st);

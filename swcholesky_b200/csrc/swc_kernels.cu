@@ -111,7 +111,8 @@ __device__ __forceinline__ void small_update(const double *Ld, int md, int wd, i
 
 // ---------------------------------------------------------------------------------------
 // Whole factorization of one small supernode s by the calling CTA (all NT threads).
-__device__ __noinline__ void factor_small_body(const DevSym &S, int s, double *smem) {
+__device__ __noinline__ void factor_small_body(const DevSym &S, const int2 *lbub, int s,
+                                               double *smem) {
   const int tid = threadIdx.x;
   const int f = S.super[s];
   const int w = S.super[s + 1] - f;
@@ -145,8 +146,8 @@ __device__ __noinline__ void factor_small_body(const DevSym &S, int s, double *s
     const int64_t rbd = S.rowptr[d];
     const int md = (int)(S.rowptr[d + 1] - rbd);
     const int *Lsd = S.Ls + rbd;
-    const int lb = wd + lbound(Lsd + wd, md - wd, f);
-    const int ub = wd + lbound(Lsd + wd, md - wd, f + w);
+    const int2 lu = lbub[q];   // d's rows at or below f, and below f + w (host-computed)
+    const int lb = lu.x, ub = lu.y;
     const int nr = md - lb;   // nSupRs
     const int n1 = ub - lb;   // ndrow1
     if (n1 <= 0 || nr > m) {
@@ -193,9 +194,10 @@ __device__ __noinline__ void factor_small_body(const DevSym &S, int s, double *s
 }
 
 // One CTA per small supernode of a level.
-__global__ void __launch_bounds__(NT) k_factor_small(DevSym S, const int *list, int count) {
+__global__ void __launch_bounds__(NT) k_factor_small(DevSym S, const int2 *lbub, const int *list,
+                                                     int count) {
   extern __shared__ double smem[];
-  factor_small_body(S, list[blockIdx.x], smem);
+  factor_small_body(S, lbub, list[blockIdx.x], smem);
 }
 
 // The small supernodes of the bottom of the tree (a set closed under descendants) in ONE
@@ -218,7 +220,8 @@ __device__ __forceinline__ void st_release_k(int *p, int v) {
   asm volatile("st.release.gpu.global.s32 [%0], %1;\n" ::"l"(p), "r"(v));
 }
 
-__global__ void __launch_bounds__(NT) k_factor_small_persist(DevSym S, const int *order, int count,
+__global__ void __launch_bounds__(NT) k_factor_small_persist(DevSym S, const int2 *lbub,
+                                                              const int *order, int count,
                                                               int *qctr) {
   extern __shared__ double smem[];
   __shared__ int item;
@@ -245,7 +248,7 @@ __global__ void __launch_bounds__(NT) k_factor_small_persist(DevSym S, const int
       }
     }
     __syncthreads();
-    factor_small_body(S, s, smem);
+    factor_small_body(S, lbub, s, smem);
     __syncthreads();
     if (threadIdx.x == 0) {
       __threadfence();
@@ -894,8 +897,8 @@ constexpr int TW = 4;
 constexpr int TINY_SLICE = (TINY_ELEMS * 8 + TINY_SLAB * 8 + 2 * TINY_M * 4 + 15) / 16 * 16;   // bytes per warp
 constexpr int TINY_SMEM = TW * TINY_SLICE;
 
-__device__ void factor_tiny_body(const DevSym &S, int s, double *P, int *rows, int *rel,
-                                 double *slab) {
+__device__ void factor_tiny_body(const DevSym &S, const int2 *lbub, int s, double *P, int *rows,
+                                 int *rel, double *slab) {
   const int lane = threadIdx.x & 31;
   const int f = S.super[s];
   const int w = S.super[s + 1] - f;
@@ -920,8 +923,8 @@ __device__ void factor_tiny_body(const DevSym &S, int s, double *P, int *rows, i
     const int64_t rbd = S.rowptr[d];
     const int md = (int)(S.rowptr[d + 1] - rbd);
     const int *Lsd = S.Ls + rbd;
-    const int lb = wd + lbound(Lsd + wd, md - wd, f);
-    const int ub = wd + lbound(Lsd + wd, md - wd, f + w);
+    const int2 lu = lbub[q];
+    const int lb = lu.x, ub = lu.y;
     const int nr = md - lb, n1 = ub - lb;
     if (n1 <= 0 || nr > m) {
       if (nr > m && lane == 0) flag_structure_error(S);
@@ -960,7 +963,8 @@ __device__ void factor_tiny_body(const DevSym &S, int s, double *P, int *rows, i
 }
 
 // qctr[1 + s]: done flags (shared with the CTA walk); qhead: this walk's queue head.
-__global__ void __launch_bounds__(TW * 32) k_factor_tiny_persist(DevSym S, const int *order,
+__global__ void __launch_bounds__(TW * 32) k_factor_tiny_persist(DevSym S, const int2 *lbub,
+                                                                 const int *order,
                                                                  int count, int *qctr,
                                                                  int *qhead) {
   extern __shared__ double smem_t[];
@@ -991,7 +995,7 @@ __global__ void __launch_bounds__(TW * 32) k_factor_tiny_persist(DevSym S, const
       }
     }
     __syncwarp();
-    factor_tiny_body(S, s, P, rows, rel, slab);
+    factor_tiny_body(S, lbub, s, P, rows, rel, slab);
     __syncwarp();
     if (lane == 0) {
       __threadfence();
@@ -1026,8 +1030,9 @@ bool kernels_configure(std::string &err) {
   return true;
 }
 
-void launch_factor_small(const DevSym &S, const int *list, int count, int smem, cudaStream_t st) {
-  if (count > 0) k_factor_small<<<count, NT, smem, st>>>(S, list, count);
+void launch_factor_small(const DevSym &S, const int2 *lbub, const int *list, int count, int smem,
+                         cudaStream_t st) {
+  if (count > 0) k_factor_small<<<count, NT, smem, st>>>(S, lbub, list, count);
 }
 int persist_ctas(int smem, int count) {
   int dev = 0, sms = 0, per = 0;
@@ -1047,13 +1052,14 @@ int tiny_ctas(int count) {
     per = 1;
   return std::max(1, std::min((count + TW - 1) / TW, sms * per));
 }
-void launch_factor_tiny_persist(const DevSym &S, const int *order, int count, int ctas,
-                                int *qctr, int *qhead, cudaStream_t st) {
-  if (count > 0) k_factor_tiny_persist<<<ctas, TW * 32, TINY_SMEM, st>>>(S, order, count, qctr, qhead);
+void launch_factor_tiny_persist(const DevSym &S, const int2 *lbub, const int *order, int count,
+                                int ctas, int *qctr, int *qhead, cudaStream_t st) {
+  if (count > 0)
+    k_factor_tiny_persist<<<ctas, TW * 32, TINY_SMEM, st>>>(S, lbub, order, count, qctr, qhead);
 }
-void launch_factor_small_persist(const DevSym &S, const int *order, int count, int smem,
-                                 int ctas, int *qctr, cudaStream_t st) {
-  if (count > 0) k_factor_small_persist<<<ctas, NT, smem, st>>>(S, order, count, qctr);
+void launch_factor_small_persist(const DevSym &S, const int2 *lbub, const int *order, int count,
+                                 int smem, int ctas, int *qctr, cudaStream_t st) {
+  if (count > 0) k_factor_small_persist<<<ctas, NT, smem, st>>>(S, lbub, order, count, qctr);
 }
 void launch_assemble(const DevSym &S, const int2 *tasks, int count, cudaStream_t st) {
   if (count > 0) k_assemble<<<(count * 32 + NT - 1) / NT, NT, 0, st>>>(S, tasks, count);
