@@ -79,10 +79,11 @@ __device__ __forceinline__ void flag_structure_error(const DevSym &S) {
 
 // Update of a small panel P (m rows, column-major) by descendant d: rows lb.. of d's panel
 // (Ld points at row lb; md = d's rows, wd = its width, nr rows from lb, the first n1 of them
-// inside the target's columns).  The rows are staged in the shared slab (capacity slab_cap
-// doubles) a column chunk at a time with independent loads from all threads, then
-// P[rel[a]][rel[b]] -= sum_k X[b][k] X[a][k] for a < n1, b >= a, from shared memory.
-// Threads t, t + nt, ...; `sync` is the barrier of the thread group (block or warp).
+// inside the target's columns).  The rows go through the shared slab (capacity slab_cap
+// doubles) a column chunk at a time, then P[rel[a]][rel[b]] -= sum_k X[b][k] X[a][k] for
+// a < n1, b >= a, from shared memory.  The first chunk is already in the slab (staged from
+// registers loaded ahead, see prefetch_chunk); later chunks load here.  Threads t, t + nt,
+// ...; the barrier is the thread group's (block or warp).
 template <bool WARP>
 __device__ __forceinline__ void small_update(const double *Ld, int md, int wd, int n1, int nr,
                                              const int *rel, double *P, int m, double *slab,
@@ -90,10 +91,11 @@ __device__ __forceinline__ void small_update(const double *Ld, int md, int wd, i
   const int kch = max(1, min(wd, slab_cap / nr));
   for (int k0 = 0; k0 < wd; k0 += kch) {
     const int kc = min(kch, wd - k0);
-    for (int e = t; e < nr * kc; e += nt) {
-      const int kk = e / nr, i = e - kk * nr;
-      slab[e] = Ld[(size_t)(k0 + kk) * md + i];
-    }
+    if (k0 > 0)
+      for (int e = t; e < nr * kc; e += nt) {
+        const int kk = e / nr, i = e - kk * nr;
+        slab[e] = Ld[(size_t)(k0 + kk) * md + i];
+      }
     if (WARP) __syncwarp(); else __syncthreads();
     const int total = n1 * nr;
     for (int idx = t; idx < total; idx += nt) {
@@ -106,6 +108,68 @@ __device__ __forceinline__ void small_update(const double *Ld, int md, int wd, i
       P[(size_t)ra * m + rbi] -= acc;
     }
     if (WARP) __syncwarp(); else __syncthreads();
+  }
+}
+
+// Loads the first slab chunk of update-list entry q into registers (element e = t + i nt of
+// the chunk in pf[i]), so the loads are in flight while the previous entry is applied.
+template <int PF>
+__device__ __forceinline__ void prefetch_chunk(const DevSym &S, const int2 *lbub, int q,
+                                               int slab_cap, int t, int nt, double (&pf)[PF]) {
+  const int d = S.upd[q];
+  const int wd = S.super[d + 1] - S.super[d];
+  const int md = (int)(S.rowptr[d + 1] - S.rowptr[d]);
+  const int lb = lbub[q].x, nr = md - lb;
+  const int cnt = nr > 0 ? nr * max(1, min(wd, slab_cap / nr)) : 0;
+  const double *Ld = S.L + S.xptr[d] + lb;
+#pragma unroll
+  for (int i = 0; i < PF; ++i) {
+    const int e = t + i * nt;
+    pf[i] = 0.0;
+    if (e < cnt) {
+      const int kk = e / nr;
+      pf[i] = Ld[(size_t)kk * md + (e - kk * nr)];
+    }
+  }
+}
+
+// Updates of panel P from every descendant of s's update list, in order, each descendant's
+// first chunk loaded while the previous one is applied.
+template <bool WARP, int PF>
+__device__ __forceinline__ void small_updates(const DevSym &S, const int2 *lbub, int s, int f,
+                                              int w, int m, const int *rows, int *rel, double *P,
+                                              double *slab, int slab_cap, int t, int nt) {
+  const int q0 = S.upd_ptr[s], q1 = S.upd_ptr[s + 1];
+  double pf[PF];
+  if (q0 < q1) prefetch_chunk<PF>(S, lbub, q0, slab_cap, t, nt, pf);
+  for (int q = q0; q < q1; ++q) {
+    const int d = S.upd[q];
+    const int wd = S.super[d + 1] - S.super[d];
+    const int64_t rbd = S.rowptr[d];
+    const int md = (int)(S.rowptr[d + 1] - rbd);
+    const int *Lsd = S.Ls + rbd;
+    const int2 lu = lbub[q];   // d's rows at or below f, and below f + w (host-computed)
+    const int lb = lu.x, ub = lu.y;
+    const int nr = md - lb;    // nSupRs
+    const int n1 = ub - lb;    // ndrow1
+    const bool skip = n1 <= 0 || nr > m;
+    if (!skip) {
+      for (int i = t; i < nr; i += nt) {
+        const int key = Lsd[lb + i];
+        int pos = lbound(rows, m, key);
+        if (pos >= m || rows[pos] != key) { flag_structure_error(S); pos = -1; }
+        rel[i] = pos;
+      }
+      const int cnt = nr * max(1, min(wd, slab_cap / nr));
+#pragma unroll
+      for (int i = 0; i < PF; ++i)
+        if (t + i * nt < cnt) slab[t + i * nt] = pf[i];
+    } else if (nr > m && t == 0) {
+      flag_structure_error(S);
+    }
+    if (q + 1 < q1) prefetch_chunk<PF>(S, lbub, q + 1, slab_cap, t, nt, pf);
+    if (skip) continue;
+    small_update<WARP>(S.L + S.xptr[d] + lb, md, wd, n1, nr, rel, P, m, slab, slab_cap, t, nt);
   }
 }
 
@@ -139,31 +203,9 @@ __device__ __noinline__ void factor_small_body(const DevSym &S, const int2 *lbub
   __syncthreads();
 
   // updates from every descendant in the prune set, in order
-  for (int q = S.upd_ptr[s]; q < S.upd_ptr[s + 1]; ++q) {
-    const int d = S.upd[q];
-    const int fd = S.super[d];
-    const int wd = S.super[d + 1] - fd;
-    const int64_t rbd = S.rowptr[d];
-    const int md = (int)(S.rowptr[d + 1] - rbd);
-    const int *Lsd = S.Ls + rbd;
-    const int2 lu = lbub[q];   // d's rows at or below f, and below f + w (host-computed)
-    const int lb = lu.x, ub = lu.y;
-    const int nr = md - lb;   // nSupRs
-    const int n1 = ub - lb;   // ndrow1
-    if (n1 <= 0 || nr > m) {
-      if (nr > m) flag_structure_error(S);
-      continue;
-    }
-    for (int i = tid; i < nr; i += NT) {
-      int key = Lsd[lb + i];
-      int pos = lbound(rows, m, key);
-      if (pos >= m || rows[pos] != key) { flag_structure_error(S); pos = -1; }
-      rel[i] = pos;
-    }
-    __syncthreads();
-    small_update<false>(S.L + S.xptr[d] + lb, md, wd, n1, nr, rel, P, m,
-                        reinterpret_cast<double *>(rel + m) + w, SMALL_SLAB, tid, NT);
-  }
+  small_updates<false, SMALL_SLAB / NT>(S, lbub, s, f, w, m, rows, rel, P,
+                                        reinterpret_cast<double *>(rel + m) + w, SMALL_SLAB,
+                                        tid, NT);
 
   // POTRF + TRSM on the tall panel: unblocked right-looking Cholesky of m x w.  Rows are
   // strided over the threads; the scaled pivot column's first w entries go through colv so
@@ -917,28 +959,7 @@ __device__ void factor_tiny_body(const DevSym &S, const int2 *lbub, int s, doubl
     }
   __syncwarp();
   // updates from the descendants of the update list, in order
-  for (int q = S.upd_ptr[s]; q < S.upd_ptr[s + 1]; ++q) {
-    const int d = S.upd[q];
-    const int wd = S.super[d + 1] - S.super[d];
-    const int64_t rbd = S.rowptr[d];
-    const int md = (int)(S.rowptr[d + 1] - rbd);
-    const int *Lsd = S.Ls + rbd;
-    const int2 lu = lbub[q];
-    const int lb = lu.x, ub = lu.y;
-    const int nr = md - lb, n1 = ub - lb;
-    if (n1 <= 0 || nr > m) {
-      if (nr > m && lane == 0) flag_structure_error(S);
-      continue;
-    }
-    for (int i = lane; i < nr; i += 32) {
-      const int key = Lsd[lb + i];
-      int pos = lbound(rows, m, key);
-      if (pos >= m || rows[pos] != key) { flag_structure_error(S); pos = -1; }
-      rel[i] = pos;
-    }
-    __syncwarp();
-    small_update<true>(S.L + S.xptr[d] + lb, md, wd, n1, nr, rel, P, m, slab, TINY_SLAB, lane, 32);
-  }
+  small_updates<true, TINY_SLAB / 32>(S, lbub, s, f, w, m, rows, rel, P, slab, TINY_SLAB, lane, 32);
   // right-looking POTRF + TRSM of the m x w panel, lanes along the rows
   for (int j = 0; j < w; ++j) {
     const double piv = P[(size_t)j * m + j];
