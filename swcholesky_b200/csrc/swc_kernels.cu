@@ -207,23 +207,42 @@ __device__ __noinline__ void factor_small_body(const DevSym &S, const int2 *lbub
                                         reinterpret_cast<double *>(rel + m) + w, SMALL_SLAB,
                                         tid, NT);
 
-  // POTRF + TRSM on the tall panel: unblocked right-looking Cholesky of m x w.  Rows are
-  // strided over the threads; the scaled pivot column's first w entries go through colv so
-  // a single barrier separates scaling from the trailing update.
-  double *colv = reinterpret_cast<double *>(rel + m);   // w doubles (8-byte aligned slot)
-  for (int j = 0; j < w; ++j) {
-    __syncthreads();
-    const double piv = P[(size_t)j * m + j];
-    const double inv = rsqrt(piv);
-    const double dsq = piv * inv;
-    if (tid == 0 && !(piv > 0.0)) atomicMin(&S.status[0], f + j + 1);
-    for (int i = j + tid; i < w; i += NT) colv[i] = (i == j) ? dsq : P[(size_t)j * m + i] * inv;
-    __syncthreads();
-    for (int i = j + tid; i < m; i += NT) {
-      const double lij = (i == j) ? dsq : P[(size_t)j * m + i] * inv;
-      P[(size_t)j * m + i] = lij;
-      const int cend = min(i, w - 1);
-      for (int c = j + 1; c <= cend; ++c) P[(size_t)c * m + i] = fma(-lij, colv[c], P[(size_t)c * m + i]);
+  // POTRF of the w x w diagonal block by warp 0 alone (warp barriers only; lanes own rows
+  // lane and lane + 32), keeping the pivots' reciprocals in rd; then every thread solves
+  // its rows below the block against it (row i of L21 = A21(i, :) L11^{-T}), two block
+  // barriers in all instead of two per column.
+  double *rd = reinterpret_cast<double *>(rel + m);   // w doubles (8-byte aligned slot)
+  if (warp == 0) {
+    for (int j = 0; j < w; ++j) {
+      const double piv = P[(size_t)j * m + j];
+      const double inv = rsqrt(piv);
+      if (lane == 0) {
+        rd[j] = inv;
+        if (!(piv > 0.0)) atomicMin(&S.status[0], f + j + 1);
+      }
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int r = lane + 32 * h;
+        if (r >= j && r < w) P[(size_t)j * m + r] = (r == j) ? piv * inv : P[(size_t)j * m + r] * inv;
+      }
+      __syncwarp();
+      for (int c = j + 1; c < w; ++c) {
+        const double lcj = P[(size_t)j * m + c];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int r = lane + 32 * h;
+          if (r >= c && r < w) P[(size_t)c * m + r] = fma(-P[(size_t)j * m + r], lcj, P[(size_t)c * m + r]);
+        }
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  for (int i = w + tid; i < m; i += NT) {
+    for (int j = 0; j < w; ++j) {
+      double acc = P[(size_t)j * m + i];
+      for (int k = 0; k < j; ++k) acc = fma(-P[(size_t)k * m + i], P[(size_t)k * m + j], acc);
+      P[(size_t)j * m + i] = acc * rd[j];
     }
   }
   __syncthreads();
