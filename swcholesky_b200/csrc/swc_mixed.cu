@@ -20,7 +20,7 @@ namespace swc {
 namespace {
 
 constexpr int MXT = 128;            // threads (4 warps, 2x2 warp grid of 32x32 sub-tiles)
-constexpr int KF = 32;              // k-chunk (4 steps of k8)
+constexpr int KF = 16;              // k-chunk (2 steps of k8, 1 of k16)
 constexpr int LDF = TB + 4;         // padded row of a staged k-slice ({hi, lo} pairs):
                                     // 64-bit fragment loads conflict-free
 constexpr int STAGEF = 2 * KF * LDF;
@@ -246,7 +246,7 @@ __device__ __forceinline__ void split_product(const float2 *__restrict__ Lf, int
 constexpr int UPDM_SMEM = 2 * STAGEF * 8 + 3 * TB * 4;
 
 template <int KIND>
-__global__ void __launch_bounds__(MXT, 3) k_update_tiles_mx(DevSym S, const int4 *tasks,
+__global__ void __launch_bounds__(MXT, 4) k_update_tiles_mx(DevSym S, const int4 *tasks,
                                                            const int *task_end,
                                                            const int4 *pairs, int count) {
   extern __shared__ float2 dynf[];
