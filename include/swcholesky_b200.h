@@ -72,6 +72,13 @@ int swc_destroy(swc_handle_t handle);
  * handle's own stream). */
 int swc_set_stream(swc_handle_t handle, void *stream);
 void *swc_get_stream(swc_handle_t handle);
+/* Execution plan used by the next swc_analyze / swc_batch_analyze on the handle: one of
+ * the candidates swc_batch_autotune tries.  0: default; 1: persistent small-supernode
+ * walk up to 100 KB of shared memory per supernode; 2: no persistent walk (one launch per
+ * level); 3: smaller small-class limits (more tiled supernodes); 4: the dense
+ * factorization of each level's tiled supernodes as one persistent dataflow launch
+ * instead of three launches per 64-column step.  SWC_INVALID_INPUT for other values. */
+int swc_set_plan(swc_handle_t handle, int plan);
 
 /* Uploads and validates the structure.  Arguments as in sw_cholesky_left_par_05
  * (values excluded).  levelPtr/parPtr/partition may be NULL: the executor derives its own
@@ -157,14 +164,16 @@ int swc_profile(swc_handle_t handle, const double *values, int values_on_device,
                 int *info, int *launches, double *ms, double *flops, double *bytes);
 
 /* Host-only: validates the structure (as swc_analyze does) and describes the execution
- * plan without touching a GPU.  stats[0..19] = levels, kernel launches per factorization,
+ * plan (candidate `plan`, as swc_set_plan) without touching a GPU; for plan 4 the dataflow
+ * task order is checked (every wait served by an earlier task) as at analysis.
+ * stats[0..19] = levels, kernel launches per factorization,
  * small-class supernodes, tiled-class supernodes, update tiles, update (tile, descendant)
  * pairs, TRSM tiles, SYRK tiles, then per kernel class (memset, small, assemble, update,
  * panel, syrk) the algorithmic flops [8..13] and DRAM bytes [14..19] of one
  * factorization.  No reference counterpart. */
 int swc_plan_stats(int n, const int *c, const int *r, const size_t *lC, const int *Ls,
                    const size_t *Li_ptr, const int *blockSet, int supNo, const int *prunePtr,
-                   const int *pruneSet, double *stats);
+                   const int *pruneSet, int plan, double *stats);
 
 /* ---- host layout builder ---------------------------------------------------------
  * Builds the BCSC layout the reference's analyze_p2 produces for a given supernode

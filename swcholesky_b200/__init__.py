@@ -42,7 +42,7 @@ EXPORTS = (
     "swc_device_L", "swc_sizes", "swc_profile", "swc_plan_stats", "swc_layout_sizes",
     "swc_layout", "swc_solve", "swc_refine", "swc_solve_noalloc", "swc_logdet",
     "swc_logdet_grad", "swc_solve_grad", "swc_supernodes", "swc_batch_analyze",
-    "swc_batch_autotune", "swc_batch_berr",
+    "swc_batch_autotune", "swc_batch_berr", "swc_set_plan",
 )
 KERNEL_CLASSES = ("memset", "small", "assemble", "update", "panel", "syrk")
 
@@ -85,7 +85,8 @@ def lib() -> ctypes.CDLL:
         L.swc_solve_noalloc.argtypes = [_VP, _VP, _VP, _I]
         L.swc_refine.argtypes = [_VP, _VP, _VP, _I, _I, ctypes.c_double, _I, _VP,
                                  ctypes.POINTER(_I), ctypes.POINTER(_I)]
-        L.swc_plan_stats.argtypes = [_I] + [_VP] * 6 + [_I] + [_VP] * 3
+        L.swc_plan_stats.argtypes = [_I] + [_VP] * 6 + [_I] + [_VP] * 2 + [_I, _VP]
+        L.swc_set_plan.argtypes = [_VP, _I]
         L.swc_layout_sizes.argtypes = [_I] + [_VP] * 3 + [_I, _VP]
         L.swc_layout.argtypes = [_I] + [_VP] * 3 + [_I] + [_VP] * 9
         L.swc_logdet.argtypes = [_VP, ctypes.POINTER(ctypes.c_double)]
@@ -183,16 +184,16 @@ PLAN_FIELDS = ("levels", "launches", "small", "tiled", "update_tiles", "update_p
                "trsm_tiles", "syrk_tiles")
 
 
-def plan_stats(n, c, r, lC, Ls, Li_ptr, blockSet, prunePtr, pruneSet):
-    """Execution plan of a structure, computed on the host (no GPU needed): counts and the
-    algorithmic flops / bytes per kernel class."""
+def plan_stats(n, c, r, lC, Ls, Li_ptr, blockSet, prunePtr, pruneSet, plan: int = 0):
+    """Execution plan (candidate ``plan``, as ``Handle.set_plan``) of a structure, computed
+    on the host (no GPU needed): counts and the algorithmic flops / bytes per kernel class."""
     st = np.zeros(8 + 2 * len(KERNEL_CLASSES))
     args = [_c(c, np.int32), _c(r, np.int32), _c(lC, np.uint64), _c(Ls, np.int32),
             _c(Li_ptr, np.uint64), _c(blockSet, np.int32), _c(prunePtr, np.int32),
             _c(pruneSet, np.int32)]
     _check(lib().swc_plan_stats(int(n), _p(args[0]), _p(args[1]), _p(args[2]), _p(args[3]),
                                 _p(args[4]), _p(args[5]), args[5].size - 1, _p(args[6]),
-                                _p(args[7]), _p(st)))
+                                _p(args[7]), int(plan), _p(st)))
     out = {k: int(st[i]) for i, k in enumerate(PLAN_FIELDS)}
     k = len(KERNEL_CLASSES)
     out["flops"] = {name: float(st[8 + i]) for i, name in enumerate(KERNEL_CLASSES)}
@@ -317,6 +318,12 @@ class Handle:
                                     float(tol), int(maxit), _p(berr), ctypes.byref(it),
                                     ctypes.byref(meth)))
         return x, berr, int(it.value), int(meth.value)
+
+    def set_plan(self, plan: int):
+        """Execution-plan candidate for the next analyze / batch_analyze (0 default, 1 larger
+        persistent supernodes, 2 no persistent walk, 3 smaller small class, 4 dense steps
+        as one dataflow launch per level)."""
+        _check(self._lib.swc_set_plan(self._h, int(plan)))
 
     def batch_analyze(self, mats):
         """Analyse independent ordered matrices (objects with n, indptr, indices: lower CSC

@@ -91,6 +91,13 @@ int swc_set_stream(swc_handle_t h, void *stream) {
   return SWC_OK;
 }
 
+int swc_set_plan(swc_handle_t h, int plan) {
+  if (!h) return fail(SWC_INVALID_INPUT, "null handle");
+  if (plan < 0 || plan >= swc::num_plans()) return fail(SWC_INVALID_INPUT, "unknown plan");
+  h->plan = plan;
+  return SWC_OK;
+}
+
 void *swc_get_stream(swc_handle_t h) { return h ? (void *)h->eng->stream() : nullptr; }
 
 int swc_analyze(swc_handle_t h, int n, const int *c, const int *r, const size_t *lC,
@@ -116,7 +123,7 @@ int swc_analyze(swc_handle_t h, int n, const int *c, const int *r, const size_t 
   h->analyzed = false;
   h->factored = false;
   h->batch.reset();
-  h->eng->set_tuning(swc::Tuning());
+  h->eng->set_tuning(swc::plan_candidate(h->plan));
   if (!h->eng->analyze(n, c, r, lc.data(), Ls, lip.data(), blockSet, supNo, prunePtr, pruneSet, err))
     return fail(err.rfind("device", 0) == 0 ? SWC_CUDA_ERROR : SWC_INVALID_INPUT, err);
   h->analyzed = true;
@@ -240,7 +247,7 @@ int swc_batch_analyze(swc_handle_t h, int nmat, const int *n, const int *c, cons
   h->factored = false;
   std::unique_ptr<swc::BatchState> b(new swc::BatchState);
   if (!b->set(nmat, n, c, r, err)) return fail(SWC_INVALID_INPUT, err);
-  if (!b->analyze(*h->eng, 0, swc::plan_candidate(0), err))
+  if (!b->analyze(*h->eng, 0, swc::plan_candidate(h->plan), err))
     return fail(err.rfind("device", 0) == 0 ? SWC_CUDA_ERROR : SWC_INVALID_INPUT, err);
   h->batch = std::move(b);
   h->analyzed = true;
@@ -385,14 +392,15 @@ int sw_cholesky_left_par_05(int n, int *c, int *r, double *values, size_t *lC, i
 
 int swc_plan_stats(int n, const int *c, const int *r, const size_t *lC, const int *Ls,
                    const size_t *Li_ptr, const int *blockSet, int supNo, const int *prunePtr,
-                   const int *pruneSet, double *stats) {
+                   const int *pruneSet, int plan, double *stats) {
   if (n <= 0 || !lC || !Li_ptr || !stats) return fail(SWC_INVALID_INPUT, "null or empty input");
+  if (plan < 0 || plan >= swc::num_plans()) return fail(SWC_INVALID_INPUT, "unknown plan");
   std::vector<int64_t> lc = to_i64(lC, n + 1), lip = to_i64(Li_ptr, n + 1);
   swc::HostSym H;
   swc::Plan P;
   std::string err;
   if (!swc::build_plan(n, c, r, lc.data(), Ls, lip.data(), blockSet, supNo, prunePtr, pruneSet,
-                       H, P, err))
+                       H, P, err, swc::plan_candidate(plan)))
     return fail(SWC_INVALID_INPUT, err);
   stats[0] = (double)P.waves.size();
   stats[1] = (double)P.launches;

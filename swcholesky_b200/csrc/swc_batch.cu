@@ -108,11 +108,13 @@ Tuning plan_candidate(int k) {
     case 1: t.persist_max_smem = 100 * 1024; break;      // bigger supernodes in the walk
     case 2: t.persist = 0; break;                        // level-by-level launches only
     case 3: t.small_max_elems = 4096; t.small_max_m = 1024; break;   // more tiled supernodes
+    case 4: t.dense_dataflow = 1; break;                 // dense steps as one dataflow launch
     default: break;
   }
   return t;
 }
-const int kNumPlans = 4;
+const int kNumPlans = 5;
+int num_plans() { return kNumPlans; }
 
 bool BatchState::set(int nm, const int *n, const int *c, const int *r, std::string &err) {
   if (nm <= 0 || !n || !c || !r) {

@@ -32,6 +32,8 @@ struct BatchState {
                 int *choice, double *best_ms, std::string &err);
 };
 
+// Execution-plan candidates of the autotuner (also selectable with swc_set_plan).
 Tuning plan_candidate(int k);
+int num_plans();
 
 }  // namespace swc

@@ -140,7 +140,7 @@ void Engine::release() {
                   d_slist_, d_cptr_, d_cidx_, d_flags_, d_fchain_, d_bchain_, d_scontrib_, d_sgather_, d_csr_rp_, d_csr_ci_,
                   d_csr_map_,
                   d_csr_val_, d_contrib_, d_work_, d_norms_, d_persist_, d_qctr_, d_npart_,
-                  d_tiny_};
+                  d_tiny_, d_dense_tasks_, d_dense_toff_, d_dense_ver_};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   release_adjoint();
@@ -156,6 +156,9 @@ void Engine::release() {
   d_dinv_ = nullptr;
   d_dinv_off_ = nullptr;
   d_diag_ = nullptr;
+  d_dense_tasks_ = nullptr;
+  d_dense_toff_ = d_dense_ver_ = nullptr;
+  dense_ver_len_ = 0;
   d_slist_ = d_cptr_ = d_cidx_ = d_flags_ = nullptr;
   d_fchain_ = d_bchain_ = nullptr;
   d_scontrib_ = d_sgather_ = nullptr;
@@ -174,6 +177,123 @@ void Engine::release() {
   }
   if (d_Lf_) cudaFree(d_Lf_);
   d_Lf_ = nullptr;
+}
+
+// Dataflow tasks of the dense factorization of one tiled-class panel (w columns, m rows),
+// see k_dense_persist.  The updates of tile (I, C) by column blocks 0 .. C-1 (0 .. C-2 for
+// a diagonal tile, whose last one its diagonal task applies) are grouped: the last block
+// alone (off-diagonal tiles), then groups of `group` blocks back to block 0, so the
+// updates the next TRSM waits for stay short and the older ones run as longer products.
+// Each task gets its bottom level: its cost plus the longest chain of costs of the tasks
+// that wait for it (diagonal block 4; full TRSM tile 1; update 0.6 + 0.4 per block;
+// scaled by the tile's fill).  Tasks are generated in a topological order; sorting by
+// decreasing bottom level keeps one (every task's bottom level exceeds its successors' by
+// at least its own cost) and starts the longest chains first.
+struct DenseTask {
+  double bl;
+  int4 t;
+};
+
+static inline int dense_code(int kind, int step, int first) {
+  return kind | (step << 2) | (first << 17);
+}
+
+static void dense_panel_tasks(int s, int w, int m, int group, std::vector<DenseTask> &out) {
+  const int nb = (w + TB - 1) / TB, mb = (m + TB - 1) / TB;
+  const double per_elem = 1.0 / (TB * TB), min_frac = 0.25;
+  struct Node {
+    int4 t;
+    double cost, succ = 0.0;
+    int pred[3] = {-1, -1, -1};
+  };
+  std::vector<Node> nodes;
+  std::vector<int> last((size_t)nb * mb, -1);      // [C * mb + I]: last task that set ver(I, C)
+  std::vector<int> trsm((size_t)nb * mb, -1);      // [J * mb + I]: aligned TRSM task of (I, J)
+  auto add = [&](int4 t, double cost, int p0, int p1, int p2) {
+    Node nd;
+    nd.t = t;
+    nd.cost = cost;
+    nd.pred[0] = p0;
+    nd.pred[1] = p1;
+    nd.pred[2] = p2;
+    nodes.push_back(nd);
+    return (int)nodes.size() - 1;
+  };
+  for (int J = 0; J < nb; ++J) {
+    const int c0 = J * TB, bw = std::min(TB, w - c0);
+    // diagonal block J: waits for the diagonal tile's updates (through J-2) and TRSM (J, J-1)
+    const int d = add(make_int4(s, c0, c0, dense_code(0, J, 0)), 4.0, last[(size_t)J * mb + J],
+                      J > 0 ? trsm[(size_t)(J - 1) * mb + J] : -1, -1);
+    last[(size_t)J * mb + J] = d;
+    // TRSM of the rows below it: waits for the diagonal block and the covered tiles' updates
+    for (int r0 = c0 + bw; r0 < m; r0 += TB) {
+      const int nr = std::min(TB, m - r0);
+      const int I0 = r0 / TB, I1 = (r0 + nr - 1) / TB;
+      const int p1 = I0 != J ? last[(size_t)J * mb + I0] : -1;
+      const int p2 = I1 != J && I1 != I0 ? last[(size_t)J * mb + I1] : -1;
+      const int t = add(make_int4(s, r0, 0, dense_code(1, J, 0)),
+                        std::max(min_frac, nr * bw * per_elem), d, p1, p2);
+      if (bw == TB) {
+        trsm[(size_t)J * mb + I0] = t;
+        last[(size_t)J * mb + I0] = t;
+      }
+    }
+    // update groups ending at block J: tile (I, C), C > J
+    for (int C = J + 1; C < nb; ++C)
+      for (int I = C; I < mb; ++I) {
+        int first;
+        if (I > C && J == C - 1) first = J;                          // the last block alone
+        else if (J <= C - 2 && (C - 2 - J) % group == 0) first = std::max(0, J - group + 1);
+        else continue;
+        const int nrow = std::min(TB, m - I * TB), ncol = std::min(TB, w - C * TB);
+        const double cost = std::max(min_frac, nrow * ncol * per_elem) * (0.6 + 0.4 * (J - first + 1));
+        const int u = add(make_int4(s, I * TB, C * TB, dense_code(2, J, first)), cost,
+                          last[(size_t)C * mb + I], trsm[(size_t)J * mb + I],
+                          trsm[(size_t)J * mb + C]);
+        last[(size_t)C * mb + I] = u;
+      }
+  }
+  // bottom levels, successors before predecessors
+  for (int k = (int)nodes.size() - 1; k >= 0; --k) {
+    const double bl = nodes[k].cost + nodes[k].succ;
+    nodes[k].succ = bl;   // now the bottom level
+    for (int q = 0; q < 3; ++q)
+      if (nodes[k].pred[q] >= 0) nodes[nodes[k].pred[q]].succ = std::max(nodes[nodes[k].pred[q]].succ, bl);
+  }
+  for (const Node &nd : nodes) out.push_back({nd.succ, nd.t});
+}
+
+// Replays the waits of k_dense_persist on the host, in list order, with the tile versions
+// every earlier task leaves: true when no task waits for a later one, i.e. the persistent
+// walk cannot stall whatever the number of resident CTAs.
+static bool dense_order_ok(const int4 *tasks, int count, const std::vector<int> &super,
+                           const std::vector<int64_t> &rowptr, const std::vector<int> &toff,
+                           std::vector<int> &ver) {
+  for (int k = 0; k < count; ++k) {
+    const int4 t = tasks[k];
+    const int s = t.x, kind = t.w & 3, step = (t.w >> 2) & 0x7fff, first = t.w >> 17;
+    const int w = super[s + 1] - super[s];
+    const int m = (int)(rowptr[s + 1] - rowptr[s]);
+    const int mb = (m + TB - 1) / TB;
+    int *V = ver.data() + toff[s];
+    if (kind == 0) {
+      if (step > 0 && (V[step * mb + step] < step - 1 || V[(step - 1) * mb + step] < step))
+        return false;
+      V[step * mb + step] = step + 1;
+    } else if (kind == 1) {
+      const int nr = std::min(TB, m - t.y);
+      if (V[step * mb + step] < step + 1) return false;
+      for (int I = t.y / TB; I <= (t.y + nr - 1) / TB; ++I)
+        if (I != step && V[step * mb + I] < step) return false;
+      if (t.y % TB == 0 && w - step * TB >= TB) V[step * mb + t.y / TB] = step + 1;
+    } else {
+      const int I = t.y / TB, C = t.z / TB;
+      if (V[C * mb + I] < first || V[step * mb + I] < step + 1 || V[step * mb + C] < step + 1)
+        return false;
+      V[C * mb + I] = step + 1;
+    }
+  }
+  return true;
 }
 
 bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int *Ls,
@@ -272,6 +392,7 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
   // ---- plan ----
   P = Plan();
   P.waves.resize(nlev);
+  P.dense_toff.assign(supNo, -1);
   std::vector<std::vector<int>> by_level(nlev);
   for (int s = 0; s < supNo; ++s) by_level[level[s]].push_back(s);
   int launches = 2;
@@ -347,9 +468,36 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
       W.syrk_cnt.push_back((int)P.syrk_tasks.size() - W.syrk_off.back());
       W.diag_cnt.push_back((int)P.diag_list.size() - W.diag_off.back());
     }
-    launches += (W.small_cnt > 0) + (W.asm_cnt > 0) + (W.upd_cnt > 0) + (W.big_cnt > 0);
-    for (int j = 0; j < maxnb; ++j)
-      launches += (W.panel_cnt[j] > 0) + (W.syrk_cnt[j] > 0) + (W.diag_cnt[j] > 0);
+    launches += (W.small_cnt > 0) + (W.asm_cnt > 0) + (W.upd_cnt > 0);
+    int widest = 0;
+    for (int s : big) widest = std::max(widest, super[s + 1] - super[s]);
+    if (T.dense_dataflow && !big.empty() && (widest + TB - 1) / TB < (1 << 14)) {
+      std::vector<DenseTask> dt;
+      for (int s : big) {
+        const int w = super[s + 1] - super[s];
+        const int m = (int)(rowptr[s + 1] - rowptr[s]);
+        P.dense_toff[s] = (int)P.dense_tiles;
+        P.dense_tiles += (int64_t)((w + TB - 1) / TB) * ((m + TB - 1) / TB);
+        if (P.dense_tiles > INT32_MAX) { err = "too many dense tiles"; return false; }
+        dense_panel_tasks(s, w, m, std::max(1, T.dense_group), dt);
+      }
+      std::stable_sort(dt.begin(), dt.end(),
+                       [](const DenseTask &a, const DenseTask &b) { return a.bl > b.bl; });
+      W.dense_off = (int)P.dense_tasks.size();
+      W.dense_cnt = (int)dt.size();
+      for (const DenseTask &d : dt) P.dense_tasks.push_back(d.t);
+      std::vector<int> ver(P.dense_tiles, 0);
+      if (!dense_order_ok(P.dense_tasks.data() + W.dense_off, W.dense_cnt, super, rowptr,
+                          P.dense_toff, ver)) {
+        err = "internal: dense task order is not topological";
+        return false;
+      }
+      launches += 1;
+    } else {
+      launches += (W.big_cnt > 0);
+      for (int j = 0; j < maxnb; ++j)
+        launches += (W.panel_cnt[j] > 0) + (W.syrk_cnt[j] > 0) + (W.diag_cnt[j] > 0);
+    }
   }
   if (!P.persist_list.empty()) launches += 1;
   if (!P.tiny_list.empty()) launches += 1;
@@ -399,6 +547,11 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
         }
         K.bytes[K_ASSEMBLE] += 12.0 * (c[super[s + 1]] - c[super[s]]) + 8.0 * m * w;
       }
+    if (!P.dense_tasks.empty()) {   // one launch does the trailing updates too: one class
+      K.flops[K_PANEL] += K.flops[K_SYRK];
+      K.bytes[K_PANEL] += K.bytes[K_SYRK];
+      K.flops[K_SYRK] = K.bytes[K_SYRK] = 0.0;
+    }
   }
   H.dinv_off.assign(supNo, -1);
   H.ndinv = 0;
@@ -550,6 +703,8 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
             upload(d_pairs_, P.upd_pairs.data(), P.upd_pairs.size(), st, err) &&
             upload(d_panel_, P.panel_tasks.data(), P.panel_tasks.size(), st, err) &&
             upload(d_syrk_, P.syrk_tasks.data(), P.syrk_tasks.size(), st, err) &&
+            upload(d_dense_tasks_, P.dense_tasks.data(), P.dense_tasks.size(), st, err) &&
+            upload(d_dense_toff_, P.dense_toff.data(), P.dense_toff.size(), st, err) &&
             upload(d_dinv_off_, H.dinv_off.data(), H.dinv_off.size(), st, err) &&
             upload(d_slist_, SP.list.data(), SP.list.size(), st, err) &&
             upload(d_cptr_, SP.cptr.data(), SP.cptr.size(), st, err) &&
@@ -576,6 +731,12 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
   if (e == cudaSuccess && !P.tiny_list.empty()) tiny_ctas_ = tiny_ctas((int)P.tiny_list.size());
   if (e == cudaSuccess && !P.persist_list.empty())
     persist_ctas_ = persist_ctas(P.persist_smem, (int)P.persist_list.size());
+  // dense dataflow: one queue head per wave, then the tile version counters
+  dense_ver_len_ = (int64_t)P.waves.size() + P.dense_tiles;
+  if (e == cudaSuccess && !P.dense_tasks.empty())
+    e = cudaMalloc(&d_dense_ver_, sizeof(int) * dense_ver_len_);
+  for (Wave &W : P.waves)
+    if (W.dense_cnt > 0) W.dense_ctas = dense_ctas(W.dense_cnt);
 
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
@@ -630,6 +791,7 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec
   mark(-1, 1);
   if (!plan_.tiny_list.empty() || !plan_.persist_list.empty())
     cudaMemsetAsync(d_qctr_, 0, sizeof(int) * (nsuper_ + 2), st);
+  if (d_dense_ver_) cudaMemsetAsync(d_dense_ver_, 0, sizeof(int) * dense_ver_len_, st);
   if (!plan_.tiny_list.empty()) {
     mark(K_SMALL, 1);
     launch_factor_tiny_persist(sym_, d_upd_lbub_, d_tiny_, (int)plan_.tiny_list.size(), tiny_ctas_,
@@ -658,6 +820,16 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec
       launch_update_tiles(sym_, d_upd_tasks_ + W.upd_off, d_upd_end_ + W.upd_off, d_pairs_,
                           W.upd_cnt, st);
     mark(-1, W.upd_cnt);
+    if (W.dense_cnt > 0) {
+      // the whole dense factorization of the wave in one dataflow launch
+      mark(K_PANEL, 1);
+      const int wave = (int)(&W - plan_.waves.data());
+      launch_dense_persist(sym_, d_dense_tasks_ + W.dense_off, W.dense_cnt, W.dense_ctas,
+                           d_dense_toff_, d_dense_ver_ + plan_.waves.size(), d_dense_ver_ + wave,
+                           st);
+      mark(-1, 1);
+      continue;
+    }
     mark(K_PANEL, W.big_cnt);
     launch_diag_step(sym_, d_big_ + W.big_off, W.big_cnt, 0, st);
     mark(-1, W.big_cnt);
@@ -774,7 +946,10 @@ int Engine::finish(int *info, std::string &err) {
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) { err = std::string("factor: ") + cudaGetErrorString(e); return -1; }
   if (h_status_[1]) { err = "symbolic structure inconsistent with the matrix pattern"; return -2; }
-  if (h_status_[3]) { err = "factorization: a supernode waited too long for its descendants"; return -1; }
+  if (h_status_[3]) {
+    err = "factorization: a persistent walk waited too long (descendant supernode or dense tile)";
+    return -1;
+  }
   if (h_status_[0] != INT_MAX) {
     if (info) *info = h_status_[0];
     err = "matrix is not positive definite";

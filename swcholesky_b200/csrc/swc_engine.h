@@ -49,6 +49,8 @@ struct Wave {
   std::vector<int> panel_off, panel_cnt;  // per column block step: TRSM tiles
   std::vector<int> syrk_off, syrk_cnt;
   std::vector<int> diag_off, diag_cnt;    // per step j: supernodes whose block j+1 exists
+  int dense_off = 0, dense_cnt = 0;       // dataflow tasks of the dense factorization
+  int dense_ctas = 0;
 };
 
 // Kernel classes, for per-kernel timing (profiled factorization) and flop accounting.
@@ -74,6 +76,9 @@ struct Plan {
   std::vector<int> diag_list;
   std::vector<int> tiny_list;      // tiny supernodes of the warp walk, in level order
   std::vector<int> persist_list;   // small supernodes of the persistent walk, in level order
+  std::vector<int4> dense_tasks;   // (s, r0, c0, step << 2 | kind), per wave in topological order
+  std::vector<int> dense_toff;     // per supernode: first tile version counter (-1: none)
+  int64_t dense_tiles = 0;         // tile version counters in total
   int persist_smem = 0;
   int launches = 0;  // kernel launches per factorization
   KernelStats work;  // algorithmic flops/bytes per kernel class
@@ -241,6 +246,9 @@ class Engine {
   int *d_dinv_off_ = nullptr;
   int *d_status_ = nullptr, *h_status_ = nullptr;
   int *d_small_ = nullptr, *d_big_ = nullptr, *d_diag_ = nullptr;
+  int4 *d_dense_tasks_ = nullptr;
+  int *d_dense_toff_ = nullptr, *d_dense_ver_ = nullptr;   // ver: wave queue heads, tile counters
+  int64_t dense_ver_len_ = 0;
   cudaStream_t aux_stream_ = nullptr;          // second branch of each dense step
   cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
   int2 *d_asm_ = nullptr, *d_panel_ = nullptr;
@@ -295,6 +303,12 @@ void launch_update_tiles(const DevSym &S, const int4 *tasks, const int *task_end
 void launch_diag_step(const DevSym &S, const int *list, int count, int step, cudaStream_t st);
 void launch_trsm_step(const DevSym &S, const int2 *tasks, int count, int step, cudaStream_t st);
 void launch_syrk_step(const DevSym &S, const int4 *tasks, int count, int step, cudaStream_t st);
+// dense factorization of a wave's tiled-class panels as one persistent dataflow launch:
+// tasks in topological order, per-supernode first tile counter (toff), tile version
+// counters and the queue head (both zeroed before the launch)
+int dense_ctas(int count);
+void launch_dense_persist(const DevSym &S, const int4 *tasks, int count, int ctas, const int *toff,
+                          int *ver, int *qhead, cudaStream_t st);
 void launch_init_status(int *status, cudaStream_t st);
 bool kernels_configure(std::string &err);
 // mixed-precision Schur updates (swc_mixed.cu)

@@ -16,5 +16,6 @@ struct swc_handle {
   int device = 0;
   bool analyzed = false;
   bool factored = false;
+  int plan = 0;                             // execution-plan candidate (swc_set_plan)
   std::unique_ptr<swc::BatchState> batch;   // set by swc_batch_analyze
 };

@@ -56,6 +56,9 @@ struct Tuning {
   int tiny = 1;                          // bottom tiny supernodes: one warp each, one launch
   int persist = 1;                       // bottom small supernodes in one persistent launch
   int persist_max_smem = 48 * 1024;      // shared-memory cap of a persistent supernode (bytes)
+  int dense_dataflow = 0;                // dense steps of a wave: one dataflow launch (else
+                                         // three launches per 64-column step)
+  int dense_group = 4;                   // column blocks per grouped trailing update
 };
 
 }  // namespace swc

@@ -600,9 +600,17 @@ __global__ void __launch_bounds__(MT, 4) k_update_tiles(DevSym S, const int4 *ta
 
 // ---- one 64x64 diagonal block: POTRF and its inverse, blocked by 8 ----------------------
 // Every 8x8 block product runs on the tensor cores (DMMA); scalar FP64 work is limited to
-// the 8x8 diagonal pieces, done by one warp with shuffles.  D and E are [column][row]
-// shared arrays with leading dimension DLD; 128 threads (4 warps).
+// the 8x8 diagonal pieces, done by one warp with shuffles.  D is a [column][row] shared
+// array with leading dimension DLD; E (the inverse, lower triangular) holds only its 36
+// lower 8x8 blocks, packed: block (bi, bk), bi >= bk, at (bi (bi + 1) / 2 + bk) * 64, each
+// block column-major.  128 threads (4 warps).
 constexpr int DLD = TB + 1;
+constexpr int E_ELEMS = 36 * 64;
+
+__device__ __forceinline__ int eix(int r, int c) {
+  const int bi = r >> 3, bk = c >> 3;
+  return ((bi * (bi + 1) / 2 + bk) << 6) + ((c & 7) << 3) + (r & 7);
+}
 
 // c += A_blk * B_blk^T for 8x8 blocks of [column][row] arrays: A_blk = rows ar0..ar0+7,
 // columns ak0..ak0+7 of Am; B_blk = rows bn0..bn0+7, columns bk0..bk0+7 of Bm.
@@ -614,19 +622,6 @@ __device__ __forceinline__ void mma8_abt(double (&c)[2], const double *Am, int a
     const double a = Am[(ak0 + 4 * t + kq) * DLD + ar0 + g];
     const double b = Bm[(bk0 + 4 * t + kq) * DLD + bn0 + g];
     dmma(c, negate_a ? neg(a) : a, b);
-  }
-}
-
-// c += A_blk * B_blk for 8x8 blocks: A_blk as above, B_blk = rows bk0..bk0+7 (the k index),
-// columns bn0..bn0+7 of Bm.
-__device__ __forceinline__ void mma8_ab(double (&c)[2], const double *Am, int ar0, int ak0,
-                                        const double *Bm, int bk0, int bn0) {
-  const int lane = threadIdx.x & 31, g = lane >> 2, kq = lane & 3;
-#pragma unroll
-  for (int t = 0; t < 2; ++t) {
-    const double a = Am[(ak0 + 4 * t + kq) * DLD + ar0 + g];
-    const double b = Bm[(bn0 + g) * DLD + bk0 + 4 * t + kq];
-    dmma(c, a, b);
   }
 }
 
@@ -690,7 +685,7 @@ __device__ void potrf8_inv8(double *D, double *E, int kb, const DevSym &S, int g
   }
   if (lane < 8) {
 #pragma unroll
-    for (int i = 0; i < 8; ++i) E[(k0 + j) * DLD + k0 + i] = t[i];
+    for (int i = 0; i < 8; ++i) E[eix(k0 + i, k0 + j)] = t[i];
   }
   __syncwarp();
 }
@@ -709,7 +704,10 @@ __device__ void potrf64_blocked(double *D, double *E, int bw, const DevSym &S, i
     // panel below: X_ib = B_ib * T_kk^T (warp 0 gets ib = kb + 1)
     for (int ib = kb + 1 + warp; ib < nbk; ib += 4) {
       double c[2] = {0.0, 0.0};
-      mma8_abt(c, D, 8 * ib, 8 * kb, E, 8 * kb, 8 * kb, false);
+      const int lane = threadIdx.x & 31, g = lane >> 2, kq = lane & 3;
+#pragma unroll
+      for (int t = 0; t < 2; ++t)   // X_ib = B_ib T_kk^T
+        dmma(c, D[(8 * kb + 4 * t + kq) * DLD + 8 * ib + g], E[eix(8 * kb + g, 8 * kb + 4 * t + kq)]);
       __syncwarp();
       store8(c, D, 8 * ib, 8 * kb, false);
     }
@@ -749,7 +747,10 @@ __device__ void trtri64_blocked(const double *D, double *E, double *W, int bw) {
   for (int k = warp; k < nbk; k += 4) {
     for (int i = k + 1; i < nbk; ++i) {
       double sacc[2] = {0.0, 0.0};
-      for (int j = k; j < i; ++j) mma8_ab(sacc, D, 8 * i, 8 * j, E, 8 * j, 8 * k);
+      for (int j = k; j < i; ++j)   // sacc += L_ij T_jk
+#pragma unroll
+        for (int t = 0; t < 2; ++t)
+          dmma(sacc, D[(8 * j + 4 * t + kq) * DLD + 8 * i + g], E[eix(8 * j + 4 * t + kq, 8 * k + g)]);
       // S (C layout) -> W[col * 8 + row], read back as the B operand of T_ii * S
       Ww[(2 * kq) * 8 + g] = sacc[0];
       Ww[(2 * kq + 1) * 8 + g] = sacc[1];
@@ -757,11 +758,12 @@ __device__ void trtri64_blocked(const double *D, double *E, double *W, int bw) {
       double c[2] = {0.0, 0.0};
 #pragma unroll
       for (int t = 0; t < 2; ++t) {
-        const double a = neg(E[(8 * i + 4 * t + kq) * DLD + 8 * i + g]);
+        const double a = neg(E[eix(8 * i + g, 8 * i + 4 * t + kq)]);
         const double b = Ww[g * 8 + 4 * t + kq];
         dmma(c, a, b);
       }
-      store8(c, E, 8 * i, 8 * k, false);
+#pragma unroll
+      for (int e = 0; e < 2; ++e) E[eix(8 * i + g, 8 * k + 2 * kq + e)] = c[e];
       __syncwarp();
     }
   }
@@ -775,11 +777,12 @@ __device__ void trtri64_blocked(const double *D, double *E, double *W, int bw) {
 // updated block never leaves the chip before its factorization; when the block is narrower
 // than 64 the tile's remaining rows are panel rows below it and go to L.
 // 128 threads, DIAG_SMEM bytes of dynamic shared memory.
-constexpr int DIAG_SMEM = (2 * TB * DLD + 4 * 64) * 8;
+// shared memory: E, W (4 x 64), then D
+constexpr int DIAG_SMEM = (E_ELEMS + 4 * 64 + TB * DLD) * 8;
 
 __device__ void factor_diag_block(const DevSym &S, int s, int c0, double *smem,
                                   const TileAcc *upd) {
-  double *D = smem, *E = smem + TB * DLD, *W = E + TB * DLD;
+  double *E = smem, *W = smem + E_ELEMS, *D = W + 4 * 64;
   const int tid = threadIdx.x;
   const int f = S.super[s];
   const int w = S.super[s + 1] - f;
@@ -787,14 +790,22 @@ __device__ void factor_diag_block(const DevSym &S, int s, int c0, double *smem,
   double *P = S.L + S.xptr[s];
   const int bw = min(TB, w - c0);
   __syncthreads();
-  for (int e = tid; e < TB * TB; e += blockDim.x) {
-    const int c = e >> 6, r = e & (TB - 1);
-    double v;
-    if (c < bw && r < bw) v = (!upd && r >= c) ? P[(size_t)(c0 + c) * m + c0 + r] : 0.0;
-    else v = (r == c) ? 1.0 : 0.0;
-    D[c * DLD + r] = v;
-    E[c * DLD + r] = 0.0;
+  // eight loads in flight per thread before the shared stores (128 threads)
+  for (int e0 = tid; e0 < TB * TB; e0 += 8 * MT) {
+    double v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int e = e0 + q * MT, c = e >> 6, r = e & (TB - 1);
+      if (c < bw && r < bw) v[q] = (!upd && r >= c) ? P[(size_t)(c0 + c) * m + c0 + r] : 0.0;
+      else v[q] = (r == c) ? 1.0 : 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int e = e0 + q * MT;
+      D[(e >> 6) * DLD + (e & (TB - 1))] = v[q];
+    }
   }
+  for (int e = tid; e < E_ELEMS; e += blockDim.x) E[e] = 0.0;
   if (upd) {
     __syncthreads();
 #pragma unroll
@@ -822,22 +833,22 @@ __device__ void factor_diag_block(const DevSym &S, int s, int c0, double *smem,
     double *T = S.dinv + ((size_t)S.dinv_off[s] + c0 / TB) * (TB * TB);
     for (int e = tid; e < TB * TB; e += blockDim.x) {
       const int c = e >> 6, r = e & (TB - 1);
-      T[e] = (c < bw && r < bw && r >= c) ? E[c * DLD + r] : 0.0;
+      T[e] = (c < bw && r < bw && r >= c) ? E[eix(r, c)] : 0.0;
     }
   }
 }
 
-// Trailing SYRK/GEMM update of one 64x64 tile of a tiled-class panel by column block
-// `kblk`: tile(r0, c0) -= L[r0:, kblk] L[c0:, kblk]^T.  The accumulator is seeded with
-// minus the tile, so the tensor cores produce -(C - A B^T).
+// Trailing SYRK/GEMM update of one 64x64 tile of a tiled-class panel by column blocks
+// kblk .. kblk + nblk - 1: tile(r0, c0) -= L[r0:, blocks] L[c0:, blocks]^T.  The
+// accumulator is seeded with minus the tile, so the tensor cores produce -(C - A B^T).
 __device__ void syrk_tile_acc(const DevSym &S, int s, int r0, int c0, int kblk, double *stages,
-                              TileAcc &acc) {
+                              TileAcc &acc, int nblk = 1) {
   const int f = S.super[s];
   const int w = S.super[s + 1] - f;
   const int m = (int)(S.rowptr[s + 1] - S.rowptr[s]);
   const double *P = S.L + S.xptr[s];
   const int k0 = kblk * TB;
-  const int bk = min(TB, w - k0);
+  const int bk = min(nblk * TB, w - k0);
   const int nrow = min(TB, m - r0), ncol = min(TB, w - c0);
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
@@ -856,14 +867,15 @@ __device__ void syrk_tile_acc(const DevSym &S, int s, int r0, int c0, int kblk, 
 }
 
 // ... stored back negated.
-__device__ void syrk_tile(const DevSym &S, int s, int r0, int c0, int kblk, double *stages) {
+__device__ void syrk_tile(const DevSym &S, int s, int r0, int c0, int kblk, double *stages,
+                          int nblk = 1) {
   const int f = S.super[s];
   const int w = S.super[s + 1] - f;
   const int m = (int)(S.rowptr[s + 1] - S.rowptr[s]);
   double *P = S.L + S.xptr[s];
   const int nrow = min(TB, m - r0), ncol = min(TB, w - c0);
   TileAcc acc;
-  syrk_tile_acc(S, s, r0, c0, kblk, stages, acc);
+  syrk_tile_acc(S, s, r0, c0, kblk, stages, acc, nblk);
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const int r = acc_row(i);
@@ -880,26 +892,26 @@ __device__ void syrk_tile(const DevSym &S, int s, int r0, int c0, int kblk, doub
 
 // One CTA per supernode of the list: bring diagonal block `step` up to date (its update by
 // column block step-1, which the SYRK launch of that step leaves out) and factor it.
-__global__ void __launch_bounds__(MT) k_diag_step(DevSym S, const int *list, int count, int step) {
-  extern __shared__ double dyn[];
-  const int s = list[blockIdx.x];
+__device__ void diag_task(const DevSym &S, int s, int step, double *smem) {
   const int c0 = step * TB;
   if (step > 0) {
     TileAcc acc;
-    syrk_tile_acc(S, s, c0, c0, step - 1, dyn, acc);
-    factor_diag_block(S, s, c0, dyn, &acc);
+    syrk_tile_acc(S, s, c0, c0, step - 1, smem, acc);
+    factor_diag_block(S, s, c0, smem, &acc);
   } else {
-    factor_diag_block(S, s, c0, dyn, nullptr);
+    factor_diag_block(S, s, c0, smem, nullptr);
   }
+}
+
+__global__ void __launch_bounds__(MT) k_diag_step(DevSym S, const int *list, int count, int step) {
+  extern __shared__ double dyn[];
+  diag_task(S, list[blockIdx.x], step, dyn);
 }
 
 // task = (s, r0): B = L[r0:r0+64, blk] := B * L_blk^{-T} = B * T^T with T = L_blk^{-1},
 // stored by the CTA that factored the block (T(r, c) at T[c * 64 + r]), as one DMMA tile
 // product.
-__global__ void __launch_bounds__(MT) k_trsm_step(DevSym S, const int2 *tasks, int count,
-                                                  int step) {
-  extern __shared__ double dyn[];
-  const int s = tasks[blockIdx.x].x, r0 = tasks[blockIdx.x].y;
+__device__ void trsm_task(const DevSym &S, int s, int r0, int step, double *dyn) {
   const int f = S.super[s];
   const int w = S.super[s + 1] - f;
   const int m = (int)(S.rowptr[s + 1] - S.rowptr[s]);
@@ -929,6 +941,12 @@ __global__ void __launch_bounds__(MT) k_trsm_step(DevSym S, const int2 *tasks, i
   }
 }
 
+__global__ void __launch_bounds__(MT) k_trsm_step(DevSym S, const int2 *tasks, int count,
+                                                  int step) {
+  extern __shared__ double dyn[];
+  trsm_task(S, tasks[blockIdx.x].x, tasks[blockIdx.x].y, step, dyn);
+}
+
 // Trailing update of step `step`: task = (s, r0, c0) with c0 >= (step+1)*64, r0 >= c0.
 // The diagonal tile of the next block is left to k_diag_step, which runs concurrently.
 constexpr int SYRK_SMEM = 2 * STAGE * 8;
@@ -938,6 +956,93 @@ __global__ void __launch_bounds__(MT) k_syrk_step(DevSym S, const int4 *tasks, i
   extern __shared__ double dyn[];
   const int4 t = tasks[blockIdx.x];
   syrk_tile(S, t.x, t.y, t.z, step, dyn);
+}
+
+// ---------------------------------------------------------------------------------------
+// The same dense factorization as ONE persistent dataflow launch per wave: every diagonal
+// block, TRSM tile and trailing-update tile of the wave's tiled-class panels is a task,
+// task = (s, r0, c0, kind | step << 2 | first << 17) with kind 0: diagonal block `step`
+// (its update by block step-1, POTRF, inverse; r0 = c0 = step * 64), 1: TRSM of rows r0..
+// of block `step`, 2: update of tile (r0, c0) by the column blocks first .. step in one
+// product (updates far from the diagonal are grouped: fewer, longer products).  Tile
+// (I, J) of a panel (64-row block I, 64-column block J; I >= J) has a version counter
+// ver[toff[s] + J * mb + I] (mb = row blocks of s): the number of column blocks applied
+// to it, plus one once it is final (factored or solved).  A task waits (acquire, bounded
+// spin) for the versions it reads, runs, and publishes its tile's new version (release):
+//   diagonal block J:  ver(J, J) >= J - 1 and ver(J, J-1) >= J;       sets ver(J, J) = J + 1
+//   TRSM (r0, J):      ver(J, J) >= J + 1, ver(I, J) >= J for the row blocks I != J it
+//                      covers;                                         sets ver(I, J) = J + 1
+//   update (I, C; F..J): ver(I, C) >= F, ver(I, J) >= J + 1, ver(C, J) >= J + 1 (a final
+//                      tile (I, J) implies final tiles (I, F..J-1));   sets ver(I, C) = J + 1
+// (the TRSM of a partial last block spans two row blocks and feeds nothing in the panel;
+// a diagonal tile C gets update tasks for blocks 0 .. C-2, its diagonal task applies C-1).
+// The list is in a topological order (decreasing length of the longest chain of tasks
+// that depends on each task), so a CTA only waits for tasks taken before its own and the
+// walk progresses whatever the number of resident CTAs.  A wait gives up after
+// PERSIST_SPIN polls (or when another one has) and records the timeout in status[3].
+constexpr int DENSE_SMEM = DIAG_SMEM > SYRK_SMEM ? DIAG_SMEM : SYRK_SMEM;
+static_assert(DENSE_SMEM >= 2 * STAGE * 8, "the TRSM stages fit");
+
+__device__ __forceinline__ bool dense_wait(const int *p, int need, int *status) {
+  long long it = 0;
+  while (ld_acquire_k(p) < need) {
+    if ((++it & 31) == 0 && *(volatile int *)&status[3]) return false;
+    if (it > PERSIST_SPIN) {
+      atomicExch(&status[3], 1);
+      return false;
+    }
+    __nanosleep(32);
+  }
+  return true;
+}
+
+__global__ void __launch_bounds__(MT, 4) k_dense_persist(DevSym S, const int4 *tasks, int count,
+                                                         const int *toff, int *ver, int *qhead) {
+  extern __shared__ double dyn[];
+  __shared__ int item, ok;
+  for (;;) {
+    if (threadIdx.x == 0) item = atomicAdd(qhead, 1);
+    __syncthreads();
+    const int idx = item;
+    if (idx >= count) break;
+    const int4 t = tasks[idx];
+    const int s = t.x, kind = t.w & 3, step = (t.w >> 2) & 0x7fff, first = t.w >> 17;
+    const int w = S.super[s + 1] - S.super[s];
+    const int m = (int)(S.rowptr[s + 1] - S.rowptr[s]);
+    const int mb = (m + TB - 1) / TB;
+    int *V = ver + toff[s];
+    if (threadIdx.x == 0) {
+      bool good = true;
+      if (kind == 0) {
+        if (step > 0)
+          good = dense_wait(V + step * mb + step, step - 1, S.status) &&
+                 dense_wait(V + (step - 1) * mb + step, step, S.status);
+      } else if (kind == 1) {
+        const int nr = min(TB, m - t.y);
+        good = dense_wait(V + step * mb + step, step + 1, S.status);
+        for (int I = t.y / TB; I <= (t.y + nr - 1) / TB && good; ++I)
+          if (I != step) good = dense_wait(V + step * mb + I, step, S.status);
+      } else {
+        const int I = t.y / TB, C = t.z / TB;
+        good = dense_wait(V + C * mb + I, first, S.status) &&
+               dense_wait(V + step * mb + I, step + 1, S.status) &&
+               dense_wait(V + step * mb + C, step + 1, S.status);
+      }
+      ok = good;
+    }
+    __syncthreads();
+    if (!ok) break;
+    if (kind == 0) diag_task(S, s, step, dyn);
+    else if (kind == 1) trsm_task(S, s, t.y, step, dyn);
+    else syrk_tile(S, s, t.y, t.z, first, dyn, step - first + 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      if (kind == 0) st_release_k(V + step * mb + step, step + 1);
+      else if (kind == 2) st_release_k(V + (t.z / TB) * mb + t.y / TB, step + 1);
+      else if (t.y % TB == 0 && w - step * TB >= TB) st_release_k(V + step * mb + t.y / TB, step + 1);
+    }
+  }
 }
 
 __global__ void k_init_status(int *status) {
@@ -1063,6 +1168,9 @@ bool kernels_configure(std::string &err) {
     e = cudaFuncSetAttribute(k_diag_step, cudaFuncAttributeMaxDynamicSharedMemorySize, DIAG_SMEM);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_syrk_step, cudaFuncAttributeMaxDynamicSharedMemorySize, SYRK_SMEM);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_dense_persist, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             DENSE_SMEM);
   if (e != cudaSuccess) {
     err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e);
     return false;
@@ -1116,6 +1224,20 @@ void launch_trsm_step(const DevSym &S, const int2 *tasks, int count, int step, c
 }
 void launch_syrk_step(const DevSym &S, const int4 *tasks, int count, int step, cudaStream_t st) {
   if (count > 0) k_syrk_step<<<count, MT, SYRK_SMEM, st>>>(S, tasks, count, step);
+}
+int dense_ctas(int count) {
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_dense_persist, MT, DENSE_SMEM) !=
+          cudaSuccess || per < 1)
+    per = 1;
+  return std::max(1, std::min(count, sms * per));
+}
+void launch_dense_persist(const DevSym &S, const int4 *tasks, int count, int ctas, const int *toff,
+                          int *ver, int *qhead, cudaStream_t st) {
+  if (count > 0)
+    k_dense_persist<<<ctas, MT, DENSE_SMEM, st>>>(S, tasks, count, toff, ver, qhead);
 }
 void launch_init_status(int *status, cudaStream_t st) { k_init_status<<<1, 1, 0, st>>>(status); }
 
