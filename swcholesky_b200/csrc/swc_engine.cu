@@ -628,9 +628,9 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
         } else {
           SP.list.push_back(s);
         }
-        for (int r0 = w; r0 < m; r0 += TB) SP.contrib_tasks.push_back(make_int2(s, r0));
+        for (int r0 = w; r0 < m; r0 += SOLVE_CONTRIB_ROWS) SP.contrib_tasks.push_back(make_int2(s, r0));
         if (m > w)
-          for (int j0 = 0; j0 < w; j0 += 32) SP.gather_tasks.push_back(make_int2(s, j0));
+          for (int j0 = 0; j0 < w; j0 += SOLVE_GATHER_COLS) SP.gather_tasks.push_back(make_int2(s, j0));
       }
     }
     SP.level_off.push_back((int)SP.list.size());

@@ -31,6 +31,11 @@ bool supernode_partition(int n, const int *c, const int *r, const int nrelax[3],
 // Tile edge used by every tiled kernel.
 constexpr int TB = 64;
 
+// Task shapes of the solve's streaming kernels: rows of an off-diagonal block per forward
+// contribution task, columns per backward gather task.
+constexpr int SOLVE_CONTRIB_ROWS = 32;
+constexpr int SOLVE_GATHER_COLS = 16;
+
 // Size classes of the executor (the B200 counterpart of the reference's triple queue,
 // cholesky/tripleQueue.c:17-170): a supernode whose whole panel fits in shared memory is
 // factored by one CTA, updates included; every other supernode goes through the tiled

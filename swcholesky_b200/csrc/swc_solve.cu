@@ -23,7 +23,7 @@ constexpr int SB = 32;    // column block of the dense triangular solves (one wa
 //                 off-diagonal row of L equal to j, in increasing supernode order), so
 //                 every column sums its own list with no barrier.
 //   k_fwd_contrib c_s = L_s[rows below the diagonal block, :] y[cols of s], one CTA per
-//                 256-row slab: the off-diagonal GEMV of every supernode runs in parallel.
+//                 32-row slab: the off-diagonal GEMV of every supernode runs in parallel.
 // c_s lives at contrib + rowptr[s] - super[s] (one entry per off-diagonal row).
 __global__ void __launch_bounds__(ST) k_fwd_diag(DevSym S, const int *list, double *y,
                                                  const double *contrib, const int *cptr,
@@ -79,35 +79,39 @@ __global__ void __launch_bounds__(ST) k_fwd_diag(DevSym S, const int *list, doub
   }
 }
 
-// task = (s, r0): rows r0..r0+63 of supernode s's off-diagonal block (r0 >= w); thread
-// (row r, group q) sums the columns k = q (mod CQ), and the CQ partial sums meet in shared
-// memory in a fixed order.  CT = 1024 threads keep enough loads in flight to stream the
-// panel from HBM when a level holds only a few wide supernodes.
-constexpr int CT = 1024, CQ = CT / TB;
+// task = (s, r0): rows r0..r0+31 of supernode s's off-diagonal block (r0 >= w); warp q
+// (lane = row) sums the columns k = q (mod CQ) with four loads in flight per lane, and the
+// CQ partial sums meet in shared memory in a fixed order.  32-row tasks and 1024 threads
+// keep enough loads in flight to stream the panel from HBM when a level holds only a few
+// wide supernodes.
+constexpr int CR = SOLVE_CONTRIB_ROWS, CT = 1024, CQ = CT / CR;
+static_assert(CR == 32, "a warp covers the rows of a task");
 __global__ void __launch_bounds__(CT) k_fwd_contrib(DevSym S, const int2 *tasks,
                                                     const double *y, double *contrib, int n,
                                                     int nrhs, int64_t cstride) {
-  __shared__ double part[CQ][TB];
+  __shared__ double part[CQ][CR];
   const int s = tasks[blockIdx.x].x, r0 = tasks[blockIdx.x].y;
   const int f = S.super[s], w = S.super[s + 1] - f;
   const int64_t rb = S.rowptr[s];
   const int m = (int)(S.rowptr[s + 1] - rb);
   const double *Ls_s = S.L + S.xptr[s];
-  const int r = threadIdx.x & (TB - 1), q = threadIdx.x >> 6;
+  const int r = threadIdx.x & (CR - 1), q = threadIdx.x / CR;
   const int a = r0 + r;
   for (int rhs = 0; rhs < nrhs; ++rhs) {
     const double *yr = y + (size_t)rhs * n + f;
-    double acc0 = 0.0, acc1 = 0.0;
+    double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
     if (a < m) {
       const double *col = Ls_s + a;
       int k = q;
-      for (; k + CQ < w; k += 2 * CQ) {
+      for (; k + 3 * CQ < w; k += 4 * CQ) {
         acc0 = fma(col[(size_t)k * m], yr[k], acc0);
         acc1 = fma(col[(size_t)(k + CQ) * m], yr[k + CQ], acc1);
+        acc2 = fma(col[(size_t)(k + 2 * CQ) * m], yr[k + 2 * CQ], acc2);
+        acc3 = fma(col[(size_t)(k + 3 * CQ) * m], yr[k + 3 * CQ], acc3);
       }
-      if (k < w) acc0 = fma(col[(size_t)k * m], yr[k], acc0);
+      for (; k < w; k += CQ) acc0 = fma(col[(size_t)k * m], yr[k], acc0);
     }
-    part[q][r] = acc0 + acc1;
+    part[q][r] = (acc0 + acc1) + (acc2 + acc3);
     __syncthreads();
     if (q == 0 && a < m) {
       double t = 0.0;
@@ -119,13 +123,12 @@ __global__ void __launch_bounds__(CT) k_fwd_contrib(DevSym S, const int2 *tasks,
   }
 }
 
-// Backward solve, level by level (root first):
 //   k_bwd_gather  x[f + j] := x[f + j] - sum_{a >= w} L(a, j) x[rows[a]] for the columns
-//                 j0..j0+31 of s (one warp per column); the rows below are columns of
-//                 ancestors, already solved.
+//                 j0..j0+15 of s (one warp per column, eight loads in flight per lane);
+//                 the rows below are columns of ancestors, already solved.
 //   k_bwd_diag    x[cols of s] := L_ss^{-T} x[cols of s], one CTA per supernode.
 constexpr int GCH = 2048;       // gathered rows staged per chunk
-constexpr int GT = 32 * SB;     // one warp per column of the task
+constexpr int GT = 32 * SOLVE_GATHER_COLS;   // one warp per column of the task
 __global__ void __launch_bounds__(GT) k_bwd_gather(DevSym S, const int2 *tasks, double *x,
                                                    int n, int nrhs) {
   __shared__ double xg[GCH];
@@ -141,7 +144,9 @@ __global__ void __launch_bounds__(GT) k_bwd_gather(DevSym S, const int2 *tasks, 
   // every column of this CTA reads the same x[rows[a]]: gather them once per chunk
   for (int rhs = 0; rhs < nrhs; ++rhs) {
     double *xr = x + (size_t)rhs * n;
-    double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
+    double acc[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) acc[u] = 0.0;
     for (int a0 = w; a0 < m; a0 += GCH) {
       const int len = min(GCH, m - a0);
       __syncthreads();
@@ -150,16 +155,13 @@ __global__ void __launch_bounds__(GT) k_bwd_gather(DevSym S, const int2 *tasks, 
       if (own) {
         const double *col = Ls_s + (size_t)j * m + a0;
         int i = lane;
-        for (; i + 96 < len; i += 128) {
-          acc0 = fma(col[i], xg[i], acc0);
-          acc1 = fma(col[i + 32], xg[i + 32], acc1);
-          acc2 = fma(col[i + 64], xg[i + 64], acc2);
-          acc3 = fma(col[i + 96], xg[i + 96], acc3);
-        }
-        for (; i < len; i += 32) acc0 = fma(col[i], xg[i], acc0);
+        for (; i + 7 * 32 < len; i += 8 * 32)
+#pragma unroll
+          for (int u = 0; u < 8; ++u) acc[u] = fma(col[i + 32 * u], xg[i + 32 * u], acc[u]);
+        for (; i < len; i += 32) acc[0] = fma(col[i], xg[i], acc[0]);
       }
     }
-    double t = (acc0 + acc1) + (acc2 + acc3);
+    double t = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
     if (lane == 0 && own) xr[f + j] -= t;
