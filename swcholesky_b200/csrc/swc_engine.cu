@@ -618,6 +618,7 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
       SP.chain_off.push_back((int)SP.fchain.size());
       SP.contrib_off.push_back((int)SP.contrib_tasks.size());
       SP.gather_off.push_back((int)SP.gather_tasks.size());
+      std::vector<int2> narrow;
       for (int s : bylev[l]) {
         const int w = super[s + 1] - super[s];
         const int m = (int)(rowptr[s + 1] - rowptr[s]);
@@ -628,10 +629,13 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
         } else {
           SP.list.push_back(s);
         }
-        for (int r0 = w; r0 < m; r0 += SOLVE_CONTRIB_ROWS) SP.contrib_tasks.push_back(make_int2(s, r0));
+        for (int r0 = w; r0 < m; r0 += SOLVE_CONTRIB_ROWS)
+          (w > SOLVE_NARROW_W ? SP.contrib_tasks : narrow).push_back(make_int2(s, r0));
         if (m > w)
           for (int j0 = 0; j0 < w; j0 += SOLVE_GATHER_COLS) SP.gather_tasks.push_back(make_int2(s, j0));
       }
+      SP.contrib_wide.push_back((int)SP.contrib_tasks.size() - SP.contrib_off.back());
+      SP.contrib_tasks.insert(SP.contrib_tasks.end(), narrow.begin(), narrow.end());
     }
     SP.level_off.push_back((int)SP.list.size());
     SP.chain_off.push_back((int)SP.fchain.size());
@@ -1032,7 +1036,7 @@ void Engine::run_solve_with(double *x, int nrhs, double *contrib) {
                        x + (size_t)r * n_, contrib + (size_t)r * cs, d_cptr_, d_cidx_, d_flags_,
                        base + 2 * r + 1, n_, cs, st);
     launch_fwd_contrib(sym_, d_scontrib_ + SP.contrib_off[l], SP.contrib_off[l + 1] - SP.contrib_off[l],
-                       x, contrib, n_, nrhs, cs, st);
+                       SP.contrib_wide[l], x, contrib, n_, nrhs, cs, st);
   }
   for (int l = nl - 1; l >= 0; --l) {
     launch_bwd_gather(sym_, d_sgather_ + SP.gather_off[l], SP.gather_off[l + 1] - SP.gather_off[l],

@@ -35,6 +35,7 @@ constexpr int TB = 64;
 // contribution task, columns per backward gather task.
 constexpr int SOLVE_CONTRIB_ROWS = 32;
 constexpr int SOLVE_GATHER_COLS = 16;
+constexpr int SOLVE_NARROW_W = 64;   // contribution tasks of supernodes this narrow: a warp each
 
 // Size classes of the executor (the B200 counterpart of the reference's triple queue,
 // cholesky/tripleQueue.c:17-170): a supernode whose whole panel fits in shared memory is

@@ -86,10 +86,41 @@ __global__ void __launch_bounds__(ST) k_fwd_diag(DevSym S, const int *list, doub
 // wide supernodes.
 constexpr int CR = SOLVE_CONTRIB_ROWS, CT = 1024, CQ = CT / CR;
 static_assert(CR == 32, "a warp covers the rows of a task");
-__global__ void __launch_bounds__(CT) k_fwd_contrib(DevSym S, const int2 *tasks,
-                                                    const double *y, double *contrib, int n,
-                                                    int nrhs, int64_t cstride) {
+// Tasks of narrow supernodes (w <= SOLVE_NARROW_W) come after the nwide wide ones, one
+// warp each (lane = row, all w columns in the warp), CQ per CTA.
+__device__ void fwd_contrib_narrow(const DevSym &S, int2 task, const double *y, double *contrib,
+                                   int n, int nrhs, int64_t cstride) {
+  const int s = task.x, r0 = task.y, lane = threadIdx.x & 31;
+  const int f = S.super[s], w = S.super[s + 1] - f;
+  const int64_t rb = S.rowptr[s];
+  const int m = (int)(S.rowptr[s + 1] - rb);
+  const int a = r0 + lane;
+  if (a >= m) return;
+  const double *col = S.L + S.xptr[s] + a;
+  for (int rhs = 0; rhs < nrhs; ++rhs) {
+    const double *yr = y + (size_t)rhs * n + f;
+    double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
+    int k = 0;
+    for (; k + 3 < w; k += 4) {
+      acc0 = fma(col[(size_t)k * m], yr[k], acc0);
+      acc1 = fma(col[(size_t)(k + 1) * m], yr[k + 1], acc1);
+      acc2 = fma(col[(size_t)(k + 2) * m], yr[k + 2], acc2);
+      acc3 = fma(col[(size_t)(k + 3) * m], yr[k + 3], acc3);
+    }
+    for (; k < w; ++k) acc0 = fma(col[(size_t)k * m], yr[k], acc0);
+    contrib[(size_t)rhs * cstride + (rb - f) + (a - w)] = (acc0 + acc1) + (acc2 + acc3);
+  }
+}
+
+__global__ void __launch_bounds__(CT) k_fwd_contrib(DevSym S, const int2 *tasks, int count,
+                                                    int nwide, const double *y, double *contrib,
+                                                    int n, int nrhs, int64_t cstride) {
   __shared__ double part[CQ][CR];
+  if ((int)blockIdx.x >= nwide) {
+    const int t = nwide + ((int)blockIdx.x - nwide) * CQ + (int)(threadIdx.x >> 5);
+    if (t < count) fwd_contrib_narrow(S, tasks[t], y, contrib, n, nrhs, cstride);
+    return;
+  }
   const int s = tasks[blockIdx.x].x, r0 = tasks[blockIdx.x].y;
   const int f = S.super[s], w = S.super[s + 1] - f;
   const int64_t rb = S.rowptr[s];
@@ -514,9 +545,12 @@ void launch_fwd_diag(const DevSym &S, const int *list, int count, int smem, doub
   if (count > 0)
     k_fwd_diag<<<count, ST, smem, st>>>(S, list, y, contrib, cptr, cidx, n, nrhs, cstride);
 }
-void launch_fwd_contrib(const DevSym &S, const int2 *tasks, int count, const double *y,
-                        double *contrib, int n, int nrhs, int64_t cstride, cudaStream_t st) {
-  if (count > 0) k_fwd_contrib<<<count, CT, 0, st>>>(S, tasks, y, contrib, n, nrhs, cstride);
+void launch_fwd_contrib(const DevSym &S, const int2 *tasks, int count, int nwide,
+                        const double *y, double *contrib, int n, int nrhs, int64_t cstride,
+                        cudaStream_t st) {
+  const int blocks = nwide + (count - nwide + CQ - 1) / CQ;
+  if (count > 0)
+    k_fwd_contrib<<<blocks, CT, 0, st>>>(S, tasks, count, nwide, y, contrib, n, nrhs, cstride);
 }
 void launch_bwd_gather(const DevSym &S, const int2 *tasks, int count, double *x, int n, int nrhs,
                        cudaStream_t st) {
