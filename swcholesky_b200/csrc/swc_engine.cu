@@ -140,7 +140,7 @@ void Engine::release() {
                   d_slist_, d_cptr_, d_cidx_, d_flags_, d_fchain_, d_bchain_, d_scontrib_, d_sgather_, d_csr_rp_, d_csr_ci_,
                   d_csr_map_,
                   d_csr_val_, d_contrib_, d_work_, d_norms_, d_persist_, d_qctr_, d_npart_,
-                  d_tiny_, d_dense_tasks_, d_dense_toff_, d_dense_ver_};
+                  d_tiny_, d_dense_tasks_, d_dense_toff_, d_dense_ver_, d_swarp_};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   release_adjoint();
@@ -160,6 +160,7 @@ void Engine::release() {
   d_dense_toff_ = d_dense_ver_ = nullptr;
   dense_ver_len_ = 0;
   d_slist_ = d_cptr_ = d_cidx_ = d_flags_ = nullptr;
+  d_swarp_ = nullptr;
   d_fchain_ = d_bchain_ = nullptr;
   d_scontrib_ = d_sgather_ = nullptr;
   d_csr_rp_ = d_csr_ci_ = d_csr_map_ = nullptr;
@@ -613,8 +614,20 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
     }
     std::vector<std::vector<int>> bylev(nl);
     for (int s = 0; s < supNo; ++s) bylev[lev[s]].push_back(s);
+    auto warp_size_ok = [&](int s) {
+      const int w = super[s + 1] - super[s];
+      const int64_t m = rowptr[s + 1] - rowptr[s];
+      return H.dinv_off[s] < 0 && w <= SOLVE_WARP_W && m - w <= SOLVE_WARP_ROWS;
+    };
+    std::vector<int> warp_level(nl, 0);
+    for (int l = 0; l < nl; ++l) {
+      int cnt = 0;
+      for (int s : bylev[l]) cnt += warp_size_ok(s);
+      warp_level[l] = cnt >= SOLVE_WARP_LEVEL_MIN;
+    }
     for (int l = 0; l < nl; ++l) {
       SP.level_off.push_back((int)SP.list.size());
+      SP.warp_off.push_back((int)SP.warp_list.size());
       SP.chain_off.push_back((int)SP.fchain.size());
       SP.contrib_off.push_back((int)SP.contrib_tasks.size());
       SP.gather_off.push_back((int)SP.gather_tasks.size());
@@ -626,6 +639,9 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
           const int nb = (w + TB - 1) / TB;
           for (int k = 0; k < nb; ++k) SP.fchain.push_back(make_int2(s, k));
           for (int k = nb - 1; k >= 0; --k) SP.bchain.push_back(make_int2(s, k));
+        } else if (warp_level[l] && warp_size_ok(s)) {
+          SP.warp_list.push_back(s);   // its contributions and gathers are done by the warp
+          continue;
         } else {
           SP.list.push_back(s);
         }
@@ -638,6 +654,7 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
       SP.contrib_tasks.insert(SP.contrib_tasks.end(), narrow.begin(), narrow.end());
     }
     SP.level_off.push_back((int)SP.list.size());
+    SP.warp_off.push_back((int)SP.warp_list.size());
     SP.chain_off.push_back((int)SP.fchain.size());
     SP.contrib_off.push_back((int)SP.contrib_tasks.size());
     SP.gather_off.push_back((int)SP.gather_tasks.size());
@@ -711,6 +728,7 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
             upload(d_dense_toff_, P.dense_toff.data(), P.dense_toff.size(), st, err) &&
             upload(d_dinv_off_, H.dinv_off.data(), H.dinv_off.size(), st, err) &&
             upload(d_slist_, SP.list.data(), SP.list.size(), st, err) &&
+            upload(d_swarp_, SP.warp_list.data(), SP.warp_list.size(), st, err) &&
             upload(d_cptr_, SP.cptr.data(), SP.cptr.size(), st, err) &&
             upload(d_cidx_, SP.cidx.data(), SP.cidx.size(), st, err) &&
             upload(d_fchain_, SP.fchain.data(), SP.fchain.size(), st, err) &&
@@ -1029,6 +1047,8 @@ void Engine::run_solve_with(double *x, int nrhs, double *contrib) {
   solve_epoch_ += 2 * nrhs;
   cudaMemsetAsync(d_status_ + 2, 0, sizeof(int), st);
   for (int l = 0; l < nl; ++l) {
+    launch_fwd_warp(sym_, d_swarp_ + SP.warp_off[l], SP.warp_off[l + 1] - SP.warp_off[l], x,
+                    contrib, d_cptr_, d_cidx_, n_, nrhs, cs, st);
     launch_fwd_diag(sym_, d_slist_ + SP.level_off[l], SP.level_off[l + 1] - SP.level_off[l], smem,
                     x, contrib, d_cptr_, d_cidx_, n_, nrhs, cs, st);
     for (int r = 0; r < nrhs; ++r)
@@ -1043,6 +1063,8 @@ void Engine::run_solve_with(double *x, int nrhs, double *contrib) {
                       x, n_, nrhs, st);
     launch_bwd_diag(sym_, d_slist_ + SP.level_off[l], SP.level_off[l + 1] - SP.level_off[l], smem,
                     x, n_, nrhs, st);
+    launch_bwd_warp(sym_, d_swarp_ + SP.warp_off[l], SP.warp_off[l + 1] - SP.warp_off[l], x, n_,
+                    nrhs, st);
     for (int r = 0; r < nrhs; ++r)
       launch_bwd_chain(sym_, d_bchain_ + SP.chain_off[l], SP.chain_off[l + 1] - SP.chain_off[l],
                        x + (size_t)r * n_, d_flags_, base + 2 * r + 2, st);

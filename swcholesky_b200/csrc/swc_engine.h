@@ -97,6 +97,13 @@ void launch_bwd_gather(const DevSym &S, const int2 *tasks, int count, double *x,
                        cudaStream_t st);
 void launch_bwd_diag(const DevSym &S, const int *list, int count, int smem, double *x, int n,
                      int nrhs, cudaStream_t st);
+// small supernodes, one warp each: forward (contributions in, diagonal solve, contributions
+// of the rows below out) and backward (gather from ancestors, transposed diagonal solve)
+void launch_fwd_warp(const DevSym &S, const int *list, int count, double *y, double *contrib,
+                     const int *cptr, const int *cidx, int n, int nrhs, int64_t cstride,
+                     cudaStream_t st);
+void launch_bwd_warp(const DevSym &S, const int *list, int count, double *x, int n, int nrhs,
+                     cudaStream_t st);
 void launch_fwd_chain(const DevSym &S, const int2 *tasks, int count, double *y,
                       const double *contrib, const int *cptr, const int *cidx, int *flags,
                       int epoch, int n, int64_t cstride, cudaStream_t st);
@@ -117,6 +124,8 @@ void launch_rowabs(int n, const int *rp, const double *val, double *out, cudaStr
 struct SolvePlan {
   std::vector<int> level_off;       // small-class supernodes of level l:
   std::vector<int> list;            //   list[level_off[l] .. level_off[l+1])
+  std::vector<int> warp_off;        // small supernodes solved by one warp each (level l):
+  std::vector<int> warp_list;       //   warp_list[warp_off[l] .. warp_off[l+1])
   std::vector<int> chain_off;       // (s, block) tasks of the tiled class in level l:
   std::vector<int2> fchain, bchain; //   forward (increasing block) / backward (decreasing)
   std::vector<int> contrib_off;     // (s, r0) tasks of level l: contrib_wide[l] tasks of
@@ -268,6 +277,7 @@ class Engine {
   // solve data
   SolvePlan splan_;
   int *d_slist_ = nullptr, *d_cptr_ = nullptr, *d_cidx_ = nullptr, *d_flags_ = nullptr;
+  int *d_swarp_ = nullptr;
   int2 *d_fchain_ = nullptr, *d_bchain_ = nullptr;
   int solve_epoch_ = 0;
   int64_t nflags_ = 0;

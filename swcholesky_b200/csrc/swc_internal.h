@@ -36,6 +36,13 @@ constexpr int TB = 64;
 constexpr int SOLVE_CONTRIB_ROWS = 32;
 constexpr int SOLVE_GATHER_COLS = 16;
 constexpr int SOLVE_NARROW_W = 64;   // contribution tasks of supernodes this narrow: a warp each
+// Supernodes of the small class at most this wide, with at most SOLVE_WARP_ROWS rows below
+// the diagonal block, are solved by one warp each (both directions, fused) on levels that
+// hold at least SOLVE_WARP_LEVEL_MIN of them (enough warps to fill the GPU; a CTA per
+// supernode is faster on levels of fewer, larger ones).
+constexpr int SOLVE_WARP_W = 32;
+constexpr int SOLVE_WARP_ROWS = 256;
+constexpr int SOLVE_WARP_LEVEL_MIN = 4096;
 
 // Size classes of the executor (the B200 counterpart of the reference's triple queue,
 // cholesky/tripleQueue.c:17-170): a supernode whose whole panel fits in shared memory is

@@ -200,6 +200,99 @@ __global__ void __launch_bounds__(GT) k_bwd_gather(DevSym S, const int2 *tasks, 
   }
 }
 
+// ---- small supernodes (w <= SOLVE_WARP_W, at most SOLVE_WARP_ROWS rows below the diagonal
+// block), one warp each, lane = column of the supernode.  Forward: the contributions the
+// descendants stored for its columns, the lower solve with the diagonal block (shuffles),
+// then its own contributions to the rows below (lane = row); backward: the gather from the
+// ancestors' solved values (lane = column, walking the rows below), then the transposed
+// solve.  Level by level like the CTA kernels; a CTA holds WPC independent warps.
+constexpr int WPC = ST / 32;
+
+__global__ void __launch_bounds__(ST) k_fwd_warp(DevSym S, const int *list, int count,
+                                                 double *y, double *contrib, const int *cptr,
+                                                 const int *cidx, int n, int nrhs,
+                                                 int64_t cstride) {
+  const int t = blockIdx.x * WPC + (threadIdx.x >> 5);
+  if (t >= count) return;
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int s = list[t];
+  const int f = S.super[s], w = S.super[s + 1] - f;
+  const int64_t rb = S.rowptr[s];
+  const int m = (int)(S.rowptr[s + 1] - rb);
+  const double *Ls_s = S.L + S.xptr[s];
+  for (int rhs = 0; rhs < nrhs; ++rhs) {
+    double *yr = y + (size_t)rhs * n;
+    double *cr = contrib + (size_t)rhs * cstride;
+    double v = 0.0;
+    if (lane < w) {
+      v = yr[f + lane];
+      for (int q = cptr[f + lane]; q < cptr[f + lane + 1]; ++q) v -= cr[cidx[q]];
+    }
+    // L_ss y = v
+#pragma unroll 4
+    for (int j = 0; j < w; ++j) {
+      const double ljj = Ls_s[(size_t)j * m + j];
+      const double lij = (lane > j && lane < w) ? Ls_s[(size_t)j * m + lane] : 0.0;
+      if (lane == j) v = v / ljj;
+      const double yj = __shfl_sync(FULL, v, j);
+      if (lane > j) v = fma(-lij, yj, v);
+    }
+    if (lane < w) yr[f + lane] = v;
+    // contributions of the rows below: c[a] = sum_j L(a, j) y_j
+    for (int a0 = w; a0 < m; a0 += 32) {
+      const int a = a0 + lane;
+      double acc = 0.0;
+#pragma unroll 4
+      for (int j = 0; j < w; ++j) {
+        const double yj = __shfl_sync(FULL, v, j);
+        if (a < m) acc = fma(Ls_s[(size_t)j * m + a], yj, acc);
+      }
+      if (a < m) cr[(rb - f) + (a - w)] = acc;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(ST) k_bwd_warp(DevSym S, const int *list, int count, double *x,
+                                                 int n, int nrhs) {
+  const int t = blockIdx.x * WPC + (threadIdx.x >> 5);
+  if (t >= count) return;
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int s = list[t];
+  const int f = S.super[s], w = S.super[s + 1] - f;
+  const int64_t rb = S.rowptr[s];
+  const int m = (int)(S.rowptr[s + 1] - rb);
+  const int *rows = S.Ls + rb;
+  const double *Ls_s = S.L + S.xptr[s];
+  for (int rhs = 0; rhs < nrhs; ++rhs) {
+    double *xr = x + (size_t)rhs * n;
+    double v = 0.0;
+    if (lane < w) {
+      // x_i - sum_{a >= w} L(a, i) x[rows[a]]
+      const double *col = Ls_s + (size_t)lane * m;
+      double a0 = 0.0, a1 = 0.0;
+      int a = w;
+      for (; a + 1 < m; a += 2) {
+        a0 = fma(col[a], xr[rows[a]], a0);
+        a1 = fma(col[a + 1], xr[rows[a + 1]], a1);
+      }
+      if (a < m) a0 = fma(col[a], xr[rows[a]], a0);
+      v = xr[f + lane] - (a0 + a1);
+    }
+    // L_ss^T x = v
+#pragma unroll 4
+    for (int j = w - 1; j >= 0; --j) {
+      const double ljj = Ls_s[(size_t)j * m + j];
+      const double lji = lane < j ? Ls_s[(size_t)lane * m + j] : 0.0;
+      if (lane == j) v = v / ljj;
+      const double xj = __shfl_sync(FULL, v, j);
+      if (lane < j) v = fma(-lji, xj, v);
+    }
+    if (lane < w) xr[f + lane] = v;
+  }
+}
+
 __global__ void __launch_bounds__(ST) k_bwd_diag(DevSym S, const int *list, double *x, int n,
                                                  int nrhs) {
   extern __shared__ double v[];
@@ -551,6 +644,17 @@ void launch_fwd_contrib(const DevSym &S, const int2 *tasks, int count, int nwide
   const int blocks = nwide + (count - nwide + CQ - 1) / CQ;
   if (count > 0)
     k_fwd_contrib<<<blocks, CT, 0, st>>>(S, tasks, count, nwide, y, contrib, n, nrhs, cstride);
+}
+void launch_fwd_warp(const DevSym &S, const int *list, int count, double *y, double *contrib,
+                     const int *cptr, const int *cidx, int n, int nrhs, int64_t cstride,
+                     cudaStream_t st) {
+  if (count > 0)
+    k_fwd_warp<<<(count + WPC - 1) / WPC, ST, 0, st>>>(S, list, count, y, contrib, cptr, cidx, n,
+                                                       nrhs, cstride);
+}
+void launch_bwd_warp(const DevSym &S, const int *list, int count, double *x, int n, int nrhs,
+                     cudaStream_t st) {
+  if (count > 0) k_bwd_warp<<<(count + WPC - 1) / WPC, ST, 0, st>>>(S, list, count, x, n, nrhs);
 }
 void launch_bwd_gather(const DevSym &S, const int2 *tasks, int count, double *x, int n, int nrhs,
                        cudaStream_t st) {
