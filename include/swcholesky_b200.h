@@ -77,7 +77,9 @@ void *swc_get_stream(swc_handle_t handle);
  * walk up to 100 KB of shared memory per supernode; 2: no persistent walk (one launch per
  * level); 3: smaller small-class limits (more tiled supernodes); 4: the dense
  * factorization of each level's tiled supernodes as one persistent dataflow launch
- * instead of three launches per 64-column step.  SWC_INVALID_INPUT for other values. */
+ * instead of three launches per 64-column step; 5: in SWC_MODE_MIXED_TF32X3, the trailing
+ * SYRK steps on the tcgen05 tensor cores (TF32 products from the split mirror, TMEM
+ * accumulators).  SWC_INVALID_INPUT for other values. */
 int swc_set_plan(swc_handle_t handle, int plan);
 
 /* Uploads and validates the structure.  Arguments as in sw_cholesky_left_par_05

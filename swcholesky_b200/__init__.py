@@ -322,7 +322,7 @@ class Handle:
     def set_plan(self, plan: int):
         """Execution-plan candidate for the next analyze / batch_analyze (0 default, 1 larger
         persistent supernodes, 2 no persistent walk, 3 smaller small class, 4 dense steps
-        as one dataflow launch per level)."""
+        as one dataflow launch per level, 5 split-TF32 SYRK steps on tcgen05)."""
         _check(self._lib.swc_set_plan(self._h, int(plan)))
 
     def batch_analyze(self, mats):

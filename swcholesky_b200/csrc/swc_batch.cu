@@ -109,11 +109,12 @@ Tuning plan_candidate(int k) {
     case 2: t.persist = 0; break;                        // level-by-level launches only
     case 3: t.small_max_elems = 4096; t.small_max_m = 1024; break;   // more tiled supernodes
     case 4: t.dense_dataflow = 1; break;                 // dense steps as one dataflow launch
+    case 5: t.syrk_tc = 1; break;                        // split-TF32 SYRK steps on tcgen05
     default: break;
   }
   return t;
 }
-const int kNumPlans = 5;
+const int kNumPlans = 6;
 int num_plans() { return kNumPlans; }
 
 bool BatchState::set(int nm, const int *n, const int *c, const int *r, std::string &err) {

@@ -583,7 +583,7 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
                      const int64_t *Li_ptr, const int *blockSet, int supNo,
                      const int *prunePtr, const int *pruneSet, std::string &err) {
   cudaSetDevice(device_);
-  if (!kernels_configure(err) || !mixed_configure(err)) return false;
+  if (!kernels_configure(err) || !mixed_configure(err) || !tc_configure(err)) return false;
   HostSym H;
   Plan P;
   if (!build_plan(n, c, r, lC, Ls, Li_ptr, blockSet, supNo, prunePtr, pruneSet, H, P, err,
@@ -798,7 +798,14 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
 
 void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec) {
   const bool mixed = prec != 0;
+  const bool syrk_tc = prec == 1 && tuning_.syrk_tc;   // split-TF32 mirror: tcgen05 SYRK
   cudaStream_t st = stream_;
+  auto syrk = [&](const int4 *tasks, int count, int step) {
+    if (syrk_tc)
+      launch_syrk_step_tc(sym_, tasks, count, syrk_tc_ctas(count), step, st);
+    else
+      launch_syrk_step(sym_, tasks, count, step, st);
+  };
   // With profiling on, every launch is preceded by an event and followed by one.
   auto mark = [&](int kind, int count) {
     if (!prof || count <= 0) return;
@@ -865,7 +872,7 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec
         launch_diag_step(sym_, d_diag_ + W.diag_off[j], W.diag_cnt[j], (int)j + 1, st);
         mark(-1, W.diag_cnt[j]);
         mark(K_SYRK, W.syrk_cnt[j]);
-        launch_syrk_step(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
+        syrk(d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j);
         mark(-1, W.syrk_cnt[j]);
       } else if (W.diag_cnt[j] > 0) {
         // fork: next diagonal block on the auxiliary stream, trailing update here; join
@@ -873,10 +880,10 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec
         cudaStreamWaitEvent(aux_stream_, ev_fork_, 0);
         launch_diag_step(sym_, d_diag_ + W.diag_off[j], W.diag_cnt[j], (int)j + 1, aux_stream_);
         cudaEventRecord(ev_join_, aux_stream_);
-        launch_syrk_step(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
+        syrk(d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j);
         cudaStreamWaitEvent(st, ev_join_, 0);
       } else {
-        launch_syrk_step(sym_, d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j, st);
+        syrk(d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j);
       }
     }
   }

@@ -323,6 +323,11 @@ void launch_dense_persist(const DevSym &S, const int4 *tasks, int count, int cta
                           int *ver, int *qhead, cudaStream_t st);
 void launch_init_status(int *status, cudaStream_t st);
 bool kernels_configure(std::string &err);
+// trailing SYRK step of the split-TF32 mode on tcgen05 (swc_tc.cu): grid of ctas CTAs
+bool tc_configure(std::string &err);
+int syrk_tc_ctas(int count);
+void launch_syrk_step_tc(const DevSym &S, const int4 *tasks, int count, int ctas, int step,
+                         cudaStream_t st);
 // mixed-precision Schur updates (swc_mixed.cu)
 bool mixed_configure(std::string &err);
 void launch_update_tiles_mx(const DevSym &S, const int4 *tasks, const int *task_end,

@@ -72,6 +72,7 @@ struct Tuning {
   int dense_dataflow = 0;                // dense steps of a wave: one dataflow launch (else
                                          // three launches per 64-column step)
   int dense_group = 4;                   // column blocks per grouped trailing update
+  int syrk_tc = 0;                       // split-TF32 mode: trailing SYRK steps on tcgen05
 };
 
 }  // namespace swc
