@@ -42,13 +42,20 @@ def test_dataflow_plan_order_and_work(name):
     assert fd["update"] == fb["update"]
 
 
-def test_dataflow_plan_own_partition():
-    """Library partition of a 3D grid (relaxed supernodes: partial last column blocks,
-    narrow tiled supernodes with many rows)."""
+@pytest.mark.parametrize("max_width", [1 << 30, 200, 130, 100, 65, 64, 40])
+def test_dataflow_plan_own_partition(max_width):
+    """Library partitions of a 3D grid with supernode width caps: the tiled supernodes' last
+    column blocks are 1 to 60 columns wide or full (width mod 64 over the caps: 0, 1, 2, 4,
+    8, 16, 24, 30, 32, 36, 40, 44, 55-60), and narrow tiled supernodes have many rows."""
     A, perm, _ = W.build("grid3d_24")
-    P = W.assemble_own(A, perm)
-    swc.plan_stats(P.n, P.A2p, P.A2i, P.lC, P.Ls, P.Li_ptr, P.super, P.prunePtr, P.pruneSet,
-                   plan=DATAFLOW)
+    P = W.assemble_own(A, perm, max_width=max_width)
+    w = np.diff(P.super)
+    assert w.max() <= max_width
+    args = (P.n, P.A2p, P.A2i, P.lC, P.Ls, P.Li_ptr, P.super, P.prunePtr, P.pruneSet)
+    base = swc.plan_stats(*args)
+    df = swc.plan_stats(*args, plan=DATAFLOW)       # raises if the order could stall
+    assert df["flops"]["panel"] == pytest.approx(base["flops"]["panel"] + base["flops"]["syrk"],
+                                                 rel=1e-12)
 
 
 def test_unknown_plan_rejected():
