@@ -154,6 +154,7 @@ __global__ void __launch_bounds__(CT) k_fwd_contrib(DevSym S, const int2 *tasks,
   }
 }
 
+// Backward solve, level by level (root first):
 //   k_bwd_gather  x[f + j] := x[f + j] - sum_{a >= w} L(a, j) x[rows[a]] for the columns
 //                 j0..j0+15 of s (one warp per column, eight loads in flight per lane);
 //                 the rows below are columns of ancestors, already solved.
