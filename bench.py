@@ -11,14 +11,19 @@ factorization is timed alongside (--mode fp64 makes it the headline).
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Our arm: values already resident in HBM, K factorizations timed with CUDA events on the
-library's stream, bracketed by barrier + synchronize; max over ranks.  `e2e` times the
-reference-facing C-ABI call sw_cholesky_left_par_05 with host buffers (upload of the
-structure and values, factorization, download of L).  The reference arm (--impl reference)
-times the reference's own CPU executor (oracle/_ref) on the host cores.
+library's stream, bracketed by barrier + synchronize; max over ranks.  `e2e` times the same
+step through the public API with host buffers (values and b uploaded, x downloaded).  After
+the timed region (rank 0, one GPU): parity of the FP64 factor against the reference's own
+factor, forward error against the FP64 solution, the CPU baseline, and one compact record
+per other configuration (``configs``).  The reference arm (--impl reference) times the
+reference's own CPU executor (oracle/_ref) on the host cores; it loads neither the product
+package nor its library (the workload generator is loaded from its file: numpy and scipy
+only).
 """
 from __future__ import annotations
 
 import argparse
+import importlib.util
 import json
 import os
 import subprocess
@@ -34,6 +39,50 @@ sys.path.insert(0, ROOT)
 METRIC = ("factorization GFLOP/s (fl = sum c_j^2 / time) of the mixed-precision factor + "
           "FP64-refined solve to backward error <= 1e-12 (FP64 factor timed alongside)")
 GOLDEN = os.path.join(ROOT, "tests", "golden")
+TOL = 1e-12
+HBM_FALLBACK_GBS = 6650.0
+
+
+def matrices_module():
+    """The workload generators (swcholesky_b200/matrices.py, numpy + scipy only), loaded from
+    their file so that the reference arm never imports the product package."""
+    name = "swc_workload_matrices"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(
+        name, os.path.join(ROOT, "swcholesky_b200", "matrices.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def workload_config(name, n, nnz_lower, nsuper, xsize, fl, nrhs):
+    """The `config` object of both arms (identical keys and values for one workload)."""
+    return {"workload": name, "n": int(n), "nnz_lower": int(nnz_lower), "nsuper": int(nsuper),
+            "xsize": int(xsize), "fl": float(fl), "nrhs": int(nrhs),
+            "backward_error_target": TOL,
+            "l2": f"inputs larger than L2 (L = {xsize * 8 / 1e9:.2f} GB)"}
+
+
+def hbm_peak():
+    """(GB/s, source) of the measured HBM copy bandwidth, else the recipe's fallback."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "of measured (MEASURED_PEAKS.json hbm_gbs)"
+    except (OSError, KeyError, ValueError):
+        return HBM_FALLBACK_GBS, "of fallback (6.65 TB/s)"
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
 
 
 def load_problem(name):
@@ -123,20 +172,22 @@ def fp64_gemm_peak(torch, dev):
     return best
 
 
-def reference_time(A, perm_in, threads, budget_s, max_reps, min_reps=1):
-    """Times the reference's own FP64 executor; returns (median seconds, reps, symbolic)."""
+def reference_time(A, perm_in, threads, budget_s, max_reps, min_reps=1, keep_L=False):
+    """Times the reference's own FP64 executor; returns (median seconds, reps, symbolic,
+    the last factor L if keep_L else None)."""
     from oracle import oracle as O
     R = O.RefSymbolic(A, perm_in)
     times = []
+    L = None
     t0 = time.time()
     while len(times) < max_reps and (len(times) < min_reps or time.time() - t0 < budget_s):
-        _, t, ret = R.factor(threads=threads)
+        L, t, ret = R.factor(threads=threads)
         if ret != 1:
             raise RuntimeError("reference factorization failed")
         times.append(t)
     sym = R.sym
     R.close()
-    return float(np.median(times)), len(times), sym
+    return float(np.median(times)), len(times), sym, (L if keep_L else None)
 
 
 def max_over_ranks(value: float, world: int, device) -> float:
@@ -172,15 +223,20 @@ def profile_traffic(kernel: str, workload: str):
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the reference's own FP64 executor (sw_cholesky_left_par_05_check,
+    built from its sources into oracle/_ref) on the host cores, on this workload; rank 0
+    alone runs and prints.  Nothing of the product is imported or loaded."""
     if rank != 0:
         return
-    A, perm_in, meta, P, fl = load_problem(args.workload)
-    threads = os.cpu_count() or 1
     from oracle import oracle as O
     if not O.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libswref.so not built"}))
         return
+    M = matrices_module()
+    A, perm_in, _ = M.workload_matrix(args.workload)
+    threads = os.cpu_count() or 1
     R = O.RefSymbolic(A, perm_in)
+    s = R.sym
     for _ in range(args.warmup):
         R.factor(threads=threads)
     times = []
@@ -190,17 +246,20 @@ def run_reference(args, rank, world):
         times.append(t)
     R.close()
     t = float(np.mean(times))
+    fl = s.flops
     val = fl / t / 1e9
     line = {
         "metric": METRIC, "value": round(val, 3), "unit": "GFLOP/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded generator, reference symbolic phase)",
-        "config": {"workload": args.workload, "n": P.n, "nnz_lower": int(P.A2p[-1]),
-                   "fl": fl, "parallelism": "host cores"},
+        "data": "synthetic (seeded generator; reference symbolic phase)",
+        "config": workload_config(args.workload, s.n, s.A2p[-1], s.nsuper, s.xsize, fl,
+                                  args.nrhs),
+        "mode": "fp64 (the reference computes in FP64 only)",
+        "parallelism": f"{threads} host threads (OpenBLAS)",
         "impl": "reference",
         "cpu_baseline": {"value": round(val, 3), "unit": "GFLOP/s", "cores": threads,
-                         "kind": "reference",
+                         "kind": "reference", "cpu_model": cpu_model(),
                          "sample": f"full {args.workload} factorization per step "
                                    f"(sw_cholesky_left_par_05_check + OpenBLAS, {threads} threads)"},
         "e2e": {"value": round(val, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": 0,
@@ -236,6 +295,18 @@ def tf32_gemm_peak(torch, dev, bf16: bool = False):
     return best
 
 
+def event_ms(torch, stream, fn, reps):
+    """Mean device milliseconds of fn() over reps calls, CUDA events on `stream`."""
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -244,7 +315,7 @@ def run_ours(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     A, perm_in, meta, P, fl = load_problem(args.workload)
-    tol = 1e-12
+    tol = TOL
 
     h = swc.Handle(local_rank)
     h.analyze(P.n, P.A2p, P.A2i, P.lC, P.Ls, P.Li_ptr, P.super, P.prunePtr, P.pruneSet,
@@ -302,6 +373,7 @@ def run_ours(args, rank, world, local_rank):
     clocks.start()
     ms = timed(step_headline, args.steps)
     clk = clocks.stop()
+    x_mixed = x.cpu().numpy().copy()
     # FP64 factor followed by a refined solve, for the like-for-like comparison
     last_fp64 = {}
 
@@ -330,6 +402,15 @@ def run_ours(args, rank, world, local_rank):
                                         "(a split-TF32 product costs three TF32 products)")
     else:
         peak, psrc = peak64, "FP64 cuBLAS DGEMM 8192^3 measured in this run"
+    hbm, hbm_src = hbm_peak()
+    # HBM-bound classes: algorithmic bytes (plan builder) / device time of the class
+    hbm_classes = {}
+    for k in ("small", "assemble"):
+        lk, mk, _, bk = prof[k]
+        if mk > 0 and bk > 0:
+            gbs = bk / (mk * 1e-3) / 1e9
+            hbm_classes[k] = {"launches": lk, "ms": round(mk, 4), "algorithmic_bytes": bk,
+                              "achieved_gbs": round(gbs, 1), "frac": round(gbs / hbm, 4)}
 
     # ---- end to end through the public API with host buffers ----
     e2e = None
@@ -377,19 +458,33 @@ def run_ours(args, rank, world, local_rank):
                 t_d.append(time.perf_counter() - t0)
         e2e["dropin_fp64_ms"] = round(float(np.mean(t_d)) * 1e3, 3)
 
+    # ---- CPU baseline (the reference's own executor) and parity against its factor ----
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import oracle as O
         if O.ref_available():
             threads = os.cpu_count() or 1
-            tref, reps, _ = reference_time(A, perm_in, threads, budget_s=15.0, max_reps=5)
+            tref, reps, rsym, L_ref = reference_time(A, perm_in, threads, budget_s=15.0,
+                                                     max_reps=5, keep_L=True)
             cpu = {"value": round(fl / tref / 1e9, 3), "unit": "GFLOP/s", "cores": threads,
-                   "kind": "reference",
+                   "kind": "reference", "cpu_model": cpu_model(),
                    "sample": f"{reps} full {args.workload} FP64 factorizations, median "
                              f"(reference sw_cholesky_left_par_05_check + OpenBLAS)"}
+            if not args.no_single_thread:
+                t1, r1, _, _ = reference_time(A, perm_in, 1, budget_s=0.0, max_reps=1)
+                cpu["single_thread"] = {"value": round(fl / t1 / 1e9, 3), "unit": "GFLOP/s",
+                                        "cores": 1, "sample": f"{r1} full {args.workload} "
+                                        f"FP64 factorization, OpenBLAS 1 thread"}
+            parity = parity_record(torch, swc, h, vals, P, rsym, L_ref, b_host, x_mixed, nrhs)
+            del L_ref
         else:
             cpu = {"value": None, "unit": "GFLOP/s", "cores": 0, "kind": "reference",
                    "sample": "unavailable: oracle/_ref/libswref.so not built"}
+
+    configs = None
+    if rank == 0 and world == 1 and not args.no_extras:
+        configs = extra_configs(torch, swc, dev)
 
     if rank == 0:
         achieved = kfl / (kms * 1e-3) / 1e12
@@ -398,18 +493,18 @@ def run_ours(args, rank, world, local_rank):
         tsrc = (f"dram__bytes_read.sum + dram__bytes_write.sum per launch, ncu capture summarised "
                 f"in profiles/{kname}_{args.workload}.md" if traffic else None)
         per_step = h.launches + (last.get("iters", 0) + 1) * (solve_launches + 5)
+        executed = float(sum(v[2] for k, v in prof.items()))
+        gs = dict(np.load(os.path.join(GOLDEN, f"sym_{args.workload}.npz")))
+        nnzl = int(gs["nnzl"]) if "nnzl" in gs else None
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": {"fp64": "f64", "mixed": "f64+tf32x3", "bf16": "f64+bf16x3"}[args.mode],
             "data": "synthetic (seeded generator; reference symbolic phase via fixture)",
-            "config": {"workload": args.workload, "n": P.n, "nnz_lower": int(P.A2p[-1]),
-                       "nsuper": P.nsuper, "xsize": P.xsize, "fl": fl, "mode": args.mode,
-                       "nrhs": nrhs,
-                       "backward_error_target": tol,
-                       "parallelism": "replicas only" if world > 1 else "single GPU",
-                       "l2": f"inputs larger than L2 (L = {P.xsize * 8 / 1e9:.2f} GB)"},
+            "config": workload_config(args.workload, P.n, P.A2p[-1], P.nsuper, P.xsize, fl, nrhs),
+            "mode": args.mode,
+            "parallelism": "replicas only" if world > 1 else "single GPU",
             "headline": {"ms_factor_plus_refined_solve": round(ms, 4),
                          "ms_factor": round(ms_fact, 4),
                          "refine_iterations": last.get("iters"),
@@ -421,6 +516,13 @@ def run_ours(args, rank, world, local_rank):
                          "fp64_backward_error": last_fp64.get("berr"),
                          "speedup_vs_fp64_factor": round(ms_fp64 / ms, 3),
                          "speedup_vs_fp64_factor_plus_solve": round(ms_fp64_solve / ms, 3)},
+            "parity": parity,
+            "work": {"fl": fl, "executed_flops": executed,
+                     "executed_over_fl": round(executed / fl, 4),
+                     "nnz_L_exact": nnzl, "xsize": int(P.xsize),
+                     "xsize_over_nnz_L": round(P.xsize / nnzl, 4) if nnzl else None,
+                     "note": "executed flops: the plan builder's per-class flop model of one "
+                             "factorization on the relaxed structure (tile padding excluded)"},
             "roofline": {"bound": "tensor", "kernel": dom, "achieved": round(achieved, 4),
                          "peak": round(peak, 3) if peak else None, "unit": "TFLOP/s",
                          "frac": round(achieved / peak, 4) if peak else None,
@@ -432,14 +534,227 @@ def run_ours(args, rank, world, local_rank):
                                          "gflop": round(v[2] / 1e9, 4)}
                                      for k, v in prof.items()},
                          "classes_fp64": ({k: {"ms": round(v[1], 4)} for k, v in prof64.items()}
-                                          if prof64 else None)},
+                                          if prof64 else None),
+                         "hbm_classes": hbm_classes, "hbm_peak_gbs": hbm,
+                         "hbm_peak_source": hbm_src},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(per_step * args.steps),
             "clocks": clk,
+            "configs": configs,
         }
         print(json.dumps(line))
     h.close()
+
+
+def parity_record(torch, swc, h, vals, P, rsym, L_ref, b_host, x_mixed, nrhs):
+    """The FP64 GPU factor against the reference's own FP64 factor of the same structure,
+    and the headline solution against the FP64 solution with the reference's factor
+    (oracle C restatement of the supernodal solves).  Outside any timed region."""
+    from oracle import oracle as O
+    same = (int(rsym.xsize) == int(P.xsize) and np.array_equal(rsym.super, P.super) and
+            np.array_equal(rsym.Ls, P.Ls))
+    rec = {"structure_matches_reference": bool(same)}
+    if not same:
+        return rec
+    assert h.factor(vals, swc.SWC_MODE_FP64) == 0
+    L = h.get_L()
+    scale = float(np.abs(L_ref).max())
+    rec["L_rel_vs_reference"] = float(np.abs(L - L_ref).max() / scale)
+    rec["L_zeros_preserved"] = bool(np.all(L[L_ref == 0.0] == 0.0))
+    del L
+    xr = O.oracle_solve(P.n, P.lC, P.Ls, P.Li_ptr, L_ref, P.super,
+                        b_host.T if nrhs > 1 else b_host)
+    xm = x_mixed.T if nrhs > 1 else x_mixed
+    fe = np.abs(xm - xr).max(axis=0) / np.abs(xr).max(axis=0)
+    rec["forward_error_vs_fp64"] = [float(v) for v in np.atleast_1d(fe)]
+    rec["forward_error_note"] = ("max |x - x_fp64| / max |x_fp64| per right-hand side; x_fp64 "
+                                 "= supernodal solve with the reference's FP64 factor")
+    return rec
+
+
+def extra_configs(torch, swc, dev):
+    """One compact record per other configuration, measured after the headline (device
+    timing with CUDA events on the handle's stream; no clocks sampling).  Each is
+    independent: a failure is recorded as its error message."""
+    out = {}
+    for name, fn in (("grid2d_100", _extra_grid2d_100), ("stencil27_40", _extra_stencil),
+                     ("stencil27_40c10", _extra_stencil), ("batch256", _extra_batch),
+                     ("gmrf_500", _extra_gmrf)):
+        t0 = time.perf_counter()
+        try:
+            rec = fn(torch, swc, dev, name)
+        except Exception as exc:   # a failed sub-record must not lose the headline line
+            rec = {"error": f"{type(exc).__name__}: {exc}"}
+        rec["wall_s"] = round(time.perf_counter() - t0, 2)
+        out[name] = rec
+        torch.cuda.empty_cache()
+    return out
+
+
+def _extra_grid2d_100(torch, swc, dev, name):
+    """Config 1: 2D 5-point 100 x 100, the reference's own symbolic arrays and factor
+    (small golden fixture).  FP64 factor time and L parity; mixed factor + refined solve."""
+    g = dict(np.load(os.path.join(GOLDEN, "small_grid2d_100.npz")))
+    h = swc.Handle(dev.index or 0)
+    h.analyze(int(g["n"]), g["A2p"], g["A2i"], g["lC"], g["Ls"], g["Li_ptr"], g["super"],
+              g["prunePtr"], g["pruneSet"], g["levelPtr"], g["parPtr"], g["partition"])
+    st = torch.cuda.ExternalStream(h.stream, device=dev)
+    vals = torch.from_numpy(g["A2x"]).to(dev)
+    b = torch.from_numpy(g["b"]).to(dev)
+    x = torch.zeros_like(b)
+    fl = float(g["fl"])
+    for _ in range(3):
+        h.factor(vals)
+    ms64 = event_ms(torch, st, lambda: h.factor(vals), 20)
+    L = h.get_L()
+    rel = float(np.abs(L - g["L"]).max() / np.abs(g["L"]).max())
+    last = {}
+
+    def mx():
+        assert h.factor(vals, swc.SWC_MODE_MIXED_TF32X3) == 0
+        _, berr, it, _ = h.refine(b, tol=TOL, maxit=60, out=x)
+        last.update(berr=float(berr.max()), it=it)
+    for _ in range(3):
+        mx()
+    msmx = event_ms(torch, st, mx, 10)
+    h.close()
+    return {"n": int(g["n"]), "fl": fl, "fp64_ms_factor": round(ms64, 4),
+            "fp64_gflops": round(fl / (ms64 * 1e-3) / 1e9, 3),
+            "L_rel_vs_reference": rel,
+            "mixed_ms_factor_plus_refined_solve": round(msmx, 4),
+            "mixed_backward_error": last.get("berr"), "mixed_refine_iterations": last.get("it")}
+
+
+def _extra_stencil(torch, swc, dev, name):
+    """Config 3: 3-dof 27-point stencil 40^3 (cond ~1e6, or ~1e10 for the c10 variant), 8
+    right-hand sides.  FP64 factor; BF16x3 factor + FP64 refinement (CG fallback when it
+    stalls); per right-hand side backward error and forward error against the FP64
+    solution (FP64 factor refined to 1e-15)."""
+    _, _, meta, P, fl = load_problem(name)
+    h = swc.Handle(dev.index or 0)
+    h.analyze(P.n, P.A2p, P.A2i, P.lC, P.Ls, P.Li_ptr, P.super, P.prunePtr, P.pruneSet)
+    st = torch.cuda.ExternalStream(h.stream, device=dev)
+    vals = torch.from_numpy(P.A2x).to(dev)
+    nrhs = 8
+    b = torch.from_numpy(np.random.default_rng(3).standard_normal((nrhs, P.n))).to(dev)
+    x64 = torch.zeros_like(b)
+    x = torch.zeros_like(b)
+    h.factor(vals)
+    ms64 = event_ms(torch, st, lambda: h.factor(vals), 3)
+    _, berr64, _, _ = h.refine(b, tol=1e-15, maxit=30, out=x64)
+    last = {}
+
+    def mx():
+        assert h.factor(vals, swc.SWC_MODE_MIXED_BF16X3) == 0
+        _, berr, it, meth = h.refine(b, tol=TOL, maxit=60, out=x)
+        last.update(berr=berr, it=it, meth=meth)
+    mx()
+    msmx = event_ms(torch, st, mx, 2)
+    msf = event_ms(torch, st, lambda: h.factor(vals, swc.SWC_MODE_MIXED_BF16X3), 2)
+    xa, xr = x.cpu().numpy(), x64.cpu().numpy()
+    fe = np.abs(xa - xr).max(axis=1) / np.abs(xr).max(axis=1)
+    h.close()
+    return {"n": P.n, "fl": fl, "cond_target": meta.get("cond"), "nrhs": nrhs,
+            "fp64_ms_factor": round(ms64, 4), "fp64_gflops": round(fl / (ms64 * 1e-3) / 1e9, 3),
+            "fp64_backward_error": [float(v) for v in berr64],
+            "bf16x3_ms_factor": round(msf, 4),
+            "bf16x3_ms_factor_plus_refined_solve": round(msmx, 4),
+            "refine_iterations": last["it"],
+            "refine_method": {0: "direct", 1: "refinement", 2: "CG fallback"}[last["meth"]],
+            "backward_error": [float(v) for v in last["berr"]],
+            "forward_error_vs_fp64": [float(v) for v in fe]}
+
+
+def _extra_batch(torch, swc, dev, name):
+    """Config 4: 256 weighted 2D grids (sides 30..200) as one batch; autotuned grouping and
+    plan per mode; matrices per second of the factor and of factor + refined solve; the
+    largest per-matrix backward error."""
+    from swcholesky_b200 import matrices as Mx
+    from swcholesky_b200 import workloads as W
+    src, sides = W.batch_sources(seed=0)
+    mats = [Mx.permute_lower(A, p) for A, p in src]
+    nmat = len(mats)
+    vals = torch.from_numpy(np.concatenate([m.data for m in mats])).to(dev)
+    h = swc.Handle(dev.index or 0)
+    h.batch_analyze(mats)
+    st = torch.cuda.ExternalStream(h.stream, device=dev)
+    b = torch.from_numpy(np.random.default_rng(0).standard_normal(h.n)).to(dev)
+    x = torch.zeros_like(b)
+    cache = os.path.join(os.environ.get("TMPDIR", "/tmp"), "swc_batch_tune.txt")
+    rec = {"matrices": nmat, "n_total": int(h.n), "sides": [int(sides.min()), int(sides.max())]}
+    for tag, mode in (("fp64", swc.SWC_MODE_FP64), ("mixed", swc.SWC_MODE_MIXED_TF32X3)):
+        choice, _ = h.batch_autotune(vals, mode, cache)
+
+        def fs():
+            assert h.factor(vals, mode) == 0
+            h.refine(b, tol=TOL, maxit=60, out=x)
+        fs()
+        msf = event_ms(torch, st, lambda: h.factor(vals, mode), 5)
+        msfs = event_ms(torch, st, fs, 3)
+        per = h.batch_berr(b, x)
+        rec[tag] = {"ms_factor": round(msf, 4), "matrices_per_s": round(nmat / (msf * 1e-3), 1),
+                    "ms_factor_plus_refined_solve": round(msfs, 4),
+                    "matrices_per_s_factor_plus_solve": round(nmat / (msfs * 1e-3), 1),
+                    "berr_max": float(per.max()), "autotune": list(choice),
+                    "launches": h.launches}
+    h.close()
+    return rec
+
+
+def _extra_gmrf(torch, swc, dev, name):
+    """Config 5: GMRF 0.1 I + weighted Laplacian 500 x 500.  Time of the log-det gradient
+    and of the solve-loss gradient (after the FP64 factor); fourth-order central finite
+    differences on 64 random nonzeros: largest |fd - ad| / |ad| (plain) and with the
+    1e-3 max|ad| floor; the split-TF32 factor's log-det gradient against the FP64 one."""
+    _, _, _, P, fl = load_problem(name)
+    h = swc.Handle(dev.index or 0)
+    h.analyze(P.n, P.A2p, P.A2i, P.lC, P.Ls, P.Li_ptr, P.super, P.prunePtr, P.pruneSet)
+    st = torch.cuda.ExternalStream(h.stream, device=dev)
+    v = torch.from_numpy(P.A2x.copy()).to(dev)
+    g = torch.zeros(P.A2x.size, dtype=torch.float64, device=dev)
+    assert h.factor(v) == 0
+    h.logdet_grad(g)
+    ms_ld = event_ms(torch, st, lambda: h.logdet_grad(g), 3)
+    ad = g.cpu().numpy()
+    rng = np.random.default_rng(2024)
+    idx = rng.choice(P.A2x.size, 64, replace=False)
+    fds = []
+    for p in idx:
+        a = float(P.A2x[p])
+        hh = 1e-3 * max(abs(a), 1.0)
+        vals = []
+        for d in (2 * hh, hh, -hh, -2 * hh):
+            v[p] = a + d
+            assert h.factor(v) == 0
+            vals.append(h.logdet())
+        v[p] = a
+        fds.append((-vals[0] + 8 * vals[1] - 8 * vals[2] + vals[3]) / (12 * hh))
+    fds = np.array(fds)
+    err = np.abs(fds - ad[idx])
+    # solve-loss gradient timing: x = A^{-1} b, lam = A^{-1}(x - y)
+    b = torch.from_numpy(rng.standard_normal(P.n)).to(dev)
+    y = torch.from_numpy(rng.standard_normal(P.n)).to(dev)
+    assert h.factor(v) == 0
+    x, _, _, _ = h.refine(b, tol=1e-15, maxit=30)
+    lam, _, _, _ = h.refine((x - y).contiguous(), tol=1e-15, maxit=30)
+    gs = torch.zeros_like(g)
+    h.solve_grad(x, lam, gs)
+    ms_sg = event_ms(torch, st, lambda: h.solve_grad(x, lam, gs), 3)
+    # split-TF32 factor: log-det gradient (selected inverse of the mixed factor)
+    assert h.factor(v, swc.SWC_MODE_MIXED_TF32X3) == 0
+    h.logdet_grad(g)
+    gm = g.cpu().numpy()
+    h.close()
+    return {"n": P.n, "fl": fl, "ms_logdet_grad": round(ms_ld, 4),
+            "ms_solve_grad": round(ms_sg, 4),
+            "fd_samples": 64,
+            "fd_logdet_max_rel_plain": float((err / np.abs(ad[idx])).max()),
+            "fd_logdet_max_rel_floored": float((err / np.maximum(np.abs(ad[idx]),
+                                                                 1e-3 * np.abs(ad).max())).max()),
+            "mixed_logdet_grad_max_rel_vs_fp64": float(np.abs(gm - ad).max() / np.abs(ad).max()),
+            "mixed_note": "the split-TF32 factor's selected inverse is FP32-class; solves are "
+                          "refined in FP64"}
 
 
 def run_batch(args, rank, world, local_rank):
@@ -542,7 +857,7 @@ def run_batch(args, rank, world, local_rank):
             threads = os.cpu_count() or 1
             tot, cnt, t0 = 0.0, 0, time.time()
             for A, p in src:
-                tref, _, _ = reference_time(A, p, threads, budget_s=0.0, max_reps=1)
+                tref, _, _, _ = reference_time(A, p, threads, budget_s=0.0, max_reps=1)
                 tot += tref
                 cnt += 1
                 if time.time() - t0 > 15.0:
@@ -584,6 +899,10 @@ def main():
     ap.add_argument("--mode", default="mixed", choices=["mixed", "bf16", "fp64"],
                     help="mixed: split-TF32 Schur updates; bf16: BF16x3; fp64")
     ap.add_argument("--nrhs", type=int, default=1, help="right-hand sides per refined solve")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the per-configuration records after the headline")
+    ap.add_argument("--no-single-thread", action="store_true",
+                    help="skip the 1-thread reference timing of the CPU baseline")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -26,6 +26,8 @@ extern "C" {
 #define SWC_CUDA_ERROR 3
 #define SWC_STRUCTURE_ERROR 4  /* pattern of A does not fit the supernodal structure */
 #define SWC_NOT_READY 5        /* call order violated (e.g. factor before analyze) */
+#define SWC_TIMEOUT 6          /* a bounded device-side wait ran out (see swc_set_wait_budget);
+                                  the kernels returned and the handle stays usable */
 
 /* factorization modes */
 #define SWC_MODE_FP64 0        /* every operation in FP64 */
@@ -81,6 +83,16 @@ void *swc_get_stream(swc_handle_t handle);
  * SYRK steps on the tcgen05 tensor cores (TF32 products from the split mirror, TMEM
  * accumulators).  SWC_INVALID_INPUT for other values. */
 int swc_set_plan(swc_handle_t handle, int plan);
+
+/* Poll budget of the handle's device-side waits: the persistent walks of the
+ * factorization (a supernode waiting for its descendants, a dense tile for its
+ * predecessors) and the chained blocks of the triangular solves (a block waiting for the
+ * one before it).  A wait that is still unserved after `polls` polls gives up, the other
+ * waits of the launch give up with it, the kernels return, and the call fails with
+ * SWC_TIMEOUT.  Default 2^24 polls (seconds); polls < 0 restores it, 0 fails every wait
+ * that is not already served.  Takes effect for the next call.  No reference counterpart
+ * (the reference's level barriers are pthread joins). */
+int swc_set_wait_budget(swc_handle_t handle, long long polls);
 
 /* Uploads and validates the structure.  Arguments as in sw_cholesky_left_par_05
  * (values excluded).  levelPtr/parPtr/partition may be NULL: the executor derives its own

@@ -31,6 +31,8 @@ SWC_INVALID_INPUT = 2
 SWC_CUDA_ERROR = 3
 SWC_STRUCTURE_ERROR = 4
 SWC_NOT_READY = 5
+SWC_TIMEOUT = 6
+DEFAULT_WAIT_BUDGET = 1 << 24
 SWC_MODE_FP64 = 0
 SWC_MODE_MIXED_TF32X3 = 1
 SWC_MODE_MIXED_BF16X3 = 2
@@ -42,7 +44,7 @@ EXPORTS = (
     "swc_device_L", "swc_sizes", "swc_profile", "swc_plan_stats", "swc_layout_sizes",
     "swc_layout", "swc_solve", "swc_refine", "swc_solve_noalloc", "swc_logdet",
     "swc_logdet_grad", "swc_solve_grad", "swc_supernodes", "swc_batch_analyze",
-    "swc_batch_autotune", "swc_batch_berr", "swc_set_plan",
+    "swc_batch_autotune", "swc_batch_berr", "swc_set_plan", "swc_set_wait_budget",
 )
 KERNEL_CLASSES = ("memset", "small", "assemble", "update", "panel", "syrk")
 
@@ -87,6 +89,7 @@ def lib() -> ctypes.CDLL:
                                  ctypes.POINTER(_I), ctypes.POINTER(_I)]
         L.swc_plan_stats.argtypes = [_I] + [_VP] * 6 + [_I] + [_VP] * 2 + [_I, _VP]
         L.swc_set_plan.argtypes = [_VP, _I]
+        L.swc_set_wait_budget.argtypes = [_VP, ctypes.c_longlong]
         L.swc_layout_sizes.argtypes = [_I] + [_VP] * 3 + [_I, _VP]
         L.swc_layout.argtypes = [_I] + [_VP] * 3 + [_I] + [_VP] * 9
         L.swc_logdet.argtypes = [_VP, ctypes.POINTER(ctypes.c_double)]
@@ -324,6 +327,11 @@ class Handle:
         persistent supernodes, 2 no persistent walk, 3 smaller small class, 4 dense steps
         as one dataflow launch per level, 5 split-TF32 SYRK steps on tcgen05)."""
         _check(self._lib.swc_set_plan(self._h, int(plan)))
+
+    def set_wait_budget(self, polls: int = -1):
+        """Poll budget of the device-side waits (persistent walks, chained solve blocks);
+        a wait that runs out makes the call fail with SWC_TIMEOUT.  -1: the default."""
+        _check(self._lib.swc_set_wait_budget(self._h, int(polls)))
 
     def batch_analyze(self, mats):
         """Analyse independent ordered matrices (objects with n, indptr, indices: lower CSC

@@ -8,6 +8,7 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -43,14 +44,17 @@ def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(LIBDIR, exist_ok=True)
     objdir = os.path.join(LIBDIR, "obj")
     os.makedirs(objdir, exist_ok=True)
-    objs = []
-    for src in sources():
+    def compile_one(src):
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
         cmd = ["nvcc", *NVCC_FLAGS, "-I", INCLUDE, "-I", CSRC, "-x", "cu", "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.run(cmd, check=True)
-        objs.append(obj)
+        return obj
+
+    # translation units compile in parallel (one nvcc process each)
+    with ThreadPoolExecutor(max_workers=max(1, min(len(sources()), os.cpu_count() or 1))) as ex:
+        objs = list(ex.map(compile_one, sources()))
     tmp = LIB + ".tmp"
     cmd = ["nvcc", "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp, *objs,
            "-lcudart_static", "-lrt", "-ldl", "-lpthread"]

@@ -26,6 +26,11 @@ int fail(int code, const std::string &msg) {
   return code;
 }
 
+// Status of a failed solve: SWC_TIMEOUT when a bounded wait ran out, else a CUDA error.
+int solve_code(const std::string &err) {
+  return err.rfind("timeout:", 0) == 0 ? SWC_TIMEOUT : SWC_CUDA_ERROR;
+}
+
 std::vector<int64_t> to_i64(const size_t *p, int count) {
   std::vector<int64_t> v(count);
   for (int i = 0; i < count; ++i) v[i] = (int64_t)p[i];
@@ -100,6 +105,13 @@ int swc_set_plan(swc_handle_t h, int plan) {
 
 void *swc_get_stream(swc_handle_t h) { return h ? (void *)h->eng->stream() : nullptr; }
 
+int swc_set_wait_budget(swc_handle_t h, long long polls) {
+  if (!h) return fail(SWC_INVALID_INPUT, "null handle");
+  std::string err;
+  if (!h->eng->set_wait_budget(polls, err)) return fail(SWC_CUDA_ERROR, err);
+  return SWC_OK;
+}
+
 int swc_analyze(swc_handle_t h, int n, const int *c, const int *r, const size_t *lC,
                 const int *Ls, const size_t *Li_ptr, const int *blockSet, int supNo,
                 const int *prunePtr, const int *pruneSet, int nLevels, const int *levelPtr,
@@ -147,6 +159,7 @@ int swc_factor(swc_handle_t h, const double *values, int values_on_device, int m
   h->factored = false;
   if (rc == 1) return fail(SWC_NOT_SPD, err);
   if (rc == -2) return fail(SWC_STRUCTURE_ERROR, err);
+  if (rc == -3) return fail(SWC_TIMEOUT, err);
   return fail(SWC_CUDA_ERROR, err);
 }
 
@@ -167,7 +180,7 @@ int swc_solve(swc_handle_t h, const double *b, double *x, int nrhs, int on_devic
   if (!b || !x || nrhs <= 0) return fail(SWC_INVALID_INPUT, "bad solve arguments");
   return with_device_vectors(h, b, x, nrhs, on_device, [&](const double *db, double *dx) {
     std::string err;
-    if (!h->eng->solve(db, dx, nrhs, err)) return fail(SWC_CUDA_ERROR, err);
+    if (!h->eng->solve(db, dx, nrhs, err)) return fail(solve_code(err), err);
     return SWC_OK;
   });
 }
@@ -180,7 +193,7 @@ int swc_refine(swc_handle_t h, const double *b, double *x, int nrhs, int on_devi
   return with_device_vectors(h, b, x, nrhs, on_device, [&](const double *db, double *dx) {
     std::string err;
     swc::RefineInfo info;
-    if (!h->eng->refine(db, dx, nrhs, tol, maxit, info, err)) return fail(SWC_CUDA_ERROR, err);
+    if (!h->eng->refine(db, dx, nrhs, tol, maxit, info, err)) return fail(solve_code(err), err);
     if (berr) for (int k = 0; k < nrhs; ++k) berr[k] = info.berr[k];
     if (iterations) *iterations = info.iterations;
     if (method) *method = info.method;

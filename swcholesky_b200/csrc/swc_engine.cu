@@ -119,7 +119,7 @@ Engine::Engine(int device) : device_(device) {
   cudaStreamCreateWithFlags(&aux_stream_, cudaStreamNonBlocking);
   cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming);
   cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming);
-  cudaMallocHost(&h_status_, 4 * sizeof(int));
+  cudaMallocHost(&h_status_, kStatusWords * sizeof(int));
 }
 
 Engine::~Engine() {
@@ -741,7 +741,10 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
   if (!ok) return false;
   cudaError_t e = cudaMalloc(&d_Ax_, sizeof(double) * std::max<int64_t>(nnz, 1));
   if (e == cudaSuccess) e = cudaMalloc(&dL_, sizeof(double) * std::max<int64_t>(xsize, 1));
-  if (e == cudaSuccess) e = cudaMalloc(&d_status_, 4 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&d_status_, kStatusWords * sizeof(int));
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_status_, 0, kStatusWords * sizeof(int), st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_status_ + 4, &wait_budget_, sizeof(int), cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMalloc(&d_flags_, sizeof(int) * std::max<int64_t>(H.ndinv, 1));
   if (e == cudaSuccess) e = cudaMemsetAsync(d_flags_, 0, sizeof(int) * std::max<int64_t>(H.ndinv, 1), st);
   if (e == cudaSuccess)
@@ -976,8 +979,9 @@ int Engine::finish(int *info, std::string &err) {
   if (e != cudaSuccess) { err = std::string("factor: ") + cudaGetErrorString(e); return -1; }
   if (h_status_[1]) { err = "symbolic structure inconsistent with the matrix pattern"; return -2; }
   if (h_status_[3]) {
-    err = "factorization: a persistent walk waited too long (descendant supernode or dense tile)";
-    return -1;
+    err = "timeout: a persistent walk of the factorization waited longer than its budget "
+          "(descendant supernode or dense tile)";
+    return -3;
   }
   if (h_status_[0] != INT_MAX) {
     if (info) *info = h_status_[0];
@@ -997,6 +1001,17 @@ bool Engine::download(double *lValues, bool to_device, std::string &err) {
   d2h_bytes_ = to_device ? 0 : (int64_t)sizeof(double) * xsize_;
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
   if (e != cudaSuccess) { err = std::string("download: ") + cudaGetErrorString(e); return false; }
+  return true;
+}
+
+bool Engine::set_wait_budget(long long polls, std::string &err) {
+  wait_budget_ = polls < 0 ? kDefaultWaitBudget : (int)std::min<long long>(polls, INT_MAX);
+  if (!d_status_) return true;   // written at the next analyze
+  cudaSetDevice(device_);
+  cudaError_t e = cudaMemcpyAsync(d_status_ + 4, &wait_budget_, sizeof(int),
+                                  cudaMemcpyHostToDevice, stream_);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+  if (e != cudaSuccess) { err = std::string("wait budget: ") + cudaGetErrorString(e); return false; }
   return true;
 }
 
@@ -1082,7 +1097,11 @@ void Engine::run_solve_with(double *x, int nrhs, double *contrib) {
 bool Engine::solve_status_ok(std::string &err) {
   cudaError_t e = cudaMemcpy(h_status_ + 2, d_status_ + 2, sizeof(int), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) { err = std::string("solve status: ") + cudaGetErrorString(e); return false; }
-  if (h_status_[2]) { err = "triangular solve: a block waited too long for its predecessor"; return false; }
+  if (h_status_[2]) {
+    err = "timeout: a chained block of the triangular solve waited longer than its budget for "
+          "its predecessor";
+    return false;
+  }
   return true;
 }
 

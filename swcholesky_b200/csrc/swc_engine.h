@@ -27,13 +27,23 @@ struct DevSym {
   double *L;              // supernodal values (the reference's lValues)
   int *status;            // [0] = smallest failing column + 1 (INT_MAX if none),
                           // [1] = structure error flag, [2] = solve wait timeout,
-                          // [3] = factorization wait timeout (persistent walk)
+                          // [3] = factorization wait timeout (persistent walk),
+                          // [4] = poll budget of every bounded wait (set by the host)
   float2 *Lf;             // split mirror of L (mixed-precision only, else null): per value
                           // {hi, lo} TF32 pair, or three bfloat16 pieces (mirror_kind)
   int mirror_kind;        // MIRROR_TF32X2 or MIRROR_BF16X3
   double *dinv;           // scratch: inverses of the 64x64 diagonal blocks of the tiled class
   const int *dinv_off;    // per supernode: first block of its inverses in dinv (-1: none)
 };
+
+// Status words per handle (see DevSym::status) and the default poll budget of a wait.
+constexpr int kStatusWords = 8;
+constexpr int kDefaultWaitBudget = 1 << 24;
+
+// Poll budget of a bounded device-side wait, as the host set it in status[4].
+__device__ __forceinline__ long long wait_budget(const int *status) {
+  return (long long)*(volatile const int *)&status[4];
+}
 
 // Formats of the split mirror (8 bytes per value).
 constexpr int MIRROR_TF32X2 = 0;   // {hi, lo} floats holding TF32 values
@@ -202,6 +212,8 @@ class Engine {
   // Plan parameters used by the next analyze.
   void set_tuning(const Tuning &t) { tuning_ = t; }
   const Tuning &tuning() const { return tuning_; }
+  // Poll budget of the device-side waits (status[4]); < 0 restores the default.
+  bool set_wait_budget(long long polls, std::string &err);
   int64_t xsize() const { return xsize_; }
   int n() const { return n_; }
   int64_t nnz() const { return nnz_; }
@@ -243,6 +255,7 @@ class Engine {
   bool set_mode(int prec, std::string &err);
   int finish(int *info, std::string &err);
   int64_t h2d_bytes_ = 0, d2h_bytes_ = 0;
+  int wait_budget_ = kDefaultWaitBudget;
   int device_ = 0;
   cudaStream_t stream_ = nullptr;
   cudaStream_t own_stream_ = nullptr;

@@ -268,9 +268,8 @@ __global__ void __launch_bounds__(NT) k_factor_small(DevSym S, const int2 *lbub,
 // CTA only waits for supernodes taken from the queue before its own, which were taken by
 // CTAs already running and waiting on even earlier ones, so the walk always progresses,
 // whatever the number of resident CTAs.  qctr[0] is the queue head, qctr[1 + s] the done
-// flag of supernode s; both are zeroed before every launch.  A wait gives up after
-// PERSIST_SPIN polls and records the timeout in status[3].
-constexpr long long PERSIST_SPIN = 1LL << 24;
+// flag of supernode s; both are zeroed before every launch.  A wait gives up after the
+// poll budget in status[4] and records the timeout in status[3].
 
 __device__ __forceinline__ int ld_acquire_k(const int *p) {
   int v;
@@ -295,11 +294,12 @@ __global__ void __launch_bounds__(NT) k_factor_small_persist(DevSym S, const int
     const int s = order[idx];
     if (threadIdx.x < 32) {   // warp 0 waits for the update sources, one lane per source
       bool timed_out = false;
+      const long long budget = wait_budget(S.status);
       for (int q = S.upd_ptr[s] + threadIdx.x; q < S.upd_ptr[s + 1] && !timed_out; q += 32) {
         const int *flag = done + S.upd[q];
         long long it = 0;
         while (ld_acquire_k(flag) == 0) {
-          if (++it > PERSIST_SPIN) {
+          if (++it > budget) {
             atomicExch(&S.status[3], 1);
             timed_out = true;
             break;
@@ -979,15 +979,16 @@ __global__ void __launch_bounds__(MT) k_syrk_step(DevSym S, const int4 *tasks, i
 // The list is in a topological order (decreasing length of the longest chain of tasks
 // that depends on each task), so a CTA only waits for tasks taken before its own and the
 // walk progresses whatever the number of resident CTAs.  A wait gives up after
-// PERSIST_SPIN polls (or when another one has) and records the timeout in status[3].
+// poll budget in status[4] (or when another one has) and records the timeout in status[3].
 constexpr int DENSE_SMEM = DIAG_SMEM > SYRK_SMEM ? DIAG_SMEM : SYRK_SMEM;
 static_assert(DENSE_SMEM >= 2 * STAGE * 8, "the TRSM stages fit");
 
 __device__ __forceinline__ bool dense_wait(const int *p, int need, int *status) {
   long long it = 0;
+  const long long budget = wait_budget(status);
   while (ld_acquire_k(p) < need) {
     if ((++it & 31) == 0 && *(volatile int *)&status[3]) return false;
-    if (it > PERSIST_SPIN) {
+    if (it > budget) {
       atomicExch(&status[3], 1);
       return false;
     }
@@ -1127,11 +1128,12 @@ __global__ void __launch_bounds__(TW * 32) k_factor_tiny_persist(DevSym S, const
     if (idx >= count) break;
     const int s = order[idx];
     bool timed_out = false;
+    const long long budget = wait_budget(S.status);
     for (int q = S.upd_ptr[s] + lane; q < S.upd_ptr[s + 1] && !timed_out; q += 32) {
       const int *flag = done + S.upd[q];
       long long it = 0;
       while (ld_acquire_k(flag) == 0) {
-        if (++it > PERSIST_SPIN) {
+        if (++it > budget) {
           atomicExch(&S.status[3], 1);
           timed_out = true;
           break;

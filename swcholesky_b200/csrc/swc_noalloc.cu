@@ -60,13 +60,16 @@ extern "C" int swc_solve_noalloc(swc_handle_t h, const double *b, double *x, int
   if (!h) return swc::set_last_error("null handle"), SWC_INVALID_INPUT;
   if (!h->factored) return swc::set_last_error("solve before a successful factor"), SWC_NOT_READY;
   if (!b || !x || nrhs <= 0) return swc::set_last_error("bad solve arguments"), SWC_INVALID_INPUT;
-  if (cudaSetDevice(h->device) != cudaSuccess) return SWC_CUDA_ERROR;
+  const cudaError_t e = cudaSetDevice(h->device);
+  if (e != cudaSuccess)
+    return swc::set_last_error(std::string("cudaSetDevice: ") + cudaGetErrorString(e)), SWC_CUDA_ERROR;
   double *scratch = nullptr;
   if (!scratch_address(h->device, &scratch)) return SWC_CUDA_ERROR;
   std::string err;
   if (!h->eng->solve_in_scratch(b, x, nrhs, scratch, SWC_SOLVE_NOALLOC_MAX, err)) {
     swc::set_last_error(err);
-    return err.rfind("solve needs", 0) == 0 ? SWC_INVALID_INPUT : SWC_CUDA_ERROR;
+    if (err.rfind("solve needs", 0) == 0) return SWC_INVALID_INPUT;
+    return err.rfind("timeout:", 0) == 0 ? SWC_TIMEOUT : SWC_CUDA_ERROR;
   }
   return SWC_OK;
 }

@@ -345,9 +345,8 @@ __global__ void __launch_bounds__(ST) k_bwd_diag(DevSym S, const int *list, doub
 // (flag == epoch), and applies its own block through the stored inverse of the 64x64
 // diagonal block (DMMA-free GEMVs: the work per block is small and latency-bound).  All
 // CTAs of a chain are resident together (a few hundred at most) and only wait on CTAs with
-// a lower blockIdx, which the hardware dispatches first.  Waits are bounded: after
-// SPIN_LIMIT polls the CTA records a timeout in status[2] and stops waiting.
-constexpr long long SPIN_LIMIT = 1LL << 24;
+// a lower blockIdx, which the hardware dispatches first.  Waits are bounded: after the poll
+// budget in status[4] the CTA records a timeout in status[2] and stops waiting.
 
 __device__ __forceinline__ int ld_acquire(const int *p) {
   int v;
@@ -358,14 +357,16 @@ __device__ __forceinline__ void st_release(int *p, int v) {
   asm volatile("st.release.gpu.global.s32 [%0], %1;\n" ::"l"(p), "r"(v));
 }
 
-// thread 0 polls, everyone waits at the barrier; returns false after a timeout
+// thread 0 polls, everyone waits at the barrier; returns false after a timeout (its own,
+// or one another block recorded: a block that gave up never publishes its flag)
 __device__ bool wait_flag(const int *flag, int val, int *status) {
   __shared__ int ok;
   if (threadIdx.x == 0) {
     long long it = 0;
+    const long long budget = wait_budget(status);
     ok = 1;
     while (ld_acquire(flag) != val) {
-      if (++it > SPIN_LIMIT) {
+      if (++it > budget || ((it & 31) == 0 && *(volatile int *)&status[2])) {
         atomicExch(&status[2], 1);
         ok = 0;
         break;

@@ -25,6 +25,8 @@ __all__ = [
     "stencil27_3dof",
     "nested_dissection",
     "permute_lower",
+    "cond_shift",
+    "workload_matrix",
 ]
 
 
@@ -211,3 +213,44 @@ def permute_lower(A: LowerCSC, perm: np.ndarray) -> LowerCSC:
     p = np.asarray(perm)
     B = full[p][:, p]
     return LowerCSC.from_scipy(B)
+
+
+def cond_shift(L: LowerCSC, cond: float) -> float:
+    """Diagonal shift giving cond(L + shift*I) = cond for a singular PSD graph Laplacian L
+    (lambda_min = 0), from a Lanczos estimate of lambda_max."""
+    import scipy.sparse.linalg as sla
+    lmax = float(sla.eigsh(L.to_scipy_full(), k=1, which="LA", return_eigenvectors=False,
+                           tol=1e-6)[0])
+    return lmax / (cond - 1.0)
+
+
+def workload_matrix(name: str):
+    """A named workload: (A as LowerCSC in the original order, user permutation, meta).
+
+    grid2d_<k>: 2D 5-point Laplacian k x k (Dirichlet); grid3d_<k>: 3D 7-point Laplacian
+    k^3 plus 1e-3 I; stencil27_<k>[c10]: 3-dof 27-point weighted stencil k^3 shifted to
+    cond ~1e6 (~1e10 with the c10 suffix); gmrf_<k>: 0.1 I + log-normal(0.7) weighted
+    5-point Laplacian k x k.  The permutation is the geometric nested dissection of the
+    grid.  Depends on numpy and scipy only."""
+    if name.startswith("grid2d_"):
+        k = int(name.split("_")[1])
+        return laplacian_2d(k), nested_dissection((k, k)), dict(kind="laplacian2d", k=k)
+    if name.startswith("grid3d_"):
+        k = int(name.split("_")[1])
+        shift = 1e-3
+        return (laplacian_3d(k, shift), nested_dissection((k, k, k)),
+                dict(kind="laplacian3d", k=k, shift=shift))
+    if name.startswith("stencil27_"):
+        tag = name.split("_")[1]
+        cond = 1e10 if tag.endswith("c10") else 1e6
+        k = int(tag.replace("c10", ""))
+        L0 = stencil27_3dof(k, sigma=1.0, shift=0.0, seed=0)
+        shift = cond_shift(L0, cond)
+        A = stencil27_3dof(k, sigma=1.0, shift=shift, seed=0)
+        return A, nested_dissection((k, k, k), dof=3), dict(kind="stencil27x3", k=k,
+                                                                 cond=cond, shift=shift)
+    if name.startswith("gmrf_"):
+        k = int(name.split("_")[1])
+        A = weighted_grid_2d(k, sigma=0.7, shift=0.1, seed=0)
+        return A, nested_dissection((k, k)), dict(kind="gmrf", k=k, kappa2=0.1)
+    raise KeyError(name)

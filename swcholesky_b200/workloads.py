@@ -31,38 +31,13 @@ __all__ = ["build", "assemble", "assemble_own", "batch_matrices", "Problem", "co
 
 
 def cond_shift(L: M.LowerCSC, cond: float) -> float:
-    """Diagonal shift giving cond(L + shift*I) = cond for a singular PSD graph Laplacian L
-    (lambda_min = 0), from a Lanczos estimate of lambda_max."""
-    import scipy.sparse.linalg as sla
-    lmax = float(sla.eigsh(L.to_scipy_full(), k=1, which="LA", return_eigenvectors=False,
-                           tol=1e-6)[0])
-    return lmax / (cond - 1.0)
+    """Diagonal shift giving cond(L + shift*I) = cond (see ``matrices.cond_shift``)."""
+    return M.cond_shift(L, cond)
 
 
 def build(name: str):
     """Returns (A as LowerCSC in the original order, user permutation, meta dict)."""
-    if name.startswith("grid2d_"):
-        k = int(name.split("_")[1])
-        return M.laplacian_2d(k), M.nested_dissection((k, k)), dict(kind="laplacian2d", k=k)
-    if name.startswith("grid3d_"):
-        k = int(name.split("_")[1])
-        shift = 1e-3
-        return (M.laplacian_3d(k, shift), M.nested_dissection((k, k, k)),
-                dict(kind="laplacian3d", k=k, shift=shift))
-    if name.startswith("stencil27_"):
-        tag = name.split("_")[1]
-        cond = 1e10 if tag.endswith("c10") else 1e6
-        k = int(tag.replace("c10", ""))
-        L0 = M.stencil27_3dof(k, sigma=1.0, shift=0.0, seed=0)
-        shift = cond_shift(L0, cond)
-        A = M.stencil27_3dof(k, sigma=1.0, shift=shift, seed=0)
-        return A, M.nested_dissection((k, k, k), dof=3), dict(kind="stencil27x3", k=k,
-                                                                   cond=cond, shift=shift)
-    if name.startswith("gmrf_"):
-        k = int(name.split("_")[1])
-        A = M.weighted_grid_2d(k, sigma=0.7, shift=0.1, seed=0)
-        return A, M.nested_dissection((k, k)), dict(kind="gmrf", k=k, kappa2=0.1)
-    raise KeyError(name)
+    return M.workload_matrix(name)
 
 
 @dataclass

@@ -10,7 +10,8 @@ is not available:
   reference's factor L, and a seeded right-hand side.  These pin the oracle and the GPU.
 * ``sym_<name>.npz`` -- large workloads: the reference's final permutation (after its
   weighted postorder), its supernode partition, and checks on the derived structure (xsize,
-  length and SHA-256 of Ls, flop count fl = sum_j c_j^2 from its exact column counts).  The
+  length and SHA-256 of Ls, flop count fl = sum_j c_j^2 and nnz(L) = sum_j c_j from its
+  exact column counts).  The
   matrix values are regenerated from the seeded generators; the layout is rebuilt from the
   partition with the library's layout builder and checked against these values.
 
@@ -58,7 +59,8 @@ def make(name: str):
         np.savez_compressed(
             os.path.join(HERE, f"sym_{name}.npz"), n=s.n, perm=s.perm, super=s.super,
             xsize=s.xsize, ls_len=s.Ls.size, ls_sha256=ls_digest(s.Ls), fl=s.flops,
-            nnz_a2=s.A2p[-1], prune_len=s.pruneSet.size, maxSupWid=s.maxSupWid)
+            nnzl=int(s.colcount.astype(np.int64).sum()), nnz_a2=s.A2p[-1],
+            prune_len=s.pruneSet.size, maxSupWid=s.maxSupWid)
         print(f"sym_{name}: n={s.n} nsuper={s.nsuper} xsize={s.xsize} fl={s.flops:.4g}")
     R.close()
 

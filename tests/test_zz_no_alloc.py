@@ -24,24 +24,42 @@ def test_solve_noalloc_matches_solve(cuda_ok):
     gs = load_sym("grid3d_24")
     A, _, _ = W.build("grid3d_24")
     P = W.assemble(A, gs["perm"], gs["super"])
-    h = swc.Handle(0)
-    h.analyze(P.n, P.A2p, P.A2i, P.lC, P.Ls, P.Li_ptr, P.super, P.prunePtr, P.pruneSet)
-    assert h.factor(P.A2x) == 0
     L = swc.lib()
     nrhs = 2
     rng = np.random.default_rng(7)
     b = torch.from_numpy(rng.standard_normal((nrhs, P.n))).cuda()   # column-major (n, nrhs)
-    x_ref = torch.zeros_like(b)
-    assert L.swc_solve(h._h, ctypes.c_void_p(b.data_ptr()), ctypes.c_void_p(x_ref.data_ptr()),
-                       nrhs, 1) == swc.SWC_OK
-    for _ in range(2):
+    # the allocation-free solve runs first on its handle (no swc_solve workspace exists)
+    h = swc.Handle(0)
+    h.analyze(P.n, P.A2p, P.A2i, P.lC, P.Ls, P.Li_ptr, P.super, P.prunePtr, P.pruneSet)
+    assert h.factor(P.A2x) == 0
+    xs = []
+    free_after_first = None
+    for call in range(2):
         x = torch.full_like(b, float("nan"))
+        torch.cuda.synchronize()   # b and the NaN fill are on torch's stream, the solve on the handle's
+        if call == 1:
+            free_after_first = torch.cuda.mem_get_info()[0]
         rc = L.swc_solve_noalloc(h._h, ctypes.c_void_p(b.data_ptr()),
                                  ctypes.c_void_p(x.data_ptr()), nrhs)
         assert rc == swc.SWC_OK, L.swc_last_error().decode()
         torch.cuda.synchronize()
-        ref = x_ref.cpu().numpy()
-        assert np.abs(x.cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
+        if call == 1:
+            # the second call allocated no device memory
+            assert torch.cuda.mem_get_info()[0] == free_after_first
+        xs.append(x.cpu().numpy())
+    # the reference result: swc_solve on a second handle with the same factor
+    h2 = swc.Handle(0)
+    h2.analyze(P.n, P.A2p, P.A2i, P.lC, P.Ls, P.Li_ptr, P.super, P.prunePtr, P.pruneSet)
+    assert h2.factor(P.A2x) == 0
+    x_ref = torch.zeros_like(b)
+    torch.cuda.synchronize()
+    assert L.swc_solve(h2._h, ctypes.c_void_p(b.data_ptr()), ctypes.c_void_p(x_ref.data_ptr()),
+                       nrhs, 1) == swc.SWC_OK
+    torch.cuda.synchronize()
+    ref = x_ref.cpu().numpy()
+    for x in xs:
+        assert np.isfinite(x).all()
+        assert np.abs(x - ref).max() <= 1e-12 * np.abs(ref).max()
 
 
 def test_solve_noalloc_rejects_oversized(cuda_ok):
