@@ -31,9 +31,13 @@ extern "C" {
 
 /* factorization modes */
 #define SWC_MODE_FP64 0        /* every operation in FP64 */
-#define SWC_MODE_MIXED_TF32X3 1 /* Schur updates of the wide supernodes as split-TF32 tensor-core
-                                   products (FP32-class accuracy, FP32/FP64 accumulation); POTRF,
-                                   TRSM and small supernodes in FP64.  Pair with swc_refine. */
+#define SWC_MODE_MIXED_TF32X3 1 /* Schur updates of the wide supernodes (descendant updates and
+                                   the trailing updates of their dense factorization) as
+                                   split-TF32 products on the tcgen05 tensor cores (each value
+                                   as hi + lo TF32 pieces, all four piece products, FP32
+                                   accumulation per group of descendants, FP64 across groups);
+                                   POTRF, TRSM and small supernodes in FP64.  Pair with
+                                   swc_refine. */
 #define SWC_MODE_MIXED_BF16X3 2 /* the same Schur updates as BF16x3 split products: each value as
                                    three bfloat16 pieces, the six piece products down to the
                                    third order, FP32 accumulation (about FP32 accuracy) */
@@ -80,8 +84,8 @@ void *swc_get_stream(swc_handle_t handle);
  * level); 3: smaller small-class limits (more tiled supernodes); 4: the dense
  * factorization of each level's tiled supernodes as one persistent dataflow launch
  * instead of three launches per 64-column step; 5: in SWC_MODE_MIXED_TF32X3, the trailing
- * SYRK steps on the tcgen05 tensor cores (TF32 products from the split mirror, TMEM
- * accumulators).  SWC_INVALID_INPUT for other values. */
+ * SYRK steps of the dense factorization in FP64 (DMMA) instead of split-TF32 tcgen05
+ * products.  SWC_INVALID_INPUT for other values. */
 int swc_set_plan(swc_handle_t handle, int plan);
 
 /* Poll budget of the handle's device-side waits: the persistent walks of the
@@ -228,6 +232,32 @@ int swc_batch_berr(swc_handle_t handle, const double *b, const double *x, int on
  * swc_layout.  No reference counterpart as a function (it is part of analyze_p2). */
 int swc_supernodes(int n, const int *c, const int *r, const int *nrelax, const double *zrelax,
                    int max_width, int *blockSet, int *supNo);
+
+/* ---- input files and fill-reducing ordering (host only) ---------------------------
+ * swc_read_mtx replaces the reference's readMatrix (common/Util.h:77-179): a Matrix Market
+ * coordinate file of a square real or integer matrix, symmetric or general (a general one
+ * must be numerically symmetric), entries in any order, duplicates summed, upper entries of
+ * a symmetric file mirrored, comments and blank lines anywhere before the entries, empty
+ * columns allowed.  Result: the lower triangle in CSC form (n + 1 column pointers, row
+ * indices sorted, the diagonal present in every column -- an explicit 0 where the file has
+ * none) in arrays allocated with malloc; release each with swc_free.  Malformed files fail
+ * with SWC_INVALID_INPUT and a message (the reference's reader returns false or silently
+ * misreads).  swc_write_mtx writes a lower CSC matrix as a symmetric coordinate file that
+ * both readers accept (1-based, column by column).
+ * swc_read_perm / swc_write_perm replace the raw permutation read of the reference's driver
+ * (examples/sw_choleskyTest01.cpp:70-82): n native size_t values, perm[k] = original index
+ * at new position k; the reader checks the file's length and that it is a permutation.
+ * swc_order_nd: the project's own fill-reducing ordering for any sparse symmetric pattern
+ * (lower or full CSC): nested dissection by breadth-first level-structure separators,
+ * exact minimum degree on subgraphs of at most `leaf` vertices (<= 64; 0 for the default
+ * 64).  The reference needs the ordering as an input file (cholesky/sw_LSparsity.h:461-468). */
+int swc_read_mtx(const char *path, int *n, int **colptr, int **rowind, double **values);
+void swc_free(void *p);
+int swc_write_mtx(const char *path, int n, const int *colptr, const int *rowind,
+                  const double *values);
+int swc_read_perm(const char *path, int n, size_t *perm);
+int swc_write_perm(const char *path, int n, const size_t *perm);
+int swc_order_nd(int n, const int *colptr, const int *rowind, int leaf, size_t *perm);
 
 #ifdef __cplusplus
 }

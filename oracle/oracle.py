@@ -1,5 +1,6 @@
 """TEST ORACLE ONLY -- Python access to the two CPU checkers for the CUDA library.
 
+* ``ref_read_matrix``: the reference's Matrix Market reader (readMatrix, common/Util.h).
 * ``RefSymbolic`` / ``ref_factor``: the reference's own host symbolic phase (analyze_p2,
   ``cholesky/sw_LSparsity.h:248-702``) and FP64 numeric executor
   (``cholesky/sw_parallel_PB_Cholesky_05_check.c:43-692``), compiled from the reference
@@ -47,6 +48,9 @@ def _load_ref():
         lib.swc_ref_factor.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                        ctypes.c_int, ctypes.c_void_p]
         lib.swc_ref_free.argtypes = [ctypes.c_void_p]
+        lib.swc_ref_read_matrix.restype = ctypes.c_int
+        lib.swc_ref_read_matrix.argtypes = [ctypes.c_char_p] + [ctypes.c_void_p] * 5
+        lib.swc_ref_free_matrix.argtypes = [ctypes.c_void_p] * 3
         _ref = lib
     return _ref
 
@@ -150,6 +154,25 @@ class RefSymbolic:
             self.close()
         except Exception:
             pass
+
+
+def ref_read_matrix(path):
+    """The reference's readMatrix (common/Util.h:77-179) on a file: (n, indptr, indices,
+    data) of the lower CSC matrix it builds, or None when it reports failure."""
+    lib = _load_ref()
+    n, nnz = ctypes.c_longlong(0), ctypes.c_longlong(0)
+    c, r = ctypes.POINTER(ctypes.c_int)(), ctypes.POINTER(ctypes.c_int)()
+    v = ctypes.POINTER(ctypes.c_double)()
+    if not lib.swc_ref_read_matrix(os.fsencode(path), ctypes.byref(n), ctypes.byref(nnz),
+                                   ctypes.byref(c), ctypes.byref(r), ctypes.byref(v)):
+        return None
+    nn, nz = int(n.value), int(nnz.value)
+    out = (nn, np.ctypeslib.as_array(c, shape=(nn + 1,)).copy(),
+           np.ctypeslib.as_array(r, shape=(nz,)).copy(),
+           np.ctypeslib.as_array(v, shape=(nz,)).copy())
+    lib.swc_ref_free_matrix(ctypes.cast(c, ctypes.c_void_p), ctypes.cast(r, ctypes.c_void_p),
+                            ctypes.cast(v, ctypes.c_void_p))
+    return out
 
 
 def oracle_factor(n, A2p, A2i, A2x, lC, Ls, Li_ptr, super_, prunePtr, pruneSet, levelPtr,

@@ -10,7 +10,9 @@
  *   - A1 = ptranspose(A, 2, L->Perm), A2 = ptranspose(A1, 2)  (:198-199)
  *   - the factor call with super_max = maxSupWid+1, col_max = maxCol+1 (:223-232)
  * and exposes every array so tests can compare against them and the bench can time the
- * reference on the same inputs.  Nothing in the product links this file. */
+ * reference on the same inputs.  swc_ref_read_matrix runs the reference's Matrix Market
+ * reader (readMatrix, common/Util.h:77-179) for the reader's parity tests.  Nothing in the
+ * product links this file. */
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -210,6 +212,28 @@ void swc_ref_free(void *hv) {
   delete[] h->A->x;
   delete h->A;
   delete h;
+}
+
+// The reference's readMatrix on a file: 1 and the lower CSC arrays (new[]-allocated, free
+// with swc_ref_free_matrix) on success, 0 when it reports failure.
+int swc_ref_read_matrix(const char *path, long long *n, long long *nnz, int **col, int **row,
+                        double **val) {
+  size_t nn = 0, nz = 0;
+  int *c = nullptr, *r = nullptr;
+  double *v = nullptr;
+  if (!readMatrix(std::string(path), nn, nz, c, r, v)) return 0;
+  *n = (long long)nn;
+  *nnz = (long long)nz;
+  *col = c;
+  *row = r;
+  *val = v;
+  return 1;
+}
+
+void swc_ref_free_matrix(int *col, int *row, double *val) {
+  delete[] col;
+  delete[] row;
+  delete[] val;
 }
 
 }  // extern "C"

@@ -21,7 +21,8 @@ import os
 import numpy as np
 
 __all__ = ["lib", "SWCError", "sw_cholesky_left_par_05", "Handle", "layout", "LIB_PATH",
-           "SWC_OK", "SWC_NOT_SPD", "SWC_MODE_FP64"]
+           "SWC_OK", "SWC_NOT_SPD", "SWC_MODE_FP64", "read_mtx", "write_mtx", "read_perm",
+           "write_perm", "order_nd", "MtxMatrix"]
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libswchol_b200.so")
 
@@ -45,6 +46,8 @@ EXPORTS = (
     "swc_layout", "swc_solve", "swc_refine", "swc_solve_noalloc", "swc_logdet",
     "swc_logdet_grad", "swc_solve_grad", "swc_supernodes", "swc_batch_analyze",
     "swc_batch_autotune", "swc_batch_berr", "swc_set_plan", "swc_set_wait_budget",
+    "swc_read_mtx", "swc_free", "swc_write_mtx", "swc_read_perm", "swc_write_perm",
+    "swc_order_nd",
 )
 KERNEL_CLASSES = ("memset", "small", "assemble", "update", "panel", "syrk")
 
@@ -90,6 +93,16 @@ def lib() -> ctypes.CDLL:
         L.swc_plan_stats.argtypes = [_I] + [_VP] * 6 + [_I] + [_VP] * 2 + [_I, _VP]
         L.swc_set_plan.argtypes = [_VP, _I]
         L.swc_set_wait_budget.argtypes = [_VP, ctypes.c_longlong]
+        L.swc_read_mtx.argtypes = [ctypes.c_char_p, ctypes.POINTER(_I),
+                                   ctypes.POINTER(ctypes.POINTER(_I)),
+                                   ctypes.POINTER(ctypes.POINTER(_I)),
+                                   ctypes.POINTER(ctypes.POINTER(ctypes.c_double))]
+        L.swc_free.restype = None
+        L.swc_free.argtypes = [_VP]
+        L.swc_write_mtx.argtypes = [ctypes.c_char_p, _I, _VP, _VP, _VP]
+        L.swc_read_perm.argtypes = [ctypes.c_char_p, _I, _VP]
+        L.swc_write_perm.argtypes = [ctypes.c_char_p, _I, _VP]
+        L.swc_order_nd.argtypes = [_I, _VP, _VP, _I, _VP]
         L.swc_layout_sizes.argtypes = [_I] + [_VP] * 3 + [_I, _VP]
         L.swc_layout.argtypes = [_I] + [_VP] * 3 + [_I] + [_VP] * 9
         L.swc_logdet.argtypes = [_VP, ctypes.POINTER(ctypes.c_double)]
@@ -181,6 +194,67 @@ def supernodes(n, c, r, max_width: int = 1 << 30, nrelax=None, zrelax=None):
     _check(lib().swc_supernodes(int(n), _p(c), _p(r), _p(nr), _p(zr), int(max_width), _p(bs),
                                 ctypes.byref(ns)))
     return bs[: ns.value + 1].copy()
+
+
+class MtxMatrix:
+    """Lower triangle of a symmetric matrix in CSC form (``n``, ``indptr``, ``indices``,
+    ``data``), as ``read_mtx`` returns it."""
+
+    def __init__(self, n, indptr, indices, data):
+        self.n = int(n)
+        self.indptr = np.ascontiguousarray(indptr, dtype=np.int32)
+        self.indices = np.ascontiguousarray(indices, dtype=np.int32)
+        self.data = np.ascontiguousarray(data, dtype=np.float64)
+
+
+def read_mtx(path: str) -> MtxMatrix:
+    """Reads a Matrix Market coordinate file (see ``swc_read_mtx``): the lower triangle,
+    rows sorted, diagonal present in every column.  Raises SWCError on a malformed file."""
+    L = lib()
+    n = _I(0)
+    c = ctypes.POINTER(_I)()
+    r = ctypes.POINTER(_I)()
+    v = ctypes.POINTER(ctypes.c_double)()
+    _check(L.swc_read_mtx(os.fsencode(path), ctypes.byref(n), ctypes.byref(c), ctypes.byref(r),
+                          ctypes.byref(v)))
+    try:
+        nn = int(n.value)
+        indptr = np.ctypeslib.as_array(c, shape=(nn + 1,)).copy()
+        nnz = int(indptr[-1])
+        indices = np.ctypeslib.as_array(r, shape=(max(nnz, 1),))[:nnz].copy()
+        data = np.ctypeslib.as_array(v, shape=(max(nnz, 1),))[:nnz].copy()
+    finally:
+        for p in (c, r, v):
+            L.swc_free(ctypes.cast(p, _VP))
+    return MtxMatrix(nn, indptr, indices, data)
+
+
+def write_mtx(path: str, n, indptr, indices, data):
+    """Writes a lower CSC matrix as a symmetric Matrix Market coordinate file."""
+    c, r, v = _c(indptr, np.int32), _c(indices, np.int32), _c(data, np.float64)
+    _check(lib().swc_write_mtx(os.fsencode(path), int(n), _p(c), _p(r), _p(v)))
+
+
+def read_perm(path: str, n: int) -> np.ndarray:
+    """Reads a permutation file of n native size_t values (checked to be a permutation)."""
+    out = np.zeros(int(n), np.uint64)
+    _check(lib().swc_read_perm(os.fsencode(path), int(n), _p(out)))
+    return out.astype(np.int64)
+
+
+def write_perm(path: str, perm):
+    """Writes perm (new position k holds original index perm[k]) as n native size_t."""
+    p = _c(perm, np.uint64)
+    _check(lib().swc_write_perm(os.fsencode(path), int(p.size), _p(p)))
+
+
+def order_nd(n, indptr, indices, leaf: int = 0) -> np.ndarray:
+    """Nested-dissection fill-reducing permutation of a sparse symmetric pattern (lower or
+    full CSC); perm[k] = original index at new position k."""
+    c, r = _c(indptr, np.int32), _c(indices, np.int32)
+    out = np.zeros(int(n), np.uint64)
+    _check(lib().swc_order_nd(int(n), _p(c), _p(r), int(leaf), _p(out)))
+    return out.astype(np.int64)
 
 
 PLAN_FIELDS = ("levels", "launches", "small", "tiled", "update_tiles", "update_pairs",
@@ -325,7 +399,7 @@ class Handle:
     def set_plan(self, plan: int):
         """Execution-plan candidate for the next analyze / batch_analyze (0 default, 1 larger
         persistent supernodes, 2 no persistent walk, 3 smaller small class, 4 dense steps
-        as one dataflow launch per level, 5 split-TF32 SYRK steps on tcgen05)."""
+        as one dataflow launch per level, 5 FP64 trailing SYRK steps in split-TF32 mode)."""
         _check(self._lib.swc_set_plan(self._h, int(plan)))
 
     def set_wait_budget(self, polls: int = -1):

@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -458,6 +459,71 @@ int swc_layout(int n, const int *c, const int *r, const int *blockSet, int supNo
   if (levelPtr) std::memcpy(levelPtr, L.levelPtr.data(), sizeof(int) * L.levelPtr.size());
   if (parPtr) std::memcpy(parPtr, L.parPtr.data(), sizeof(int) * L.parPtr.size());
   if (partition) std::memcpy(partition, L.partition.data(), sizeof(int) * L.partition.size());
+  return SWC_OK;
+}
+
+// ---- input files and ordering (host only) --------------------------------------------
+
+int swc_read_mtx(const char *path, int *n, int **colptr, int **rowind, double **values) {
+  if (!path || !n || !colptr || !rowind || !values) return fail(SWC_INVALID_INPUT, "null argument");
+  swc::MtxLower M;
+  std::string err;
+  if (!swc::read_matrix_market(path, M, err)) return fail(SWC_INVALID_INPUT, err);
+  const size_t nnz = M.rowind.size();
+  int *c = static_cast<int *>(std::malloc(sizeof(int) * ((size_t)M.n + 1)));
+  int *r = static_cast<int *>(std::malloc(sizeof(int) * std::max<size_t>(nnz, 1)));
+  double *v = static_cast<double *>(std::malloc(sizeof(double) * std::max<size_t>(nnz, 1)));
+  if (!c || !r || !v) {
+    std::free(c);
+    std::free(r);
+    std::free(v);
+    return fail(SWC_INVALID_INPUT, "out of host memory");
+  }
+  std::memcpy(c, M.colptr.data(), sizeof(int) * ((size_t)M.n + 1));
+  std::memcpy(r, M.rowind.data(), sizeof(int) * nnz);
+  std::memcpy(v, M.values.data(), sizeof(double) * nnz);
+  *n = M.n;
+  *colptr = c;
+  *rowind = r;
+  *values = v;
+  return SWC_OK;
+}
+
+void swc_free(void *p) { std::free(p); }
+
+int swc_write_mtx(const char *path, int n, const int *c, const int *r, const double *values) {
+  if (!path) return fail(SWC_INVALID_INPUT, "null path");
+  std::string err;
+  if (!swc::write_matrix_market(path, n, c, r, values, err)) return fail(SWC_INVALID_INPUT, err);
+  return SWC_OK;
+}
+
+int swc_read_perm(const char *path, int n, size_t *perm) {
+  if (!path || !perm) return fail(SWC_INVALID_INPUT, "null argument");
+  std::vector<int64_t> p;
+  std::string err;
+  if (!swc::read_perm_file(path, n, p, err)) return fail(SWC_INVALID_INPUT, err);
+  for (int k = 0; k < n; ++k) perm[k] = (size_t)p[k];
+  return SWC_OK;
+}
+
+int swc_write_perm(const char *path, int n, const size_t *perm) {
+  if (!path || !perm) return fail(SWC_INVALID_INPUT, "null argument");
+  std::vector<int64_t> p(n > 0 ? n : 0);
+  for (int k = 0; k < n; ++k) p[k] = perm[k] > (size_t)INT32_MAX ? -1 : (int64_t)perm[k];
+  std::string err;
+  if (!swc::write_perm_file(path, n, p.data(), err)) return fail(SWC_INVALID_INPUT, err);
+  return SWC_OK;
+}
+
+int swc_order_nd(int n, const int *c, const int *r, int leaf, size_t *perm) {
+  if (!perm) return fail(SWC_INVALID_INPUT, "null perm");
+  swc::NdOptions opt;
+  if (leaf > 0) opt.leaf = leaf;
+  std::vector<int64_t> p;
+  std::string err;
+  if (!swc::nested_dissection_order(n, c, r, opt, p, err)) return fail(SWC_INVALID_INPUT, err);
+  for (int k = 0; k < n; ++k) perm[k] = (size_t)p[k];
   return SWC_OK;
 }
 

@@ -109,7 +109,7 @@ Tuning plan_candidate(int k) {
     case 2: t.persist = 0; break;                        // level-by-level launches only
     case 3: t.small_max_elems = 4096; t.small_max_m = 1024; break;   // more tiled supernodes
     case 4: t.dense_dataflow = 1; break;                 // dense steps as one dataflow launch
-    case 5: t.syrk_tc = 1; break;                        // split-TF32 SYRK steps on tcgen05
+    case 5: t.syrk_fp64 = 1; break;                      // split-TF32 mode: FP64 SYRK steps
     default: break;
   }
   return t;

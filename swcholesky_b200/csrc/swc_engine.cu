@@ -41,8 +41,12 @@ int64_t small_smem(int w, int64_t m) {
 struct TileWork {
   int4 task;                 // (s, r0, c0, first pair -- filled when flattened)
   std::vector<int4> pairs;   // (d, a0, b0, na | nb << 16)
+  std::vector<TcPair> tc;    // the same pairs with the tile rows / columns they feed
   double flops = 0, bytes = 0;
 };
+
+// Mask of the first n bits (n <= 64).
+inline unsigned long long low_bits(int n) { return n >= 64 ? ~0ULL : ((1ULL << n) - 1ULL); }
 
 // Splits every update d -> s of the prune set into the 64x64 tiles of s it touches.  The
 // rows of d at or below s's first column map monotonically into s's row list, so each
@@ -83,10 +87,18 @@ bool build_update_pairs(int s, int f, int w, int m, const std::vector<int> &supe
     for (const Run &cr : runs) {
       if ((int64_t)cr.tile * TB >= w) break;   // column runs: positions < w only
       int nb = 0;
-      for (int i = cr.start - lb; i < cr.start - lb + cr.count; ++i) nb += pos[i] < w;
+      unsigned long long cmask = 0;
+      for (int i = cr.start - lb; i < cr.start - lb + cr.count; ++i)
+        if (pos[i] < w) {
+          ++nb;
+          cmask |= 1ULL << (pos[i] - cr.tile * TB);
+        }
       if (nb == 0) continue;
       for (const Run &rr : runs) {
         if (rr.tile < cr.tile) continue;
+        unsigned long long rmask = 0;
+        for (int i = rr.start - lb; i < rr.start - lb + rr.count; ++i)
+          rmask |= 1ULL << (pos[i] - rr.tile * TB);
         const int key = rr.tile * ntc + cr.tile;
         if (tile_of[key] < 0) {
           tile_of[key] = (int)tiles.size();
@@ -96,6 +108,7 @@ bool build_update_pairs(int s, int f, int w, int m, const std::vector<int> &supe
         }
         TileWork &tw = tiles[tile_of[key]];
         tw.pairs.push_back(make_int4(d, rr.start, cr.start, rr.count | (nb << 16)));
+        tw.tc.push_back(TcPair{d, rr.start, cr.start, wd << 16, rmask, cmask});
         tw.flops += 2.0 * rr.count * nb * wd;
         tw.bytes += 8.0 * (rr.count + nb) * wd;
       }
@@ -140,7 +153,8 @@ void Engine::release() {
                   d_slist_, d_cptr_, d_cidx_, d_flags_, d_fchain_, d_bchain_, d_scontrib_, d_sgather_, d_csr_rp_, d_csr_ci_,
                   d_csr_map_,
                   d_csr_val_, d_contrib_, d_work_, d_norms_, d_persist_, d_qctr_, d_npart_,
-                  d_tiny_, d_dense_tasks_, d_dense_toff_, d_dense_ver_, d_swarp_};
+                  d_tiny_, d_dense_tasks_, d_dense_toff_, d_dense_ver_, d_swarp_,
+                  d_Lk_, d_xk_, d_tmaps_, d_tc_pairs_, d_syrk_pairs_, d_syrk_end_};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   release_adjoint();
@@ -166,6 +180,12 @@ void Engine::release() {
   d_csr_rp_ = d_csr_ci_ = d_csr_map_ = nullptr;
   d_csr_val_ = d_contrib_ = d_work_ = d_norms_ = nullptr;
   d_persist_ = d_qctr_ = d_tiny_ = nullptr;
+  d_Lk_ = nullptr;
+  d_xk_ = nullptr;
+  d_tmaps_ = nullptr;
+  d_tc_pairs_ = d_syrk_pairs_ = nullptr;
+  d_syrk_end_ = nullptr;
+  kmirror_len_ = 0;
   tiny_ctas_ = 0;
   d_npart_ = nullptr;
   persist_ctas_ = 0;
@@ -441,6 +461,7 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
     for (TileWork &tw : wave_tiles) {
       tw.task.w = (int)P.upd_pairs.size();
       P.upd_pairs.insert(P.upd_pairs.end(), tw.pairs.begin(), tw.pairs.end());
+      P.tc_pairs.insert(P.tc_pairs.end(), tw.tc.begin(), tw.tc.end());
       P.upd_tasks.push_back(tw.task);
       P.upd_end.push_back((int)P.upd_pairs.size());
       P.work.flops[K_UPDATE] += tw.flops;
@@ -461,8 +482,14 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
         for (int r0 = c0 + bw; r0 < m; r0 += TB) P.panel_tasks.push_back(make_int2(s, r0));
         for (int cc = c0 + TB; cc < w; cc += TB)
           for (int r0 = cc; r0 < m; r0 += TB)
-            if (!(cc == c0 + TB && r0 == cc))   // next diagonal tile: k_diag_step
-              P.syrk_tasks.push_back(make_int4(s, r0, cc, 0));
+            if (!(cc == c0 + TB && r0 == cc)) {   // next diagonal tile: k_diag_step
+              // .w: the task's own index, its single product for the tcgen05 kernel
+              P.syrk_pairs.push_back(TcPair{s, r0, cc, c0 | (bw << 16),
+                                            low_bits(std::min(TB, m - r0)),
+                                            low_bits(std::min(TB, w - cc))});
+              P.syrk_tasks.push_back(make_int4(s, r0, cc, (int)P.syrk_tasks.size()));
+              P.syrk_end.push_back((int)P.syrk_tasks.size());
+            }
         if (c0 + TB < w) P.diag_list.push_back(s);
       }
       W.panel_cnt.push_back((int)P.panel_tasks.size() - W.panel_off.back());
@@ -583,7 +610,7 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
                      const int64_t *Li_ptr, const int *blockSet, int supNo,
                      const int *prunePtr, const int *pruneSet, std::string &err) {
   cudaSetDevice(device_);
-  if (!kernels_configure(err) || !mixed_configure(err) || !tc_configure(err)) return false;
+  if (!kernels_configure(err) || !mixed_configure(err) || !update_tc_configure(err)) return false;
   HostSym H;
   Plan P;
   if (!build_plan(n, c, r, lC, Ls, Li_ptr, blockSet, supNo, prunePtr, pruneSet, H, P, err,
@@ -724,6 +751,9 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
             upload(d_pairs_, P.upd_pairs.data(), P.upd_pairs.size(), st, err) &&
             upload(d_panel_, P.panel_tasks.data(), P.panel_tasks.size(), st, err) &&
             upload(d_syrk_, P.syrk_tasks.data(), P.syrk_tasks.size(), st, err) &&
+            upload(d_syrk_pairs_, P.syrk_pairs.data(), P.syrk_pairs.size(), st, err) &&
+            upload(d_syrk_end_, P.syrk_end.data(), P.syrk_end.size(), st, err) &&
+            upload(d_tc_pairs_, P.tc_pairs.data(), P.tc_pairs.size(), st, err) &&
             upload(d_dense_tasks_, P.dense_tasks.data(), P.dense_tasks.size(), st, err) &&
             upload(d_dense_toff_, P.dense_toff.data(), P.dense_toff.size(), st, err) &&
             upload(d_dinv_off_, H.dinv_off.data(), H.dinv_off.size(), st, err) &&
@@ -792,7 +822,9 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
   sym_.status = d_status_;
   sym_.dinv = d_dinv_;
   sym_.Lf = nullptr;
+  sym_.xk = nullptr;
   sym_.dinv_off = d_dinv_off_;
+  kmirror_len_ = kmirror_layout(H.super, H.rowptr, h_xk_);
   hsym_ = H;
   h_Ls_.assign(Ls, Ls + nls);
 
@@ -800,12 +832,13 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
 }
 
 void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec) {
-  const bool mixed = prec != 0;
-  const bool syrk_tc = prec == 1 && tuning_.syrk_tc;   // split-TF32 mirror: tcgen05 SYRK
+  const bool tf32 = prec == 1;                          // split-TF32 products on tcgen05
+  const bool syrk_tc = tf32 && !tuning_.syrk_fp64;
   cudaStream_t st = stream_;
   auto syrk = [&](const int4 *tasks, int count, int step) {
     if (syrk_tc)
-      launch_syrk_step_tc(sym_, tasks, count, syrk_tc_ctas(count), step, st);
+      launch_update_tc(sym_, d_tmaps_, tasks, d_syrk_end_ + (tasks - d_syrk_), d_syrk_pairs_,
+                       count, st);
     else
       launch_syrk_step(sym_, tasks, count, step, st);
   };
@@ -845,7 +878,10 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec
     launch_assemble(sym_, d_asm_ + W.asm_off, W.asm_cnt, st);
     mark(-1, W.asm_cnt);
     mark(K_UPDATE, W.upd_cnt);
-    if (mixed)
+    if (tf32)
+      launch_update_tc(sym_, d_tmaps_, d_upd_tasks_ + W.upd_off, d_upd_end_ + W.upd_off,
+                       d_tc_pairs_, W.upd_cnt, st);
+    else if (prec == 2)
       launch_update_tiles_mx(sym_, d_upd_tasks_ + W.upd_off, d_upd_end_ + W.upd_off, d_pairs_,
                              W.upd_cnt, st);
     else
@@ -893,8 +929,7 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec
 }
 
 bool Engine::set_mode(int prec, std::string &err) {
-  const bool mixed = prec != 0;
-  if (mixed && !d_Lf_) {
+  if (prec == 2 && !d_Lf_) {   // BF16x3 mirror, indexed as L
     cudaError_t e = cudaMalloc(&d_Lf_, sizeof(float2) * std::max<int64_t>(xsize_, 1));
     if (e != cudaSuccess) {
       d_Lf_ = nullptr;
@@ -902,8 +937,26 @@ bool Engine::set_mode(int prec, std::string &err) {
       return false;
     }
   }
-  sym_.Lf = mixed ? d_Lf_ : nullptr;
-  sym_.mirror_kind = prec == 2 ? MIRROR_BF16X3 : MIRROR_TF32X2;
+  if (prec == 1 && !d_Lk_) {   // split-TF32 K-major mirror and its tensor maps
+    const size_t mb = tensor_map_bytes() * (size_t)nsuper_;
+    std::vector<unsigned char> maps(mb);
+    cudaError_t e = cudaMalloc(&d_Lk_, sizeof(float) * std::max<int64_t>(kmirror_len_, 4));
+    if (e == cudaSuccess) e = cudaMalloc(&d_xk_, sizeof(int64_t) * std::max<size_t>(h_xk_.size(), 1));
+    if (e == cudaSuccess) e = cudaMalloc(&d_tmaps_, std::max<size_t>(mb, 128));
+    if (e != cudaSuccess) {
+      err = std::string("mirror allocation: ") + cudaGetErrorString(e);
+      return false;
+    }
+    if (!build_tensor_maps(hsym_.super, hsym_.rowptr, h_xk_, d_Lk_, maps.data(), err)) return false;
+    e = cudaMemcpy(d_xk_, h_xk_.data(), sizeof(int64_t) * h_xk_.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_tmaps_, maps.data(), mb, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      err = std::string("mirror set-up: ") + cudaGetErrorString(e);
+      return false;
+    }
+  }
+  sym_.Lf = prec == 2 ? d_Lf_ : prec == 1 ? reinterpret_cast<float2 *>(d_Lk_) : nullptr;
+  sym_.xk = prec == 1 ? d_xk_ : nullptr;
   return true;
 }
 

@@ -29,9 +29,12 @@ struct DevSym {
                           // [1] = structure error flag, [2] = solve wait timeout,
                           // [3] = factorization wait timeout (persistent walk),
                           // [4] = poll budget of every bounded wait (set by the host)
-  float2 *Lf;             // split mirror of L (mixed-precision only, else null): per value
-                          // {hi, lo} TF32 pair, or three bfloat16 pieces (mirror_kind)
-  int mirror_kind;        // MIRROR_TF32X2 or MIRROR_BF16X3
+  float2 *Lf;             // split mirror of L (mixed-precision modes only, else null)
+  const int64_t *xk;      // null: Lf is the BF16x3 mirror, same indexing as L, per value
+                          // three bfloat16 pieces.  Else Lf holds the split-TF32 mirror in
+                          // K-major form: supernode s at (float *)Lf + xk[s], hi plane rows
+                          // 0..m-1 then lo plane rows m..2m-1, rows of (w rounded up to 4)
+                          // floats
   double *dinv;           // scratch: inverses of the 64x64 diagonal blocks of the tiled class
   const int *dinv_off;    // per supernode: first block of its inverses in dinv (-1: none)
 };
@@ -45,9 +48,15 @@ __device__ __forceinline__ long long wait_budget(const int *status) {
   return (long long)*(volatile const int *)&status[4];
 }
 
-// Formats of the split mirror (8 bytes per value).
-constexpr int MIRROR_TF32X2 = 0;   // {hi, lo} floats holding TF32 values
-constexpr int MIRROR_BF16X3 = 1;   // bits: x = hi | mid << 16, y = lo (bfloat16 pieces)
+// BF16x3 mirror entry bits: x = hi | mid << 16, y = lo (bfloat16 pieces).
+
+// One (64x64 tile, descendant) product of the tcgen05 update kernel: rows a0.. of
+// supernode d feed the tile rows set in rmask (in order), rows b0.. the tile columns set in
+// cmask; the product runs over columns k0 .. k0 + kcnt - 1 of d (kk = k0 | kcnt << 16).
+struct __align__(16) TcPair {
+  int d, a0, b0, kk;
+  unsigned long long rmask, cmask;
+};
 
 // One level of the schedule (supernodes whose descendants all belong to earlier levels).
 struct Wave {
@@ -81,6 +90,9 @@ struct Plan {
   std::vector<int4> upd_tasks;     // (s, r0, c0, first pair)
   std::vector<int> upd_end;        // one past the last pair of each task
   std::vector<int4> upd_pairs;     // (d, a0, b0, na | nb << 16)
+  std::vector<TcPair> tc_pairs;    // the same pairs for the tcgen05 kernel (tile masks)
+  std::vector<TcPair> syrk_pairs;  // per SYRK task: its product (s, r0, c0, step block)
+  std::vector<int> syrk_end;       // per SYRK task: one past its pair (its index + 1)
   std::vector<int2> panel_tasks;
   std::vector<int4> syrk_tasks;
   std::vector<int> diag_list;
@@ -280,7 +292,14 @@ class Engine {
   int *d_upd_end_ = nullptr;
   cudaGraph_t graph_[3] = {nullptr, nullptr, nullptr};          // one per precision mode
   cudaGraphExec_t graph_exec_[3] = {nullptr, nullptr, nullptr};
-  float2 *d_Lf_ = nullptr;
+  float2 *d_Lf_ = nullptr;                     // BF16x3 mirror
+  float *d_Lk_ = nullptr;                      // split-TF32 K-major mirror
+  int64_t *d_xk_ = nullptr;                    // its per-supernode offsets
+  void *d_tmaps_ = nullptr;                    // one tensor map per supernode (over d_Lk_)
+  std::vector<int64_t> h_xk_;
+  int64_t kmirror_len_ = 0;
+  TcPair *d_tc_pairs_ = nullptr, *d_syrk_pairs_ = nullptr;
+  int *d_syrk_end_ = nullptr;
   bool use_graph_ = true;
   Tuning tuning_;
   int *d_persist_ = nullptr, *d_qctr_ = nullptr, *d_tiny_ = nullptr;
@@ -336,12 +355,19 @@ void launch_dense_persist(const DevSym &S, const int4 *tasks, int count, int cta
                           int *ver, int *qhead, cudaStream_t st);
 void launch_init_status(int *status, cudaStream_t st);
 bool kernels_configure(std::string &err);
-// trailing SYRK step of the split-TF32 mode on tcgen05 (swc_tc.cu): grid of ctas CTAs
-bool tc_configure(std::string &err);
-int syrk_tc_ctas(int count);
-void launch_syrk_step_tc(const DevSym &S, const int4 *tasks, int count, int ctas, int step,
-                         cudaStream_t st);
-// mixed-precision Schur updates (swc_mixed.cu)
+// split-TF32 tile updates on tcgen05 fed by TMA gathers (swc_update_tc.cu): K-major mirror
+// layout (offsets per supernode, total floats), one tensor map per supernode (host array
+// of nsuper entries of tensor_map_bytes() each), the launch over tile tasks
+bool update_tc_configure(std::string &err);
+int64_t kmirror_layout(const std::vector<int> &super, const std::vector<int64_t> &rowptr,
+                       std::vector<int64_t> &xk);
+bool build_tensor_maps(const std::vector<int> &super, const std::vector<int64_t> &rowptr,
+                       const std::vector<int64_t> &xk, float *Lk, void *maps_host,
+                       std::string &err);
+size_t tensor_map_bytes();
+void launch_update_tc(const DevSym &S, const void *maps, const int4 *tasks, const int *task_end,
+                      const TcPair *pairs, int count, cudaStream_t st);
+// BF16x3 Schur updates (swc_mixed.cu)
 bool mixed_configure(std::string &err);
 void launch_update_tiles_mx(const DevSym &S, const int4 *tasks, const int *task_end,
                             const int4 *pairs, int count, cudaStream_t st);

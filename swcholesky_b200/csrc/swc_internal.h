@@ -28,6 +28,30 @@ bool supernode_partition(int n, const int *c, const int *r, const int nrelax[3],
                          const double zrelax[3], int max_width, std::vector<int> &super,
                          std::string &err);
 
+// A symmetric matrix read from a Matrix Market file: its lower triangle in CSC form, rows
+// sorted, diagonal present (explicit zero when the file has none) in every column.
+struct MtxLower {
+  int n = 0;
+  std::vector<int> colptr, rowind;
+  std::vector<double> values;
+};
+bool read_matrix_market(const char *path, MtxLower &out, std::string &err);
+bool write_matrix_market(const char *path, int n, const int *c, const int *r, const double *v,
+                         std::string &err);
+// Raw permutation files: n native size_t values (new position k holds original index perm[k]).
+bool read_perm_file(const char *path, int n, std::vector<int64_t> &perm, std::string &err);
+bool write_perm_file(const char *path, int n, const int64_t *perm, std::string &err);
+
+// Fill-reducing ordering of a general sparse symmetric matrix given by its lower (or full)
+// CSC pattern: nested dissection by level-structure vertex separators, minimum degree on
+// the leaves.  perm[k] = original index at new position k.
+struct NdOptions {
+  int leaf = 64;           // subgraphs at most this large are ordered by minimum degree
+  int trials = 3;          // pseudo-peripheral starting vertices tried per bisection
+};
+bool nested_dissection_order(int n, const int *c, const int *r, const NdOptions &opt,
+                             std::vector<int64_t> &perm, std::string &err);
+
 // Tile edge used by every tiled kernel.
 constexpr int TB = 64;
 
@@ -72,7 +96,8 @@ struct Tuning {
   int dense_dataflow = 0;                // dense steps of a wave: one dataflow launch (else
                                          // three launches per 64-column step)
   int dense_group = 4;                   // column blocks per grouped trailing update
-  int syrk_tc = 0;                       // split-TF32 mode: trailing SYRK steps on tcgen05
+  int syrk_fp64 = 0;                     // split-TF32 mode: trailing SYRK steps in FP64
+                                         // (DMMA) instead of split-TF32 on tcgen05
 };
 
 }  // namespace swc

@@ -68,9 +68,43 @@ __device__ __forceinline__ float2 split_bf16x3(double x) {
   return make_float2(__uint_as_float(bx), __uint_as_float(by));
 }
 
-// The mirror entry of value x in the format of this factorization.
-__device__ __forceinline__ float2 mirror_value(const DevSym &S, double x) {
-  return S.mirror_kind == MIRROR_BF16X3 ? split_bf16x3(x) : split_tf32(x);
+// The mirror entries of value x of row r, column c of supernode s (m rows, w columns):
+// the BF16x3 triple at L's index, or hi / lo of the split-TF32 K-major planes.
+__device__ __forceinline__ void store_mirror(const DevSym &S, int s, int m, int w, int r, int c,
+                                             double x) {
+  if (!S.xk) {
+    S.Lf[S.xptr[s] + (size_t)c * m + r] = split_bf16x3(x);
+  } else {
+    const float2 v = split_tf32(x);
+    float *row = reinterpret_cast<float *>(S.Lf) + S.xk[s] + (size_t)r * ((w + 3) & ~3) + c;
+    row[0] = v.x;
+    row[(size_t)m * ((w + 3) & ~3)] = v.y;
+  }
+}
+
+// The whole m x w panel P (column-major, ld m) of supernode s into the mirror; threads
+// t, t + nt, ... (consecutive threads write consecutive mirror entries).
+__device__ __forceinline__ void store_mirror_panel(const DevSym &S, int s, int m, int w,
+                                                   const double *P, int t, int nt) {
+  if (!S.xk) {
+    float2 *dstf = S.Lf + S.xptr[s];
+    for (int i = t; i < m * w; i += nt) dstf[i] = split_bf16x3(P[i]);
+  } else {
+    const int wp = (w + 3) & ~3;
+    float *hi = reinterpret_cast<float *>(S.Lf) + S.xk[s], *lo = hi + (size_t)m * wp;
+    for (int e = t; e < m * w; e += nt) {
+      const int r = e / w, c = e - r * w;
+      const float2 v = split_tf32(P[(size_t)c * m + r]);
+      hi[(size_t)r * wp + c] = v.x;
+      lo[(size_t)r * wp + c] = v.y;
+    }
+  }
+}
+
+// The same for one warp, out of line (keeps the warp-per-supernode kernel's registers).
+__device__ __noinline__ void store_mirror_panel_warp(const DevSym &S, int s, int m, int w,
+                                                     const double *P) {
+  store_mirror_panel(S, s, m, w, P, threadIdx.x & 31, 32);
 }
 
 __device__ __forceinline__ void flag_structure_error(const DevSym &S) {
@@ -248,10 +282,8 @@ __device__ __noinline__ void factor_small_body(const DevSym &S, const int2 *lbub
   __syncthreads();
   double *dst = S.L + S.xptr[s];
   for (int i = tid; i < m * w; i += NT) dst[i] = P[i];
-  if (S.Lf) {   // mixed-precision factorization: split mirror for the Schur updates
-    float2 *dstf = S.Lf + S.xptr[s];
-    for (int i = tid; i < m * w; i += NT) dstf[i] = mirror_value(S, P[i]);
-  }
+  if (S.Lf)   // mixed-precision factorization: split mirror for the Schur updates
+    store_mirror_panel(S, s, m, w, P, tid, NT);
 }
 
 // One CTA per small supernode of a level.
@@ -935,13 +967,13 @@ __device__ void trsm_task(const DevSym &S, int s, int r0, int step, double *dyn)
         const int c = acc_col(j, e);
         if (c < bw) {
           P[(size_t)(c0 + c) * m + r0 + r] = acc.v[i][j][e];
-          if (S.Lf) S.Lf[S.xptr[s] + (size_t)(c0 + c) * m + r0 + r] = mirror_value(S, acc.v[i][j][e]);
+          if (S.Lf) store_mirror(S, s, m, w, r0 + r, c0 + c, acc.v[i][j][e]);
         }
       }
   }
 }
 
-__global__ void __launch_bounds__(MT) k_trsm_step(DevSym S, const int2 *tasks, int count,
+__global__ void __launch_bounds__(MT, 4) k_trsm_step(DevSym S, const int2 *tasks, int count,
                                                   int step) {
   extern __shared__ double dyn[];
   trsm_task(S, tasks[blockIdx.x].x, tasks[blockIdx.x].y, step, dyn);
@@ -1102,10 +1134,7 @@ __device__ void factor_tiny_body(const DevSym &S, const int2 *lbub, int s, doubl
   }
   double *dst = S.L + S.xptr[s];
   for (int i = lane; i < m * w; i += 32) dst[i] = P[i];
-  if (S.Lf) {
-    float2 *dstf = S.Lf + S.xptr[s];
-    for (int i = lane; i < m * w; i += 32) dstf[i] = mirror_value(S, P[i]);
-  }
+  if (S.Lf) store_mirror_panel_warp(S, s, m, w, P);
 }
 
 // qctr[1 + s]: done flags (shared with the CTA walk); qhead: this walk's queue head.

@@ -1,14 +1,16 @@
-// Mixed-precision Schur updates: the SYRK/GEMM updates of the tiled class (the bulk of the
-// flops) computed as FP32-accurate split-TF32 products on the tensor cores, with FP32
+// BF16x3 Schur updates (SWC_MODE_MIXED_BF16X3): the SYRK/GEMM updates of the tiled class
+// (the bulk of the flops) computed as split-bfloat16 products on the tensor cores, with FP32
 // accumulation inside one descendant's product and FP64 accumulation across descendants.
 //
 // Every finished panel (small-class supernodes, TRSM'd tiles of the tiled class) also
-// writes a split copy of itself (the "mirror", same indexing as L): each value x as the
-// pair {hi, lo} with hi = tf32(x) and lo = tf32(x - hi), so the tensor-core kernels load
-// fragments without any conversion.  A product is hi*hi' + hi*lo' + lo*hi' (three TF32
-// MMAs, the lo*lo' term dropped), about 2^-21 relative error -- the FP32-class accuracy that
-// FP64 iterative refinement then removes.  POTRF, TRSM, the diagonal tiles and the small
-// supernodes stay FP64.
+// writes a split copy of itself (the "mirror", same indexing as L): each value x as three
+// bfloat16 pieces hi = bf16(x), mid = bf16(x - hi), lo = bf16(x - hi - mid), so the
+// tensor-core kernel loads fragments without any conversion.  A product sums the six piece
+// products whose order is at most two pieces below the leading one (the split-bfloat16
+// method of Henry, Tang and Heinecke, ARITH 2019), about 2^-24 relative error -- the
+// FP32-class accuracy that FP64 iterative refinement then removes.  POTRF, TRSM, the
+// diagonal tiles and the small supernodes stay FP64.  (The split-TF32 mode runs its updates
+// on tcgen05: swc_update_tc.cu.)
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -44,14 +46,6 @@ __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_grou
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
-
-__device__ __forceinline__ void mma_tf32(float (&c)[4], const unsigned (&a)[4], const unsigned (&b)[2]) {
-  asm(
-      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};\n"
-      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
 
 // Accumulator of one warp's 32x32 sub-tile: 2 x 4 MMA tiles of 16x8, fragment layout of
 // m16n8k8: c0 (g, 2t), c1 (g, 2t+1), c2 (g+8, 2t), c3 (g+8, 2t+1), g = lane/4, t = lane%4.
@@ -99,50 +93,6 @@ __device__ __forceinline__ void mma_bf16(float (&c)[4], const unsigned (&a)[4], 
       "{%0,%1,%2,%3};\n"
       : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
-
-// One staged k-chunk, split-TF32: elements are {hi, lo} float pairs; per k8 step the three
-// partial products lo*hi', hi*lo', hi*hi' (each issued over all tiles before the next: the
-// products of one tile depend on each other through the accumulator).
-__device__ __forceinline__ void chunk_tf32(const float2 *As, const float2 *Bs, int wr, int wc,
-                                           int g, int t, unsigned rmask, unsigned cmask,
-                                           Acc32 &acc) {
-#pragma unroll
-  for (int k8 = 0; k8 < KF; k8 += 8) {
-    unsigned ah[2][4], al[2][4], bh[4][2], bl[4][2];
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      const int r = wr + 16 * i + g;
-      const float2 x0 = As[(k8 + t) * LDF + r], x1 = As[(k8 + t) * LDF + r + 8];
-      const float2 x2 = As[(k8 + t + 4) * LDF + r], x3 = As[(k8 + t + 4) * LDF + r + 8];
-      ah[i][0] = __float_as_uint(x0.x); al[i][0] = __float_as_uint(x0.y);
-      ah[i][1] = __float_as_uint(x1.x); al[i][1] = __float_as_uint(x1.y);
-      ah[i][2] = __float_as_uint(x2.x); al[i][2] = __float_as_uint(x2.y);
-      ah[i][3] = __float_as_uint(x3.x); al[i][3] = __float_as_uint(x3.y);
-    }
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int n = wc + 8 * j + g;
-      const float2 y0 = Bs[(k8 + t) * LDF + n], y1 = Bs[(k8 + t + 4) * LDF + n];
-      bh[j][0] = __float_as_uint(y0.x); bl[j][0] = __float_as_uint(y0.y);
-      bh[j][1] = __float_as_uint(y1.x); bl[j][1] = __float_as_uint(y1.y);
-    }
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-        if (((rmask >> i) & (cmask >> j)) & 1u) mma_tf32(acc.v[i][j], al[i], bh[j]);
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-        if (((rmask >> i) & (cmask >> j)) & 1u) mma_tf32(acc.v[i][j], ah[i], bl[j]);
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-        if (((rmask >> i) & (cmask >> j)) & 1u) mma_tf32(acc.v[i][j], ah[i], bh[j]);
-  }
 }
 
 // Two BF16x3 elements (bits: x = hi | mid << 16, y = lo) -> one register of component p for
@@ -205,10 +155,8 @@ __device__ __forceinline__ void chunk_bf16(const float2 *Asf, const float2 *Bsf,
   }
 }
 
-// acc += A B^T over K columns from the mirror (split-TF32 or BF16x3 by KIND), with A / B
-// rows gathered through ia / ib.  rmask / cmask: this warp's non-empty 16-row and 8-column
-// groups.
-template <int KIND>
+// acc += A B^T over K columns from the BF16x3 mirror, with A / B rows gathered through
+// ia / ib.  rmask / cmask: this warp's non-empty 16-row and 8-column groups.
 __device__ __forceinline__ void split_product(const float2 *__restrict__ Lf, int ld, const int *ia,
                                               const int *ib, int K, float2 *stages, Acc32 &acc) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -234,10 +182,7 @@ __device__ __forceinline__ void split_product(const float2 *__restrict__ Lf, int
     }
     __syncthreads();
     const float2 *As = stages + (c & 1) * STAGEF, *Bs = As + KF * LDF;
-    if (rmask && cmask) {
-      if (KIND == MIRROR_BF16X3) chunk_bf16(As, Bs, wr, wc, g, t, rmask, cmask, acc);
-      else chunk_tf32(As, Bs, wr, wc, g, t, rmask, cmask, acc);
-    }
+    if (rmask && cmask) chunk_bf16(As, Bs, wr, wc, g, t, rmask, cmask, acc);
     __syncthreads();
   }
 }
@@ -245,7 +190,6 @@ __device__ __forceinline__ void split_product(const float2 *__restrict__ Lf, int
 // Mixed-precision tile-owner update (same tasks and pair lists as the FP64 kernel).
 constexpr int UPDM_SMEM = 2 * STAGEF * 8 + 3 * TB * 4;
 
-template <int KIND>
 __global__ void __launch_bounds__(MXT, 4) k_update_tiles_mx(DevSym S, const int4 *tasks,
                                                            const int *task_end,
                                                            const int4 *pairs, int count) {
@@ -294,7 +238,7 @@ __global__ void __launch_bounds__(MXT, 4) k_update_tiles_mx(DevSym S, const int4
     }
     Acc32 acc;
     acc.zero();
-    split_product<KIND>(S.Lf + S.xptr[d], md, ia, ib, wd, stages, acc);
+    split_product(S.Lf + S.xptr[d], md, ia, ib, wd, stages, acc);
 #pragma unroll
     for (int i = 0; i < 2; ++i)
 #pragma unroll
@@ -318,11 +262,8 @@ __global__ void __launch_bounds__(MXT, 4) k_update_tiles_mx(DevSym S, const int4
 }  // namespace
 
 bool mixed_configure(std::string &err) {
-  cudaError_t e = cudaFuncSetAttribute(k_update_tiles_mx<MIRROR_TF32X2>,
+  cudaError_t e = cudaFuncSetAttribute(k_update_tiles_mx,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, UPDM_SMEM);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_update_tiles_mx<MIRROR_BF16X3>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, UPDM_SMEM);
   if (e != cudaSuccess) {
     err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e);
     return false;
@@ -333,10 +274,7 @@ bool mixed_configure(std::string &err) {
 void launch_update_tiles_mx(const DevSym &S, const int4 *tasks, const int *task_end,
                             const int4 *pairs, int count, cudaStream_t st) {
   if (count <= 0) return;
-  if (S.mirror_kind == MIRROR_BF16X3)
-    k_update_tiles_mx<MIRROR_BF16X3><<<count, MXT, UPDM_SMEM, st>>>(S, tasks, task_end, pairs, count);
-  else
-    k_update_tiles_mx<MIRROR_TF32X2><<<count, MXT, UPDM_SMEM, st>>>(S, tasks, task_end, pairs, count);
+  k_update_tiles_mx<<<count, MXT, UPDM_SMEM, st>>>(S, tasks, task_end, pairs, count);
 }
 
 }  // namespace swc

@@ -27,6 +27,7 @@ __all__ = [
     "permute_lower",
     "cond_shift",
     "workload_matrix",
+    "random_geometric",
 ]
 
 
@@ -213,6 +214,25 @@ def permute_lower(A: LowerCSC, perm: np.ndarray) -> LowerCSC:
     p = np.asarray(perm)
     B = full[p][:, p]
     return LowerCSC.from_scipy(B)
+
+
+def random_geometric(n: int, dim: int = 3, degree: float = 10.0, sigma: float = 0.5,
+                     shift: float = 1e-2, seed: int = 0) -> LowerCSC:
+    """SPD matrix of a random geometric graph, a structure with no grid to dissect: n points
+    uniform in the unit square (dim 2) or cube (dim 3), joined when closer than the radius
+    that gives `degree` neighbours on average; log-normal(sigma) edge weights; the weighted
+    graph Laplacian plus shift * I."""
+    from scipy.spatial import cKDTree
+    rng = np.random.default_rng(seed)
+    X = rng.random((n, dim))
+    vol = np.pi if dim == 2 else 4.0 / 3.0 * np.pi
+    radius = (degree / (n * vol)) ** (1.0 / dim)
+    pairs = cKDTree(X).query_pairs(radius, output_type="ndarray")
+    w = rng.lognormal(0.0, sigma, len(pairs))
+    W = sp.coo_matrix((w, (pairs[:, 0], pairs[:, 1])), shape=(n, n))
+    W = (W + W.T).tocsc()
+    Lap = sp.diags(np.asarray(W.sum(axis=1)).ravel()) - W + shift * sp.identity(n)
+    return LowerCSC.from_scipy(Lap)
 
 
 def cond_shift(L: LowerCSC, cond: float) -> float:

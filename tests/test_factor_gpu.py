@@ -161,3 +161,33 @@ def test_full_size_matches_reference_factor(cuda_ok, name):
     b = np.random.default_rng(0).standard_normal(s.n)
     x = O.oracle_solve(s.n, s.lC, s.Ls, s.Li_ptr, L, s.super, b)
     assert backward_error(s.n, s.A2p, s.A2i, s.A2x, x, b) <= 1e-13
+
+
+def test_general_graph_from_files_matches_reference(cuda_ok, tmp_path):
+    """A matrix with no grid structure (random geometric graph in 3D, n = 30,000) through
+    the reference driver's file path with the library's own inputs: Matrix Market file ->
+    the library's reader -> its nested-dissection ordering -> a permutation file -> the
+    reference's analyze_p2 (GIVEN) -> the drop-in factorization on the GPU, against the
+    reference's own FP64 factor at <= 1e-12."""
+    import os
+    from swcholesky_b200 import matrices as M
+    if not O.ref_available():
+        pytest.skip("oracle/_ref/libswref.so not built")
+    A = M.random_geometric(30000, dim=3, degree=12, seed=11)
+    fm, fp = str(tmp_path / "rgg.mtx"), str(tmp_path / "rgg.perm")
+    swc.write_mtx(fm, A.n, A.indptr, A.indices, A.data)
+    B = swc.read_mtx(fm)
+    swc.write_perm(fp, swc.order_nd(B.n, B.indptr, B.indices))
+    R = O.RefSymbolic(M.LowerCSC(B.n, B.indptr, B.indices, B.data), swc.read_perm(fp, B.n))
+    s = R.sym
+    L_ref, _, ret = R.factor(threads=os.cpu_count() or 1)
+    R.close()
+    assert ret == 1
+    g = dict(n=s.n, A2p=s.A2p, A2i=s.A2i, A2x=s.A2x, lC=s.lC, Ls=s.Ls, Li_ptr=s.Li_ptr,
+             super=s.super, prunePtr=s.prunePtr, pruneSet=s.pruneSet, levelPtr=s.levelPtr,
+             parPtr=s.parPtr, partition=s.partition, maxSupWid=s.maxSupWid, maxCol=s.maxCol,
+             xsize=s.xsize)
+    ret, L = dropin(g)
+    assert ret == 1, swc.lib().swc_last_error()
+    assert rel_diff(L, L_ref) <= RTOL_L
+    assert np.all(L[L_ref == 0.0] == 0.0)
