@@ -377,6 +377,9 @@ def run_ours(args, rank, world, local_rank):
         last_fp64.update(berr=float(berr.max()), iters=iters)
     ms_fp64_solve = timed(step_fp64_solve, max(1, args.steps // 2))
     value = world * fl / (ms * 1e-3) / 1e9
+    # one supernodal solve (forward + backward) with the FP64 factor, for the breakdown
+    h.solve(b, out=x)
+    ms_solve = timed(lambda: h.solve(b, out=x), args.steps)
 
     # ---- per-kernel roofline (a separate profiled factorization in the headline mode) ----
     prof64 = h.profile(vals, swc.SWC_MODE_FP64) if mixed else None
@@ -508,6 +511,7 @@ def run_ours(args, rank, world, local_rank):
                          "fp64_gflops": round(world * fl / (ms_fp64 * 1e-3) / 1e9, 3),
                          "fp64_ms_factor_plus_refined_solve": round(ms_fp64_solve, 4),
                          "fp64_backward_error": last_fp64.get("berr"),
+                         "ms_one_solve": round(ms_solve, 4),
                          "speedup_vs_fp64_factor": round(ms_fp64 / ms, 3),
                          "speedup_vs_fp64_factor_plus_solve": round(ms_fp64_solve / ms, 3)},
             "parity": parity,

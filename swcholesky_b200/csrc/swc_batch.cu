@@ -110,11 +110,12 @@ Tuning plan_candidate(int k) {
     case 3: t.small_max_elems = 4096; t.small_max_m = 1024; break;   // more tiled supernodes
     case 4: t.dense_dataflow = 1; break;                 // dense steps as one dataflow launch
     case 5: t.syrk_fp64 = 1; break;                      // split-TF32 mode: FP64 SYRK steps
+    case 6: t.tc_tma = 1; break;                         // split-TF32 mode: TMA gather4 staging
     default: break;
   }
   return t;
 }
-const int kNumPlans = 6;
+const int kNumPlans = 7;
 int num_plans() { return kNumPlans; }
 
 bool BatchState::set(int nm, const int *n, const int *c, const int *r, std::string &err) {

@@ -189,6 +189,9 @@ void Engine::release() {
   tiny_ctas_ = 0;
   d_npart_ = nullptr;
   persist_ctas_ = 0;
+  release_solve_graphs();
+  if (d_sx_) cudaFree(d_sx_);
+  d_sx_ = nullptr;
   work_nrhs_ = 0;
   for (int k = 0; k < 3; ++k) {
     if (graph_exec_[k]) cudaGraphExecDestroy(graph_exec_[k]);
@@ -480,16 +483,27 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
         if (c0 >= w) continue;
         int bw = std::min(TB, w - c0);
         for (int r0 = c0 + bw; r0 < m; r0 += TB) P.panel_tasks.push_back(make_int2(s, r0));
-        for (int cc = c0 + TB; cc < w; cc += TB)
+        // trailing updates of step j: column j+1 (the next TRSM reads it) by block j alone;
+        // a column C >= j+2 by the group of blocks that closes at step j (blocks j-G+1..j,
+        // at the steps j = C-2, C-2-G, ...), so it receives blocks 0..C-2 in groups and
+        // block C-1 at step C-1, and every tile is read and written once per group
+        const int G = std::max(1, T.dense_group);
+        for (int cc = c0 + TB; cc < w; cc += TB) {
+          const int C = cc / TB;
+          int first;
+          if (C == j + 1) first = j;
+          else if ((C - 2 - j) % G == 0) first = std::max(0, j - G + 1);
+          else continue;
           for (int r0 = cc; r0 < m; r0 += TB)
-            if (!(cc == c0 + TB && r0 == cc)) {   // next diagonal tile: k_diag_step
-              // .w: the task's own index, its single product for the tcgen05 kernel
-              P.syrk_pairs.push_back(TcPair{s, r0, cc, c0 | (bw << 16),
+            if (!(cc == c0 + TB && r0 == cc)) {   // next diagonal tile: the TRSM task's update
+              // .w: the task's own index: its product (column blocks first..j) in syrk_pairs
+              P.syrk_pairs.push_back(TcPair{s, r0, cc, (first * TB) | ((c0 + bw - first * TB) << 16),
                                             low_bits(std::min(TB, m - r0)),
                                             low_bits(std::min(TB, w - cc))});
               P.syrk_tasks.push_back(make_int4(s, r0, cc, (int)P.syrk_tasks.size()));
               P.syrk_end.push_back((int)P.syrk_tasks.size());
             }
+        }
         if (c0 + TB < w) P.diag_list.push_back(s);
       }
       W.panel_cnt.push_back((int)P.panel_tasks.size() - W.panel_off.back());
@@ -559,8 +573,9 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
       int s = t.x, w = super[s + 1] - super[s];
       int64_t m = rowptr[s + 1] - rowptr[s];
       int nrow = (int)std::min<int64_t>(TB, m - t.y), ncol = std::min(TB, w - t.z);
-      K.flops[K_SYRK] += 2.0 * nrow * ncol * TB;
-      K.bytes[K_SYRK] += 8.0 * (2.0 * nrow * ncol + (nrow + ncol) * TB);
+      const int kc = P.syrk_pairs[t.w].kk >> 16;
+      K.flops[K_SYRK] += 2.0 * nrow * ncol * kc;
+      K.bytes[K_SYRK] += 8.0 * (2.0 * nrow * ncol + (nrow + ncol) * kc);
     }
     // dense factorization of the tiled class: POTRF + TRSM per column block
     for (int lv = 0; lv < nlev; ++lv)
@@ -573,7 +588,9 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
           K.flops[K_PANEL] += (double)bw * bw * bw / 3.0 + (double)(m - c0 - bw) * bw * bw;
           K.bytes[K_PANEL] += 16.0 * (m - c0) * bw;
         }
-        K.bytes[K_ASSEMBLE] += 12.0 * (c[super[s + 1]] - c[super[s]]) + 8.0 * m * w;
+        // each entry of A in the supernode's columns: row index and value read, one value of
+        // the panel written (the rest of the panel is zeroed by the memset)
+        K.bytes[K_ASSEMBLE] += 20.0 * (c[super[s + 1]] - c[super[s]]);
       }
     if (!P.dense_tasks.empty()) {   // one launch does the trailing updates too: one class
       K.flops[K_PANEL] += K.flops[K_SYRK];
@@ -804,7 +821,6 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
   nnz_ = nnz;
   plan_ = std::move(P);
   splan_ = std::move(SP);
-  solve_epoch_ = 0;
   nflags_ = H.ndinv;
   csr_nnz_ = (int64_t)csr_ci.size();
   sym_.n = n;
@@ -835,12 +851,12 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec
   const bool tf32 = prec == 1;                          // split-TF32 products on tcgen05
   const bool syrk_tc = tf32 && !tuning_.syrk_fp64;
   cudaStream_t st = stream_;
-  auto syrk = [&](const int4 *tasks, int count, int step) {
+  auto syrk = [&](const int4 *tasks, int count, int) {
     if (syrk_tc)
       launch_update_tc(sym_, d_tmaps_, tasks, d_syrk_end_ + (tasks - d_syrk_), d_syrk_pairs_,
-                       count, st);
+                       count, tuning_.tc_tma != 0, st);
     else
-      launch_syrk_step(sym_, tasks, count, step, st);
+      launch_syrk_step(sym_, tasks, d_syrk_pairs_, count, st);
   };
   // With profiling on, every launch is preceded by an event and followed by one.
   auto mark = [&](int kind, int count) {
@@ -880,7 +896,7 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec
     mark(K_UPDATE, W.upd_cnt);
     if (tf32)
       launch_update_tc(sym_, d_tmaps_, d_upd_tasks_ + W.upd_off, d_upd_end_ + W.upd_off,
-                       d_tc_pairs_, W.upd_cnt, st);
+                       d_tc_pairs_, W.upd_cnt, tuning_.tc_tma != 0, st);
     else if (prec == 2)
       launch_update_tiles_mx(sym_, d_upd_tasks_ + W.upd_off, d_upd_end_ + W.upd_off, d_pairs_,
                              W.upd_cnt, st);
@@ -1087,6 +1103,9 @@ double *Engine::staging(size_t doubles, std::string &err) {
 
 bool Engine::ensure_work(int nrhs, std::string &err) {
   if (nrhs <= work_nrhs_) return true;
+  release_solve_graphs();   // they hold the old buffers
+  if (d_sx_) cudaFree(d_sx_);
+  d_sx_ = nullptr;
   if (d_contrib_) cudaFree(d_contrib_);
   if (d_work_) cudaFree(d_work_);
   if (d_norms_) cudaFree(d_norms_);
@@ -1099,6 +1118,7 @@ bool Engine::ensure_work(int nrhs, std::string &err) {
   if (e == cudaSuccess) e = cudaMalloc(&d_norms_, sizeof(double) * 8 * (nrhs + 1));
   if (e == cudaSuccess) e = cudaMallocHost(&h_norms_, sizeof(double) * 8 * (nrhs + 1));
   if (e == cudaSuccess) e = cudaMalloc(&d_npart_, sizeof(double) * norm_scratch_doubles(nrhs));
+  if (e == cudaSuccess) e = cudaMalloc(&d_sx_, sizeof(double) * (size_t)n_ * nrhs);
   if (e != cudaSuccess) {
     err = std::string("solve workspace: ") + cudaGetErrorString(e);
     work_nrhs_ = 0;
@@ -1108,18 +1128,59 @@ bool Engine::ensure_work(int nrhs, std::string &err) {
   return true;
 }
 
-void Engine::run_solve(double *x, int nrhs) { run_solve_with(x, nrhs, d_contrib_); }
+void Engine::release_solve_graphs() {
+  for (auto &g : solve_graphs_) cudaGraphExecDestroy(g.second);
+  solve_graphs_.clear();
+}
+
+// The solve of nrhs right-hand sides held in d_sx_ as one CUDA graph (its launch sequence
+// and buffers are fixed by the structure and nrhs); captured on first use, nullptr when the
+// capture fails (the caller then launches directly).
+cudaGraphExec_t Engine::solve_graph(int nrhs) {
+  for (auto &g : solve_graphs_)
+    if (g.first == nrhs) return g.second;
+  cudaStream_t st = stream_;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return nullptr;
+  run_solve_with(d_sx_, nrhs, d_contrib_);
+  cudaError_t e = cudaStreamEndCapture(st, &graph);
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+  if (graph) cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  solve_graphs_.emplace_back(nrhs, exec);
+  return exec;
+}
+
+// x := (L L^T)^{-1} x for device x (n x nrhs): the solve graph on a copy of x in d_sx_,
+// or direct launches without graphs.
+void Engine::run_solve(double *x, int nrhs) {
+  cudaGraphExec_t g = use_graph_ ? solve_graph(nrhs) : nullptr;
+  if (!g) {
+    run_solve_with(x, nrhs, d_contrib_);
+    return;
+  }
+  const size_t bytes = sizeof(double) * (size_t)n_ * nrhs;
+  cudaMemcpyAsync(d_sx_, x, bytes, cudaMemcpyDeviceToDevice, stream_);
+  cudaGraphLaunch(g, stream_);
+  cudaMemcpyAsync(x, d_sx_, bytes, cudaMemcpyDeviceToDevice, stream_);
+}
 
 // Forward then backward supernodal solve, level by level, with the contribution scratch
-// `contrib` (one double per off-diagonal row of L per right-hand side).
+// `contrib` (one double per off-diagonal row of L per right-hand side).  The chained blocks'
+// flags are cleared first, so the epochs of every solve are the same (2r + 1 forward, 2r + 2
+// backward for right-hand side r) and a graph of this sequence can be replayed.
 void Engine::run_solve_with(double *x, int nrhs, double *contrib) {
   cudaStream_t st = stream_;
   const SolvePlan &SP = splan_;
   const int nl = (int)SP.level_off.size() - 1;
   const int smem = (int)sizeof(double) * std::max(SP.max_w, 1);
   const int64_t cs = std::max<int64_t>(SP.contrib_len, 1);
-  const int base = solve_epoch_;
-  solve_epoch_ += 2 * nrhs;
+  const int base = 0;
+  cudaMemsetAsync(d_flags_, 0, sizeof(int) * std::max<int64_t>(nflags_, 1), st);
   cudaMemsetAsync(d_status_ + 2, 0, sizeof(int), st);
   for (int l = 0; l < nl; ++l) {
     launch_fwd_warp(sym_, d_swarp_ + SP.warp_off[l], SP.warp_off[l + 1] - SP.warp_off[l], x,

@@ -311,8 +311,11 @@ class Engine {
   int *d_slist_ = nullptr, *d_cptr_ = nullptr, *d_cidx_ = nullptr, *d_flags_ = nullptr;
   int *d_swarp_ = nullptr;
   int2 *d_fchain_ = nullptr, *d_bchain_ = nullptr;
-  int solve_epoch_ = 0;
   int64_t nflags_ = 0;
+  double *d_sx_ = nullptr;                                         // solve graphs' vectors
+  std::vector<std::pair<int, cudaGraphExec_t>> solve_graphs_;      // per nrhs
+  cudaGraphExec_t solve_graph(int nrhs);
+  void release_solve_graphs();
   int2 *d_scontrib_ = nullptr, *d_sgather_ = nullptr;
   int *d_csr_rp_ = nullptr, *d_csr_ci_ = nullptr, *d_csr_map_ = nullptr;
   double *d_csr_val_ = nullptr;
@@ -346,7 +349,9 @@ void launch_update_tiles(const DevSym &S, const int4 *tasks, const int *task_end
                          const int4 *pairs, int count, cudaStream_t st);
 void launch_diag_step(const DevSym &S, const int *list, int count, int step, cudaStream_t st);
 void launch_trsm_step(const DevSym &S, const int2 *tasks, int count, int step, cudaStream_t st);
-void launch_syrk_step(const DevSym &S, const int4 *tasks, int count, int step, cudaStream_t st);
+// tasks (s, r0, c0, product index): prod[index].kk names the column blocks applied
+void launch_syrk_step(const DevSym &S, const int4 *tasks, const TcPair *prod, int count,
+                      cudaStream_t st);
 // dense factorization of a wave's tiled-class panels as one persistent dataflow launch:
 // tasks in topological order, per-supernode first tile counter (toff), tile version
 // counters and the queue head (both zeroed before the launch)
@@ -365,8 +370,9 @@ bool build_tensor_maps(const std::vector<int> &super, const std::vector<int64_t>
                        const std::vector<int64_t> &xk, float *Lk, void *maps_host,
                        std::string &err);
 size_t tensor_map_bytes();
+// tma: stage operands with TMA tile::gather4 loads, else with cp.async (four producer warps)
 void launch_update_tc(const DevSym &S, const void *maps, const int4 *tasks, const int *task_end,
-                      const TcPair *pairs, int count, cudaStream_t st);
+                      const TcPair *pairs, int count, bool tma, cudaStream_t st);
 // BF16x3 Schur updates (swc_mixed.cu)
 bool mixed_configure(std::string &err);
 void launch_update_tiles_mx(const DevSym &S, const int4 *tasks, const int *task_end,

@@ -98,6 +98,8 @@ struct Tuning {
   int dense_group = 4;                   // column blocks per grouped trailing update
   int syrk_fp64 = 0;                     // split-TF32 mode: trailing SYRK steps in FP64
                                          // (DMMA) instead of split-TF32 on tcgen05
+  int tc_tma = 0;                        // split-TF32 tcgen05 updates: stage operands with
+                                         // TMA gather4 loads instead of cp.async
 };
 
 }  // namespace swc

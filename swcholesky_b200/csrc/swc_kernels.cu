@@ -624,10 +624,11 @@ __global__ void __launch_bounds__(MT, 4) k_update_tiles(DevSym S, const int4 *ta
 
 // ---------------------------------------------------------------------------------------
 // Dense factorization of a tiled-class panel, blocked by 64 columns (right-looking):
-//   step j:  TRSM of the tiles below diagonal block j (k_trsm_step), then, concurrently,
-//            the trailing SYRK/GEMM update of the column blocks after j (k_syrk_step) and
-//            the update + POTRF + inverse of diagonal block j+1 (k_diag_step), so every
-//            diagonal block is factored before the next step's TRSM reads it.
+//   step j:  TRSM of the tiles below diagonal block j (k_trsm_step; its first row block's
+//            task also applies the update of diagonal tile j+1 by block j), then,
+//            concurrently, the trailing SYRK/GEMM update of the column blocks after j
+//            (k_syrk_step) and the POTRF + inverse of diagonal block j+1 (k_diag_step), so
+//            every diagonal block is factored before the next step's TRSM reads it.
 //   block 0 is factored by k_diag_step with step 0.
 
 // ---- one 64x64 diagonal block: POTRF and its inverse, blocked by 8 ----------------------
@@ -725,8 +726,9 @@ __device__ void potrf8_inv8(double *D, double *E, int kb, const DevSym &S, int g
 // D: bw x bw lower block padded to a multiple of 8 with identity.  Factors it in place
 // (right-looking over 8-column blocks) and leaves the inverses of its 8x8 diagonal blocks
 // in E.  Look-ahead: in the trailing update of step kb, warp 0 updates diagonal block kb+1
-// first and factors it while warps 1-3 update the other blocks, so each step costs one
-// panel phase and one trailing phase (two barriers).
+// first and factors it while the other NW - 1 warps update the other blocks, so each step
+// costs one panel phase and one trailing phase (two barriers).  NW warps (32 NW threads).
+template <int NW>
 __device__ void potrf64_blocked(double *D, double *E, int bw, const DevSym &S, int gcol0) {
   const int warp = threadIdx.x >> 5;
   const int nbk = (bw + 7) >> 3;
@@ -734,7 +736,7 @@ __device__ void potrf64_blocked(double *D, double *E, int bw, const DevSym &S, i
   __syncthreads();
   for (int kb = 0; kb < nbk; ++kb) {
     // panel below: X_ib = B_ib * T_kk^T (warp 0 gets ib = kb + 1)
-    for (int ib = kb + 1 + warp; ib < nbk; ib += 4) {
+    for (int ib = kb + 1 + warp; ib < nbk; ib += NW) {
       double c[2] = {0.0, 0.0};
       const int lane = threadIdx.x & 31, g = lane >> 2, kq = lane & 3;
 #pragma unroll
@@ -759,7 +761,7 @@ __device__ void potrf64_blocked(double *D, double *E, int bw, const DevSym &S, i
       for (int jb = kb + 1; jb < nbk; ++jb)
         for (int ib = jb; ib < nbk; ++ib) {
           if (ib == kb + 1) continue;   // (kb+1, kb+1) belongs to warp 0
-          if ((q++ % 3) != warp - 1) continue;
+          if ((q++ % (NW - 1)) != warp - 1) continue;
           double c[2];
           load8(c, D, 8 * ib, 8 * jb);
           mma8_abt(c, D, 8 * ib, 8 * kb, D, 8 * jb, 8 * kb, true);
@@ -772,11 +774,12 @@ __device__ void potrf64_blocked(double *D, double *E, int bw, const DevSym &S, i
 
 // Inverse of the factored block: off-diagonal 8x8 blocks T_ik = -T_ii sum_{j=k}^{i-1}
 // L_ij T_jk, one column block per warp (E holds T_kk on entry; W: 64 doubles per warp).
+template <int NW>
 __device__ void trtri64_blocked(const double *D, double *E, double *W, int bw) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, kq = lane & 3;
   const int nbk = (bw + 7) >> 3;
   double *Ww = W + warp * 64;
-  for (int k = warp; k < nbk; k += 4) {
+  for (int k = warp; k < nbk; k += NW) {
     for (int i = k + 1; i < nbk; ++i) {
       double sacc[2] = {0.0, 0.0};
       for (int j = k; j < i; ++j)   // sacc += L_ij T_jk
@@ -808,13 +811,17 @@ __device__ void trtri64_blocked(const double *D, double *E, double *W, int bw) {
 // a tile accumulator by syrk_tile_acc (its update by the previous column block), so the
 // updated block never leaves the chip before its factorization; when the block is narrower
 // than 64 the tile's remaining rows are panel rows below it and go to L.
-// 128 threads, DIAG_SMEM bytes of dynamic shared memory.
-// shared memory: E, W (4 x 64), then D
-constexpr int DIAG_SMEM = (E_ELEMS + 4 * 64 + TB * DLD) * 8;
+// NW warps (upd needs NW = 4: the tile accumulator's layout), diag_smem(NW) bytes of
+// dynamic shared memory: E, W (NW x 64), then D.
+constexpr int diag_smem(int nw) { return (E_ELEMS + nw * 64 + TB * DLD) * 8; }
+constexpr int DIAG_SMEM = diag_smem(4);
+constexpr int DIAG_NW = 8;   // warps of the per-step diagonal-block kernel
 
+template <int NW>
 __device__ void factor_diag_block(const DevSym &S, int s, int c0, double *smem,
                                   const TileAcc *upd) {
-  double *E = smem, *W = smem + E_ELEMS, *D = W + 4 * 64;
+  constexpr int NTH = 32 * NW;
+  double *E = smem, *W = smem + E_ELEMS, *D = W + NW * 64;
   const int tid = threadIdx.x;
   const int f = S.super[s];
   const int w = S.super[s + 1] - f;
@@ -822,18 +829,18 @@ __device__ void factor_diag_block(const DevSym &S, int s, int c0, double *smem,
   double *P = S.L + S.xptr[s];
   const int bw = min(TB, w - c0);
   __syncthreads();
-  // eight loads in flight per thread before the shared stores (128 threads)
-  for (int e0 = tid; e0 < TB * TB; e0 += 8 * MT) {
+  // eight loads in flight per thread before the shared stores
+  for (int e0 = tid; e0 < TB * TB; e0 += 8 * NTH) {
     double v[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-      const int e = e0 + q * MT, c = e >> 6, r = e & (TB - 1);
+      const int e = e0 + q * NTH, c = e >> 6, r = e & (TB - 1);
       if (c < bw && r < bw) v[q] = (!upd && r >= c) ? P[(size_t)(c0 + c) * m + c0 + r] : 0.0;
       else v[q] = (r == c) ? 1.0 : 0.0;
     }
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-      const int e = e0 + q * MT;
+      const int e = e0 + q * NTH;
       D[(e >> 6) * DLD + (e & (TB - 1))] = v[q];
     }
   }
@@ -855,13 +862,13 @@ __device__ void factor_diag_block(const DevSym &S, int s, int c0, double *smem,
     }
   }
   __syncthreads();
-  potrf64_blocked(D, E, bw, S, f + c0);
+  potrf64_blocked<NW>(D, E, bw, S, f + c0);
   for (int e = tid; e < TB * TB; e += blockDim.x) {
     const int c = e >> 6, r = e & (TB - 1);
     if (c < bw && r < bw && r >= c) P[(size_t)(c0 + c) * m + c0 + r] = D[c * DLD + r];
   }
   {   // the inverse serves the TRSM of the rows below and the chained triangular solves
-    trtri64_blocked(D, E, W, bw);
+    trtri64_blocked<NW>(D, E, W, bw);
     double *T = S.dinv + ((size_t)S.dinv_off[s] + c0 / TB) * (TB * TB);
     for (int e = tid; e < TB * TB; e += blockDim.x) {
       const int c = e >> 6, r = e & (TB - 1);
@@ -922,22 +929,25 @@ __device__ void syrk_tile(const DevSym &S, int s, int r0, int c0, int kblk, doub
   }
 }
 
-// One CTA per supernode of the list: bring diagonal block `step` up to date (its update by
-// column block step-1, which the SYRK launch of that step leaves out) and factor it.
+// Dataflow plan: one task brings diagonal block `step` up to date (its update by column
+// block step-1, which the trailing-update tasks of that step leave out) and factors it.
 __device__ void diag_task(const DevSym &S, int s, int step, double *smem) {
   const int c0 = step * TB;
   if (step > 0) {
     TileAcc acc;
     syrk_tile_acc(S, s, c0, c0, step - 1, smem, acc);
-    factor_diag_block(S, s, c0, smem, &acc);
+    factor_diag_block<4>(S, s, c0, smem, &acc);
   } else {
-    factor_diag_block(S, s, c0, smem, nullptr);
+    factor_diag_block<4>(S, s, c0, smem, nullptr);
   }
 }
 
-__global__ void __launch_bounds__(MT) k_diag_step(DevSym S, const int *list, int count, int step) {
+// Per-step launches: one CTA per supernode of the list factors diagonal block `step`, whose
+// update by column block step-1 the TRSM launch of that step has applied.
+__global__ void __launch_bounds__(DIAG_NW * 32) k_diag_step(DevSym S, const int *list, int count,
+                                                           int step) {
   extern __shared__ double dyn[];
-  diag_task(S, list[blockIdx.x], step, dyn);
+  factor_diag_block<DIAG_NW>(S, list[blockIdx.x], step * TB, dyn, nullptr);
 }
 
 // task = (s, r0): B = L[r0:r0+64, blk] := B * L_blk^{-T} = B * T^T with T = L_blk^{-1},
@@ -973,21 +983,35 @@ __device__ void trsm_task(const DevSym &S, int s, int r0, int step, double *dyn)
   }
 }
 
+// TRSM tiles of step `step`.  The task of the first row block below the diagonal block
+// holds the rows of the next diagonal tile: after solving them it applies that tile's
+// update by this column block itself (FP64, the rows it just wrote, still on chip or in
+// L2), so the next diagonal block's kernel only factors and the chain of dependent
+// launches (TRSM -> diagonal block -> TRSM) does not re-read the column block.
 __global__ void __launch_bounds__(MT, 4) k_trsm_step(DevSym S, const int2 *tasks, int count,
                                                   int step) {
   extern __shared__ double dyn[];
-  trsm_task(S, tasks[blockIdx.x].x, tasks[blockIdx.x].y, step, dyn);
+  const int s = tasks[blockIdx.x].x, r0 = tasks[blockIdx.x].y;
+  trsm_task(S, s, r0, step, dyn);
+  const int c0 = step * TB, w = S.super[s + 1] - S.super[s];
+  if (c0 + TB < w && r0 == c0 + TB) {
+    __syncthreads();   // the solved rows are in L (visible to the whole CTA)
+    syrk_tile(S, s, r0, r0, step, dyn);
+  }
 }
 
-// Trailing update of step `step`: task = (s, r0, c0) with c0 >= (step+1)*64, r0 >= c0.
-// The diagonal tile of the next block is left to k_diag_step, which runs concurrently.
+// Trailing update of a step: task = (s, r0, c0, product index) with c0 >= (step+1)*64,
+// r0 >= c0; the product names the column blocks applied (the step's block, or a group of
+// blocks ending with it).  The diagonal tile of the next block is updated by the TRSM
+// launch of the step and factored by k_diag_step, which runs concurrently.
 constexpr int SYRK_SMEM = 2 * STAGE * 8;
 
-__global__ void __launch_bounds__(MT) k_syrk_step(DevSym S, const int4 *tasks, int count,
-                                                  int step) {
+__global__ void __launch_bounds__(MT) k_syrk_step(DevSym S, const int4 *tasks, const TcPair *prod,
+                                                  int count) {
   extern __shared__ double dyn[];
   const int4 t = tasks[blockIdx.x];
-  syrk_tile(S, t.x, t.y, t.z, step, dyn);
+  const int kk = prod[t.w].kk;   // the task's column blocks: first = k0 / 64, then kcnt columns
+  syrk_tile(S, t.x, t.y, t.z, (kk & 0xffff) / TB, dyn, ((kk >> 16) + TB - 1) / TB);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1196,7 +1220,8 @@ bool kernels_configure(std::string &err) {
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_trsm_step, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * STAGE * 8);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_diag_step, cudaFuncAttributeMaxDynamicSharedMemorySize, DIAG_SMEM);
+    e = cudaFuncSetAttribute(k_diag_step, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             diag_smem(DIAG_NW));
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_syrk_step, cudaFuncAttributeMaxDynamicSharedMemorySize, SYRK_SMEM);
   if (e == cudaSuccess)
@@ -1248,13 +1273,14 @@ void launch_update_tiles(const DevSym &S, const int4 *tasks, const int *task_end
   if (count > 0) k_update_tiles<<<count, MT, UPD_SMEM, st>>>(S, tasks, task_end, pairs, count);
 }
 void launch_diag_step(const DevSym &S, const int *list, int count, int step, cudaStream_t st) {
-  if (count > 0) k_diag_step<<<count, MT, DIAG_SMEM, st>>>(S, list, count, step);
+  if (count > 0) k_diag_step<<<count, DIAG_NW * 32, diag_smem(DIAG_NW), st>>>(S, list, count, step);
 }
 void launch_trsm_step(const DevSym &S, const int2 *tasks, int count, int step, cudaStream_t st) {
   if (count > 0) k_trsm_step<<<count, MT, 2 * STAGE * 8, st>>>(S, tasks, count, step);
 }
-void launch_syrk_step(const DevSym &S, const int4 *tasks, int count, int step, cudaStream_t st) {
-  if (count > 0) k_syrk_step<<<count, MT, SYRK_SMEM, st>>>(S, tasks, count, step);
+void launch_syrk_step(const DevSym &S, const int4 *tasks, const TcPair *prod, int count,
+                      cudaStream_t st) {
+  if (count > 0) k_syrk_step<<<count, MT, SYRK_SMEM, st>>>(S, tasks, prod, count);
 }
 int dense_ctas(int count) {
   int dev = 0, sms = 0, per = 0;

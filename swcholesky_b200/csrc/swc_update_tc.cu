@@ -53,7 +53,8 @@ namespace swc {
 
 namespace {
 
-constexpr int UT_THREADS = 192;
+// threads: 4 epilogue warps, the producer warp(s), the MMA warp
+constexpr int ut_threads(bool tma) { return 32 * (tma ? 6 : 9); }
 constexpr int UT_STAGES = 4;
 constexpr int UT_KCHUNK = 32;                       // K columns per stage (128 bytes of TF32)
 constexpr int UT_OPB = 16 * 1024;                   // bytes of one 128-row operand chunk
@@ -196,9 +197,21 @@ __device__ __forceinline__ int gather_row(uint64_t mask, int s0, int i, int p, i
   return p * md + s0 + rank;
 }
 
-__global__ void __launch_bounds__(UT_THREADS, 1)
+// 16-byte copy global -> shared with zero fill beyond `bytes` (0..16) of the source.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, int bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(bytes)
+               : "memory");
+}
+
+// TMA = true: one producer warp stages with tile::gather4 loads; false: four producer warps
+// stage with 16-byte cp.async copies into the same swizzled layout and hand each stage to
+// the MMA warp through its mbarrier after a proxy fence.
+template <bool TMA>
+__global__ void __launch_bounds__(ut_threads(TMA), 1)
     k_update_tc(DevSym S, const CUtensorMap *__restrict__ maps, const int4 *__restrict__ tasks,
                 const int *__restrict__ task_end, const TcPair *__restrict__ pairs, int count) {
+  constexpr int NPROD = TMA ? 1 : 4;          // producer warps: 4 .. 3 + NPROD
+  constexpr int MMA_WARP = 4 + NPROD;
   extern __shared__ unsigned char ut_dyn[];
   __shared__ __align__(8) uint64_t full_bar[UT_STAGES], empty_bar[UT_STAGES];
   __shared__ __align__(8) uint64_t accf_bar[2], acce_bar[2], done_bar;
@@ -214,9 +227,9 @@ __global__ void __launch_bounds__(UT_THREADS, 1)
                  "r"(UT_TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
   }
-  if (tid == 160) {
+  if (tid == 32 * MMA_WARP) {
     for (int s = 0; s < UT_STAGES; ++s) {
-      mbar_init(smem_u32(&full_bar[s]), 1);
+      mbar_init(smem_u32(&full_bar[s]), TMA ? 1 : NPROD);
       mbar_init(smem_u32(&empty_bar[s]), 1);
     }
     for (int b = 0; b < 2; ++b) {
@@ -232,8 +245,67 @@ __global__ void __launch_bounds__(UT_THREADS, 1)
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = tmem_base;
 
-  if (warp == 4) {
-    // ------------------------------ producer ------------------------------
+  if (!TMA && warp >= 4 && warp < 4 + NPROD) {
+    // ------------------------- producers (cp.async) ------------------------
+    // warp pw fills rows' 32 pw .. 32 pw + 31 of A' and B': per instruction four rows' of
+    // 128 bytes (lane = row' (lane / 8), 16-byte chunk lane % 8), swizzled as the MMA reads
+    // them; a chunk completes two chunks later (wait_group 2), then proxy fence and arrival.
+    const int pw = warp - 4;
+    int stage = 0;
+    uint32_t phase = 0;
+    int pend[2] = {-1, -1};   // stages issued one and two chunks ago
+    bool ok = true;
+    const float *mir = reinterpret_cast<const float *>(S.Lf);
+    const int c = lane & 7;
+    for (int t = blockIdx.x; t < count && ok; t += gridDim.x) {
+      const int p_end = task_end[t];
+      for (int q = tasks[t].w; q < p_end && ok; ++q) {
+        const TcPair pr = pairs[q];
+        const int wd = S.super[pr.d + 1] - S.super[pr.d], wp = (wd + 3) & ~3;
+        const int md = (int)(S.rowptr[pr.d + 1] - S.rowptr[pr.d]);
+        const float *base = mir + S.xk[pr.d];
+        const int k0 = pr.kk & 0xffff, kend = k0 + (pr.kk >> 16);
+        for (int k = k0; k < kend; k += UT_KCHUNK) {
+          if (!mbar_wait_warp(smem_u32(&empty_bar[stage]), phase ^ 1u, &abort_flag, S.status)) {
+            ok = false;
+            break;
+          }
+          const uint32_t sa = sbase + stage * UT_STAGE_BYTES;
+          const int kk = k + 4 * c;
+          const int bytes = kend - kk >= 4 ? 16 : (kend > kk ? 4 * (kend - kk) : 0);
+#pragma unroll 4
+          for (int j = 0; j < 8; ++j) {
+            const int R = 32 * pw + 4 * j + (lane >> 3);
+            const int a = R >> 3, u = R & 7, p = u >> 2, i = 4 * a + (u & 3);
+            const uint32_t off = (uint32_t)(a * 1024 + u * 128 + ((c ^ u) << 4));
+            const int ya = gather_row(pr.rmask, pr.a0, i, p, md);
+            const int yb = gather_row(pr.cmask, pr.b0, i, p, md);
+            const bool va = ya < 2 * md && bytes > 0, vb = yb < 2 * md && bytes > 0;
+            cp_async16(sa + off, va ? base + (size_t)ya * wp + kk : base, va ? bytes : 0);
+            cp_async16(sa + UT_OPB + off, vb ? base + (size_t)yb * wp + kk : base, vb ? bytes : 0);
+          }
+          asm volatile("cp.async.commit_group;\n" ::: "memory");
+          if (pend[1] >= 0) {   // the chunk issued two chunks ago has landed: hand it over
+            asm volatile("cp.async.wait_group 2;\n" ::: "memory");
+            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&full_bar[pend[1]]));
+          }
+          pend[1] = pend[0];
+          pend[0] = stage;
+          if (++stage == UT_STAGES) { stage = 0; phase ^= 1u; }
+        }
+      }
+    }
+    // the last chunks (and, after an abort, every copy in flight) land before leaving
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    __syncwarp();
+    if (lane == 0)
+      for (int k = 1; k >= 0; --k)
+        if (pend[k] >= 0) mbar_arrive(smem_u32(&full_bar[pend[k]]));
+  } else if (TMA && warp == 4) {
+    // --------------------------- producer (TMA) ---------------------------
     int stage = 0;
     uint32_t phase = 0;
     int armed[UT_STAGES];
@@ -274,7 +346,7 @@ __global__ void __launch_bounds__(UT_THREADS, 1)
     if (lane == 0)
       for (int s = 0; s < UT_STAGES; ++s)
         if (armed[s] > 0) mbar_drain(smem_u32(&full_bar[s]), (uint32_t)(armed[s] - 1) & 1u, S.status);
-  } else if (warp == 5) {
+  } else if (warp == MMA_WARP) {
     // ------------------------------ MMA issuer ----------------------------
     if (lane == 0) {
       int stage = 0, buf = 0;
@@ -421,8 +493,11 @@ EncodeTiled encode_fn() {
 }  // namespace
 
 bool update_tc_configure(std::string &err) {
-  cudaError_t e = cudaFuncSetAttribute(k_update_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       UT_SMEM);
+  cudaError_t e = cudaFuncSetAttribute(k_update_tc<true>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, UT_SMEM);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_update_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             UT_SMEM);
   if (e != cudaSuccess) {
     err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e);
     return false;
@@ -482,10 +557,14 @@ int update_tc_ctas(int count) {
 }
 
 void launch_update_tc(const DevSym &S, const void *maps, const int4 *tasks, const int *task_end,
-                      const TcPair *pairs, int count, cudaStream_t st) {
+                      const TcPair *pairs, int count, bool tma, cudaStream_t st) {
   if (count <= 0) return;
-  k_update_tc<<<update_tc_ctas(count), UT_THREADS, UT_SMEM, st>>>(
-      S, static_cast<const CUtensorMap *>(maps), tasks, task_end, pairs, count);
+  if (tma)
+    k_update_tc<true><<<update_tc_ctas(count), ut_threads(true), UT_SMEM, st>>>(
+        S, static_cast<const CUtensorMap *>(maps), tasks, task_end, pairs, count);
+  else
+    k_update_tc<false><<<update_tc_ctas(count), ut_threads(false), UT_SMEM, st>>>(
+        S, static_cast<const CUtensorMap *>(maps), tasks, task_end, pairs, count);
 }
 
 }  // namespace swc

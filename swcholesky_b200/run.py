@@ -1,13 +1,17 @@
 """Runs the numeric factorization of a named workload a given number of times.
 
     python -m swcholesky_b200.run --workload grid3d_60 --mode fp64 --reps 1 [--solve]
+                                  [--plan K] [--profile]
     python -m swcholesky_b200.run --workload batch256 --mode mixed --reps 1 [--batch-count 64]
 
 The single-matrix workloads use the supernode partition stored in tests/golden (the
 reference's symbolic phase) when present, else the library's own partition; ``batch256``
 is the batched workload.  Prints one line with the sizes and the device milliseconds of
 the last factorization.  Meant as the command under a profiler: no warm-up, no extra
-kernels besides the factorization (and the solve with ``--solve``).
+kernels besides the factorization (and the solve with ``--solve``).  ``--plan`` selects an
+execution-plan candidate (``Handle.set_plan``); ``--profile`` adds, after the runs, one
+factorization with per-class event timing and the device time of factorizations and
+solves (not for use under a profiler).
 """
 from __future__ import annotations
 
@@ -17,7 +21,7 @@ import time
 
 import numpy as np
 
-from . import SWC_MODE_FP64, SWC_MODE_MIXED_TF32X3, Handle
+from . import SWC_MODE_FP64, SWC_MODE_MIXED_BF16X3, SWC_MODE_MIXED_TF32X3, Handle
 from . import matrices as M
 from . import workloads as W
 
@@ -44,7 +48,9 @@ def load(name: str, batch_count: int = 256):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", default="grid3d_60")
-    ap.add_argument("--mode", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--mode", default="fp64", choices=["fp64", "mixed", "bf16"])
+    ap.add_argument("--plan", type=int, default=0)
+    ap.add_argument("--profile", action="store_true")
     ap.add_argument("--reps", type=int, default=1)
     ap.add_argument("--solve", action="store_true")
     ap.add_argument("--tune-cache", default=None,
@@ -52,9 +58,11 @@ def main():
     ap.add_argument("--batch-count", type=int, default=256,
                     help="matrices of the batched workload (a smaller batch for profiling)")
     args = ap.parse_args()
-    mode = SWC_MODE_MIXED_TF32X3 if args.mode == "mixed" else SWC_MODE_FP64
+    mode = {"fp64": SWC_MODE_FP64, "mixed": SWC_MODE_MIXED_TF32X3,
+            "bf16": SWC_MODE_MIXED_BF16X3}[args.mode]
     prob, vals = load(args.workload, args.batch_count)
     h = Handle(0)
+    h.set_plan(args.plan)
     if isinstance(prob, list):
         h.batch_analyze(prob)
         if args.tune_cache:
@@ -79,6 +87,27 @@ def main():
             h.refine(b, tol=1e-12)
     print(f"workload {args.workload} n {h.n} nsuper {h.nsuper} xsize {h.xsize} "
           f"launches {h.launches} last factor {ms:.3f} ms (host clock)")
+    if args.profile:
+        prof = h.profile(v, mode)
+        print("classes (launches, device ms): " +
+              ", ".join(f"{k} {la} {t:.3f}" for k, (la, t, _, _) in prof.items()))
+        st = torch.cuda.ExternalStream(h.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(5):
+            h.factor(v, mode)
+        e1.record(st)
+        torch.cuda.synchronize()
+        x = torch.zeros_like(b)
+        h.solve(b, out=x)
+        e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e2.record(st)
+        for _ in range(10):
+            h.solve(b, out=x)
+        e3.record(st)
+        torch.cuda.synchronize()
+        print(f"factor {e0.elapsed_time(e1) / 5:.3f} ms, solve {e2.elapsed_time(e3) / 10:.3f} ms "
+              f"(device, CUDA events)")
     h.close()
 
 

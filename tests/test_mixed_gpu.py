@@ -73,3 +73,25 @@ def test_stencil27_40_eight_rhs(cuda_ok, name, mode):
     assert berr.shape == (8,) and berr.max() <= 1e-12, (berr, iters, method)
     fwd = ((xmx - x64).abs().amax(dim=1) / x64.abs().amax(dim=1)).cpu().numpy()
     assert fwd.max() <= meta["cond"] * 1e-13, fwd
+
+
+@pytest.mark.parametrize("plan", [0, 5, 6])
+def test_split_tf32_plan_variants(cuda_ok, plan):
+    """The split-TF32 factor under each of its execution-plan variants (0: tcgen05 updates
+    staged with cp.async, 5: trailing SYRK steps kept in FP64, 6: tcgen05 updates staged with
+    TMA tile::gather4 loads) agrees with the default plan's to FP32-class accuracy and
+    refines to the FP64 backward error."""
+    gs = load_sym("grid3d_24")
+    A, _, _ = W.build("grid3d_24")
+    P = W.assemble(A, gs["perm"], gs["super"])
+    h = swc.Handle(0)
+    h.set_plan(plan)
+    h.analyze(P.n, P.A2p, P.A2i, P.lC, P.Ls, P.Li_ptr, P.super, P.prunePtr, P.pruneSet)
+    assert h.factor(P.A2x, swc.SWC_MODE_FP64) == 0
+    L64 = h.get_L()
+    assert h.factor(P.A2x, swc.SWC_MODE_MIXED_TF32X3) == 0
+    rel = np.abs(h.get_L() - L64).max() / np.abs(L64).max()
+    assert 1e-12 < rel < 1e-5, rel
+    b = np.random.default_rng(4).standard_normal(P.n)
+    _, berr, _, _ = h.refine(b, tol=1e-14, maxit=30)
+    assert berr.max() <= 1e-14
