@@ -390,13 +390,15 @@ def run_ours(args, rank, world, local_rank):
     peak64 = fp64_gemm_peak(torch, dev) if rank == 0 else None
     bf16 = mode == swc.SWC_MODE_MIXED_BF16X3
     peak32 = tf32_gemm_peak(torch, dev, bf16) if rank == 0 and mixed else None
-    if mixed and dom == "update":
+    if mixed and dom in ("update", "syrk"):
         if bf16:
-            peak, psrc = peak32 / 6.0, ("cuBLAS BF16 GEMM 8192^3 measured in this run, divided by 6 "
-                                        "(a BF16x3 product costs six BF16 products)")
+            peak, psrc = peak32 / 8.0, ("cuBLAS BF16 GEMM 8192^3 measured in this run, divided by 8 "
+                                        "(a BF16x3 product executes eight BF16 piece products on "
+                                        "tcgen05: [hi;mid][hi;mid]^T and [lo;hi][lo;hi]^T)")
         else:
-            peak, psrc = peak32 / 3.0, ("cuBLAS TF32 GEMM 8192^3 measured in this run, divided by 3 "
-                                        "(a split-TF32 product costs three TF32 products)")
+            peak, psrc = peak32 / 4.0, ("cuBLAS TF32 GEMM 8192^3 measured in this run, divided by 4 "
+                                        "(a split-TF32 product executes four TF32 piece products on "
+                                        "tcgen05: [hi;lo][hi;lo]^T)")
     else:
         peak, psrc = peak64, "FP64 cuBLAS DGEMM 8192^3 measured in this run"
     hbm, hbm_src = hbm_peak()
@@ -485,7 +487,8 @@ def run_ours(args, rank, world, local_rank):
 
     if rank == 0:
         achieved = kfl / (kms * 1e-3) / 1e12
-        kname = {"update": "k_update_tiles_mx" if mixed else "k_update_tiles"}.get(dom)
+        kname = {"update": "k_update_tc" if mixed else "k_update_tiles",
+                 "syrk": "k_update_tc" if mixed else "k_syrk_step"}.get(dom)
         traffic = profile_traffic(kname, args.workload) if kname else None
         tsrc = (f"dram__bytes_read.sum + dram__bytes_write.sum per launch, ncu capture summarised "
                 f"in profiles/{kname}_{args.workload}.md" if traffic else None)

@@ -38,9 +38,10 @@ extern "C" {
                                    accumulation per group of descendants, FP64 across groups);
                                    POTRF, TRSM and small supernodes in FP64.  Pair with
                                    swc_refine. */
-#define SWC_MODE_MIXED_BF16X3 2 /* the same Schur updates as BF16x3 split products: each value as
-                                   three bfloat16 pieces, the six piece products down to the
-                                   third order, FP32 accumulation (about FP32 accuracy) */
+#define SWC_MODE_MIXED_BF16X3 2 /* the same Schur updates as BF16x3 split products on tcgen05:
+                                   each value as three bfloat16 pieces, the six piece products
+                                   down to the third order, FP32 accumulation per group of
+                                   descendants, FP64 across groups (about FP32 accuracy) */
 
 typedef struct swc_handle *swc_handle_t;
 

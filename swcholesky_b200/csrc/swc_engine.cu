@@ -154,7 +154,7 @@ void Engine::release() {
                   d_csr_map_,
                   d_csr_val_, d_contrib_, d_work_, d_norms_, d_persist_, d_qctr_, d_npart_,
                   d_tiny_, d_dense_tasks_, d_dense_toff_, d_dense_ver_, d_swarp_,
-                  d_Lk_, d_xk_, d_tmaps_, d_tc_pairs_, d_syrk_pairs_, d_syrk_end_};
+                  d_Lk_, d_xk_, d_xk16_, d_tmaps_, d_tc_pairs_, d_syrk_pairs_, d_syrk_end_};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   release_adjoint();
@@ -181,7 +181,7 @@ void Engine::release() {
   d_csr_val_ = d_contrib_ = d_work_ = d_norms_ = nullptr;
   d_persist_ = d_qctr_ = d_tiny_ = nullptr;
   d_Lk_ = nullptr;
-  d_xk_ = nullptr;
+  d_xk_ = d_xk16_ = nullptr;
   d_tmaps_ = nullptr;
   d_tc_pairs_ = d_syrk_pairs_ = nullptr;
   d_syrk_end_ = nullptr;
@@ -199,8 +199,6 @@ void Engine::release() {
     graph_exec_[k] = nullptr;
     graph_[k] = nullptr;
   }
-  if (d_Lf_) cudaFree(d_Lf_);
-  d_Lf_ = nullptr;
 }
 
 // Dataflow tasks of the dense factorization of one tiled-class panel (w columns, m rows),
@@ -627,7 +625,7 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
                      const int64_t *Li_ptr, const int *blockSet, int supNo,
                      const int *prunePtr, const int *pruneSet, std::string &err) {
   cudaSetDevice(device_);
-  if (!kernels_configure(err) || !mixed_configure(err) || !update_tc_configure(err)) return false;
+  if (!kernels_configure(err) || !update_tc_configure(err)) return false;
   HostSym H;
   Plan P;
   if (!build_plan(n, c, r, lC, Ls, Li_ptr, blockSet, supNo, prunePtr, pruneSet, H, P, err,
@@ -848,13 +846,15 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
 }
 
 void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec) {
-  const bool tf32 = prec == 1;                          // split-TF32 products on tcgen05
-  const bool syrk_tc = tf32 && !tuning_.syrk_fp64;
+  // split products on tcgen05: split-TF32 (cp.async or TMA staging) or BF16x3
+  const int variant = prec == 2 ? UT_VARIANT_BF16
+                                : (tuning_.tc_tma ? UT_VARIANT_TF32_TMA : UT_VARIANT_TF32);
+  const bool syrk_tc = prec != 0 && !tuning_.syrk_fp64;
   cudaStream_t st = stream_;
   auto syrk = [&](const int4 *tasks, int count, int) {
     if (syrk_tc)
       launch_update_tc(sym_, d_tmaps_, tasks, d_syrk_end_ + (tasks - d_syrk_), d_syrk_pairs_,
-                       count, tuning_.tc_tma != 0, st);
+                       count, variant, st);
     else
       launch_syrk_step(sym_, tasks, d_syrk_pairs_, count, st);
   };
@@ -894,12 +894,9 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec
     launch_assemble(sym_, d_asm_ + W.asm_off, W.asm_cnt, st);
     mark(-1, W.asm_cnt);
     mark(K_UPDATE, W.upd_cnt);
-    if (tf32)
+    if (prec != 0)
       launch_update_tc(sym_, d_tmaps_, d_upd_tasks_ + W.upd_off, d_upd_end_ + W.upd_off,
-                       d_tc_pairs_, W.upd_cnt, tuning_.tc_tma != 0, st);
-    else if (prec == 2)
-      launch_update_tiles_mx(sym_, d_upd_tasks_ + W.upd_off, d_upd_end_ + W.upd_off, d_pairs_,
-                             W.upd_cnt, st);
+                       d_tc_pairs_, W.upd_cnt, variant, st);
     else
       launch_update_tiles(sym_, d_upd_tasks_ + W.upd_off, d_upd_end_ + W.upd_off, d_pairs_,
                           W.upd_cnt, st);
@@ -945,34 +942,31 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec
 }
 
 bool Engine::set_mode(int prec, std::string &err) {
-  if (prec == 2 && !d_Lf_) {   // BF16x3 mirror, indexed as L
-    cudaError_t e = cudaMalloc(&d_Lf_, sizeof(float2) * std::max<int64_t>(xsize_, 1));
-    if (e != cudaSuccess) {
-      d_Lf_ = nullptr;
-      err = std::string("mirror allocation: ") + cudaGetErrorString(e);
-      return false;
-    }
-  }
-  if (prec == 1 && !d_Lk_) {   // split-TF32 K-major mirror and its tensor maps
+  if (prec != 0 && !d_Lk_) {   // the K-major split mirror, its format arrays, tensor maps
     const size_t mb = tensor_map_bytes() * (size_t)nsuper_;
+    const size_t nx = h_xk_.size();   // nsuper + 1: offsets, then the format entry
     std::vector<unsigned char> maps(mb);
-    cudaError_t e = cudaMalloc(&d_Lk_, sizeof(float) * std::max<int64_t>(kmirror_len_, 4));
-    if (e == cudaSuccess) e = cudaMalloc(&d_xk_, sizeof(int64_t) * std::max<size_t>(h_xk_.size(), 1));
+    std::vector<int64_t> xk16(h_xk_);
+    xk16[nx - 1] = 1;
+    cudaError_t e = cudaMalloc(&d_Lk_, sizeof(float) * std::max<int64_t>(kmirror_len_, 8));
+    if (e == cudaSuccess) e = cudaMalloc(&d_xk_, sizeof(int64_t) * nx);
+    if (e == cudaSuccess) e = cudaMalloc(&d_xk16_, sizeof(int64_t) * nx);
     if (e == cudaSuccess) e = cudaMalloc(&d_tmaps_, std::max<size_t>(mb, 128));
     if (e != cudaSuccess) {
       err = std::string("mirror allocation: ") + cudaGetErrorString(e);
       return false;
     }
     if (!build_tensor_maps(hsym_.super, hsym_.rowptr, h_xk_, d_Lk_, maps.data(), err)) return false;
-    e = cudaMemcpy(d_xk_, h_xk_.data(), sizeof(int64_t) * h_xk_.size(), cudaMemcpyHostToDevice);
+    e = cudaMemcpy(d_xk_, h_xk_.data(), sizeof(int64_t) * nx, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_xk16_, xk16.data(), sizeof(int64_t) * nx, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(d_tmaps_, maps.data(), mb, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
       err = std::string("mirror set-up: ") + cudaGetErrorString(e);
       return false;
     }
   }
-  sym_.Lf = prec == 2 ? d_Lf_ : prec == 1 ? reinterpret_cast<float2 *>(d_Lk_) : nullptr;
-  sym_.xk = prec == 1 ? d_xk_ : nullptr;
+  sym_.Lf = prec != 0 ? reinterpret_cast<float2 *>(d_Lk_) : nullptr;
+  sym_.xk = prec == 2 ? d_xk16_ : prec == 1 ? d_xk_ : nullptr;
   return true;
 }
 

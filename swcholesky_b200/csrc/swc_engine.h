@@ -29,12 +29,11 @@ struct DevSym {
                           // [1] = structure error flag, [2] = solve wait timeout,
                           // [3] = factorization wait timeout (persistent walk),
                           // [4] = poll budget of every bounded wait (set by the host)
-  float2 *Lf;             // split mirror of L (mixed-precision modes only, else null)
-  const int64_t *xk;      // null: Lf is the BF16x3 mirror, same indexing as L, per value
-                          // three bfloat16 pieces.  Else Lf holds the split-TF32 mirror in
-                          // K-major form: supernode s at (float *)Lf + xk[s], hi plane rows
-                          // 0..m-1 then lo plane rows m..2m-1, rows of (w rounded up to 4)
-                          // floats
+  float2 *Lf;             // split mirror of L in K-major form (mixed-precision modes only,
+                          // else null): supernode s at (float *)Lf + xk[s]
+  const int64_t *xk;      // per supernode: offset of its mirror; xk[nsuper]: the format, 0
+                          // hi / lo TF32 planes (rows of w rounded up to 4 floats), 1 hi / mid
+                          // / lo bfloat16 planes (rows of w rounded up to 8 values)
   double *dinv;           // scratch: inverses of the 64x64 diagonal blocks of the tiled class
   const int *dinv_off;    // per supernode: first block of its inverses in dinv (-1: none)
 };
@@ -292,9 +291,8 @@ class Engine {
   int *d_upd_end_ = nullptr;
   cudaGraph_t graph_[3] = {nullptr, nullptr, nullptr};          // one per precision mode
   cudaGraphExec_t graph_exec_[3] = {nullptr, nullptr, nullptr};
-  float2 *d_Lf_ = nullptr;                     // BF16x3 mirror
-  float *d_Lk_ = nullptr;                      // split-TF32 K-major mirror
-  int64_t *d_xk_ = nullptr;                    // its per-supernode offsets
+  float *d_Lk_ = nullptr;                      // K-major split mirror (either mixed mode)
+  int64_t *d_xk_ = nullptr, *d_xk16_ = nullptr;   // its offsets + format (TF32 / BF16x3)
   void *d_tmaps_ = nullptr;                    // one tensor map per supernode (over d_Lk_)
   std::vector<int64_t> h_xk_;
   int64_t kmirror_len_ = 0;
@@ -360,9 +358,10 @@ void launch_dense_persist(const DevSym &S, const int4 *tasks, int count, int cta
                           int *ver, int *qhead, cudaStream_t st);
 void launch_init_status(int *status, cudaStream_t st);
 bool kernels_configure(std::string &err);
-// split-TF32 tile updates on tcgen05 fed by TMA gathers (swc_update_tc.cu): K-major mirror
-// layout (offsets per supernode, total floats), one tensor map per supernode (host array
-// of nsuper entries of tensor_map_bytes() each), the launch over tile tasks
+// split-precision tile updates on tcgen05 (swc_update_tc.cu): K-major mirror layout
+// (offsets per supernode and the format entry, total floats), one tensor map per supernode
+// for the TMA staging (host array of nsuper entries of tensor_map_bytes() each), the launch
+// over tile tasks
 bool update_tc_configure(std::string &err);
 int64_t kmirror_layout(const std::vector<int> &super, const std::vector<int64_t> &rowptr,
                        std::vector<int64_t> &xk);
@@ -370,12 +369,11 @@ bool build_tensor_maps(const std::vector<int> &super, const std::vector<int64_t>
                        const std::vector<int64_t> &xk, float *Lk, void *maps_host,
                        std::string &err);
 size_t tensor_map_bytes();
-// tma: stage operands with TMA tile::gather4 loads, else with cp.async (four producer warps)
+// variants: split-TF32 staged with cp.async (four producer warps) or with TMA gather4 loads;
+// BF16x3 staged with cp.async
+constexpr int UT_VARIANT_TF32 = 0, UT_VARIANT_TF32_TMA = 1, UT_VARIANT_BF16 = 2;
+int update_tc_ctas(int count);   // CTAs of a launch over `count` tiles (at most one per SM)
 void launch_update_tc(const DevSym &S, const void *maps, const int4 *tasks, const int *task_end,
-                      const TcPair *pairs, int count, bool tma, cudaStream_t st);
-// BF16x3 Schur updates (swc_mixed.cu)
-bool mixed_configure(std::string &err);
-void launch_update_tiles_mx(const DevSym &S, const int4 *tasks, const int *task_end,
-                            const int4 *pairs, int count, cudaStream_t st);
+                      const TcPair *pairs, int count, int variant, cudaStream_t st);
 
 }  // namespace swc

@@ -56,47 +56,65 @@ __device__ __forceinline__ float2 split_tf32(double x) {
 }
 
 // Three bfloat16 pieces of x: hi = bf16(x), mid = bf16(x - hi), lo = bf16(x - hi - mid)
-// (the remainders are exact in FP64), packed as x = hi | mid << 16, y = lo.
-__device__ __forceinline__ float2 split_bf16x3(double x) {
+// (the remainders are exact in FP64).
+struct Bf16x3 {
+  unsigned short hi, mid, lo;
+};
+__device__ __forceinline__ Bf16x3 split_bf16x3(double x) {
   const __nv_bfloat16 hi = __float2bfloat16_rn((float)x);
   const double r1 = x - (double)__bfloat162float(hi);
   const __nv_bfloat16 mid = __float2bfloat16_rn((float)r1);
   const double r2 = r1 - (double)__bfloat162float(mid);
   const __nv_bfloat16 lo = __float2bfloat16_rn((float)r2);
-  const unsigned bx = (unsigned)__bfloat16_as_ushort(hi) | ((unsigned)__bfloat16_as_ushort(mid) << 16);
-  const unsigned by = (unsigned)__bfloat16_as_ushort(lo);
-  return make_float2(__uint_as_float(bx), __uint_as_float(by));
+  return Bf16x3{__bfloat16_as_ushort(hi), __bfloat16_as_ushort(mid), __bfloat16_as_ushort(lo)};
 }
 
-// The mirror entries of value x of row r, column c of supernode s (m rows, w columns):
-// the BF16x3 triple at L's index, or hi / lo of the split-TF32 K-major planes.
+// The mirror entries of value x of row r, column c of supernode s (m rows, w columns), in
+// the K-major split mirror at (float *)Lf + xk[s], format xk[nsuper]: 0, hi / lo TF32
+// planes of rows of w rounded up to 4 floats; 1, hi / mid / lo bfloat16 planes of rows of
+// w rounded up to 8 values.
 __device__ __forceinline__ void store_mirror(const DevSym &S, int s, int m, int w, int r, int c,
                                              double x) {
-  if (!S.xk) {
-    S.Lf[S.xptr[s] + (size_t)c * m + r] = split_bf16x3(x);
-  } else {
+  float *base = reinterpret_cast<float *>(S.Lf) + S.xk[s];
+  if (S.xk[S.nsuper] == 0) {
+    const int wp = (w + 3) & ~3;
     const float2 v = split_tf32(x);
-    float *row = reinterpret_cast<float *>(S.Lf) + S.xk[s] + (size_t)r * ((w + 3) & ~3) + c;
-    row[0] = v.x;
-    row[(size_t)m * ((w + 3) & ~3)] = v.y;
+    base[(size_t)r * wp + c] = v.x;
+    base[((size_t)m + r) * wp + c] = v.y;
+  } else {
+    const int wq = (w + 7) & ~7;
+    unsigned short *b = reinterpret_cast<unsigned short *>(base);
+    const Bf16x3 v = split_bf16x3(x);
+    b[(size_t)r * wq + c] = v.hi;
+    b[((size_t)m + r) * wq + c] = v.mid;
+    b[((size_t)2 * m + r) * wq + c] = v.lo;
   }
 }
 
 // The whole m x w panel P (column-major, ld m) of supernode s into the mirror; threads
-// t, t + nt, ... (consecutive threads write consecutive mirror entries).
+// t, t + nt, ... (consecutive threads write consecutive mirror entries of a row).
 __device__ __forceinline__ void store_mirror_panel(const DevSym &S, int s, int m, int w,
                                                    const double *P, int t, int nt) {
-  if (!S.xk) {
-    float2 *dstf = S.Lf + S.xptr[s];
-    for (int i = t; i < m * w; i += nt) dstf[i] = split_bf16x3(P[i]);
-  } else {
+  float *base = reinterpret_cast<float *>(S.Lf) + S.xk[s];
+  if (S.xk[S.nsuper] == 0) {
     const int wp = (w + 3) & ~3;
-    float *hi = reinterpret_cast<float *>(S.Lf) + S.xk[s], *lo = hi + (size_t)m * wp;
+    float *hi = base, *lo = hi + (size_t)m * wp;
     for (int e = t; e < m * w; e += nt) {
       const int r = e / w, c = e - r * w;
       const float2 v = split_tf32(P[(size_t)c * m + r]);
       hi[(size_t)r * wp + c] = v.x;
       lo[(size_t)r * wp + c] = v.y;
+    }
+  } else {
+    const int wq = (w + 7) & ~7;
+    unsigned short *hi = reinterpret_cast<unsigned short *>(base);
+    unsigned short *mid = hi + (size_t)m * wq, *lo = mid + (size_t)m * wq;
+    for (int e = t; e < m * w; e += nt) {
+      const int r = e / w, c = e - r * w;
+      const Bf16x3 v = split_bf16x3(P[(size_t)c * m + r]);
+      hi[(size_t)r * wq + c] = v.hi;
+      mid[(size_t)r * wq + c] = v.mid;
+      lo[(size_t)r * wq + c] = v.lo;
     }
   }
 }

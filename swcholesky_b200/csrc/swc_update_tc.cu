@@ -1,46 +1,66 @@
-// Split-TF32 Schur updates of the tiled class on the 5th-generation tensor cores.
+// Split-precision Schur updates of the tiled class on the 5th-generation tensor cores.
 //
 // The reference forms every update of a target supernode from a descendant as a dense
 // SYRK + GEMM into a contribution buffer and scatters it through relative indices
 // (cholesky/sw_parallel_PB_Cholesky_05.c:299-378).  Here a 64x64 tile of a target panel
 // owns its updates: for every (tile, descendant) pair the descendant's rows that fall in
-// the tile are GATHERED by the tensor memory accelerator straight into the tile's own row
-// and column positions, so the product lands in the tile's coordinates and no scatter is
-// needed; the tile leaves the chip once, after all its descendants.  The same kernel runs
-// the trailing SYRK/GEMM steps of the blocked dense factorization of wide supernodes (a
-// "pair" whose descendant is the supernode itself and whose K range is one 64-column block).
+// the tile are gathered straight into the tile's own row and column positions in shared
+// memory, so the product lands in the tile's coordinates and no scatter is needed; the tile
+// leaves the chip once, after all its descendants.  The same kernel runs the trailing
+// SYRK/GEMM steps of the blocked dense factorization of wide supernodes (a "pair" whose
+// descendant is the supernode itself and whose K range is one or more 64-column blocks).
 //
-// Operands: the split mirror of L in K-major form.  Every value x of supernode d (md rows,
-// wd columns, pitch wp = wd rounded up to 4) is stored as hi = tf32(x) in row r of the hi
-// plane and lo = tf32(x - hi) in row md + r of the lo plane (rows of wp floats).  One 2D
-// tensor map per supernode covers both planes ({wd, 2 md}, 128-byte swizzle); a
-// cp.async.bulk.tensor ... tile::gather4 load copies four rows of 32 values (any four
-// row coordinates: a row outside the map, used for tile rows no descendant row feeds,
-// reads zeros) into one half of a 1024-byte swizzle atom.  A stage holds the 128-row
-// operands A' and B' of one 32-column K chunk: atom a holds tile rows 4a..4a+3, hi pieces
-// in its first 512 bytes and lo pieces in its second.
+// Operands: the split mirror of L in K-major form, supernode d (md rows, wd columns) at
+// (float *)Lf + xk[d]; xk[nsuper] names the format:
+//   0  split-TF32: hi = tf32(x) in row r of the hi plane, lo = tf32(x - hi) in row md + r
+//      of the lo plane; rows of wp = wd rounded up to 4 floats;
+//   1  BF16x3: hi = bf16(x), mid = bf16(x - hi), lo = bf16(x - hi - mid) in rows r, md + r,
+//      2 md + r of three planes; rows of wq = wd rounded up to 8 bfloat16 values.
+// A stage holds one 32-column K chunk of the 128-row operands, each in the canonical K-major
+// layout the MMA reads with a swizzle (128-byte rows, 128-byte swizzle for TF32; 64-byte
+// rows, 64-byte swizzle for BF16): atom a (8 rows) holds tile rows 4a..4a+3 twice, one piece
+// in its first four rows and another in its last four.  A tile row that no descendant row
+// feeds is zero-filled.
 //
-// Product: one tcgen05.mma kind::tf32 with M = N = 128 and K = 8 multiplies A' by B'^T, so
-// the accumulator D' (128 x 128 FP32 in TMEM) holds all four piece products of every
-// (row, column) pair: C(i, j) = hi hi' + hi lo' + lo hi' + lo lo', about 2^-22 relative
-// error (the accuracy of the split); the four entries are folded in the epilogue.
+// Products (one CTA, M = N = 128, accumulators in TMEM, FP32):
+//   split-TF32: operands A' = [hi; lo] and B' = [hi; lo]; one kind::tf32 MMA per 8 columns of
+//     K gives every piece product: C(i, j) = hi hi' + hi lo' + lo hi' + lo lo' (about 2^-22
+//     relative error, the accuracy of the split);
+//   BF16x3: operands A1 = [hi; mid], A2 = [lo; hi] (and B1, B2 alike); per 16 columns of K one
+//     kind::f16 MMA accumulates D1 = A1 B1^T and one D2 = A2 B2^T; the epilogue takes all of
+//     D1 and the lo hi' and hi lo' blocks of D2: the six piece products down to the third
+//     order (the split-bfloat16 method of Henry, Tang and Heinecke, ARITH 2019), about 2^-24
+//     relative error.
+// The pieces are folded in the epilogue (one shuffle: the two rows of a tile row's pieces
+// are lanes t and t ^ 4).
 //
-// Roles (192 threads, one CTA per SM, persistent over the tile list):
-//   warp 4   producer: per K chunk, waits for a free stage, arms its "full" mbarrier with
-//            the stage's byte count and issues 64 gather4 loads (two per lane);
-//   warp 5   MMA issuer (one thread): per chunk, waits for the stage, issues 4 MMAs into
-//            one of two TMEM accumulators and commits the stage back to the producer;
-//            after a group of descendants (at least 8 chunks, or the tile's last) commits
-//            the accumulator to the epilogue and switches to the other one;
-//   warps 0-3 epilogue (TMEM lane quarter = warp): per group, reads the accumulator,
-//            folds the pieces, adds it in FP64 to the tile held in registers (seeded with
-//            minus the tile's FP64 values), releases the accumulator; stores the tile
-//            once per tile.  The next tile's FP64 values load while the MMAs of its first
-//            group run.
-// Every wait is bounded; a wait that runs out sets status[3] and an abort flag that stops
-// the other roles; the kernel then waits (bounded) for its copies and MMAs in flight,
-// frees its TMEM and returns.
+// Staging (per K chunk, 32 KB):
+//   cp.async  four producer warps copy 16 bytes per lane, a warp instruction covering 512
+//             contiguous shared-memory bytes (four 128-byte or eight 64-byte rows: no bank
+//             conflicts) and 128- or 64-byte runs of global memory; a chunk is handed to the
+//             MMA warp two chunks later (cp.async.wait_group 2, proxy fence, mbarrier
+//             arrival of each producer warp);
+//   TMA       (split-TF32, plan 6) one producer warp issues 64 cp.async.bulk.tensor.2d ...
+//             tile::gather4 loads (four rows of 32 values each, into one half of a swizzle
+//             atom) from one 2D tensor map per supernode ({wd, 2 md}, 128-byte swizzle, zero
+//             fill outside); measured slower than the cp.async path on this workload.
+//
+// Roles (one CTA per SM, persistent over the launch's tile list):
+//   warps 0-3  epilogue (TMEM lane quarter = warp): per group of descendants (at least 8
+//              chunks, or the tile's last), reads the accumulator(s), folds the pieces, adds
+//              them in FP64 to the tile held in registers (seeded with minus the tile's FP64
+//              values), releases the accumulator; stores the tile once per tile.  The next
+//              tile's values load while the MMAs of its first group run;
+//   producers  as above;
+//   MMA warp   one thread: per chunk waits for the stage, issues the MMAs into one of two
+//              accumulator sets and commits the stage back to the producers
+//              (tcgen05.commit); at the end of a group commits the accumulators to the
+//              epilogue and switches sets.
+// Every mbarrier wait is bounded (2 s of %globaltimer): a wait that runs out sets status[3]
+// and an abort flag that stops the other roles; the kernel then waits (bounded) for its
+// copies and MMAs in flight, frees its TMEM and returns.
 #include <cuda.h>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -53,29 +73,49 @@ namespace swc {
 
 namespace {
 
-// threads: 4 epilogue warps, the producer warp(s), the MMA warp
-constexpr int ut_threads(bool tma) { return 32 * (tma ? 6 : 9); }
+// variants of the kernel
+constexpr int V_TF32 = UT_VARIANT_TF32;           // split-TF32, cp.async staging
+constexpr int V_TF32_TMA = UT_VARIANT_TF32_TMA;   // split-TF32, TMA gather4 staging
+constexpr int V_BF16 = UT_VARIANT_BF16;           // BF16x3, cp.async staging
+
 constexpr int UT_STAGES = 4;
-constexpr int UT_KCHUNK = 32;                       // K columns per stage (128 bytes of TF32)
-constexpr int UT_OPB = 16 * 1024;                   // bytes of one 128-row operand chunk
-constexpr int UT_STAGE_BYTES = 2 * UT_OPB;          // A' and B'
+constexpr int UT_KCHUNK = 32;                       // K columns per stage
+constexpr int UT_STAGE_BYTES = 32 * 1024;           // the operand chunks of one stage
 constexpr int UT_SMEM = UT_STAGES * UT_STAGE_BYTES + 1024;   // + alignment slack
-constexpr int UT_TMEM_COLS = 256;                   // two 128-column FP32 accumulators
 constexpr int UT_GROUP_CHUNKS = 8;                  // chunks of one FP32 accumulation group
 constexpr unsigned long long UT_WAIT_NS = 2000000000ULL;   // a pipeline wait gives up after 2 s
-// instruction descriptor: D F32, A and B TF32, both K-major, N = 128, M = 128
-constexpr uint32_t UT_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((128u >> 3) << 17) |
-                              ((128u >> 4) << 24);
+
+// Per-variant constants: element bytes, row bytes of an operand chunk (= its swizzle span),
+// operands per stage, bytes of one operand chunk, TMEM columns (two accumulator sets),
+// producer warps, threads, instruction descriptor (D F32, K-major A and B, N = M = 128;
+// A/B format TF32 = 2 or BF16 = 1), descriptor layout type (SWIZZLE_128B = 2, _64B = 4).
+template <int V>
+struct Ut {
+  static constexpr bool BF16 = V == V_BF16;
+  static constexpr int ELEM = BF16 ? 2 : 4;
+  static constexpr int ROW = UT_KCHUNK * ELEM;               // 128 (TF32) or 64 (BF16)
+  static constexpr int ATOM = 8 * ROW;                       // bytes of an 8-row atom
+  static constexpr int NOPS = BF16 ? 4 : 2;                  // A1, A2, B1, B2 / A', B'
+  static constexpr int OPB = 128 * ROW;                      // bytes of one operand chunk
+  static constexpr int TMEM_COLS = BF16 ? 512 : 256;
+  static constexpr int NPROD = V == V_TF32_TMA ? 1 : 4;
+  static constexpr int THREADS = 32 * (5 + NPROD);
+  static constexpr int FMT = BF16 ? 1 : 2;
+  static constexpr uint32_t IDESC = (1u << 4) | ((uint32_t)FMT << 7) | ((uint32_t)FMT << 10) |
+                                    ((128u >> 3) << 17) | ((128u >> 4) << 24);
+  static constexpr uint64_t LAYOUT = BF16 ? 4 : 2;
+  static_assert(NOPS * OPB == UT_STAGE_BYTES, "a stage holds the operand chunks");
+};
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-// Shared-memory matrix descriptor, K-major operand with the 128-byte swizzle: 8-row groups
-// 1024 bytes apart (SBO), leading offset 16 bytes (unused by this layout), version 1.
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
-  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
-         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+// Shared-memory matrix descriptor of a K-major swizzled operand: 8-row groups `sbo` bytes
+// apart, leading offset 16 bytes (unused by the swizzled K-major layouts), version 1.
+__device__ __forceinline__ uint64_t sw_desc(uint32_t saddr, uint32_t sbo, uint64_t layout) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | ((uint64_t)1 << 46) | (layout << 61);
 }
 
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
@@ -154,12 +194,27 @@ __device__ __forceinline__ void tma_gather4(uint32_t dst, const CUtensorMap *map
       : "memory");
 }
 
-__device__ __forceinline__ void mma_tf32(uint32_t tmem, uint64_t adesc, uint64_t bdesc,
-                                         uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
-      "l"(adesc), "l"(bdesc), "r"(UT_IDESC), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+// 16-byte copy global -> shared with zero fill beyond `bytes` (0..16) of the source.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, int bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(bytes)
+               : "memory");
+}
+
+template <int V>
+__device__ __forceinline__ void mma_issue(uint32_t tmem, uint64_t adesc, uint64_t bdesc,
+                                          uint32_t accumulate) {
+  if (Ut<V>::BF16)
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+            tmem),
+        "l"(adesc), "l"(bdesc), "r"(Ut<V>::IDESC), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+  else
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+            tmem),
+        "l"(adesc), "l"(bdesc), "r"(Ut<V>::IDESC), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
 }
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
   asm volatile(
@@ -183,35 +238,31 @@ __device__ __forceinline__ void tmem_ld32(uint32_t addr, float (&v)[32]) {
   for (int q = 0; q < 32; ++q) v[q] = __uint_as_float(r[q]);
 }
 
-// K chunks of a pair, and whether the accumulation group closes after it.
+// K chunks of a pair.
 __device__ __forceinline__ int pair_chunks(const TcPair &pr) {
   return ((pr.kk >> 16) + UT_KCHUNK - 1) / UT_KCHUNK;
 }
 
-// Row coordinate of tile row i of the pair's operand (mask, first source row s0) in the
-// map of a supernode with md rows: plane p (0 hi, 1 lo), or a row outside the map (zeros)
-// when no source row feeds it.
-__device__ __forceinline__ int gather_row(uint64_t mask, int s0, int i, int p, int md) {
-  if (!((mask >> i) & 1ull)) return 2 * md;
-  const int rank = __popcll(mask & ((1ull << i) - 1ull));
-  return p * md + s0 + rank;
+// Row of the source supernode (md rows) that feeds tile row i of the pair's operand (mask,
+// first source row s0), in plane p of the mirror, or -1 when no source row feeds it.
+__device__ __forceinline__ int source_row(uint64_t mask, int s0, int i, int p, int md) {
+  if (!((mask >> i) & 1ull)) return -1;
+  return p * md + s0 + __popcll(mask & ((1ull << i) - 1ull));
 }
 
-// 16-byte copy global -> shared with zero fill beyond `bytes` (0..16) of the source.
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, int bytes) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(bytes)
-               : "memory");
+// Mirror plane of piece slot p (0: first four rows of an atom, 1: last four) of operand o.
+template <int V>
+__device__ __forceinline__ int operand_plane(int o, int p) {
+  if (!Ut<V>::BF16) return p;                    // A', B': hi, lo
+  return (o & 1) == 0 ? p : (p == 0 ? 2 : 0);    // A1, B1: hi, mid;  A2, B2: lo, hi
 }
 
-// TMA = true: one producer warp stages with tile::gather4 loads; false: four producer warps
-// stage with 16-byte cp.async copies into the same swizzled layout and hand each stage to
-// the MMA warp through its mbarrier after a proxy fence.
-template <bool TMA>
-__global__ void __launch_bounds__(ut_threads(TMA), 1)
+template <int V>
+__global__ void __launch_bounds__(Ut<V>::THREADS, 1)
     k_update_tc(DevSym S, const CUtensorMap *__restrict__ maps, const int4 *__restrict__ tasks,
                 const int *__restrict__ task_end, const TcPair *__restrict__ pairs, int count) {
-  constexpr int NPROD = TMA ? 1 : 4;          // producer warps: 4 .. 3 + NPROD
-  constexpr int MMA_WARP = 4 + NPROD;
+  using T = Ut<V>;
+  constexpr int MMA_WARP = 4 + T::NPROD;
   extern __shared__ unsigned char ut_dyn[];
   __shared__ __align__(8) uint64_t full_bar[UT_STAGES], empty_bar[UT_STAGES];
   __shared__ __align__(8) uint64_t accf_bar[2], acce_bar[2], done_bar;
@@ -224,12 +275,12 @@ __global__ void __launch_bounds__(ut_threads(TMA), 1)
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
                      smem_u32(&tmem_base)),
-                 "r"(UT_TMEM_COLS));
+                 "r"(T::TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
   }
   if (tid == 32 * MMA_WARP) {
     for (int s = 0; s < UT_STAGES; ++s) {
-      mbar_init(smem_u32(&full_bar[s]), TMA ? 1 : NPROD);
+      mbar_init(smem_u32(&full_bar[s]), T::NPROD);
       mbar_init(smem_u32(&empty_bar[s]), 1);
     }
     for (int b = 0; b < 2; ++b) {
@@ -245,25 +296,50 @@ __global__ void __launch_bounds__(ut_threads(TMA), 1)
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = tmem_base;
 
-  if (!TMA && warp >= 4 && warp < 4 + NPROD) {
+  if (V != V_TF32_TMA && warp >= 4 && warp < 4 + T::NPROD) {
     // ------------------------- producers (cp.async) ------------------------
-    // warp pw fills rows' 32 pw .. 32 pw + 31 of A' and B': per instruction four rows' of
-    // 128 bytes (lane = row' (lane / 8), 16-byte chunk lane % 8), swizzled as the MMA reads
-    // them; a chunk completes two chunks later (wait_group 2), then proxy fence and arrival.
-    const int pw = warp - 4;
+    // warp pw fills rows' 32 pw .. 32 pw + 31 of every operand chunk; an instruction covers
+    // RPI rows' of T::ROW bytes (lane: row' RPI j + lane / CPR, 16-byte column chunk
+    // lane % CPR), written where the swizzled K-major layout puts them.  The lane's NSLOT
+    // shared-memory slots are fixed for the kernel and its source rows for a pair, so a
+    // chunk costs one add and one copy per slot.  A chunk completes two chunks later
+    // (wait_group 2), then proxy fence and the warp's arrival on the stage.
+    constexpr int CPR = T::ROW / 16, RPI = 32 / CPR, JS = 32 / RPI, NSLOT = T::NOPS * JS;
+    const int pw = warp - 4, cc = lane % CPR, rsub = lane / CPR;
+    uint32_t soff[NSLOT];   // shared-memory offset of each slot within a stage
+#pragma unroll
+    for (int o = 0; o < T::NOPS; ++o)
+#pragma unroll
+      for (int j = 0; j < JS; ++j) {
+        const int R = 32 * pw + RPI * j + rsub, a = R >> 3, u = R & 7;
+        const int swz = T::BF16 ? (u >> 1) : u;
+        soff[o * JS + j] = (uint32_t)(o * T::OPB + a * T::ATOM + u * T::ROW + ((cc ^ swz) << 4));
+      }
     int stage = 0;
     uint32_t phase = 0;
     int pend[2] = {-1, -1};   // stages issued one and two chunks ago
     bool ok = true;
-    const float *mir = reinterpret_cast<const float *>(S.Lf);
-    const int c = lane & 7;
+    const unsigned char *mir = reinterpret_cast<const unsigned char *>(S.Lf);
     for (int t = blockIdx.x; t < count && ok; t += gridDim.x) {
       const int p_end = task_end[t];
       for (int q = tasks[t].w; q < p_end && ok; ++q) {
         const TcPair pr = pairs[q];
-        const int wd = S.super[pr.d + 1] - S.super[pr.d], wp = (wd + 3) & ~3;
+        const int wd = S.super[pr.d + 1] - S.super[pr.d];
+        const int pitch = T::BF16 ? ((wd + 7) & ~7) : ((wd + 3) & ~3);   // elements per row
         const int md = (int)(S.rowptr[pr.d + 1] - S.rowptr[pr.d]);
-        const float *base = mir + S.xk[pr.d];
+        const unsigned char *base = mir + 4 * S.xk[pr.d];
+        // element offset of each slot's source row (plane row * pitch), -1: zeros
+        int64_t goff[NSLOT];
+#pragma unroll
+        for (int o = 0; o < T::NOPS; ++o)
+#pragma unroll
+          for (int j = 0; j < JS; ++j) {
+            const bool isA = o < T::NOPS / 2;
+            const int R = 32 * pw + RPI * j + rsub, u = R & 7;
+            const int y = source_row(isA ? pr.rmask : pr.cmask, isA ? pr.a0 : pr.b0,
+                                     4 * (R >> 3) + (u & 3), operand_plane<V>(o, u >> 2), md);
+            goff[o * JS + j] = y >= 0 ? (int64_t)y * pitch : -1;
+          }
         const int k0 = pr.kk & 0xffff, kend = k0 + (pr.kk >> 16);
         for (int k = k0; k < kend; k += UT_KCHUNK) {
           if (!mbar_wait_warp(smem_u32(&empty_bar[stage]), phase ^ 1u, &abort_flag, S.status)) {
@@ -271,18 +347,13 @@ __global__ void __launch_bounds__(ut_threads(TMA), 1)
             break;
           }
           const uint32_t sa = sbase + stage * UT_STAGE_BYTES;
-          const int kk = k + 4 * c;
-          const int bytes = kend - kk >= 4 ? 16 : (kend > kk ? 4 * (kend - kk) : 0);
-#pragma unroll 4
-          for (int j = 0; j < 8; ++j) {
-            const int R = 32 * pw + 4 * j + (lane >> 3);
-            const int a = R >> 3, u = R & 7, p = u >> 2, i = 4 * a + (u & 3);
-            const uint32_t off = (uint32_t)(a * 1024 + u * 128 + ((c ^ u) << 4));
-            const int ya = gather_row(pr.rmask, pr.a0, i, p, md);
-            const int yb = gather_row(pr.cmask, pr.b0, i, p, md);
-            const bool va = ya < 2 * md && bytes > 0, vb = yb < 2 * md && bytes > 0;
-            cp_async16(sa + off, va ? base + (size_t)ya * wp + kk : base, va ? bytes : 0);
-            cp_async16(sa + UT_OPB + off, vb ? base + (size_t)yb * wp + kk : base, vb ? bytes : 0);
+          const int kk = k + cc * (16 / T::ELEM);
+          const int left = (kend - kk) * T::ELEM;
+          const int bytes = left >= 16 ? 16 : (left > 0 ? left : 0);
+#pragma unroll
+          for (int e = 0; e < NSLOT; ++e) {
+            const bool v = goff[e] >= 0;
+            cp_async16(sa + soff[e], base + (v ? goff[e] + kk : 0) * T::ELEM, v ? bytes : 0);
           }
           asm volatile("cp.async.commit_group;\n" ::: "memory");
           if (pend[1] >= 0) {   // the chunk issued two chunks ago has landed: hand it over
@@ -301,10 +372,11 @@ __global__ void __launch_bounds__(ut_threads(TMA), 1)
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncwarp();
-    if (lane == 0)
-      for (int k = 1; k >= 0; --k)
-        if (pend[k] >= 0) mbar_arrive(smem_u32(&full_bar[pend[k]]));
-  } else if (TMA && warp == 4) {
+    if (lane == 0) {
+      if (pend[1] >= 0) mbar_arrive(smem_u32(&full_bar[pend[1]]));
+      if (pend[0] >= 0) mbar_arrive(smem_u32(&full_bar[pend[0]]));
+    }
+  } else if (V == V_TF32_TMA && warp == 4) {
     // --------------------------- producer (TMA) ---------------------------
     int stage = 0;
     uint32_t phase = 0;
@@ -321,9 +393,11 @@ __global__ void __launch_bounds__(ut_threads(TMA), 1)
         const CUtensorMap *map = maps + pr.d;
         int ya[4], yb[4];
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          ya[r] = gather_row(pr.rmask, pr.a0, 4 * a + r, p, md);
-          yb[r] = gather_row(pr.cmask, pr.b0, 4 * a + r, p, md);
+        for (int r = 0; r < 4; ++r) {   // a row outside the map (2 md) reads zeros
+          ya[r] = source_row(pr.rmask, pr.a0, 4 * a + r, p, md);
+          yb[r] = source_row(pr.cmask, pr.b0, 4 * a + r, p, md);
+          if (ya[r] < 0) ya[r] = 2 * md;
+          if (yb[r] < 0) yb[r] = 2 * md;
         }
         const int k0 = pr.kk & 0xffff, kend = k0 + (pr.kk >> 16);
         for (int k = k0; k < kend; k += UT_KCHUNK) {
@@ -335,9 +409,9 @@ __global__ void __launch_bounds__(ut_threads(TMA), 1)
           if (lane == 0) mbar_arrive_tx(fb, UT_STAGE_BYTES);
           armed[stage] += 1;
           __syncwarp();
-          const uint32_t dst = sbase + stage * UT_STAGE_BYTES + a * 1024 + p * 512;
+          const uint32_t dst = sbase + stage * UT_STAGE_BYTES + a * T::ATOM + p * (T::ATOM / 2);
           tma_gather4(dst, map, fb, k, ya[0], ya[1], ya[2], ya[3]);
-          tma_gather4(dst + UT_OPB, map, fb, k, yb[0], yb[1], yb[2], yb[3]);
+          tma_gather4(dst + T::OPB, map, fb, k, yb[0], yb[1], yb[2], yb[3]);
           if (++stage == UT_STAGES) { stage = 0; phase ^= 1u; }
         }
       }
@@ -358,25 +432,39 @@ __global__ void __launch_bounds__(ut_threads(TMA), 1)
         for (int q = tasks[t].w; q < p_end && ok; ++q) {
           const int nch = pair_chunks(pairs[q]);
           const bool open = gchunks == 0;
-          if (open) {   // the epilogue has drained this accumulator
+          if (open) {   // the epilogue has drained this accumulator set
             if (!mbar_wait(smem_u32(&acce_bar[buf]), accphase[buf] ^ 1u, &abort_flag, S.status)) {
               ok = false;
               break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
           }
-          const uint32_t dt = tmem + (uint32_t)buf * 128u;
+          const uint32_t dt = tmem + (uint32_t)buf * (T::TMEM_COLS / 2);
           for (int c = 0; c < nch; ++c) {
             if (!mbar_wait(smem_u32(&full_bar[stage]), phase, &abort_flag, S.status)) {
               ok = false;
               break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-            const uint32_t sa = sbase + stage * UT_STAGE_BYTES, sb = sa + UT_OPB;
+            const uint32_t sa = sbase + stage * UT_STAGE_BYTES;
+            if (T::BF16) {
+              // 16 columns of K per MMA: D1 += A1 B1^T, D2 += A2 B2^T
 #pragma unroll
-            for (int kk = 0; kk < UT_KCHUNK / 8; ++kk)
-              mma_tf32(dt, sw128_desc(sa + 32 * kk), sw128_desc(sb + 32 * kk),
-                       (open && c == 0 && kk == 0) ? 0u : 1u);
+              for (int kk = 0; kk < UT_KCHUNK / 16; ++kk) {
+                const uint32_t acc = (open && c == 0 && kk == 0) ? 0u : 1u;
+                mma_issue<V>(dt, sw_desc(sa + 32 * kk, T::ATOM, T::LAYOUT),
+                             sw_desc(sa + 2 * T::OPB + 32 * kk, T::ATOM, T::LAYOUT), acc);
+                mma_issue<V>(dt + 128, sw_desc(sa + T::OPB + 32 * kk, T::ATOM, T::LAYOUT),
+                             sw_desc(sa + 3 * T::OPB + 32 * kk, T::ATOM, T::LAYOUT), acc);
+              }
+            } else {
+              // 8 columns of K per MMA: D += A' B'^T
+#pragma unroll
+              for (int kk = 0; kk < UT_KCHUNK / 8; ++kk)
+                mma_issue<V>(dt, sw_desc(sa + 32 * kk, T::ATOM, T::LAYOUT),
+                             sw_desc(sa + T::OPB + 32 * kk, T::ATOM, T::LAYOUT),
+                             (open && c == 0 && kk == 0) ? 0u : 1u);
+            }
             mma_commit(smem_u32(&empty_bar[stage]));   // stage free once these MMAs are done
             if (++stage == UT_STAGES) { stage = 0; phase ^= 1u; }
           }
@@ -395,9 +483,10 @@ __global__ void __launch_bounds__(ut_threads(TMA), 1)
       mbar_drain(smem_u32(&done_bar), 0u, S.status);
     }
     __syncwarp();
-  } else {
+  } else if (warp < 4) {
     // ------------------------------ epilogue ------------------------------
-    // thread tid owns TMEM lane tid: row' tid = atom a, piece p, tile row i = 4a + r
+    // thread tid owns TMEM lane tid: row' tid = atom a, piece slot p, tile row i = 4a + r;
+    // lanes tid and tid ^ 4 hold the two slots of the same tile row
     const int a = tid >> 3, p = (tid >> 2) & 1, i = 4 * a + (tid & 3);
     int buf = 0;
     uint32_t accphase[2] = {0, 0};
@@ -431,18 +520,22 @@ __global__ void __launch_bounds__(ut_threads(TMA), 1)
         }
         accphase[buf] ^= 1u;
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-        const uint32_t ta = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)buf * 128u;
+        const uint32_t ta = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)buf * (T::TMEM_COLS / 2);
 #pragma unroll
         for (int cc = 0; cc < 4; ++cc) {
-          float v[32];
+          float v[32], v2[32];
           tmem_ld32(ta + 32u * cc, v);
+          if (T::BF16) tmem_ld32(ta + 128u + 32u * cc, v2);
 #pragma unroll
           for (int bb = 0; bb < 4; ++bb) {
             float f[4];
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
-              f[c] = v[8 * bb + c] + v[8 * bb + 4 + c];          // hi' + lo' of column 4b + c
-              f[c] += __shfl_xor_sync(0xffffffffu, f[c], 4);   // + the other piece of row i
+              // column 4b + c: both pieces of the column from D (D1) ...
+              f[c] = v[8 * bb + c] + v[8 * bb + 4 + c];
+              // ... and, for BF16x3, D2's lo hi' (slot 0 rows, slot 1 columns) or hi lo'
+              if (T::BF16) f[c] += p == 0 ? v2[8 * bb + 4 + c] : v2[8 * bb + c];
+              f[c] += __shfl_xor_sync(0xffffffffu, f[c], 4);   // + the other slot of row i
             }
             const int b = 4 * cc + bb;
             acc[b][0] += (double)(p ? f[2] : f[0]);
@@ -469,7 +562,7 @@ __global__ void __launch_bounds__(ut_threads(TMA), 1)
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
-                 "r"(UT_TMEM_COLS));
+                 "r"(T::TMEM_COLS));
 }
 
 using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
@@ -490,13 +583,23 @@ EncodeTiled encode_fn() {
   return fn;
 }
 
+template <int V>
+void launch_variant(const DevSym &S, const void *maps, const int4 *tasks, const int *task_end,
+                    const TcPair *pairs, int count, cudaStream_t st) {
+  k_update_tc<V><<<update_tc_ctas(count), Ut<V>::THREADS, UT_SMEM, st>>>(
+      S, static_cast<const CUtensorMap *>(maps), tasks, task_end, pairs, count);
+}
+
 }  // namespace
 
 bool update_tc_configure(std::string &err) {
-  cudaError_t e = cudaFuncSetAttribute(k_update_tc<true>,
+  cudaError_t e = cudaFuncSetAttribute(k_update_tc<V_TF32>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, UT_SMEM);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_update_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(k_update_tc<V_TF32_TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             UT_SMEM);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_update_tc<V_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              UT_SMEM);
   if (e != cudaSuccess) {
     err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e);
@@ -508,13 +611,17 @@ bool update_tc_configure(std::string &err) {
 int64_t kmirror_layout(const std::vector<int> &super, const std::vector<int64_t> &rowptr,
                        std::vector<int64_t> &xk) {
   const int ns = (int)super.size() - 1;
-  xk.resize(ns);
+  xk.resize(ns + 1);
   int64_t off = 0;
   for (int d = 0; d < ns; ++d) {
     const int64_t w = super[d + 1] - super[d], m = rowptr[d + 1] - rowptr[d];
+    // floats: two TF32 planes of rows of w rounded up to 4, or three BF16 planes of rows of
+    // w rounded up to 8; the larger, rounded up to 32 bytes
+    const int64_t tf32 = 2 * m * ((w + 3) & ~3LL), bf16 = (3 * m * ((w + 7) & ~7LL) + 1) / 2;
     xk[d] = off;
-    off += 2 * m * ((w + 3) & ~3LL);
+    off += ((tf32 > bf16 ? tf32 : bf16) + 7) & ~7LL;
   }
+  xk[ns] = 0;   // the format entry, set per mode
   return off;
 }
 
@@ -557,14 +664,14 @@ int update_tc_ctas(int count) {
 }
 
 void launch_update_tc(const DevSym &S, const void *maps, const int4 *tasks, const int *task_end,
-                      const TcPair *pairs, int count, bool tma, cudaStream_t st) {
+                      const TcPair *pairs, int count, int variant, cudaStream_t st) {
   if (count <= 0) return;
-  if (tma)
-    k_update_tc<true><<<update_tc_ctas(count), ut_threads(true), UT_SMEM, st>>>(
-        S, static_cast<const CUtensorMap *>(maps), tasks, task_end, pairs, count);
+  if (variant == UT_VARIANT_BF16)
+    launch_variant<V_BF16>(S, maps, tasks, task_end, pairs, count, st);
+  else if (variant == UT_VARIANT_TF32_TMA)
+    launch_variant<V_TF32_TMA>(S, maps, tasks, task_end, pairs, count, st);
   else
-    k_update_tc<false><<<update_tc_ctas(count), ut_threads(false), UT_SMEM, st>>>(
-        S, static_cast<const CUtensorMap *>(maps), tasks, task_end, pairs, count);
+    launch_variant<V_TF32>(S, maps, tasks, task_end, pairs, count, st);
 }
 
 }  // namespace swc
