@@ -280,8 +280,10 @@ bool BatchState::autotune(Engine &eng, const double *d_values, int mixed, const 
     ok = measure(p, 0, ms);
     if (ok && ms < best) { best = ms; bp = p; bl = 0; }
   }
-  // stage 2: plan, best partition
+  // stage 2: plan, best partition (only the plans that change something in this mode:
+  // 5 applies to both mixed modes, 6 to the split-TF32 mode)
   for (int k = 1; k < kNumPlans && ok; ++k) {
+    if ((k == 5 && mode == 0) || (k == 6 && mode != 1)) continue;
     double ms;
     ok = measure(bp, k, ms);
     if (ok && ms < best) { best = ms; bl = k; }

@@ -36,10 +36,10 @@
 //
 // Staging (per K chunk, 32 KB):
 //   cp.async  four producer warps copy 16 bytes per lane, a warp instruction covering 512
-//             contiguous shared-memory bytes (four 128-byte or eight 64-byte rows: no bank
-//             conflicts) and 128- or 64-byte runs of global memory; a chunk is handed to the
-//             MMA warp two chunks later (cp.async.wait_group 2, proxy fence, mbarrier
-//             arrival of each producer warp);
+//             contiguous shared-memory bytes (four 128-byte or eight 64-byte rows) and 128-
+//             or 64-byte runs of global memory; each thread's copies arrive on the stage's
+//             mbarrier when they land (cp.async.mbarrier.arrive.noinc), and the MMA thread
+//             fences the async proxy after its wait;
 //   TMA       (split-TF32, plan 6) one producer warp issues 64 cp.async.bulk.tensor.2d ...
 //             tile::gather4 loads (four rows of 32 values each, into one half of a swizzle
 //             atom) from one 2D tensor map per supernode ({wd, 2 md}, 128-byte swizzle, zero
@@ -194,6 +194,12 @@ __device__ __forceinline__ void tma_gather4(uint32_t dst, const CUtensorMap *map
       : "memory");
 }
 
+// Arrival on the mbarrier once every cp.async this thread issued so far has landed (the
+// barrier's count includes this arrival: no increment).
+__device__ __forceinline__ void cp_async_arrive(uint32_t bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(bar) : "memory");
+}
+
 // 16-byte copy global -> shared with zero fill beyond `bytes` (0..16) of the source.
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, int bytes) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(bytes)
@@ -280,7 +286,8 @@ __global__ void __launch_bounds__(Ut<V>::THREADS, 1)
   }
   if (tid == 32 * MMA_WARP) {
     for (int s = 0; s < UT_STAGES; ++s) {
-      mbar_init(smem_u32(&full_bar[s]), T::NPROD);
+      // cp.async staging: one hardware arrival per producer thread; TMA: the arming thread
+      mbar_init(smem_u32(&full_bar[s]), V == V_TF32_TMA ? 1 : 32 * T::NPROD);
       mbar_init(smem_u32(&empty_bar[s]), 1);
     }
     for (int b = 0; b < 2; ++b) {
@@ -302,8 +309,9 @@ __global__ void __launch_bounds__(Ut<V>::THREADS, 1)
     // RPI rows' of T::ROW bytes (lane: row' RPI j + lane / CPR, 16-byte column chunk
     // lane % CPR), written where the swizzled K-major layout puts them.  The lane's NSLOT
     // shared-memory slots are fixed for the kernel and its source rows for a pair, so a
-    // chunk costs one add and one copy per slot.  A chunk completes two chunks later
-    // (wait_group 2), then proxy fence and the warp's arrival on the stage.
+    // chunk costs one add and one copy per slot.  Each thread's copies arrive on the stage's
+    // mbarrier when they land (cp.async.mbarrier.arrive.noinc), so up to UT_STAGES chunks
+    // are in flight.
     constexpr int CPR = T::ROW / 16, RPI = 32 / CPR, JS = 32 / RPI, NSLOT = T::NOPS * JS;
     const int pw = warp - 4, cc = lane % CPR, rsub = lane / CPR;
     uint32_t soff[NSLOT];   // shared-memory offset of each slot within a stage
@@ -317,7 +325,6 @@ __global__ void __launch_bounds__(Ut<V>::THREADS, 1)
       }
     int stage = 0;
     uint32_t phase = 0;
-    int pend[2] = {-1, -1};   // stages issued one and two chunks ago
     bool ok = true;
     const unsigned char *mir = reinterpret_cast<const unsigned char *>(S.Lf);
     for (int t = blockIdx.x; t < count && ok; t += gridDim.x) {
@@ -355,27 +362,13 @@ __global__ void __launch_bounds__(Ut<V>::THREADS, 1)
             const bool v = goff[e] >= 0;
             cp_async16(sa + soff[e], base + (v ? goff[e] + kk : 0) * T::ELEM, v ? bytes : 0);
           }
-          asm volatile("cp.async.commit_group;\n" ::: "memory");
-          if (pend[1] >= 0) {   // the chunk issued two chunks ago has landed: hand it over
-            asm volatile("cp.async.wait_group 2;\n" ::: "memory");
-            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-            __syncwarp();
-            if (lane == 0) mbar_arrive(smem_u32(&full_bar[pend[1]]));
-          }
-          pend[1] = pend[0];
-          pend[0] = stage;
+          cp_async_arrive(smem_u32(&full_bar[stage]));
           if (++stage == UT_STAGES) { stage = 0; phase ^= 1u; }
         }
       }
     }
-    // the last chunks (and, after an abort, every copy in flight) land before leaving
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-    __syncwarp();
-    if (lane == 0) {
-      if (pend[1] >= 0) mbar_arrive(smem_u32(&full_bar[pend[1]]));
-      if (pend[0] >= 0) mbar_arrive(smem_u32(&full_bar[pend[0]]));
-    }
+    // every copy in flight lands before the CTA leaves
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
   } else if (V == V_TF32_TMA && warp == 4) {
     // --------------------------- producer (TMA) ---------------------------
     int stage = 0;
@@ -445,6 +438,9 @@ __global__ void __launch_bounds__(Ut<V>::THREADS, 1)
               ok = false;
               break;
             }
+            // the stage's bytes (written by cp.async in the generic proxy, or by TMA) are
+            // read by the MMAs through the async proxy
+            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
             const uint32_t sa = sbase + stage * UT_STAGE_BYTES;
             if (T::BF16) {
