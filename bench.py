@@ -390,15 +390,16 @@ def run_ours(args, rank, world, local_rank):
     peak64 = fp64_gemm_peak(torch, dev) if rank == 0 else None
     bf16 = mode == swc.SWC_MODE_MIXED_BF16X3
     peak32 = tf32_gemm_peak(torch, dev, bf16) if rank == 0 and mixed else None
-    if mixed and dom in ("update", "syrk"):
+    # the trailing SYRK steps run in FP64 (DMMA) in every mode by default
+    if mixed and dom == "update":
         if bf16:
             peak, psrc = peak32 / 8.0, ("cuBLAS BF16 GEMM 8192^3 measured in this run, divided by 8 "
                                         "(a BF16x3 product executes eight BF16 piece products on "
                                         "tcgen05: [hi;mid][hi;mid]^T and [lo;hi][lo;hi]^T)")
         else:
-            peak, psrc = peak32 / 4.0, ("cuBLAS TF32 GEMM 8192^3 measured in this run, divided by 4 "
-                                        "(a split-TF32 product executes four TF32 piece products on "
-                                        "tcgen05: [hi;lo][hi;lo]^T)")
+            peak, psrc = peak32 / 3.0, ("cuBLAS TF32 GEMM 8192^3 measured in this run, divided by 3 "
+                                        "(a split-TF32 product executes three TF32 piece products "
+                                        "on tcgen05: hi hi' + lo hi' + hi lo')")
     else:
         peak, psrc = peak64, "FP64 cuBLAS DGEMM 8192^3 measured in this run"
     hbm, hbm_src = hbm_peak()
@@ -487,12 +488,13 @@ def run_ours(args, rank, world, local_rank):
 
     if rank == 0:
         achieved = kfl / (kms * 1e-3) / 1e12
-        kname = {"update": "k_update_tc" if mixed else "k_update_tiles",
-                 "syrk": "k_update_tc" if mixed else "k_syrk_step"}.get(dom)
+        kname = {"update": ("k_update_tc" if bf16 else "k_scatter_tc") if mixed
+                 else "k_update_tiles", "syrk": "k_syrk_step"}.get(dom)
         traffic = profile_traffic(kname, args.workload) if kname else None
         tsrc = (f"dram__bytes_read.sum + dram__bytes_write.sum per launch, ncu capture summarised "
                 f"in profiles/{kname}_{args.workload}.md" if traffic else None)
-        per_step = h.launches + (last.get("iters", 0) + 1) * (solve_launches + 5)
+        factor_launches = int(sum(v[0] for v in prof.values()))   # this mode's launch list
+        per_step = factor_launches + (last.get("iters", 0) + 1) * (solve_launches + 5)
         executed = float(sum(v[2] for k, v in prof.items()))
         gs = dict(np.load(os.path.join(GOLDEN, f"sym_{args.workload}.npz")))
         nnzl = int(gs["nnzl"]) if "nnzl" in gs else None

@@ -154,7 +154,8 @@ void Engine::release() {
                   d_csr_map_,
                   d_csr_val_, d_contrib_, d_work_, d_norms_, d_persist_, d_qctr_, d_npart_,
                   d_tiny_, d_dense_tasks_, d_dense_toff_, d_dense_ver_, d_swarp_,
-                  d_Lk_, d_xk_, d_xk16_, d_tmaps_, d_tc_pairs_, d_syrk_pairs_, d_syrk_end_};
+                  d_Lk_, d_xk_, d_xk16_, d_tmaps_, d_tc_pairs_, d_syrk_pairs_, d_syrk_end_,
+                  d_sc_tiles_, d_sc_base_, d_sc_coff_, d_sc_rel_, d_sc_relidx_, d_sc_maps_};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   release_adjoint();
@@ -185,6 +186,10 @@ void Engine::release() {
   d_tmaps_ = nullptr;
   d_tc_pairs_ = d_syrk_pairs_ = nullptr;
   d_syrk_end_ = nullptr;
+  d_sc_tiles_ = nullptr;
+  d_sc_base_ = d_sc_coff_ = nullptr;
+  d_sc_rel_ = d_sc_relidx_ = nullptr;
+  d_sc_maps_ = nullptr;
   kmirror_len_ = 0;
   tiny_ctas_ = 0;
   d_npart_ = nullptr;
@@ -543,6 +548,86 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
   if (!P.tiny_list.empty()) launches += 1;
   P.launches = launches;
 
+  // ---- right-looking updates of the split-TF32 mode: the contribution of every descendant
+  // d to tiled-class targets, C = B B^T over the rows of d from the first one whose column
+  // belongs to a tiled supernode, as 128x128 tiles of one dense product, launched in the
+  // level after d's own (every target sits on a later level) ----
+  if (T.scatter && !P.big_list.empty()) {
+    std::vector<char> tiled(supNo, 0);
+    for (int s : P.big_list) tiled[s] = 1;
+    std::vector<std::vector<int4>> by_wave(nlev);
+    P.sc_coff.assign(supNo, 0);
+    P.sc_used.assign(supNo, 0);
+    for (int d = 0; d < supNo; ++d) {
+      const int wd = super[d + 1] - super[d];
+      const int md = (int)(rowptr[d + 1] - rowptr[d]);
+      const int *rd = Ls + rowptr[d];
+      int c0 = wd;
+      while (c0 < md && !tiled[col2sup[rd[c0]]]) ++c0;
+      if (c0 == md) continue;
+      P.sc_coff[d] = (int64_t)P.sc_base.size() - c0;
+      for (int j = c0; j < md;) {
+        const int s = col2sup[rd[j]];
+        int je = j;
+        while (je < md && col2sup[rd[je]] == s) ++je;
+        if (!tiled[s]) {
+          P.sc_base.insert(P.sc_base.end(), (size_t)(je - j), (int64_t)-1);
+          P.sc_rel.insert(P.sc_rel.end(), (size_t)(je - j), 0);
+        } else {
+          // positions of rows j.. of d in the row list of s (contained in it: s is an
+          // ancestor of d)
+          const int *rs = Ls + rowptr[s];
+          const int ms = (int)(rowptr[s + 1] - rowptr[s]);
+          const int64_t rbase = (int64_t)P.sc_relidx.size() - j;
+          if ((int64_t)P.sc_relidx.size() + (md - j) > INT32_MAX) {
+            err = "relative indices of the right-looking updates exceed 2^31 entries";
+            return false;
+          }
+          int k = (int)(std::lower_bound(rs, rs + ms, rd[j]) - rs);
+          for (int i = j; i < md; ++i) {
+            while (k < ms && rs[k] < rd[i]) ++k;
+            if (k == ms || rs[k] != rd[i]) {
+              err = "row structure of a descendant is not contained in its ancestor's";
+              return false;
+            }
+            P.sc_relidx.push_back(k);
+          }
+          for (int q = j; q < je; ++q) {
+            P.sc_base.push_back(xptr[s] + (int64_t)(rd[q] - super[s]) * ms);
+            P.sc_rel.push_back((int)rbase);
+          }
+        }
+        j = je;
+      }
+      const int nk = (wd + 31) / 32;
+      for (int i0 = c0; i0 < md; i0 += 128)
+        for (int j0 = c0; j0 <= i0; j0 += 128) {
+          by_wave[level[d] + 1].push_back(make_int4(d, i0, j0, nk));
+          P.sc_flops += 2.0 * 128 * 128 * wd;
+        }
+      P.sc_used[d] = 1;
+    }
+    // per level: larger K first (a shorter tail); one descendant's tiles stay together
+    int sc_launches = 0;
+    for (int lv = 0; lv < nlev; ++lv) {
+      std::vector<int4> &v = by_wave[lv];
+      std::stable_sort(v.begin(), v.end(), [](const int4 &a, const int4 &b) { return a.w > b.w; });
+      P.waves[lv].sc_off = (int)P.sc_tiles.size();
+      P.waves[lv].sc_cnt = (int)v.size();
+      P.sc_tiles.insert(P.sc_tiles.end(), v.begin(), v.end());
+      sc_launches += !v.empty();
+    }
+    // one assemble launch up front instead of one per level; scatter instead of tile-owner
+    int asm_l = 0, upd_l = 0;
+    for (const Wave &W : P.waves) {
+      asm_l += W.asm_cnt > 0;
+      upd_l += W.upd_cnt > 0;
+    }
+    P.launches_scatter = launches - asm_l - upd_l + (asm_l > 0) + sc_launches;
+  } else {
+    P.launches_scatter = launches;
+  }
+
   // ---- algorithmic work per kernel class (one factorization) ----
   {
     KernelStats &K = P.work;
@@ -625,7 +710,8 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
                      const int64_t *Li_ptr, const int *blockSet, int supNo,
                      const int *prunePtr, const int *pruneSet, std::string &err) {
   cudaSetDevice(device_);
-  if (!kernels_configure(err) || !update_tc_configure(err)) return false;
+  if (!kernels_configure(err) || !update_tc_configure(err) || !scatter_tc_configure(err))
+    return false;
   HostSym H;
   Plan P;
   if (!build_plan(n, c, r, lC, Ls, Li_ptr, blockSet, supNo, prunePtr, pruneSet, H, P, err,
@@ -769,6 +855,11 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
             upload(d_syrk_pairs_, P.syrk_pairs.data(), P.syrk_pairs.size(), st, err) &&
             upload(d_syrk_end_, P.syrk_end.data(), P.syrk_end.size(), st, err) &&
             upload(d_tc_pairs_, P.tc_pairs.data(), P.tc_pairs.size(), st, err) &&
+            upload(d_sc_tiles_, P.sc_tiles.data(), P.sc_tiles.size(), st, err) &&
+            upload(d_sc_base_, P.sc_base.data(), P.sc_base.size(), st, err) &&
+            upload(d_sc_coff_, P.sc_coff.data(), P.sc_coff.size(), st, err) &&
+            upload(d_sc_rel_, P.sc_rel.data(), P.sc_rel.size(), st, err) &&
+            upload(d_sc_relidx_, P.sc_relidx.data(), P.sc_relidx.size(), st, err) &&
             upload(d_dense_tasks_, P.dense_tasks.data(), P.dense_tasks.size(), st, err) &&
             upload(d_dense_toff_, P.dense_toff.data(), P.dense_toff.size(), st, err) &&
             upload(d_dinv_off_, H.dinv_off.data(), H.dinv_off.size(), st, err) &&
@@ -854,7 +945,7 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec
   auto syrk = [&](const int4 *tasks, int count, int) {
     if (syrk_tc)
       launch_update_tc(sym_, d_tmaps_, tasks, d_syrk_end_ + (tasks - d_syrk_), d_syrk_pairs_,
-                       count, variant, st);
+                       count, variant, true, st);
     else
       launch_syrk_step(sym_, tasks, d_syrk_pairs_, count, st);
   };
@@ -866,10 +957,19 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec
     cudaEventRecord(ev, st);
     prof->emplace_back(kind, ev);
   };
+  // split-TF32 mode with right-looking updates: contributions reach a target from the level
+  // after each descendant's, so every tiled panel is assembled up front
+  const bool scatter = prec == 1 && !plan_.sc_coff.empty();
+  const ScatterCols sc_cols{d_sc_base_, d_sc_rel_, d_sc_coff_, d_sc_relidx_};
   mark(K_MEMSET, 1);
   cudaMemsetAsync(dL_, 0, sizeof(double) * xsize_, st);
   launch_init_status(d_status_, st);
   mark(-1, 1);
+  if (scatter && !plan_.asm_tasks.empty()) {
+    mark(K_ASSEMBLE, 1);
+    launch_assemble(sym_, d_asm_, (int)plan_.asm_tasks.size(), st);
+    mark(-1, 1);
+  }
   if (!plan_.tiny_list.empty() || !plan_.persist_list.empty())
     cudaMemsetAsync(d_qctr_, 0, sizeof(int) * (nsuper_ + 2), st);
   if (d_dense_ver_) cudaMemsetAsync(d_dense_ver_, 0, sizeof(int) * dense_ver_len_, st);
@@ -890,17 +990,23 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec
     mark(K_SMALL, W.small_cnt);
     launch_factor_small(sym_, d_upd_lbub_, d_small_ + W.small_off, W.small_cnt, W.small_smem, st);
     mark(-1, W.small_cnt);
+    if (scatter) {
+      mark(K_UPDATE, W.sc_cnt);
+      launch_scatter_tc(sym_, d_sc_maps_, d_sc_tiles_ + W.sc_off, W.sc_cnt, sc_cols, st);
+      mark(-1, W.sc_cnt);
+    } else {
     mark(K_ASSEMBLE, W.asm_cnt);
     launch_assemble(sym_, d_asm_ + W.asm_off, W.asm_cnt, st);
     mark(-1, W.asm_cnt);
     mark(K_UPDATE, W.upd_cnt);
     if (prec != 0)
       launch_update_tc(sym_, d_tmaps_, d_upd_tasks_ + W.upd_off, d_upd_end_ + W.upd_off,
-                       d_tc_pairs_, W.upd_cnt, variant, st);
+                       d_tc_pairs_, W.upd_cnt, variant, false, st);
     else
       launch_update_tiles(sym_, d_upd_tasks_ + W.upd_off, d_upd_end_ + W.upd_off, d_pairs_,
                           W.upd_cnt, st);
     mark(-1, W.upd_cnt);
+    }
     if (W.dense_cnt > 0) {
       // the whole dense factorization of the wave in one dataflow launch
       mark(K_PANEL, 1);
@@ -957,6 +1063,18 @@ bool Engine::set_mode(int prec, std::string &err) {
       return false;
     }
     if (!build_tensor_maps(hsym_.super, hsym_.rowptr, h_xk_, d_Lk_, maps.data(), err)) return false;
+    if (!plan_.sc_coff.empty()) {   // hi / lo plane maps of the right-looking update tiles
+      std::vector<unsigned char> sm(2 * mb, 0);
+      if (!build_scatter_maps(hsym_.super, hsym_.rowptr, h_xk_, plan_.sc_used, d_Lk_, sm.data(),
+                              err))
+        return false;
+      e = cudaMalloc(&d_sc_maps_, sm.size());
+      if (e == cudaSuccess) e = cudaMemcpy(d_sc_maps_, sm.data(), sm.size(), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) {
+        err = std::string("scatter tensor maps: ") + cudaGetErrorString(e);
+        return false;
+      }
+    }
     e = cudaMemcpy(d_xk_, h_xk_.data(), sizeof(int64_t) * nx, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(d_xk16_, xk16.data(), sizeof(int64_t) * nx, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(d_tmaps_, maps.data(), mb, cudaMemcpyHostToDevice);

@@ -31,9 +31,9 @@ struct DevSym {
                           // [4] = poll budget of every bounded wait (set by the host)
   float2 *Lf;             // split mirror of L in K-major form (mixed-precision modes only,
                           // else null): supernode s at (float *)Lf + xk[s]
-  const int64_t *xk;      // per supernode: offset of its mirror; xk[nsuper]: the format, 0
-                          // hi / lo TF32 planes (rows of w rounded up to 4 floats), 1 hi / mid
-                          // / lo bfloat16 planes (rows of w rounded up to 8 values)
+  const int64_t *xk;      // per supernode: offset (floats) of its mirror; xk[nsuper]: the
+                          // format, 0 hi / lo TF32 planes, 1 hi / mid / lo bfloat16 planes
+                          // (rows of kmirror_pitch_tf32 / _bf16 elements)
   double *dinv;           // scratch: inverses of the 64x64 diagonal blocks of the tiled class
   const int *dinv_off;    // per supernode: first block of its inverses in dinv (-1: none)
 };
@@ -47,7 +47,11 @@ __device__ __forceinline__ long long wait_budget(const int *status) {
   return (long long)*(volatile const int *)&status[4];
 }
 
-// BF16x3 mirror entry bits: x = hi | mid << 16, y = lo (bfloat16 pieces).
+// Row pitch (elements) of a supernode of width w in the K-major split mirror: rows start on
+// 128-byte boundaries, so every 32-column K chunk of a row is one aligned 128-byte (TF32) or
+// 64-byte (bfloat16) run.
+__host__ __device__ __forceinline__ int kmirror_pitch_tf32(int w) { return (w + 31) & ~31; }
+__host__ __device__ __forceinline__ int kmirror_pitch_bf16(int w) { return (w + 63) & ~63; }
 
 // One (64x64 tile, descendant) product of the tcgen05 update kernel: rows a0.. of
 // supernode d feed the tile rows set in rmask (in order), rows b0.. the tile columns set in
@@ -69,6 +73,8 @@ struct Wave {
   std::vector<int> diag_off, diag_cnt;    // per step j: supernodes whose block j+1 exists
   int dense_off = 0, dense_cnt = 0;       // dataflow tasks of the dense factorization
   int dense_ctas = 0;
+  int sc_off = 0, sc_cnt = 0;   // right-looking update tiles of the descendants of the level
+                                // before (split-TF32 mode)
 };
 
 // Kernel classes, for per-kernel timing (profiled factorization) and flop accounting.
@@ -100,8 +106,16 @@ struct Plan {
   std::vector<int4> dense_tasks;   // (s, r0, c0, step << 2 | kind), per wave in topological order
   std::vector<int> dense_toff;     // per supernode: first tile version counter (-1: none)
   int64_t dense_tiles = 0;         // tile version counters in total
+  // right-looking updates (split-TF32 mode): tiles, the column table and relative indices
+  // (ScatterCols), supernodes that own tiles
+  std::vector<int4> sc_tiles;
+  std::vector<int64_t> sc_base, sc_coff;
+  std::vector<int> sc_rel, sc_relidx;
+  std::vector<char> sc_used;
+  double sc_flops = 0;               // executed flops of the tiles (128x128 blocks)
   int persist_smem = 0;
   int launches = 0;  // kernel launches per factorization
+  int launches_scatter = 0;  // the same in the split-TF32 mode with right-looking updates
   KernelStats work;  // algorithmic flops/bytes per kernel class
 };
 
@@ -231,7 +245,10 @@ class Engine {
   int nsuper() const { return nsuper_; }
   const Plan &plan() const { return plan_; }
   double *device_L() const { return dL_; }
-  int launches_per_factor() const { return plan_.launches; }
+  // kernel launches of one factorization in the given mode
+  int launches_per_factor(int prec = 0) const {
+    return prec == 1 ? plan_.launches_scatter : plan_.launches;
+  }
 
   // Adjoint (swc_adjoint.cu), on the current factor; device pointers, grad has one entry
   // per stored nonzero of A.
@@ -298,6 +315,10 @@ class Engine {
   int64_t kmirror_len_ = 0;
   TcPair *d_tc_pairs_ = nullptr, *d_syrk_pairs_ = nullptr;
   int *d_syrk_end_ = nullptr;
+  int4 *d_sc_tiles_ = nullptr;                 // right-looking update tiles and their tables
+  int64_t *d_sc_base_ = nullptr, *d_sc_coff_ = nullptr;
+  int *d_sc_rel_ = nullptr, *d_sc_relidx_ = nullptr;
+  void *d_sc_maps_ = nullptr;                  // two tensor maps per supernode (over d_Lk_)
   bool use_graph_ = true;
   Tuning tuning_;
   int *d_persist_ = nullptr, *d_qctr_ = nullptr, *d_tiny_ = nullptr;
@@ -373,7 +394,29 @@ size_t tensor_map_bytes();
 // BF16x3 staged with cp.async
 constexpr int UT_VARIANT_TF32 = 0, UT_VARIANT_TF32_TMA = 1, UT_VARIANT_BF16 = 2;
 int update_tc_ctas(int count);   // CTAs of a launch over `count` tiles (at most one per SM)
+// shared_sm: the launch runs next to another kernel (the diagonal-block kernel of the dense
+// steps) and keeps shared memory for it
 void launch_update_tc(const DevSym &S, const void *maps, const int4 *tasks, const int *task_end,
-                      const TcPair *pairs, int count, int variant, cudaStream_t st);
+                      const TcPair *pairs, int count, int variant, bool shared_sm,
+                      cudaStream_t st);
+
+// Right-looking split-TF32 updates (swc_scatter_tc.cu).  Tiles (d, i0, j0, K chunks): the
+// 128x128 block of d's contribution whose rows start at row i0 and columns at row j0 of d's
+// row list.  Column table: entry coff[d] + j (row j of d, used as a column of C) holds the
+// first entry in L of the target column (-1: the target is not of the tiled class) and the
+// offset r such that relidx[r + i] is the position of d's row i in that target's row list.
+struct ScatterCols {
+  const int64_t *base;
+  const int *rel;
+  const int64_t *coff;
+  const int *relidx;
+};
+bool scatter_tc_configure(std::string &err);
+// two tensor maps per supernode d with used[d] (hi plane, lo plane; 128-row boxes)
+bool build_scatter_maps(const std::vector<int> &super, const std::vector<int64_t> &rowptr,
+                        const std::vector<int64_t> &xk, const std::vector<char> &used, float *Lk,
+                        void *maps_host, std::string &err);
+void launch_scatter_tc(const DevSym &S, const void *maps, const int4 *tiles, int count,
+                       const ScatterCols &C, cudaStream_t st);
 
 }  // namespace swc

@@ -71,18 +71,17 @@ __device__ __forceinline__ Bf16x3 split_bf16x3(double x) {
 
 // The mirror entries of value x of row r, column c of supernode s (m rows, w columns), in
 // the K-major split mirror at (float *)Lf + xk[s], format xk[nsuper]: 0, hi / lo TF32
-// planes of rows of w rounded up to 4 floats; 1, hi / mid / lo bfloat16 planes of rows of
-// w rounded up to 8 values.
+// planes; 1, hi / mid / lo bfloat16 planes (row pitch kmirror_pitch_tf32 / _bf16 (w)).
 __device__ __forceinline__ void store_mirror(const DevSym &S, int s, int m, int w, int r, int c,
                                              double x) {
   float *base = reinterpret_cast<float *>(S.Lf) + S.xk[s];
   if (S.xk[S.nsuper] == 0) {
-    const int wp = (w + 3) & ~3;
+    const int wp = kmirror_pitch_tf32(w);
     const float2 v = split_tf32(x);
     base[(size_t)r * wp + c] = v.x;
     base[((size_t)m + r) * wp + c] = v.y;
   } else {
-    const int wq = (w + 7) & ~7;
+    const int wq = kmirror_pitch_bf16(w);
     unsigned short *b = reinterpret_cast<unsigned short *>(base);
     const Bf16x3 v = split_bf16x3(x);
     b[(size_t)r * wq + c] = v.hi;
@@ -97,7 +96,7 @@ __device__ __forceinline__ void store_mirror_panel(const DevSym &S, int s, int m
                                                    const double *P, int t, int nt) {
   float *base = reinterpret_cast<float *>(S.Lf) + S.xk[s];
   if (S.xk[S.nsuper] == 0) {
-    const int wp = (w + 3) & ~3;
+    const int wp = kmirror_pitch_tf32(w);
     float *hi = base, *lo = hi + (size_t)m * wp;
     for (int e = t; e < m * w; e += nt) {
       const int r = e / w, c = e - r * w;
@@ -106,7 +105,7 @@ __device__ __forceinline__ void store_mirror_panel(const DevSym &S, int s, int m
       lo[(size_t)r * wp + c] = v.y;
     }
   } else {
-    const int wq = (w + 7) & ~7;
+    const int wq = kmirror_pitch_bf16(w);
     unsigned short *hi = reinterpret_cast<unsigned short *>(base);
     unsigned short *mid = hi + (size_t)m * wq, *lo = mid + (size_t)m * wq;
     for (int e = t; e < m * w; e += nt) {

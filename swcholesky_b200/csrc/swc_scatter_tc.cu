@@ -1,0 +1,432 @@
+// Right-looking split-TF32 Schur updates of the tiled class on the 5th-generation tensor
+// cores, scattered into the targets with FP64 atomic adds.
+//
+// The reference forms the update of every target supernode by every descendant d as a dense
+// SYRK/GEMM of d's rows below the target's first column into a contribution buffer, then
+// adds it to the target through relative indices (cholesky/sw_parallel_PB_Cholesky_05.c:
+// 299-378).  Here, in the split-TF32 mode, d's whole contribution is formed at once, as soon
+// as d is factored: C = B B^T with B the rows of d (below its own columns) whose column
+// index falls in a tiled-class supernode onwards, a dense product of 128x128 tiles over K =
+// the width of d, and each entry of the lower triangle of C is added to its target entry of
+// L (the supernode s owning C's column, at the target's row of C's row) by one FP64 atomic
+// add.  Operands are plain 2D tiles of d's K-major split mirror (no gather), so every tile
+// is a full 128x128x(width) product; the only padding is the diagonal tiles' upper halves and
+// the ragged last tiles.  Concurrent contributions to one target entry are summed by the
+// atomics in an unspecified order (results reproduce to rounding, not bit for bit); the FP64
+// mode keeps the deterministic tile-owner kernels.
+//
+// Split-TF32 products: x = hi + lo with hi = tf32(x) and lo = tf32(x - hi) (the mirror's two
+// planes); per 8 columns of K three kind::tf32 MMAs (M = N = 128) accumulate
+// hi hi' + lo hi' + hi lo' in one FP32 accumulator in TMEM (the lo lo' term, below 2^-22 of
+// the product, is dropped).
+//
+// Roles (192 threads, one CTA per SM, persistent over the launch's tile list, tile t handled
+// by CTA t mod gridDim.x):
+//   warps 0-3  epilogue: thread = TMEM lane = tile row; reads the 128 FP32 columns of its
+//              row, releases the accumulator, then adds minus each lower-triangle entry to L;
+//   warp 4     TMA producer (one thread): per 32-column K chunk, four 2D tiled loads (A hi,
+//              A lo, B hi, B lo; 128 rows x 128 bytes each, 128-byte swizzle) into a stage,
+//              two for a diagonal tile (B = A);
+//   warp 5     MMA issuer (one thread): twelve MMAs per stage into one of two accumulators,
+//              tcgen05.commit frees the stage and, after the tile's last chunk, hands the
+//              accumulator to the epilogue.
+// Every mbarrier wait is bounded (2 s of %globaltimer): a wait that runs out sets status[3]
+// and an abort flag that stops the other roles; the kernel then waits (bounded) for its loads
+// and MMAs in flight, frees its TMEM and returns.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "swc_engine.h"
+
+namespace swc {
+
+namespace {
+
+constexpr int SC_STAGES = 3;
+constexpr int SC_KCHUNK = 32;                 // K columns per stage
+constexpr int SC_OP = 128 * 128;              // bytes of one operand chunk (128 rows x 128 B)
+constexpr int SC_STAGE = 4 * SC_OP;           // A hi, A lo, B hi, B lo
+constexpr int SC_SMEM = SC_STAGES * SC_STAGE + 1024;   // + alignment slack
+constexpr int SC_THREADS = 192;
+constexpr int SC_TMEM_COLS = 256;             // two 128-column FP32 accumulators
+constexpr unsigned long long SC_WAIT_NS = 2000000000ULL;
+// D F32 (bit 4), A and B TF32 (2 at bits 7 and 10), K-major, N >> 3 at 17, M >> 4 at 24
+constexpr uint32_t SC_IDESC =
+    (1u << 4) | (2u << 7) | (2u << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// K-major operand with the 128-byte swizzle: 8-row groups 1024 bytes apart, version 1,
+// layout type 2.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n\t"
+      "selp.b32 %0, 1, 0, P1;\n\t}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity), "r"(20000)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+  return t;
+}
+// Bounded wait for the phase of the given parity; false when it ran out (recorded in
+// status[3] and the abort flag) or another role aborted.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort_flag,
+                                          int *status) {
+  if (mbar_try(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (long long it = 1;; ++it) {
+    if (mbar_try(bar, parity)) return true;
+    if ((it & 63) == 0) {
+      if (*abort_flag) return false;
+      if (global_ns() - t0 > SC_WAIT_NS) {
+        *abort_flag = 1;
+        atomicExch(&status[3], 1);
+        return false;
+      }
+    }
+  }
+}
+// Lane 0 waits for the warp (a warp-uniform result).
+__device__ __forceinline__ bool mbar_wait_warp(uint32_t bar, uint32_t parity,
+                                               volatile int *abort_flag, int *status) {
+  int ok = 1;
+  if ((threadIdx.x & 31) == 0) ok = mbar_wait(bar, parity, abort_flag, status);
+  ok = __shfl_sync(0xffffffffu, ok, 0);
+  __syncwarp();
+  return ok != 0;
+}
+// Bounded wait used while shutting down (ignores the abort flag).
+__device__ __forceinline__ void mbar_drain(uint32_t bar, uint32_t parity, int *status) {
+  const unsigned long long t0 = global_ns();
+  for (long long it = 0;; ++it) {
+    if (mbar_try(bar, parity)) return;
+    if ((it & 63) == 63 && global_ns() - t0 > SC_WAIT_NS) break;
+  }
+  atomicExch(&status[3], 1);
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, uint32_t bar,
+                                            int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];\n" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem, uint64_t adesc, uint64_t bdesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+          tmem),
+      "l"(adesc), "l"(bdesc), "r"(SC_IDESC), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar)
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t addr, float *v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(addr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+  for (int q = 0; q < 32; ++q) v[q] = __uint_as_float(r[q]);
+}
+
+// Barriers of the four epilogue warps: a plain one, and one that returns the AND of every
+// thread's flag (so all four warps take the same exit after a bounded wait).
+__device__ __forceinline__ void epi_bar() {
+  asm volatile("bar.sync 1, 128;\n" ::: "memory");
+}
+__device__ __forceinline__ bool epi_bar_and(bool ok) {
+  int r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.s32 q, %1, 0;\n\tbar.red.and.pred p, 2, 128, q;\n\t"
+      "selp.s32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(r)
+      : "r"((int)ok)
+      : "memory");
+  return r != 0;
+}
+
+__global__ void __launch_bounds__(SC_THREADS, 1)
+    k_scatter_tc(DevSym S, const CUtensorMap *__restrict__ maps, const int4 *__restrict__ tiles,
+                 int count, ScatterCols C) {
+  extern __shared__ unsigned char sc_dyn[];
+  __shared__ __align__(8) uint64_t full_bar[SC_STAGES], empty_bar[SC_STAGES];
+  __shared__ __align__(8) uint64_t accf_bar[2], acce_bar[2], done_bar;
+  __shared__ int64_t col_base[128];   // per tile column: target column's first entry in L
+  __shared__ int col_rel[128];        //   and the offset of its run's relative indices
+  __shared__ uint32_t tmem_base;
+  __shared__ volatile int abort_flag;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t sbase = (smem_u32(sc_dyn) + 1023u) & ~1023u;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     smem_u32(&tmem_base)),
+                 "r"(SC_TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  if (tid == 160) {
+    for (int s = 0; s < SC_STAGES; ++s) {
+      mbar_init(smem_u32(&full_bar[s]), 1);
+      mbar_init(smem_u32(&empty_bar[s]), 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(smem_u32(&accf_bar[b]), 1);
+      mbar_init(smem_u32(&acce_bar[b]), 4);
+    }
+    mbar_init(smem_u32(&done_bar), 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = tmem_base;
+
+  if (warp == 4) {
+    // ------------------------------ TMA producer ------------------------------
+    if (lane == 0) {
+      int stage = 0, armed[SC_STAGES];
+      uint32_t phase = 0;
+      for (int s = 0; s < SC_STAGES; ++s) armed[s] = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < count && ok; t += gridDim.x) {
+        const int4 tl = tiles[t];
+        const CUtensorMap *hi = maps + 2 * tl.x, *lo = hi + 1;
+        const bool diag = tl.y == tl.z;
+        const uint32_t bytes = diag ? 2 * SC_OP : 4 * SC_OP;
+        for (int kc = 0; kc < tl.w; ++kc) {
+          if (!mbar_wait(smem_u32(&empty_bar[stage]), phase ^ 1u, &abort_flag, S.status)) {
+            ok = false;
+            break;
+          }
+          const uint32_t fb = smem_u32(&full_bar[stage]);
+          const uint32_t sa = sbase + stage * SC_STAGE;
+          mbar_arrive_tx(fb, bytes);
+          armed[stage] += 1;
+          const int x = kc * SC_KCHUNK;
+          tma_load_2d(sa, hi, fb, x, tl.y);
+          tma_load_2d(sa + SC_OP, lo, fb, x, tl.y);
+          if (!diag) {
+            tma_load_2d(sa + 2 * SC_OP, hi, fb, x, tl.z);
+            tma_load_2d(sa + 3 * SC_OP, lo, fb, x, tl.z);
+          }
+          if (++stage == SC_STAGES) { stage = 0; phase ^= 1u; }
+        }
+      }
+      // loads in flight land before the CTA leaves
+      for (int s = 0; s < SC_STAGES; ++s)
+        if (armed[s] > 0) mbar_drain(smem_u32(&full_bar[s]), (uint32_t)(armed[s] - 1) & 1u, S.status);
+    }
+    __syncwarp();
+  } else if (warp == 5) {
+    // ------------------------------- MMA issuer -------------------------------
+    if (lane == 0) {
+      int stage = 0, buf = 0;
+      uint32_t phase = 0, accphase[2] = {0, 0};
+      bool ok = true;
+      for (int t = blockIdx.x; t < count && ok; t += gridDim.x) {
+        const int4 tl = tiles[t];
+        const bool diag = tl.y == tl.z;
+        if (!mbar_wait(smem_u32(&acce_bar[buf]), accphase[buf] ^ 1u, &abort_flag, S.status)) break;
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        const uint32_t dt = tmem + (uint32_t)buf * 128u;
+        for (int kc = 0; kc < tl.w; ++kc) {
+          if (!mbar_wait(smem_u32(&full_bar[stage]), phase, &abort_flag, S.status)) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+          const uint32_t ah = sbase + stage * SC_STAGE, al = ah + SC_OP;
+          const uint32_t bh = diag ? ah : ah + 2 * SC_OP, bl = diag ? al : ah + 3 * SC_OP;
+#pragma unroll
+          for (int kk = 0; kk < SC_KCHUNK / 8; ++kk) {
+            const uint32_t o = 32u * kk;   // 8 TF32 columns = 32 bytes along the swizzled row
+            mma_tf32(dt, sw128_desc(ah + o), sw128_desc(bh + o), (kc | kk) != 0);
+            mma_tf32(dt, sw128_desc(al + o), sw128_desc(bh + o), 1u);
+            mma_tf32(dt, sw128_desc(ah + o), sw128_desc(bl + o), 1u);
+          }
+          mma_commit(smem_u32(&empty_bar[stage]));   // the stage is free once these are done
+          if (++stage == SC_STAGES) { stage = 0; phase ^= 1u; }
+        }
+        if (!ok) break;
+        mma_commit(smem_u32(&accf_bar[buf]));          // the tile's product: to the epilogue
+        accphase[buf] ^= 1u;
+        buf ^= 1;
+      }
+      // every MMA issued has completed before TMEM is freed
+      mma_commit(smem_u32(&done_bar));
+      mbar_drain(smem_u32(&done_bar), 0u, S.status);
+    }
+    __syncwarp();
+  } else {
+    // -------------------------------- epilogue --------------------------------
+    int buf = 0;
+    uint32_t accphase[2] = {0, 0};
+    for (int t = blockIdx.x; t < count; t += gridDim.x) {
+      const int4 tl = tiles[t];
+      const int d = tl.x;
+      const int md = (int)(S.rowptr[d + 1] - S.rowptr[d]);
+      const int64_t co = C.coff[d];
+      // the tile's column table (the previous tile's readers are past the first barrier, the
+      // second publishes it)
+      epi_bar();
+      {
+        const int j = tl.z + tid;
+        col_base[tid] = j < md ? C.base[co + j] : -1;
+        col_rel[tid] = j < md ? C.rel[co + j] : 0;
+      }
+      const bool ok = mbar_wait_warp(smem_u32(&accf_bar[buf]), accphase[buf], &abort_flag, S.status);
+      if (!epi_bar_and(ok)) break;
+      accphase[buf] ^= 1u;
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      float v[128];
+      const uint32_t ta = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)buf * 128u;
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) tmem_ld32(ta + 32u * cc, v + 32 * cc);
+      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&acce_bar[buf]));
+      buf ^= 1;
+      // row i of d: add minus C(i, j) for every column j <= i whose target is tiled
+      const int i = tl.y + tid;
+      if (i < md) {
+        int cur = -1;
+        int pos = 0;
+        const int jn = min(128, i - tl.z + 1);   // columns j = tl.z + c with j <= i
+#pragma unroll
+        for (int c = 0; c < 128; ++c) {
+          if (c < jn) {
+            const int64_t cb = col_base[c];
+            if (cb >= 0) {
+              const int ro = col_rel[c];
+              if (ro != cur) {
+                cur = ro;
+                pos = C.relidx[ro + i];
+              }
+              atomicAdd(S.L + cb + pos, -(double)v[c]);
+            }
+          }
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
+                 "r"(SC_TMEM_COLS));
+}
+
+using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                 const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                 const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                 CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_fn() {
+  static EncodeTiled fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiled>(p);
+  }
+  return fn;
+}
+
+}  // namespace
+
+bool scatter_tc_configure(std::string &err) {
+  cudaError_t e =
+      cudaFuncSetAttribute(k_scatter_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, SC_SMEM);
+  if (e != cudaSuccess) {
+    err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e);
+    return false;
+  }
+  return true;
+}
+
+bool build_scatter_maps(const std::vector<int> &super, const std::vector<int64_t> &rowptr,
+                        const std::vector<int64_t> &xk, const std::vector<char> &used, float *Lk,
+                        void *maps_host, std::string &err) {
+  EncodeTiled enc = encode_fn();
+  if (!enc) {
+    err = "cuTensorMapEncodeTiled is not available from the driver";
+    return false;
+  }
+  CUtensorMap *maps = static_cast<CUtensorMap *>(maps_host);
+  const int ns = (int)super.size() - 1;
+  for (int d = 0; d < ns; ++d) {
+    if (!used[d]) continue;
+    const uint64_t w = super[d + 1] - super[d], m = rowptr[d + 1] - rowptr[d];
+    const uint64_t wp = (uint64_t)kmirror_pitch_tf32((int)w);
+    const cuuint64_t dims[2] = {w, m};
+    const cuuint64_t strides[1] = {wp * sizeof(float)};
+    const cuuint32_t box[2] = {SC_KCHUNK, 128};
+    const cuuint32_t estr[2] = {1, 1};
+    for (int p = 0; p < 2; ++p) {   // hi plane, lo plane (rows outside a plane read zeros)
+      CUresult r = enc(&maps[2 * d + p], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                       Lk + xk[d] + (int64_t)p * m * wp, dims, strides, box, estr,
+                       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                       CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r != CUDA_SUCCESS) {
+        err = "cuTensorMapEncodeTiled failed for supernode " + std::to_string(d) + " (code " +
+              std::to_string((int)r) + ")";
+        return false;
+      }
+    }
+  }
+  return true;
+}
+
+void launch_scatter_tc(const DevSym &S, const void *maps, const int4 *tiles, int count,
+                       const ScatterCols &C, cudaStream_t st) {
+  if (count <= 0) return;
+  k_scatter_tc<<<update_tc_ctas(count), SC_THREADS, SC_SMEM, st>>>(
+      S, static_cast<const CUtensorMap *>(maps), tiles, count, C);
+}
+
+}  // namespace swc

@@ -11,11 +11,12 @@
 // descendant is the supernode itself and whose K range is one or more 64-column blocks).
 //
 // Operands: the split mirror of L in K-major form, supernode d (md rows, wd columns) at
-// (float *)Lf + xk[d]; xk[nsuper] names the format:
+// (float *)Lf + xk[d] (128-byte aligned); xk[nsuper] names the format:
 //   0  split-TF32: hi = tf32(x) in row r of the hi plane, lo = tf32(x - hi) in row md + r
-//      of the lo plane; rows of wp = wd rounded up to 4 floats;
+//      of the lo plane; rows of wd rounded up to 32 floats (128 bytes);
 //   1  BF16x3: hi = bf16(x), mid = bf16(x - hi), lo = bf16(x - hi - mid) in rows r, md + r,
-//      2 md + r of three planes; rows of wq = wd rounded up to 8 bfloat16 values.
+//      2 md + r of three planes; rows of wd rounded up to 64 bfloat16 values.
+// A 32-column K chunk of a row is then one aligned 128-byte (or 64-byte) run of memory.
 // A stage holds one 32-column K chunk of the 128-row operands, each in the canonical K-major
 // layout the MMA reads with a swizzle (128-byte rows, 128-byte swizzle for TF32; 64-byte
 // rows, 64-byte swizzle for BF16): atom a (8 rows) holds tile rows 4a..4a+3 twice, one piece
@@ -78,10 +79,11 @@ constexpr int V_TF32 = UT_VARIANT_TF32;           // split-TF32, cp.async stagin
 constexpr int V_TF32_TMA = UT_VARIANT_TF32_TMA;   // split-TF32, TMA gather4 staging
 constexpr int V_BF16 = UT_VARIANT_BF16;           // BF16x3, cp.async staging
 
-constexpr int UT_STAGES = 4;
+constexpr int UT_MAX_STAGES = 6;
 constexpr int UT_KCHUNK = 32;                       // K columns per stage
 constexpr int UT_STAGE_BYTES = 32 * 1024;           // the operand chunks of one stage
-constexpr int UT_SMEM = UT_STAGES * UT_STAGE_BYTES + 1024;   // + alignment slack
+// dynamic shared memory of a launch with `stages` stages (+ alignment slack)
+constexpr int ut_smem(int stages) { return stages * UT_STAGE_BYTES + 1024; }
 constexpr int UT_GROUP_CHUNKS = 8;                  // chunks of one FP32 accumulation group
 constexpr unsigned long long UT_WAIT_NS = 2000000000ULL;   // a pipeline wait gives up after 2 s
 
@@ -121,13 +123,15 @@ __device__ __forceinline__ uint64_t sw_desc(uint32_t saddr, uint32_t sbo, uint64
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
 }
+// One bounded try: the thread sleeps until the phase completes or about 20 us pass, so
+// waiting warps do not take issue slots from the producers.
 __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
-      "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+      "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n\t"
       "selp.b32 %0, 1, 0, P1;\n\t}\n"
       : "=r"(ok)
-      : "r"(bar), "r"(parity)
+      : "r"(bar), "r"(parity), "r"(20000)
       : "memory");
   return ok != 0;
 }
@@ -266,11 +270,12 @@ __device__ __forceinline__ int operand_plane(int o, int p) {
 template <int V>
 __global__ void __launch_bounds__(Ut<V>::THREADS, 1)
     k_update_tc(DevSym S, const CUtensorMap *__restrict__ maps, const int4 *__restrict__ tasks,
-                const int *__restrict__ task_end, const TcPair *__restrict__ pairs, int count) {
+                const int *__restrict__ task_end, const TcPair *__restrict__ pairs, int count,
+                int nst) {
   using T = Ut<V>;
   constexpr int MMA_WARP = 4 + T::NPROD;
   extern __shared__ unsigned char ut_dyn[];
-  __shared__ __align__(8) uint64_t full_bar[UT_STAGES], empty_bar[UT_STAGES];
+  __shared__ __align__(8) uint64_t full_bar[UT_MAX_STAGES], empty_bar[UT_MAX_STAGES];
   __shared__ __align__(8) uint64_t accf_bar[2], acce_bar[2], done_bar;
   __shared__ uint32_t tmem_base;
   __shared__ volatile int abort_flag;
@@ -285,7 +290,7 @@ __global__ void __launch_bounds__(Ut<V>::THREADS, 1)
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
   }
   if (tid == 32 * MMA_WARP) {
-    for (int s = 0; s < UT_STAGES; ++s) {
+    for (int s = 0; s < nst; ++s) {
       // cp.async staging: one hardware arrival per producer thread; TMA: the arming thread
       mbar_init(smem_u32(&full_bar[s]), V == V_TF32_TMA ? 1 : 32 * T::NPROD);
       mbar_init(smem_u32(&empty_bar[s]), 1);
@@ -310,8 +315,8 @@ __global__ void __launch_bounds__(Ut<V>::THREADS, 1)
     // lane % CPR), written where the swizzled K-major layout puts them.  The lane's NSLOT
     // shared-memory slots are fixed for the kernel and its source rows for a pair, so a
     // chunk costs one add and one copy per slot.  Each thread's copies arrive on the stage's
-    // mbarrier when they land (cp.async.mbarrier.arrive.noinc), so up to UT_STAGES chunks
-    // are in flight.
+    // mbarrier when they land (cp.async.mbarrier.arrive.noinc), so up to nst chunks are in
+    // flight.
     constexpr int CPR = T::ROW / 16, RPI = 32 / CPR, JS = 32 / RPI, NSLOT = T::NOPS * JS;
     const int pw = warp - 4, cc = lane % CPR, rsub = lane / CPR;
     uint32_t soff[NSLOT];   // shared-memory offset of each slot within a stage
@@ -332,11 +337,11 @@ __global__ void __launch_bounds__(Ut<V>::THREADS, 1)
       for (int q = tasks[t].w; q < p_end && ok; ++q) {
         const TcPair pr = pairs[q];
         const int wd = S.super[pr.d + 1] - S.super[pr.d];
-        const int pitch = T::BF16 ? ((wd + 7) & ~7) : ((wd + 3) & ~3);   // elements per row
+        const int pitch = T::BF16 ? kmirror_pitch_bf16(wd) : kmirror_pitch_tf32(wd);
         const int md = (int)(S.rowptr[pr.d + 1] - S.rowptr[pr.d]);
         const unsigned char *base = mir + 4 * S.xk[pr.d];
-        // element offset of each slot's source row (plane row * pitch), -1: zeros
-        int64_t goff[NSLOT];
+        // each slot's source row (plane row * pitch elements from base), null: zeros
+        const unsigned char *src[NSLOT];
 #pragma unroll
         for (int o = 0; o < T::NOPS; ++o)
 #pragma unroll
@@ -345,7 +350,7 @@ __global__ void __launch_bounds__(Ut<V>::THREADS, 1)
             const int R = 32 * pw + RPI * j + rsub, u = R & 7;
             const int y = source_row(isA ? pr.rmask : pr.cmask, isA ? pr.a0 : pr.b0,
                                      4 * (R >> 3) + (u & 3), operand_plane<V>(o, u >> 2), md);
-            goff[o * JS + j] = y >= 0 ? (int64_t)y * pitch : -1;
+            src[o * JS + j] = y >= 0 ? base + (size_t)y * pitch * T::ELEM : nullptr;
           }
         const int k0 = pr.kk & 0xffff, kend = k0 + (pr.kk >> 16);
         for (int k = k0; k < kend; k += UT_KCHUNK) {
@@ -357,13 +362,12 @@ __global__ void __launch_bounds__(Ut<V>::THREADS, 1)
           const int kk = k + cc * (16 / T::ELEM);
           const int left = (kend - kk) * T::ELEM;
           const int bytes = left >= 16 ? 16 : (left > 0 ? left : 0);
+          const size_t kb = (size_t)kk * T::ELEM;
 #pragma unroll
-          for (int e = 0; e < NSLOT; ++e) {
-            const bool v = goff[e] >= 0;
-            cp_async16(sa + soff[e], base + (v ? goff[e] + kk : 0) * T::ELEM, v ? bytes : 0);
-          }
+          for (int e = 0; e < NSLOT; ++e)
+            cp_async16(sa + soff[e], src[e] ? src[e] + kb : base, src[e] ? bytes : 0);
           cp_async_arrive(smem_u32(&full_bar[stage]));
-          if (++stage == UT_STAGES) { stage = 0; phase ^= 1u; }
+          if (++stage == nst) { stage = 0; phase ^= 1u; }
         }
       }
     }
@@ -373,9 +377,9 @@ __global__ void __launch_bounds__(Ut<V>::THREADS, 1)
     // --------------------------- producer (TMA) ---------------------------
     int stage = 0;
     uint32_t phase = 0;
-    int armed[UT_STAGES];
+    int armed[UT_MAX_STAGES];
 #pragma unroll
-    for (int s = 0; s < UT_STAGES; ++s) armed[s] = 0;
+    for (int s = 0; s < UT_MAX_STAGES; ++s) armed[s] = 0;
     const int a = lane >> 1, p = lane & 1;   // this lane's swizzle atom and piece
     bool ok = true;
     for (int t = blockIdx.x; t < count && ok; t += gridDim.x) {
@@ -405,13 +409,13 @@ __global__ void __launch_bounds__(Ut<V>::THREADS, 1)
           const uint32_t dst = sbase + stage * UT_STAGE_BYTES + a * T::ATOM + p * (T::ATOM / 2);
           tma_gather4(dst, map, fb, k, ya[0], ya[1], ya[2], ya[3]);
           tma_gather4(dst + T::OPB, map, fb, k, yb[0], yb[1], yb[2], yb[3]);
-          if (++stage == UT_STAGES) { stage = 0; phase ^= 1u; }
+          if (++stage == nst) { stage = 0; phase ^= 1u; }
         }
       }
     }
     // copies in flight complete before the CTA leaves
     if (lane == 0)
-      for (int s = 0; s < UT_STAGES; ++s)
+      for (int s = 0; s < nst; ++s)
         if (armed[s] > 0) mbar_drain(smem_u32(&full_bar[s]), (uint32_t)(armed[s] - 1) & 1u, S.status);
   } else if (warp == MMA_WARP) {
     // ------------------------------ MMA issuer ----------------------------
@@ -462,7 +466,7 @@ __global__ void __launch_bounds__(Ut<V>::THREADS, 1)
                              (open && c == 0 && kk == 0) ? 0u : 1u);
             }
             mma_commit(smem_u32(&empty_bar[stage]));   // stage free once these MMAs are done
-            if (++stage == UT_STAGES) { stage = 0; phase ^= 1u; }
+            if (++stage == nst) { stage = 0; phase ^= 1u; }
           }
           if (!ok) break;
           gchunks += nch;
@@ -581,22 +585,23 @@ EncodeTiled encode_fn() {
 
 template <int V>
 void launch_variant(const DevSym &S, const void *maps, const int4 *tasks, const int *task_end,
-                    const TcPair *pairs, int count, cudaStream_t st) {
-  k_update_tc<V><<<update_tc_ctas(count), Ut<V>::THREADS, UT_SMEM, st>>>(
-      S, static_cast<const CUtensorMap *>(maps), tasks, task_end, pairs, count);
+                    const TcPair *pairs, int count, int nst, cudaStream_t st) {
+  k_update_tc<V><<<update_tc_ctas(count), Ut<V>::THREADS, ut_smem(nst), st>>>(
+      S, static_cast<const CUtensorMap *>(maps), tasks, task_end, pairs, count, nst);
 }
 
 }  // namespace
 
 bool update_tc_configure(std::string &err) {
+  const int smem = ut_smem(UT_MAX_STAGES);
   cudaError_t e = cudaFuncSetAttribute(k_update_tc<V_TF32>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, UT_SMEM);
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_update_tc<V_TF32_TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             UT_SMEM);
+                             smem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_update_tc<V_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             UT_SMEM);
+                             smem);
   if (e != cudaSuccess) {
     err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e);
     return false;
@@ -611,11 +616,12 @@ int64_t kmirror_layout(const std::vector<int> &super, const std::vector<int64_t>
   int64_t off = 0;
   for (int d = 0; d < ns; ++d) {
     const int64_t w = super[d + 1] - super[d], m = rowptr[d + 1] - rowptr[d];
-    // floats: two TF32 planes of rows of w rounded up to 4, or three BF16 planes of rows of
-    // w rounded up to 8; the larger, rounded up to 32 bytes
-    const int64_t tf32 = 2 * m * ((w + 3) & ~3LL), bf16 = (3 * m * ((w + 7) & ~7LL) + 1) / 2;
+    // floats: two TF32 planes or three bfloat16 planes (rows of 128-byte multiples); the
+    // larger, so every supernode starts on a 128-byte boundary
+    const int64_t tf32 = 2 * m * kmirror_pitch_tf32((int)w);
+    const int64_t bf16 = (3 * m * kmirror_pitch_bf16((int)w) + 1) / 2;
     xk[d] = off;
-    off += ((tf32 > bf16 ? tf32 : bf16) + 7) & ~7LL;
+    off += ((tf32 > bf16 ? tf32 : bf16) + 31) & ~31LL;
   }
   xk[ns] = 0;   // the format entry, set per mode
   return off;
@@ -633,7 +639,7 @@ bool build_tensor_maps(const std::vector<int> &super, const std::vector<int64_t>
   const int ns = (int)super.size() - 1;
   for (int d = 0; d < ns; ++d) {
     const uint64_t w = super[d + 1] - super[d], m = rowptr[d + 1] - rowptr[d];
-    const uint64_t wp = (w + 3) & ~3ULL;
+    const uint64_t wp = (uint64_t)kmirror_pitch_tf32((int)w);
     const cuuint64_t dims[2] = {w, 2 * m};
     const cuuint64_t strides[1] = {wp * sizeof(float)};
     const cuuint32_t box[2] = {UT_KCHUNK, 1};
@@ -660,14 +666,17 @@ int update_tc_ctas(int count) {
 }
 
 void launch_update_tc(const DevSym &S, const void *maps, const int4 *tasks, const int *task_end,
-                      const TcPair *pairs, int count, int variant, cudaStream_t st) {
+                      const TcPair *pairs, int count, int variant, bool shared_sm,
+                      cudaStream_t st) {
   if (count <= 0) return;
+  // alone on the GPU: 6 stages (193 KB); next to the diagonal-block kernel: 4 (129 KB)
+  const int nst = shared_sm ? 4 : UT_MAX_STAGES;
   if (variant == UT_VARIANT_BF16)
-    launch_variant<V_BF16>(S, maps, tasks, task_end, pairs, count, st);
+    launch_variant<V_BF16>(S, maps, tasks, task_end, pairs, count, nst, st);
   else if (variant == UT_VARIANT_TF32_TMA)
-    launch_variant<V_TF32_TMA>(S, maps, tasks, task_end, pairs, count, st);
+    launch_variant<V_TF32_TMA>(S, maps, tasks, task_end, pairs, count, nst, st);
   else
-    launch_variant<V_TF32>(S, maps, tasks, task_end, pairs, count, st);
+    launch_variant<V_TF32>(S, maps, tasks, task_end, pairs, count, nst, st);
 }
 
 }  // namespace swc

@@ -65,7 +65,7 @@ def test_batch_autotune_and_cache(cuda_ok, tmp_path):
     h.batch_analyze(mats)
     cache = str(tmp_path / "tune.txt")
     choice, ms = h.batch_autotune(v, S.SWC_MODE_FP64, cache)
-    assert 0 <= choice[0] < 3 and 0 <= choice[1] < 5 and ms > 0   # plans 5, 6: mixed modes
+    assert 0 <= choice[0] < 3 and 0 <= choice[1] < 5 and ms > 0   # plans 5-7: mixed modes
     # the tuned handle factors and solves correctly
     assert h.factor(v) == 0
     b = np.random.default_rng(3).standard_normal(h.n)

@@ -33,9 +33,14 @@ def test_mixed_factor_then_refine(cuda_ok, name, lbound, mode):
     Lmx = h.get_L()
     rel = np.abs(Lmx - L64).max() / np.abs(L64).max()
     assert 1e-12 < rel < lbound, rel
-    # deterministic
+    # BF16x3 (tile-owner updates): bit for bit; split-TF32 (right-looking updates summed by
+    # FP64 atomics in no fixed order): to rounding, far below the mixed-vs-FP64 difference
     assert h.factor(P.A2x, mode) == 0
-    assert np.array_equal(h.get_L(), Lmx)
+    if mode == swc.SWC_MODE_MIXED_BF16X3:
+        assert np.array_equal(h.get_L(), Lmx)
+    else:
+        rerun = np.abs(h.get_L() - Lmx).max() / np.abs(L64).max()
+        assert rerun <= 1e-12 and rerun <= 1e-3 * rel, (rerun, rel)
     rng = np.random.default_rng(0)
     b = rng.standard_normal((P.n, 2))
     x, berr, iters, method = h.refine(b, tol=1e-14, maxit=30)
@@ -75,12 +80,13 @@ def test_stencil27_40_eight_rhs(cuda_ok, name, mode):
     assert fwd.max() <= meta["cond"] * 1e-13, fwd
 
 
-@pytest.mark.parametrize("plan", [0, 5, 6])
+@pytest.mark.parametrize("plan", [0, 5, 6, 7])
 def test_split_tf32_plan_variants(cuda_ok, plan):
-    """The split-TF32 factor under each of its execution-plan variants (0: tcgen05 updates
-    staged with cp.async, 5: trailing SYRK steps kept in FP64, 6: tcgen05 updates staged with
-    TMA tile::gather4 loads) agrees with the default plan's to FP32-class accuracy and
-    refines to the FP64 backward error."""
+    """The split-TF32 factor under each of its execution-plan variants (0: right-looking
+    tcgen05 updates scattered by FP64 atomics, trailing SYRK steps in FP64; 5: the trailing
+    SYRK steps as split-TF32 tcgen05 products; 6, 7: tile-owner tcgen05 updates staged with TMA
+    tile::gather4 loads or with cp.async) agrees with the FP64 factor to FP32-class accuracy
+    and refines to the FP64 backward error."""
     gs = load_sym("grid3d_24")
     A, _, _ = W.build("grid3d_24")
     P = W.assemble(A, gs["perm"], gs["super"])
