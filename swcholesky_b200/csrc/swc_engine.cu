@@ -155,7 +155,8 @@ void Engine::release() {
                   d_csr_val_, d_contrib_, d_work_, d_norms_, d_persist_, d_qctr_, d_npart_,
                   d_tiny_, d_dense_tasks_, d_dense_toff_, d_dense_ver_, d_swarp_,
                   d_Lk_, d_xk_, d_xk16_, d_tmaps_, d_tc_pairs_, d_syrk_pairs_, d_syrk_end_,
-                  d_sc_tiles_, d_sc_base_, d_sc_coff_, d_sc_rel_, d_sc_relidx_, d_sc_maps_};
+                  d_sc_tiles_, d_sc_base_, d_sc_coff_, d_sc_rel_, d_sc_relidx_, d_sc_maps_,
+                  d_sc_small_};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   release_adjoint();
@@ -187,6 +188,7 @@ void Engine::release() {
   d_tc_pairs_ = d_syrk_pairs_ = nullptr;
   d_syrk_end_ = nullptr;
   d_sc_tiles_ = nullptr;
+  d_sc_small_ = nullptr;
   d_sc_base_ = d_sc_coff_ = nullptr;
   d_sc_rel_ = d_sc_relidx_ = nullptr;
   d_sc_maps_ = nullptr;
@@ -555,7 +557,8 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
   if (T.scatter && !P.big_list.empty()) {
     std::vector<char> tiled(supNo, 0);
     for (int s : P.big_list) tiled[s] = 1;
-    std::vector<std::vector<int4>> by_wave(nlev);
+    std::vector<std::vector<ScTile>> by_wave(nlev);
+    std::vector<std::vector<int2>> small_by_wave(nlev);
     P.sc_coff.assign(supNo, 0);
     P.sc_used.assign(supNo, 0);
     for (int d = 0; d < supNo; ++d) {
@@ -599,10 +602,14 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
         }
         j = je;
       }
-      const int nk = (wd + 31) / 32;
+      const int nk = (wd + 31) / 32, r = md - c0;
+      if (r <= 128 && (int64_t)wd * ((r + 31) & ~31) <= SC_SMALL_ELEMS) {
+        small_by_wave[level[d] + 1].push_back(make_int2(d, c0));   // FP64 on the CUDA cores
+        continue;
+      }
       for (int i0 = c0; i0 < md; i0 += 128)
         for (int j0 = c0; j0 <= i0; j0 += 128) {
-          by_wave[level[d] + 1].push_back(make_int4(d, i0, j0, nk));
+          by_wave[level[d] + 1].push_back(ScTile{d, i0, j0, nk, md, 0, P.sc_coff[d]});
           P.sc_flops += 2.0 * 128 * 128 * wd;
         }
       P.sc_used[d] = 1;
@@ -610,12 +617,16 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
     // per level: larger K first (a shorter tail); one descendant's tiles stay together
     int sc_launches = 0;
     for (int lv = 0; lv < nlev; ++lv) {
-      std::vector<int4> &v = by_wave[lv];
-      std::stable_sort(v.begin(), v.end(), [](const int4 &a, const int4 &b) { return a.w > b.w; });
+      std::vector<ScTile> &v = by_wave[lv];
+      std::stable_sort(v.begin(), v.end(),
+                       [](const ScTile &a, const ScTile &b) { return a.nk > b.nk; });
       P.waves[lv].sc_off = (int)P.sc_tiles.size();
       P.waves[lv].sc_cnt = (int)v.size();
       P.sc_tiles.insert(P.sc_tiles.end(), v.begin(), v.end());
-      sc_launches += !v.empty();
+      P.waves[lv].scs_off = (int)P.sc_small.size();
+      P.waves[lv].scs_cnt = (int)small_by_wave[lv].size();
+      P.sc_small.insert(P.sc_small.end(), small_by_wave[lv].begin(), small_by_wave[lv].end());
+      sc_launches += !v.empty() + !small_by_wave[lv].empty();
     }
     // one assemble launch up front instead of one per level; scatter instead of tile-owner
     int asm_l = 0, upd_l = 0;
@@ -856,6 +867,7 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
             upload(d_syrk_end_, P.syrk_end.data(), P.syrk_end.size(), st, err) &&
             upload(d_tc_pairs_, P.tc_pairs.data(), P.tc_pairs.size(), st, err) &&
             upload(d_sc_tiles_, P.sc_tiles.data(), P.sc_tiles.size(), st, err) &&
+            upload(d_sc_small_, P.sc_small.data(), P.sc_small.size(), st, err) &&
             upload(d_sc_base_, P.sc_base.data(), P.sc_base.size(), st, err) &&
             upload(d_sc_coff_, P.sc_coff.data(), P.sc_coff.size(), st, err) &&
             upload(d_sc_rel_, P.sc_rel.data(), P.sc_rel.size(), st, err) &&
@@ -991,6 +1003,9 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec
     launch_factor_small(sym_, d_upd_lbub_, d_small_ + W.small_off, W.small_cnt, W.small_smem, st);
     mark(-1, W.small_cnt);
     if (scatter) {
+      mark(K_UPDATE, W.scs_cnt);
+      launch_scatter_small(sym_, d_sc_small_ + W.scs_off, W.scs_cnt, sc_cols, st);
+      mark(-1, W.scs_cnt);
       mark(K_UPDATE, W.sc_cnt);
       launch_scatter_tc(sym_, d_sc_maps_, d_sc_tiles_ + W.sc_off, W.sc_cnt, sc_cols, st);
       mark(-1, W.sc_cnt);

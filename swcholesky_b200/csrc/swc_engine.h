@@ -61,6 +61,23 @@ struct __align__(16) TcPair {
   unsigned long long rmask, cmask;
 };
 
+// Right-looking split-TF32 updates (swc_scatter_tc.cu).  Tiles (d, i0, j0, K chunks): the
+// 128x128 block of d's contribution whose rows start at row i0 and columns at row j0 of d's
+// row list.  Column table: entry coff[d] + j (row j of d, used as a column of C) holds the
+// first entry in L of the target column (-1: the target is not of the tiled class) and the
+// offset r such that relidx[r + i] is the position of d's row i in that target's row list.
+struct ScatterCols {
+  const int64_t *base;
+  const int *rel;
+  const int64_t *coff;
+  const int *relidx;
+};
+// One 128x128 tile of a descendant's contribution: supernode d, first row i0 and first column
+// j0 (rows of d's row list), K chunks of 32 columns, d's rows and its column-table offset.
+struct __align__(16) ScTile {
+  int d, i0, j0, nk, md, pad;
+  int64_t co;
+};
 // One level of the schedule (supernodes whose descendants all belong to earlier levels).
 struct Wave {
   int small_off = 0, small_cnt = 0;
@@ -75,6 +92,7 @@ struct Wave {
   int dense_ctas = 0;
   int sc_off = 0, sc_cnt = 0;   // right-looking update tiles of the descendants of the level
                                 // before (split-TF32 mode)
+  int scs_off = 0, scs_cnt = 0; // the same level's small contributions
 };
 
 // Kernel classes, for per-kernel timing (profiled factorization) and flop accounting.
@@ -108,7 +126,8 @@ struct Plan {
   int64_t dense_tiles = 0;         // tile version counters in total
   // right-looking updates (split-TF32 mode): tiles, the column table and relative indices
   // (ScatterCols), supernodes that own tiles
-  std::vector<int4> sc_tiles;
+  std::vector<ScTile> sc_tiles;
+  std::vector<int2> sc_small;        // (d, c0) tasks of the small contributions
   std::vector<int64_t> sc_base, sc_coff;
   std::vector<int> sc_rel, sc_relidx;
   std::vector<char> sc_used;
@@ -315,7 +334,8 @@ class Engine {
   int64_t kmirror_len_ = 0;
   TcPair *d_tc_pairs_ = nullptr, *d_syrk_pairs_ = nullptr;
   int *d_syrk_end_ = nullptr;
-  int4 *d_sc_tiles_ = nullptr;                 // right-looking update tiles and their tables
+  ScTile *d_sc_tiles_ = nullptr;               // right-looking update tiles and their tables
+  int2 *d_sc_small_ = nullptr;
   int64_t *d_sc_base_ = nullptr, *d_sc_coff_ = nullptr;
   int *d_sc_rel_ = nullptr, *d_sc_relidx_ = nullptr;
   void *d_sc_maps_ = nullptr;                  // two tensor maps per supernode (over d_Lk_)
@@ -400,23 +420,19 @@ void launch_update_tc(const DevSym &S, const void *maps, const int4 *tasks, cons
                       const TcPair *pairs, int count, int variant, bool shared_sm,
                       cudaStream_t st);
 
-// Right-looking split-TF32 updates (swc_scatter_tc.cu).  Tiles (d, i0, j0, K chunks): the
-// 128x128 block of d's contribution whose rows start at row i0 and columns at row j0 of d's
-// row list.  Column table: entry coff[d] + j (row j of d, used as a column of C) holds the
-// first entry in L of the target column (-1: the target is not of the tiled class) and the
-// offset r such that relidx[r + i] is the position of d's row i in that target's row list.
-struct ScatterCols {
-  const int64_t *base;
-  const int *rel;
-  const int64_t *coff;
-  const int *relidx;
-};
+// Right-looking split-TF32 updates (swc_scatter_tc.cu): ScatterCols, ScTile above.
 bool scatter_tc_configure(std::string &err);
 // two tensor maps per supernode d with used[d] (hi plane, lo plane; 128-row boxes)
 bool build_scatter_maps(const std::vector<int> &super, const std::vector<int64_t> &rowptr,
                         const std::vector<int64_t> &xk, const std::vector<char> &used, float *Lk,
                         void *maps_host, std::string &err);
-void launch_scatter_tc(const DevSym &S, const void *maps, const int4 *tiles, int count,
+void launch_scatter_tc(const DevSym &S, const void *maps, const ScTile *tiles, int count,
                        const ScatterCols &C, cudaStream_t st);
+// Small contributions (a descendant whose rows from c0 number at most 128 and whose width
+// times those rows, rounded up to 32, is at most SC_SMALL_ELEMS): one CTA per (d, c0) task,
+// FP64 products from L on the CUDA cores, the same atomic scatter.
+constexpr int SC_SMALL_ELEMS = 4096;
+void launch_scatter_small(const DevSym &S, const int2 *tasks, int count, const ScatterCols &C,
+                          cudaStream_t st);
 
 }  // namespace swc

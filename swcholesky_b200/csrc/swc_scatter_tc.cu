@@ -20,22 +20,30 @@
 // hi hi' + lo hi' + hi lo' in one FP32 accumulator in TMEM (the lo lo' term, below 2^-22 of
 // the product, is dropped).
 //
-// Roles (192 threads, one CTA per SM, persistent over the launch's tile list, tile t handled
+// Roles (608 threads, one CTA per SM, persistent over the launch's tile list, tile t handled
 // by CTA t mod gridDim.x):
-//   warps 0-3  epilogue: thread = TMEM lane = tile row; reads the 128 FP32 columns of its
-//              row, releases the accumulator, then adds minus each lower-triangle entry to L;
-//   warp 4     TMA producer (one thread): per 32-column K chunk, four 2D tiled loads (A hi,
+//   warps 0-15 epilogue: warp w owns tile rows 32 (w % 4) .. + 31 (its TMEM lane quarter) and
+//              columns 32 (w / 4) .. + 31; reads its 32 FP32 values, releases the
+//              accumulator, then adds minus each lower-triangle entry to L at the address the
+//              tile's scatter table gives (shared memory only); sixteen warps keep enough
+//              atomic adds in flight;
+//   warp 16    TMA producer (one thread): per 32-column K chunk, four 2D tiled loads (A hi,
 //              A lo, B hi, B lo; 128 rows x 128 bytes each, 128-byte swizzle) into a stage,
 //              two for a diagonal tile (B = A);
-//   warp 5     MMA issuer (one thread): twelve MMAs per stage into one of two accumulators,
+//   warp 17    MMA issuer (one thread): twelve MMAs per stage into one of two accumulators,
 //              tcgen05.commit frees the stage and, after the tile's last chunk, hands the
-//              accumulator to the epilogue.
+//              accumulator to the epilogue;
+//   warp 18    table warp: builds the next tile's scatter table in shared memory (two
+//              tables in a ring): the target base and run slot of every column and, per
+//              run, the target position of every tile row, loaded as independent reads so
+//              the epilogue meets no chain of dependent global loads.
 // Every mbarrier wait is bounded (2 s of %globaltimer): a wait that runs out sets status[3]
 // and an abort flag that stops the other roles; the kernel then waits (bounded) for its loads
 // and MMAs in flight, frees its TMEM and returns.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <climits>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -51,7 +59,9 @@ constexpr int SC_KCHUNK = 32;                 // K columns per stage
 constexpr int SC_OP = 128 * 128;              // bytes of one operand chunk (128 rows x 128 B)
 constexpr int SC_STAGE = 4 * SC_OP;           // A hi, A lo, B hi, B lo
 constexpr int SC_SMEM = SC_STAGES * SC_STAGE + 1024;   // + alignment slack
-constexpr int SC_THREADS = 192;
+constexpr int SC_EPI_WARPS = 16;              // epilogue: (row quarter, 32-column group)
+constexpr int SC_PRODUCER = 16, SC_MMA = 17, SC_TABLE = 18;   // warps of the other roles
+constexpr int SC_THREADS = 32 * 19;
 constexpr int SC_TMEM_COLS = 256;             // two 128-column FP32 accumulators
 constexpr unsigned long long SC_WAIT_NS = 2000000000ULL;
 // D F32 (bit 4), A and B TF32 (2 at bits 7 and 10), K-major, N >> 3 at 17, M >> 4 at 24
@@ -170,30 +180,27 @@ __device__ __forceinline__ void tmem_ld32(uint32_t addr, float *v) {
   for (int q = 0; q < 32; ++q) v[q] = __uint_as_float(r[q]);
 }
 
-// Barriers of the four epilogue warps: a plain one, and one that returns the AND of every
-// thread's flag (so all four warps take the same exit after a bounded wait).
-__device__ __forceinline__ void epi_bar() {
-  asm volatile("bar.sync 1, 128;\n" ::: "memory");
-}
-__device__ __forceinline__ bool epi_bar_and(bool ok) {
-  int r;
-  asm volatile(
-      "{\n\t.reg .pred p, q;\n\tsetp.ne.s32 q, %1, 0;\n\tbar.red.and.pred p, 2, 128, q;\n\t"
-      "selp.s32 %0, 1, 0, p;\n\t}\n"
-      : "=r"(r)
-      : "r"((int)ok)
-      : "memory");
-  return r != 0;
-}
+// Scatter table of one tile, built by the table warp ahead of the epilogue: per column the
+// target's first entry in L (-1: no tiled target) and its run slot (a run: consecutive
+// columns with one target supernode); per slot the offset of the run's relative indices and
+// its first column; for the first SC_RUNS slots the target position of every tile row.
+constexpr int SC_RUNS = 16;
+struct ScTable {
+  int64_t base[128];
+  int slot[128];
+  int ro[128];
+  int rj[SC_RUNS];
+  int pos[SC_RUNS][128];
+  int md, i0, j0, nslots;
+};
 
 __global__ void __launch_bounds__(SC_THREADS, 1)
-    k_scatter_tc(DevSym S, const CUtensorMap *__restrict__ maps, const int4 *__restrict__ tiles,
+    k_scatter_tc(DevSym S, const CUtensorMap *__restrict__ maps, const ScTile *__restrict__ tiles,
                  int count, ScatterCols C) {
   extern __shared__ unsigned char sc_dyn[];
   __shared__ __align__(8) uint64_t full_bar[SC_STAGES], empty_bar[SC_STAGES];
-  __shared__ __align__(8) uint64_t accf_bar[2], acce_bar[2], done_bar;
-  __shared__ int64_t col_base[128];   // per tile column: target column's first entry in L
-  __shared__ int col_rel[128];        //   and the offset of its run's relative indices
+  __shared__ __align__(8) uint64_t accf_bar[2], acce_bar[2], tblf_bar[2], tble_bar[2], done_bar;
+  __shared__ __align__(16) ScTable tbl[2];
   __shared__ uint32_t tmem_base;
   __shared__ volatile int abort_flag;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -205,14 +212,16 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                  "r"(SC_TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
   }
-  if (tid == 160) {
+  if (tid == 32 * SC_MMA) {
     for (int s = 0; s < SC_STAGES; ++s) {
       mbar_init(smem_u32(&full_bar[s]), 1);
       mbar_init(smem_u32(&empty_bar[s]), 1);
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(smem_u32(&accf_bar[b]), 1);
-      mbar_init(smem_u32(&acce_bar[b]), 4);
+      mbar_init(smem_u32(&acce_bar[b]), SC_EPI_WARPS);
+      mbar_init(smem_u32(&tblf_bar[b]), 32);
+      mbar_init(smem_u32(&tble_bar[b]), SC_EPI_WARPS);
     }
     mbar_init(smem_u32(&done_bar), 1);
     abort_flag = 0;
@@ -223,7 +232,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = tmem_base;
 
-  if (warp == 4) {
+  if (warp == SC_PRODUCER) {
     // ------------------------------ TMA producer ------------------------------
     if (lane == 0) {
       int stage = 0, armed[SC_STAGES];
@@ -231,11 +240,11 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
       for (int s = 0; s < SC_STAGES; ++s) armed[s] = 0;
       bool ok = true;
       for (int t = blockIdx.x; t < count && ok; t += gridDim.x) {
-        const int4 tl = tiles[t];
-        const CUtensorMap *hi = maps + 2 * tl.x, *lo = hi + 1;
-        const bool diag = tl.y == tl.z;
+        const ScTile tl = tiles[t];
+        const CUtensorMap *hi = maps + 2 * tl.d, *lo = hi + 1;
+        const bool diag = tl.i0 == tl.j0;
         const uint32_t bytes = diag ? 2 * SC_OP : 4 * SC_OP;
-        for (int kc = 0; kc < tl.w; ++kc) {
+        for (int kc = 0; kc < tl.nk; ++kc) {
           if (!mbar_wait(smem_u32(&empty_bar[stage]), phase ^ 1u, &abort_flag, S.status)) {
             ok = false;
             break;
@@ -245,11 +254,11 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
           mbar_arrive_tx(fb, bytes);
           armed[stage] += 1;
           const int x = kc * SC_KCHUNK;
-          tma_load_2d(sa, hi, fb, x, tl.y);
-          tma_load_2d(sa + SC_OP, lo, fb, x, tl.y);
+          tma_load_2d(sa, hi, fb, x, tl.i0);
+          tma_load_2d(sa + SC_OP, lo, fb, x, tl.i0);
           if (!diag) {
-            tma_load_2d(sa + 2 * SC_OP, hi, fb, x, tl.z);
-            tma_load_2d(sa + 3 * SC_OP, lo, fb, x, tl.z);
+            tma_load_2d(sa + 2 * SC_OP, hi, fb, x, tl.j0);
+            tma_load_2d(sa + 3 * SC_OP, lo, fb, x, tl.j0);
           }
           if (++stage == SC_STAGES) { stage = 0; phase ^= 1u; }
         }
@@ -259,19 +268,19 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
         if (armed[s] > 0) mbar_drain(smem_u32(&full_bar[s]), (uint32_t)(armed[s] - 1) & 1u, S.status);
     }
     __syncwarp();
-  } else if (warp == 5) {
+  } else if (warp == SC_MMA) {
     // ------------------------------- MMA issuer -------------------------------
     if (lane == 0) {
       int stage = 0, buf = 0;
       uint32_t phase = 0, accphase[2] = {0, 0};
       bool ok = true;
       for (int t = blockIdx.x; t < count && ok; t += gridDim.x) {
-        const int4 tl = tiles[t];
-        const bool diag = tl.y == tl.z;
+        const int i0 = tiles[t].i0, j0 = tiles[t].j0, nk = tiles[t].nk;
+        const bool diag = i0 == j0;
         if (!mbar_wait(smem_u32(&acce_bar[buf]), accphase[buf] ^ 1u, &abort_flag, S.status)) break;
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
         const uint32_t dt = tmem + (uint32_t)buf * 128u;
-        for (int kc = 0; kc < tl.w; ++kc) {
+        for (int kc = 0; kc < nk; ++kc) {
           if (!mbar_wait(smem_u32(&full_bar[stage]), phase, &abort_flag, S.status)) {
             ok = false;
             break;
@@ -299,56 +308,125 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
       mbar_drain(smem_u32(&done_bar), 0u, S.status);
     }
     __syncwarp();
-  } else {
-    // -------------------------------- epilogue --------------------------------
-    int buf = 0;
-    uint32_t accphase[2] = {0, 0};
+  } else if (warp == SC_TABLE) {
+    // ------------------------------- table warp -------------------------------
+    // lane: columns 4 lane .. 4 lane + 3 of the tile, rows lane + 32 k
+    int b = 0;
+    uint32_t tph[2] = {0, 0};
     for (int t = blockIdx.x; t < count; t += gridDim.x) {
-      const int4 tl = tiles[t];
-      const int d = tl.x;
-      const int md = (int)(S.rowptr[d + 1] - S.rowptr[d]);
-      const int64_t co = C.coff[d];
-      // the tile's column table (the previous tile's readers are past the first barrier, the
-      // second publishes it)
-      epi_bar();
-      {
-        const int j = tl.z + tid;
-        col_base[tid] = j < md ? C.base[co + j] : -1;
-        col_rel[tid] = j < md ? C.rel[co + j] : 0;
+      if (!mbar_wait_warp(smem_u32(&tble_bar[b]), tph[b] ^ 1u, &abort_flag, S.status)) break;
+      const ScTile tl = tiles[t];
+      const int md = tl.md;
+      const int64_t co = tl.co;
+      ScTable &T = tbl[b];
+      int64_t cb[4];
+      int ro[4], fl[4], nf = 0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int j = tl.j0 + 4 * lane + q;
+        cb[q] = j < md ? C.base[co + j] : -1;
+        ro[q] = j < md ? C.rel[co + j] : 0;
       }
-      const bool ok = mbar_wait_warp(smem_u32(&accf_bar[buf]), accphase[buf], &abort_flag, S.status);
-      if (!epi_bar_and(ok)) break;
+      // a run starts at a tiled column whose predecessor is untiled or has another run
+      int64_t pcb = __shfl_up_sync(0xffffffffu, cb[3], 1);
+      const int pro = __shfl_up_sync(0xffffffffu, ro[3], 1);
+      if (lane == 0) pcb = -1;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int64_t prevb = q ? cb[q - 1] : pcb;
+        const int prevr = q ? ro[q - 1] : pro;
+        fl[q] = cb[q] >= 0 && (prevb < 0 || prevr != ro[q]);
+        nf += fl[q];
+      }
+      int incl = nf;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      int sl = incl - nf;   // runs started before my first column
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int c = 4 * lane + q;
+        sl += fl[q];
+        T.base[c] = cb[q];
+        T.slot[c] = cb[q] >= 0 ? sl - 1 : -1;
+        if (fl[q]) {
+          T.ro[sl - 1] = ro[q];
+          if (sl - 1 < SC_RUNS) T.rj[sl - 1] = tl.j0 + c;
+        }
+      }
+      const int nslots = __shfl_sync(0xffffffffu, incl, 31);
+      if (lane == 0) {
+        T.md = md;
+        T.i0 = tl.i0;
+        T.j0 = tl.j0;
+        T.nslots = nslots;
+      }
+      __syncwarp();
+      // target positions of the tile rows for the first SC_RUNS runs (rows before a run's
+      // first column have no position in its target and are not read)
+      const int ns = min(nslots, SC_RUNS);
+      for (int s0 = 0; s0 < ns; s0 += 4) {
+        int pv[4][4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int s = s0 + u;
+          const int rro = s < ns ? T.ro[s] : 0, rj = s < ns ? T.rj[s] : INT_MAX;
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const int i = tl.i0 + lane + 32 * k;
+            pv[u][k] = (i < md && i >= rj) ? C.relidx[rro + i] : 0;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (s0 + u < ns)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) T.pos[s0 + u][lane + 32 * k] = pv[u][k];
+      }
+      __syncwarp();
+      mbar_arrive(smem_u32(&tblf_bar[b]));   // every lane: its writes are released
+      tph[b] ^= 1u;
+      b ^= 1;
+    }
+  } else if (warp < SC_EPI_WARPS) {
+    // -------------------------------- epilogue --------------------------------
+    // warp w: tile rows 32 (w % 4) + lane (its TMEM lane quarter), columns 32 (w / 4) ..
+    const int rt = 32 * (warp & 3) + lane, c0 = 32 * (warp >> 2);
+    int buf = 0, b = 0;
+    uint32_t accphase[2] = {0, 0}, tph[2] = {0, 0};
+    for (int t = blockIdx.x; t < count; t += gridDim.x) {
+      if (!mbar_wait_warp(smem_u32(&tblf_bar[b]), tph[b], &abort_flag, S.status)) break;
+      if (!mbar_wait_warp(smem_u32(&accf_bar[buf]), accphase[buf], &abort_flag, S.status)) break;
       accphase[buf] ^= 1u;
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-      float v[128];
-      const uint32_t ta = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)buf * 128u;
-#pragma unroll
-      for (int cc = 0; cc < 4; ++cc) tmem_ld32(ta + 32u * cc, v + 32 * cc);
+      float v[32];
+      tmem_ld32(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)buf * 128u + (uint32_t)c0, v);
       asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
       __syncwarp();
       if (lane == 0) mbar_arrive(smem_u32(&acce_bar[buf]));
       buf ^= 1;
       // row i of d: add minus C(i, j) for every column j <= i whose target is tiled
-      const int i = tl.y + tid;
-      if (i < md) {
-        int cur = -1;
-        int pos = 0;
-        const int jn = min(128, i - tl.z + 1);   // columns j = tl.z + c with j <= i
+      const ScTable &T = tbl[b];
+      const int i = T.i0 + rt;
+      if (i < T.md) {
+        const int jn = min(32, i - T.j0 - c0 + 1);   // columns j = j0 + c0 + q with j <= i
 #pragma unroll
-        for (int c = 0; c < 128; ++c) {
-          if (c < jn) {
-            const int64_t cb = col_base[c];
-            if (cb >= 0) {
-              const int ro = col_rel[c];
-              if (ro != cur) {
-                cur = ro;
-                pos = C.relidx[ro + i];
-              }
-              atomicAdd(S.L + cb + pos, -(double)v[c]);
+        for (int q = 0; q < 32; ++q) {
+          if (q < jn) {
+            const int sl = T.slot[c0 + q];
+            if (sl >= 0) {
+              const int pos = sl < SC_RUNS ? T.pos[sl][rt] : C.relidx[T.ro[sl] + i];
+              atomicAdd(S.L + T.base[c0 + q] + pos, -(double)v[q]);
             }
           }
         }
       }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&tble_bar[b]));
+      tph[b] ^= 1u;
+      b ^= 1;
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -357,6 +435,48 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
                  "r"(SC_TMEM_COLS));
+}
+
+// Small contributions in FP64: CTA = one descendant d from row c0 (r = md - c0 <= 128 rows);
+// its rows c0.. are staged column by column in shared memory (V[k][row], rows padded to a
+// multiple of 32, at most SC_SMALL_ELEMS values); thread t owns row i = c0 + t and adds
+// minus sum_k L(i, k) L(j, k) to the target entry of every column j <= i with a tiled target.
+__global__ void __launch_bounds__(128) k_scatter_small(DevSym S, const int2 *__restrict__ tasks,
+                                                       ScatterCols C) {
+  __shared__ double V[SC_SMALL_ELEMS];
+  __shared__ int64_t cbase[128];
+  __shared__ int crel[128];
+  const int d = tasks[blockIdx.x].x, c0 = tasks[blockIdx.x].y;
+  const int wd = S.super[d + 1] - S.super[d];
+  const int md = (int)(S.rowptr[d + 1] - S.rowptr[d]);
+  const int r = md - c0, R = (r + 31) & ~31;
+  const double *Ld = S.L + S.xptr[d];
+  const int64_t co = C.coff[d];
+  for (int e = threadIdx.x; e < wd * R; e += blockDim.x) {
+    const int k = e / R, q = e - k * R;
+    V[e] = q < r ? Ld[(size_t)k * md + c0 + q] : 0.0;
+  }
+  for (int q = threadIdx.x; q < r; q += blockDim.x) {
+    cbase[q] = C.base[co + c0 + q];
+    crel[q] = C.rel[co + c0 + q];
+  }
+  __syncthreads();
+  const int t = threadIdx.x;
+  if (t >= r) return;
+  const int i = c0 + t;
+  int cur = INT_MIN, pos = 0;
+  for (int q = 0; q <= t; ++q) {
+    const int64_t b = cbase[q];
+    if (b < 0) continue;
+    double acc = 0.0;
+    for (int k = 0; k < wd; ++k) acc = fma(V[k * R + t], V[k * R + q], acc);
+    const int ro = crel[q];
+    if (ro != cur) {
+      cur = ro;
+      pos = C.relidx[ro + i];
+    }
+    atomicAdd(S.L + b + pos, -acc);
+  }
 }
 
 using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
@@ -422,11 +542,17 @@ bool build_scatter_maps(const std::vector<int> &super, const std::vector<int64_t
   return true;
 }
 
-void launch_scatter_tc(const DevSym &S, const void *maps, const int4 *tiles, int count,
+void launch_scatter_tc(const DevSym &S, const void *maps, const ScTile *tiles, int count,
                        const ScatterCols &C, cudaStream_t st) {
   if (count <= 0) return;
   k_scatter_tc<<<update_tc_ctas(count), SC_THREADS, SC_SMEM, st>>>(
       S, static_cast<const CUtensorMap *>(maps), tiles, count, C);
+}
+
+void launch_scatter_small(const DevSym &S, const int2 *tasks, int count, const ScatterCols &C,
+                          cudaStream_t st) {
+  if (count <= 0) return;
+  k_scatter_small<<<count, 128, 0, st>>>(S, tasks, C);
 }
 
 }  // namespace swc
