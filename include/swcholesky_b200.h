@@ -31,18 +31,19 @@ extern "C" {
 
 /* factorization modes */
 #define SWC_MODE_FP64 0        /* every operation in FP64 */
-#define SWC_MODE_MIXED_TF32X3 1 /* the descendant updates of the wide supernodes as split-TF32
-                                   products on the tcgen05 tensor cores (each value as hi + lo
-                                   TF32 pieces, the products hi hi' + lo hi' + hi lo', FP32
-                                   accumulation over a descendant's width), added to L in FP64;
-                                   POTRF, TRSM, the trailing updates of the dense
-                                   factorization (plan 5: split-TF32 too) and small supernodes
-                                   in FP64.  Pair with swc_refine. */
-#define SWC_MODE_MIXED_BF16X3 2 /* the same descendant updates as BF16x3 split products on
-                                   tcgen05: each value as three bfloat16 pieces, the six piece
-                                   products down to the third order, FP32 accumulation per
-                                   group of descendants, FP64 across groups (about FP32
-                                   accuracy) */
+#define SWC_MODE_MIXED_TF32X3 1 /* the Schur updates of the wide supernodes (descendant updates
+                                   and the trailing updates of their dense factorization) as
+                                   split-TF32 products on the tcgen05 tensor cores (each value
+                                   as hi + lo TF32 pieces, the products hi hi' + lo hi' +
+                                   hi lo', FP32 accumulation over a descendant's width or
+                                   over the column blocks of one trailing update), added to L
+                                   in FP64; POTRF, TRSM and small supernodes in FP64.  Pair
+                                   with swc_refine. */
+#define SWC_MODE_MIXED_BF16X3 2 /* the descendant updates as BF16x3 split products on tcgen05:
+                                   each value as three bfloat16 pieces, the six piece products
+                                   down to the third order, FP32 accumulation per group of
+                                   descendants, FP64 across groups (about FP32 accuracy); the
+                                   trailing updates in FP64 */
 
 typedef struct swc_handle *swc_handle_t;
 
@@ -85,12 +86,12 @@ void *swc_get_stream(swc_handle_t handle);
  * walk up to 100 KB of shared memory per supernode; 2: no persistent walk (one launch per
  * level); 3: smaller small-class limits (more tiled supernodes); 4: the dense
  * factorization of each level's tiled supernodes as one persistent dataflow launch
- * instead of three launches per 64-column step; 5: in the mixed modes, the trailing SYRK
- * steps of the dense factorization as split products on tcgen05 instead of FP64 (DMMA);
- * 6 and 7: in SWC_MODE_MIXED_TF32X3, the updates of the tiled class by the tile-owner
+ * instead of three launches per 64-column step; 5: in SWC_MODE_MIXED_TF32X3, the trailing
+ * SYRK steps of the dense factorization in FP64 (DMMA) instead of split-TF32 tcgen05
+ * tiles; 6 and 7: in SWC_MODE_MIXED_TF32X3, the descendant updates by the tile-owner
  * gather kernel (operands staged by TMA gather4 loads, 6, or by cp.async, 7) instead of
- * the right-looking dense products with an FP64 atomic scatter.  SWC_INVALID_INPUT for
- * other values. */
+ * the right-looking dense products with an FP64 atomic scatter, and the trailing SYRK
+ * steps in FP64.  SWC_INVALID_INPUT for other values. */
 int swc_set_plan(swc_handle_t handle, int plan);
 
 /* Poll budget of the handle's device-side waits: the persistent walks of the

@@ -156,7 +156,7 @@ void Engine::release() {
                   d_tiny_, d_dense_tasks_, d_dense_toff_, d_dense_ver_, d_swarp_,
                   d_Lk_, d_xk_, d_xk16_, d_tmaps_, d_tc_pairs_, d_syrk_pairs_, d_syrk_end_,
                   d_sc_tiles_, d_sc_base_, d_sc_coff_, d_sc_rel_, d_sc_relidx_, d_sc_maps_,
-                  d_sc_small_};
+                  d_sc_small_, d_sc_dense_};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   release_adjoint();
@@ -189,6 +189,7 @@ void Engine::release() {
   d_syrk_end_ = nullptr;
   d_sc_tiles_ = nullptr;
   d_sc_small_ = nullptr;
+  d_sc_dense_ = nullptr;
   d_sc_base_ = d_sc_coff_ = nullptr;
   d_sc_rel_ = d_sc_relidx_ = nullptr;
   d_sc_maps_ = nullptr;
@@ -481,6 +482,7 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
       W.panel_off.push_back((int)P.panel_tasks.size());
       W.syrk_off.push_back((int)P.syrk_tasks.size());
       W.diag_off.push_back((int)P.diag_list.size());
+      W.scd_off.push_back((int)P.sc_dense.size());
       for (int s : big) {
         int w = super[s + 1] - super[s];
         int m = (int)(rowptr[s + 1] - rowptr[s]);
@@ -499,6 +501,12 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
           if (C == j + 1) first = j;
           else if ((C - 2 - j) % G == 0) first = std::max(0, j - G + 1);
           else continue;
+          if (T.scatter) {   // the same update as 128-row x one-column-block dense tiles
+            const int kc = c0 + bw - first * TB;
+            for (int r0 = cc == c0 + TB ? cc + TB : cc; r0 < m; r0 += 128)
+              P.sc_dense.push_back(ScTile{s, r0, cc, (kc + 31) / 32, m, first * TB,
+                                          std::min(TB, w - cc), 1, 0, 0});
+          }
           for (int r0 = cc; r0 < m; r0 += TB)
             if (!(cc == c0 + TB && r0 == cc)) {   // next diagonal tile: the TRSM task's update
               // .w: the task's own index: its product (column blocks first..j) in syrk_pairs
@@ -514,6 +522,7 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
       W.panel_cnt.push_back((int)P.panel_tasks.size() - W.panel_off.back());
       W.syrk_cnt.push_back((int)P.syrk_tasks.size() - W.syrk_off.back());
       W.diag_cnt.push_back((int)P.diag_list.size() - W.diag_off.back());
+      W.scd_cnt.push_back((int)P.sc_dense.size() - W.scd_off.back());
     }
     launches += (W.small_cnt > 0) + (W.asm_cnt > 0) + (W.upd_cnt > 0);
     int widest = 0;
@@ -609,11 +618,19 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
       }
       for (int i0 = c0; i0 < md; i0 += 128)
         for (int j0 = c0; j0 <= i0; j0 += 128) {
-          by_wave[level[d] + 1].push_back(ScTile{d, i0, j0, nk, md, 0, P.sc_coff[d]});
+          by_wave[level[d] + 1].push_back(ScTile{d, i0, j0, nk, md, 0, 128, 0, P.sc_coff[d], 0});
           P.sc_flops += 2.0 * 128 * 128 * wd;
         }
-      P.sc_used[d] = 1;
+      P.sc_used[d] |= 1;
     }
+    // dense tiles of its own factorization: A operands through the 128-row maps, B through
+    // the 64-row maps
+    for (int s : P.big_list) P.sc_used[s] |= 3;
+    // every tile's supernode has the maps its loads use
+    for (const ScTile &t : P.sc_tiles)
+      if (!(P.sc_used[t.d] & 1)) { err = "internal: scatter tile without its tensor maps"; return false; }
+    for (const ScTile &t : P.sc_dense)
+      if ((P.sc_used[t.d] & 3) != 3) { err = "internal: dense tile without its tensor maps"; return false; }
     // per level: larger K first (a shorter tail); one descendant's tiles stay together
     int sc_launches = 0;
     for (int lv = 0; lv < nlev; ++lv) {
@@ -868,6 +885,7 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
             upload(d_tc_pairs_, P.tc_pairs.data(), P.tc_pairs.size(), st, err) &&
             upload(d_sc_tiles_, P.sc_tiles.data(), P.sc_tiles.size(), st, err) &&
             upload(d_sc_small_, P.sc_small.data(), P.sc_small.size(), st, err) &&
+            upload(d_sc_dense_, P.sc_dense.data(), P.sc_dense.size(), st, err) &&
             upload(d_sc_base_, P.sc_base.data(), P.sc_base.size(), st, err) &&
             upload(d_sc_coff_, P.sc_coff.data(), P.sc_coff.size(), st, err) &&
             upload(d_sc_rel_, P.sc_rel.data(), P.sc_rel.size(), st, err) &&
@@ -952,14 +970,16 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec
   // split products on tcgen05: split-TF32 (cp.async or TMA staging) or BF16x3
   const int variant = prec == 2 ? UT_VARIANT_BF16
                                 : (tuning_.tc_tma ? UT_VARIANT_TF32_TMA : UT_VARIANT_TF32);
-  const bool syrk_tc = prec != 0 && !tuning_.syrk_fp64;
   cudaStream_t st = stream_;
-  auto syrk = [&](const int4 *tasks, int count, int) {
+  // the trailing updates of the dense steps: split-TF32 dense tiles of the scatter kernel
+  // (two SMs left to the concurrent diagonal-block kernel), else FP64
+  const bool syrk_tc = prec == 1 && !tuning_.syrk_fp64 && !plan_.sc_coff.empty();
+  auto syrk = [&](const Wave &W, int j) {
     if (syrk_tc)
-      launch_update_tc(sym_, d_tmaps_, tasks, d_syrk_end_ + (tasks - d_syrk_), d_syrk_pairs_,
-                       count, variant, true, st);
+      launch_scatter_tc(sym_, d_sc_maps_, d_sc_dense_ + W.scd_off[j], W.scd_cnt[j], scatter_cols(),
+                        2, st);
     else
-      launch_syrk_step(sym_, tasks, d_syrk_pairs_, count, st);
+      launch_syrk_step(sym_, d_syrk_ + W.syrk_off[j], d_syrk_pairs_, W.syrk_cnt[j], st);
   };
   // With profiling on, every launch is preceded by an event and followed by one.
   auto mark = [&](int kind, int count) {
@@ -972,7 +992,7 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec
   // split-TF32 mode with right-looking updates: contributions reach a target from the level
   // after each descendant's, so every tiled panel is assembled up front
   const bool scatter = prec == 1 && !plan_.sc_coff.empty();
-  const ScatterCols sc_cols{d_sc_base_, d_sc_rel_, d_sc_coff_, d_sc_relidx_};
+  const ScatterCols sc_cols = scatter_cols();
   mark(K_MEMSET, 1);
   cudaMemsetAsync(dL_, 0, sizeof(double) * xsize_, st);
   launch_init_status(d_status_, st);
@@ -1007,7 +1027,7 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec
       launch_scatter_small(sym_, d_sc_small_ + W.scs_off, W.scs_cnt, sc_cols, st);
       mark(-1, W.scs_cnt);
       mark(K_UPDATE, W.sc_cnt);
-      launch_scatter_tc(sym_, d_sc_maps_, d_sc_tiles_ + W.sc_off, W.sc_cnt, sc_cols, st);
+      launch_scatter_tc(sym_, d_sc_maps_, d_sc_tiles_ + W.sc_off, W.sc_cnt, sc_cols, 0, st);
       mark(-1, W.sc_cnt);
     } else {
     mark(K_ASSEMBLE, W.asm_cnt);
@@ -1045,7 +1065,7 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec
         launch_diag_step(sym_, d_diag_ + W.diag_off[j], W.diag_cnt[j], (int)j + 1, st);
         mark(-1, W.diag_cnt[j]);
         mark(K_SYRK, W.syrk_cnt[j]);
-        syrk(d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j);
+        syrk(W, (int)j);
         mark(-1, W.syrk_cnt[j]);
       } else if (W.diag_cnt[j] > 0) {
         // fork: next diagonal block on the auxiliary stream, trailing update here; join
@@ -1053,10 +1073,10 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec
         cudaStreamWaitEvent(aux_stream_, ev_fork_, 0);
         launch_diag_step(sym_, d_diag_ + W.diag_off[j], W.diag_cnt[j], (int)j + 1, aux_stream_);
         cudaEventRecord(ev_join_, aux_stream_);
-        syrk(d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j);
+        syrk(W, (int)j);
         cudaStreamWaitEvent(st, ev_join_, 0);
       } else {
-        syrk(d_syrk_ + W.syrk_off[j], W.syrk_cnt[j], (int)j);
+        syrk(W, (int)j);
       }
     }
   }
@@ -1079,7 +1099,7 @@ bool Engine::set_mode(int prec, std::string &err) {
     }
     if (!build_tensor_maps(hsym_.super, hsym_.rowptr, h_xk_, d_Lk_, maps.data(), err)) return false;
     if (!plan_.sc_coff.empty()) {   // hi / lo plane maps of the right-looking update tiles
-      std::vector<unsigned char> sm(2 * mb, 0);
+      std::vector<unsigned char> sm(4 * mb, 0);
       if (!build_scatter_maps(hsym_.super, hsym_.rowptr, h_xk_, plan_.sc_used, d_Lk_, sm.data(),
                               err))
         return false;

@@ -72,11 +72,14 @@ struct ScatterCols {
   const int64_t *coff;
   const int *relidx;
 };
-// One 128x128 tile of a descendant's contribution: supernode d, first row i0 and first column
-// j0 (rows of d's row list), K chunks of 32 columns, d's rows and its column-table offset.
+// One tile of a contribution: supernode d, first row i0 and first column j0 (rows of d's row
+// list), nk K chunks of 32 columns from column k0 of d, d's rows md, ncol columns (128, or at
+// most 64 for a dense tile) and d's column-table offset co.  dense: a trailing update of the
+// dense factorization of d itself (target = d's own columns j0.., row i at position i; no
+// table), else a descendant's contribution to its tiled-class ancestors (128x128).
 struct __align__(16) ScTile {
-  int d, i0, j0, nk, md, pad;
-  int64_t co;
+  int d, i0, j0, nk, md, k0, ncol, dense;
+  int64_t co, pad;
 };
 // One level of the schedule (supernodes whose descendants all belong to earlier levels).
 struct Wave {
@@ -88,6 +91,8 @@ struct Wave {
   std::vector<int> panel_off, panel_cnt;  // per column block step: TRSM tiles
   std::vector<int> syrk_off, syrk_cnt;
   std::vector<int> diag_off, diag_cnt;    // per step j: supernodes whose block j+1 exists
+  std::vector<int> scd_off, scd_cnt;      // per step j: the trailing updates as dense tiles
+                                          // (split-TF32 mode)
   int dense_off = 0, dense_cnt = 0;       // dataflow tasks of the dense factorization
   int dense_ctas = 0;
   int sc_off = 0, sc_cnt = 0;   // right-looking update tiles of the descendants of the level
@@ -128,6 +133,7 @@ struct Plan {
   // (ScatterCols), supernodes that own tiles
   std::vector<ScTile> sc_tiles;
   std::vector<int2> sc_small;        // (d, c0) tasks of the small contributions
+  std::vector<ScTile> sc_dense;      // trailing updates of the dense steps as tiles
   std::vector<int64_t> sc_base, sc_coff;
   std::vector<int> sc_rel, sc_relidx;
   std::vector<char> sc_used;
@@ -336,9 +342,11 @@ class Engine {
   int *d_syrk_end_ = nullptr;
   ScTile *d_sc_tiles_ = nullptr;               // right-looking update tiles and their tables
   int2 *d_sc_small_ = nullptr;
+  ScTile *d_sc_dense_ = nullptr;
   int64_t *d_sc_base_ = nullptr, *d_sc_coff_ = nullptr;
   int *d_sc_rel_ = nullptr, *d_sc_relidx_ = nullptr;
-  void *d_sc_maps_ = nullptr;                  // two tensor maps per supernode (over d_Lk_)
+  void *d_sc_maps_ = nullptr;                  // four tensor maps per supernode (over d_Lk_)
+  ScatterCols scatter_cols() const { return {d_sc_base_, d_sc_rel_, d_sc_coff_, d_sc_relidx_}; }
   bool use_graph_ = true;
   Tuning tuning_;
   int *d_persist_ = nullptr, *d_qctr_ = nullptr, *d_tiny_ = nullptr;
@@ -422,12 +430,16 @@ void launch_update_tc(const DevSym &S, const void *maps, const int4 *tasks, cons
 
 // Right-looking split-TF32 updates (swc_scatter_tc.cu): ScatterCols, ScTile above.
 bool scatter_tc_configure(std::string &err);
-// two tensor maps per supernode d with used[d] (hi plane, lo plane; 128-row boxes)
+// tensor maps over the K-major split mirror, 4 nsuper entries: [2 d], [2 d + 1] the hi and lo
+// planes of supernode d with 128-row boxes (used[d] & 1), [2 (nsuper + d)] and + 1 the same
+// with 64-row boxes (used[d] & 2)
 bool build_scatter_maps(const std::vector<int> &super, const std::vector<int64_t> &rowptr,
                         const std::vector<int64_t> &xk, const std::vector<char> &used, float *Lk,
                         void *maps_host, std::string &err);
+// reserve: SMs left free for a kernel running at the same time (the diagonal-block kernel
+// of the dense steps)
 void launch_scatter_tc(const DevSym &S, const void *maps, const ScTile *tiles, int count,
-                       const ScatterCols &C, cudaStream_t st);
+                       const ScatterCols &C, int reserve, cudaStream_t st);
 // Small contributions (a descendant whose rows from c0 number at most 128 and whose width
 // times those rows, rounded up to 32, is at most SC_SMALL_ELEMS): one CTA per (d, c0) task,
 // FP64 products from L on the CUDA cores, the same atomic scatter.

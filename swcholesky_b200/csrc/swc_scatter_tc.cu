@@ -43,6 +43,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <climits>
 #include <cstdint>
 #include <string>
@@ -64,9 +65,11 @@ constexpr int SC_PRODUCER = 16, SC_MMA = 17, SC_TABLE = 18;   // warps of the ot
 constexpr int SC_THREADS = 32 * 19;
 constexpr int SC_TMEM_COLS = 256;             // two 128-column FP32 accumulators
 constexpr unsigned long long SC_WAIT_NS = 2000000000ULL;
-// D F32 (bit 4), A and B TF32 (2 at bits 7 and 10), K-major, N >> 3 at 17, M >> 4 at 24
-constexpr uint32_t SC_IDESC =
-    (1u << 4) | (2u << 7) | (2u << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
+// Instruction descriptor: D F32 (bit 4), A and B TF32 (2 at bits 7 and 10), K-major, N >> 3
+// at bit 17, M >> 4 at bit 24; M = 128, N = 128 or 64.
+__host__ __device__ constexpr uint32_t sc_idesc(uint32_t n) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((n >> 3) << 17) | ((128u >> 4) << 24);
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -151,12 +154,12 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map
 }
 
 __device__ __forceinline__ void mma_tf32(uint32_t tmem, uint64_t adesc, uint64_t bdesc,
-                                         uint32_t accumulate) {
+                                         uint32_t idesc, uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
           tmem),
-      "l"(adesc), "l"(bdesc), "r"(SC_IDESC), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
 }
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
   asm volatile(
@@ -242,8 +245,11 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
       for (int t = blockIdx.x; t < count && ok; t += gridDim.x) {
         const ScTile tl = tiles[t];
         const CUtensorMap *hi = maps + 2 * tl.d, *lo = hi + 1;
-        const bool diag = tl.i0 == tl.j0;
-        const uint32_t bytes = diag ? 2 * SC_OP : 4 * SC_OP;
+        // B: 128-row boxes, or 64-row boxes for a tile of at most 64 columns
+        const bool narrow = tl.ncol <= 64;
+        const CUtensorMap *bhi = narrow ? maps + 2 * (S.nsuper + tl.d) : hi, *blo = bhi + 1;
+        const bool diag = tl.i0 == tl.j0;   // B = the first ncol rows of A
+        const uint32_t bytes = 2 * SC_OP + (diag ? 0 : (narrow ? SC_OP : 2 * SC_OP));
         for (int kc = 0; kc < tl.nk; ++kc) {
           if (!mbar_wait(smem_u32(&empty_bar[stage]), phase ^ 1u, &abort_flag, S.status)) {
             ok = false;
@@ -253,12 +259,12 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
           const uint32_t sa = sbase + stage * SC_STAGE;
           mbar_arrive_tx(fb, bytes);
           armed[stage] += 1;
-          const int x = kc * SC_KCHUNK;
+          const int x = tl.k0 + kc * SC_KCHUNK;
           tma_load_2d(sa, hi, fb, x, tl.i0);
           tma_load_2d(sa + SC_OP, lo, fb, x, tl.i0);
           if (!diag) {
-            tma_load_2d(sa + 2 * SC_OP, hi, fb, x, tl.j0);
-            tma_load_2d(sa + 3 * SC_OP, lo, fb, x, tl.j0);
+            tma_load_2d(sa + 2 * SC_OP, bhi, fb, x, tl.j0);
+            tma_load_2d(sa + 3 * SC_OP, blo, fb, x, tl.j0);
           }
           if (++stage == SC_STAGES) { stage = 0; phase ^= 1u; }
         }
@@ -277,6 +283,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
       for (int t = blockIdx.x; t < count && ok; t += gridDim.x) {
         const int i0 = tiles[t].i0, j0 = tiles[t].j0, nk = tiles[t].nk;
         const bool diag = i0 == j0;
+        const uint32_t idesc = sc_idesc(tiles[t].ncol <= 64 ? 64u : 128u);
         if (!mbar_wait(smem_u32(&acce_bar[buf]), accphase[buf] ^ 1u, &abort_flag, S.status)) break;
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
         const uint32_t dt = tmem + (uint32_t)buf * 128u;
@@ -291,9 +298,9 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
 #pragma unroll
           for (int kk = 0; kk < SC_KCHUNK / 8; ++kk) {
             const uint32_t o = 32u * kk;   // 8 TF32 columns = 32 bytes along the swizzled row
-            mma_tf32(dt, sw128_desc(ah + o), sw128_desc(bh + o), (kc | kk) != 0);
-            mma_tf32(dt, sw128_desc(al + o), sw128_desc(bh + o), 1u);
-            mma_tf32(dt, sw128_desc(ah + o), sw128_desc(bl + o), 1u);
+            mma_tf32(dt, sw128_desc(ah + o), sw128_desc(bh + o), idesc, (kc | kk) != 0);
+            mma_tf32(dt, sw128_desc(al + o), sw128_desc(bh + o), idesc, 1u);
+            mma_tf32(dt, sw128_desc(ah + o), sw128_desc(bl + o), idesc, 1u);
           }
           mma_commit(smem_u32(&empty_bar[stage]));   // the stage is free once these are done
           if (++stage == SC_STAGES) { stage = 0; phase ^= 1u; }
@@ -319,6 +326,33 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
       const int md = tl.md;
       const int64_t co = tl.co;
       ScTable &T = tbl[b];
+      if (tl.dense) {
+        // d's own columns j0 .. j0 + ncol - 1, one run, row i at position i
+        const int wdd = S.super[tl.d + 1] - S.super[tl.d];
+        const int64_t xp = S.xptr[tl.d];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int c = 4 * lane + q, j = tl.j0 + c;
+          const int64_t cbv = (c < tl.ncol && j < wdd) ? xp + (int64_t)j * md : -1;
+          T.base[c] = cbv;
+          T.slot[c] = cbv >= 0 ? 0 : -1;
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) T.pos[0][lane + 32 * k] = tl.i0 + lane + 32 * k;
+        if (lane == 0) {
+          T.ro[0] = 0;
+          T.rj[0] = tl.j0;
+          T.md = md;
+          T.i0 = tl.i0;
+          T.j0 = tl.j0;
+          T.nslots = 1;
+        }
+        __syncwarp();
+        mbar_arrive(smem_u32(&tblf_bar[b]));
+        tph[b] ^= 1u;
+        b ^= 1;
+        continue;
+      }
       int64_t cb[4];
       int ro[4], fl[4], nf = 0;
 #pragma unroll
@@ -519,16 +553,17 @@ bool build_scatter_maps(const std::vector<int> &super, const std::vector<int64_t
   }
   CUtensorMap *maps = static_cast<CUtensorMap *>(maps_host);
   const int ns = (int)super.size() - 1;
-  for (int d = 0; d < ns; ++d) {
-    if (!used[d]) continue;
+  for (int q = 0; q < 2 * ns; ++q) {
+    const int d = q % ns, rows = q < ns ? 128 : 64;
+    if (!(used[d] & (q < ns ? 1 : 2))) continue;
     const uint64_t w = super[d + 1] - super[d], m = rowptr[d + 1] - rowptr[d];
     const uint64_t wp = (uint64_t)kmirror_pitch_tf32((int)w);
     const cuuint64_t dims[2] = {w, m};
     const cuuint64_t strides[1] = {wp * sizeof(float)};
-    const cuuint32_t box[2] = {SC_KCHUNK, 128};
+    const cuuint32_t box[2] = {SC_KCHUNK, (cuuint32_t)rows};
     const cuuint32_t estr[2] = {1, 1};
     for (int p = 0; p < 2; ++p) {   // hi plane, lo plane (rows outside a plane read zeros)
-      CUresult r = enc(&maps[2 * d + p], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+      CUresult r = enc(&maps[2 * q + p], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
                        Lk + xk[d] + (int64_t)p * m * wp, dims, strides, box, estr,
                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -543,10 +578,14 @@ bool build_scatter_maps(const std::vector<int> &super, const std::vector<int64_t
 }
 
 void launch_scatter_tc(const DevSym &S, const void *maps, const ScTile *tiles, int count,
-                       const ScatterCols &C, cudaStream_t st) {
+                       const ScatterCols &C, int reserve, cudaStream_t st) {
   if (count <= 0) return;
-  k_scatter_tc<<<update_tc_ctas(count), SC_THREADS, SC_SMEM, st>>>(
-      S, static_cast<const CUtensorMap *>(maps), tiles, count, C);
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int ctas = std::max(1, std::min(count, sms - reserve));
+  k_scatter_tc<<<ctas, SC_THREADS, SC_SMEM, st>>>(S, static_cast<const CUtensorMap *>(maps), tiles,
+                                                  count, C);
 }
 
 void launch_scatter_small(const DevSym &S, const int2 *tasks, int count, const ScatterCols &C,
