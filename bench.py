@@ -389,19 +389,54 @@ def run_ours(args, rank, world, local_rank):
     la, kms, kfl, kby = kinds[dom]
     peak64 = fp64_gemm_peak(torch, dev) if rank == 0 else None
     bf16 = mode == swc.SWC_MODE_MIXED_BF16X3
+    tf32 = mode == swc.SWC_MODE_MIXED_TF32X3
     peak32 = tf32_gemm_peak(torch, dev, bf16) if rank == 0 and mixed else None
-    # the trailing SYRK steps run in FP64 (DMMA) in every mode by default
-    if mixed and dom == "update":
-        if bf16:
-            peak, psrc = peak32 / 8.0, ("cuBLAS BF16 GEMM 8192^3 measured in this run, divided by 8 "
-                                        "(a BF16x3 product executes eight BF16 piece products on "
-                                        "tcgen05: [hi;mid][hi;mid]^T and [lo;hi][lo;hi]^T)")
-        else:
-            peak, psrc = peak32 / 3.0, ("cuBLAS TF32 GEMM 8192^3 measured in this run, divided by 3 "
-                                        "(a split-TF32 product executes three TF32 piece products "
-                                        "on tcgen05: hi hi' + lo hi' + hi lo')")
+    src64 = "FP64 cuBLAS DGEMM 8192^3 measured in this run"
+    src_tf32 = ("cuBLAS TF32 GEMM 8192^3 measured in this run, divided by 3 (a split-TF32 product "
+                "executes three TF32 piece products on tcgen05: hi hi' + lo hi' + hi lo')")
+    src_bf16 = ("cuBLAS BF16 GEMM 8192^3 measured in this run, divided by 8 (a BF16x3 product "
+                "executes eight BF16 piece products on tcgen05: [hi;mid][hi;mid]^T and "
+                "[lo;hi][lo;hi]^T)")
+    # per compute class: its kernel(s) and the peak of the arithmetic it runs in this mode
+    # (split-TF32 mode: descendant updates and trailing SYRK steps on tcgen05; BF16x3 mode:
+    # descendant updates on tcgen05, SYRK in FP64; the panel chain always FP64)
+    if tf32:
+        cls_kernel = {"update": ("k_scatter_tc", peak32 / 3.0, src_tf32),
+                      "syrk": ("k_scatter_tc", peak32 / 3.0, src_tf32)}
+    elif bf16:
+        cls_kernel = {"update": ("k_update_tc", peak32 / 8.0, src_bf16),
+                      "syrk": ("k_syrk_step", peak64, src64)}
     else:
-        peak, psrc = peak64, "FP64 cuBLAS DGEMM 8192^3 measured in this run"
+        cls_kernel = {"update": ("k_update_tiles", peak64, src64),
+                      "syrk": ("k_syrk_step", peak64, src64)}
+    cls_kernel["panel"] = ("k_diag_step + k_trsm_step", peak64, src64)
+    cls_kernel["small"] = ("k_factor_small*", peak64, src64)
+    # the dominant kernel: classes grouped by the kernel that runs them (the split-TF32 scatter
+    # kernel runs both the descendant updates and the trailing SYRK steps); the panel class is
+    # two kernels (TRSM, diagonal block) of about equal share
+    groups = {}
+    for k in ("update", "syrk", "panel", "small"):
+        kn = cls_kernel[k][0]
+        g = groups.setdefault(kn, {"classes": [], "ms": 0.0, "flops": 0.0, "launches": 0})
+        g["classes"].append(k)
+        g["ms"] += kinds[k][1]
+        g["flops"] += kinds[k][2]
+        g["launches"] += kinds[k][0]
+    kname = max(groups, key=lambda kn: groups[kn]["ms"] / (2.0 if kn.startswith("k_diag") else 1.0))
+    dom = "+".join(groups[kname]["classes"])
+    la, kms, kfl = groups[kname]["launches"], groups[kname]["ms"], groups[kname]["flops"]
+    peak, psrc = {cls_kernel[k][0]: cls_kernel[k][1:] for k in cls_kernel}[kname]
+    rooflines = {}
+    for k in ("update", "syrk", "panel"):
+        lk, mk, fk, _ = kinds[k]
+        kn, pk, ps = cls_kernel[k]
+        if mk > 0 and pk:
+            ach = fk / (mk * 1e-3) / 1e12
+            tr = profile_traffic(kn, args.workload) if rank == 0 else None
+            rooflines[k] = {"kernel": kn, "launches": lk, "ms": round(mk, 4),
+                            "achieved": round(ach, 4), "peak": round(pk, 3), "unit": "TFLOP/s",
+                            "frac": round(ach / pk, 4), "peak_source": ps,
+                            "traffic_bytes_per_launch": tr}
     hbm, hbm_src = hbm_peak()
     # HBM-bound classes: algorithmic bytes (plan builder) / device time of the class
     hbm_classes = {}
@@ -488,8 +523,6 @@ def run_ours(args, rank, world, local_rank):
 
     if rank == 0:
         achieved = kfl / (kms * 1e-3) / 1e12
-        kname = {"update": ("k_update_tc" if bf16 else "k_scatter_tc") if mixed
-                 else "k_update_tiles", "syrk": "k_syrk_step"}.get(dom)
         traffic = profile_traffic(kname, args.workload) if kname else None
         tsrc = (f"dram__bytes_read.sum + dram__bytes_write.sum per launch, ncu capture summarised "
                 f"in profiles/{kname}_{args.workload}.md" if traffic else None)
@@ -526,7 +559,8 @@ def run_ours(args, rank, world, local_rank):
                      "xsize_over_nnz_L": round(P.xsize / nnzl, 4) if nnzl else None,
                      "note": "executed flops: the plan builder's per-class flop model of one "
                              "factorization on the relaxed structure (tile padding excluded)"},
-            "roofline": {"bound": "tensor", "kernel": dom, "achieved": round(achieved, 4),
+            "roofline": {"bound": "tensor", "class": dom, "kernel": kname,
+                         "achieved": round(achieved, 4),
                          "peak": round(peak, 3) if peak else None, "unit": "TFLOP/s",
                          "frac": round(achieved / peak, 4) if peak else None,
                          "traffic": traffic, "traffic_source": tsrc, "peak_source": psrc,
@@ -539,7 +573,7 @@ def run_ours(args, rank, world, local_rank):
                          "classes_fp64": ({k: {"ms": round(v[1], 4)} for k, v in prof64.items()}
                                           if prof64 else None),
                          "hbm_classes": hbm_classes, "hbm_peak_gbs": hbm,
-                         "hbm_peak_source": hbm_src},
+                         "hbm_peak_source": hbm_src, "rooflines": rooflines},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(per_step * args.steps),

@@ -399,7 +399,8 @@ class Handle:
     def set_plan(self, plan: int):
         """Execution-plan candidate for the next analyze / batch_analyze (0 default, 1 larger
         persistent supernodes, 2 no persistent walk, 3 smaller small class, 4 dense steps
-        as one dataflow launch per level, 5 FP64 trailing SYRK steps in split-TF32 mode)."""
+        as one dataflow launch per level, 5 FP64 trailing SYRK steps in split-TF32 mode, 6 and
+        7 tile-owner descendant updates in split-TF32 mode, staged by TMA or cp.async)."""
         _check(self._lib.swc_set_plan(self._h, int(plan)))
 
     def set_wait_budget(self, polls: int = -1):
