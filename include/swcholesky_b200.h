@@ -39,11 +39,10 @@ extern "C" {
                                    over the column blocks of one trailing update), added to L
                                    in FP64; POTRF, TRSM and small supernodes in FP64.  Pair
                                    with swc_refine. */
-#define SWC_MODE_MIXED_BF16X3 2 /* the descendant updates as BF16x3 split products on tcgen05:
-                                   each value as three bfloat16 pieces, the six piece products
-                                   down to the third order, FP32 accumulation per group of
-                                   descendants, FP64 across groups (about FP32 accuracy); the
-                                   trailing updates in FP64 */
+#define SWC_MODE_MIXED_BF16X3 2 /* the same Schur updates as BF16x3 split products on
+                                   tcgen05: each value as three bfloat16 pieces, the six piece
+                                   products down to the third order (about FP32 accuracy),
+                                   FP32 accumulation, added to L in FP64 */
 
 typedef struct swc_handle *swc_handle_t;
 
@@ -86,11 +85,11 @@ void *swc_get_stream(swc_handle_t handle);
  * walk up to 100 KB of shared memory per supernode; 2: no persistent walk (one launch per
  * level); 3: smaller small-class limits (more tiled supernodes); 4: the dense
  * factorization of each level's tiled supernodes as one persistent dataflow launch
- * instead of three launches per 64-column step; 5: in SWC_MODE_MIXED_TF32X3, the trailing
- * SYRK steps of the dense factorization in FP64 (DMMA) instead of split-TF32 tcgen05
- * tiles; 6 and 7: in SWC_MODE_MIXED_TF32X3, the descendant updates by the tile-owner
- * gather kernel (operands staged by TMA gather4 loads, 6, or by cp.async, 7) instead of
- * the right-looking dense products with an FP64 atomic scatter, and the trailing SYRK
+ * instead of three launches per 64-column step; 5: in the mixed modes, the trailing SYRK
+ * steps of the dense factorization in FP64 (DMMA) instead of split tcgen05 tiles; 6 and 7:
+ * in the mixed modes, the descendant updates by the tile-owner gather kernel (split-TF32
+ * operands staged by TMA gather4 loads, 6, or by cp.async, 7; BF16x3 by cp.async) instead
+ * of the right-looking dense products with an FP64 atomic scatter, and the trailing SYRK
  * steps in FP64.  SWC_INVALID_INPUT for other values. */
 int swc_set_plan(swc_handle_t handle, int plan);
 

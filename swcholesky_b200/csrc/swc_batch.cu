@@ -109,9 +109,9 @@ Tuning plan_candidate(int k) {
     case 2: t.persist = 0; break;                        // level-by-level launches only
     case 3: t.small_max_elems = 4096; t.small_max_m = 1024; break;   // more tiled supernodes
     case 4: t.dense_dataflow = 1; break;                 // dense steps as one dataflow launch
-    case 5: t.syrk_fp64 = 1; break;                      // split-TF32: FP64 SYRK steps
-    case 6: t.scatter = 0; t.tc_tma = 1; break;          // split-TF32: tile-owner updates, TMA
-    case 7: t.scatter = 0; break;                        // split-TF32: tile-owner, cp.async
+    case 5: t.syrk_fp64 = 1; break;                      // mixed modes: FP64 SYRK steps
+    case 6: t.scatter = 0; t.tc_tma = 1; break;          // mixed: tile-owner updates (TMA for TF32)
+    case 7: t.scatter = 0; break;                        // mixed: tile-owner, cp.async
     default: break;
   }
   return t;
@@ -282,9 +282,9 @@ bool BatchState::autotune(Engine &eng, const double *d_values, int mixed, const 
     if (ok && ms < best) { best = ms; bp = p; bl = 0; }
   }
   // stage 2: plan, best partition (only the plans that change something in this mode:
-  // 5 to 7 apply to the split-TF32 mode)
+  // 5 to 7 apply to the mixed modes, 6 differs from 7 in the split-TF32 mode only)
   for (int k = 1; k < kNumPlans && ok; ++k) {
-    if (k >= 5 && mode != 1) continue;
+    if ((k >= 5 && mode == 0) || (k == 6 && mode != 1)) continue;
     double ms;
     ok = measure(bp, k, ms);
     if (ok && ms < best) { best = ms; bl = k; }

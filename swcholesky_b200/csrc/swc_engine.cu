@@ -156,6 +156,7 @@ void Engine::release() {
                   d_tiny_, d_dense_tasks_, d_dense_toff_, d_dense_ver_, d_swarp_,
                   d_Lk_, d_xk_, d_xk16_, d_tmaps_, d_tc_pairs_, d_syrk_pairs_, d_syrk_end_,
                   d_sc_tiles_, d_sc_base_, d_sc_coff_, d_sc_rel_, d_sc_relidx_, d_sc_maps_,
+                  d_sc_maps16_,
                   d_sc_small_, d_sc_dense_};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -192,7 +193,7 @@ void Engine::release() {
   d_sc_dense_ = nullptr;
   d_sc_base_ = d_sc_coff_ = nullptr;
   d_sc_rel_ = d_sc_relidx_ = nullptr;
-  d_sc_maps_ = nullptr;
+  d_sc_maps_ = d_sc_maps16_ = nullptr;
   kmirror_len_ = 0;
   tiny_ctas_ = 0;
   d_npart_ = nullptr;
@@ -971,13 +972,18 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec
   const int variant = prec == 2 ? UT_VARIANT_BF16
                                 : (tuning_.tc_tma ? UT_VARIANT_TF32_TMA : UT_VARIANT_TF32);
   cudaStream_t st = stream_;
-  // the trailing updates of the dense steps: split-TF32 dense tiles of the scatter kernel
-  // (two SMs left to the concurrent diagonal-block kernel), else FP64
-  const bool syrk_tc = prec == 1 && !tuning_.syrk_fp64 && !plan_.sc_coff.empty();
+  // mixed modes: right-looking descendant updates through the scatter kernel (tensor maps
+  // of the mode's mirror format), unless a tile-owner plan (split-TF32 plans 6, 7) is set
+  const bool scatter = prec != 0 && !plan_.sc_coff.empty();
+  const bool bf16 = prec == 2;
+  void *sc_maps = bf16 ? d_sc_maps16_ : d_sc_maps_;
+  // the trailing updates of the dense steps: split dense tiles of the scatter kernel (two
+  // SMs left to the concurrent diagonal-block kernel), else FP64
+  const bool syrk_tc = scatter && !tuning_.syrk_fp64;
   auto syrk = [&](const Wave &W, int j) {
     if (syrk_tc)
-      launch_scatter_tc(sym_, d_sc_maps_, d_sc_dense_ + W.scd_off[j], W.scd_cnt[j], scatter_cols(),
-                        2, st);
+      launch_scatter_tc(sym_, sc_maps, d_sc_dense_ + W.scd_off[j], W.scd_cnt[j], scatter_cols(),
+                        2, bf16, st);
     else
       launch_syrk_step(sym_, d_syrk_ + W.syrk_off[j], d_syrk_pairs_, W.syrk_cnt[j], st);
   };
@@ -989,9 +995,8 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec
     cudaEventRecord(ev, st);
     prof->emplace_back(kind, ev);
   };
-  // split-TF32 mode with right-looking updates: contributions reach a target from the level
-  // after each descendant's, so every tiled panel is assembled up front
-  const bool scatter = prec == 1 && !plan_.sc_coff.empty();
+  // right-looking updates: contributions reach a target from the level after each
+  // descendant's, so every tiled panel is assembled up front
   const ScatterCols sc_cols = scatter_cols();
   mark(K_MEMSET, 1);
   cudaMemsetAsync(dL_, 0, sizeof(double) * xsize_, st);
@@ -1027,7 +1032,7 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec
       launch_scatter_small(sym_, d_sc_small_ + W.scs_off, W.scs_cnt, sc_cols, st);
       mark(-1, W.scs_cnt);
       mark(K_UPDATE, W.sc_cnt);
-      launch_scatter_tc(sym_, d_sc_maps_, d_sc_tiles_ + W.sc_off, W.sc_cnt, sc_cols, 0, st);
+      launch_scatter_tc(sym_, sc_maps, d_sc_tiles_ + W.sc_off, W.sc_cnt, sc_cols, 0, bf16, st);
       mark(-1, W.sc_cnt);
     } else {
     mark(K_ASSEMBLE, W.asm_cnt);
@@ -1098,13 +1103,15 @@ bool Engine::set_mode(int prec, std::string &err) {
       return false;
     }
     if (!build_tensor_maps(hsym_.super, hsym_.rowptr, h_xk_, d_Lk_, maps.data(), err)) return false;
-    if (!plan_.sc_coff.empty()) {   // hi / lo plane maps of the right-looking update tiles
-      std::vector<unsigned char> sm(4 * mb, 0);
-      if (!build_scatter_maps(hsym_.super, hsym_.rowptr, h_xk_, plan_.sc_used, d_Lk_, sm.data(),
-                              err))
+    for (int f = 0; f < 2 && !plan_.sc_coff.empty(); ++f) {
+      // plane maps of the right-looking update tiles, split-TF32 (f = 0) and BF16x3 layouts
+      std::vector<unsigned char> sm(tensor_map_bytes() * scatter_maps_count(nsuper_, f == 1), 0);
+      if (!build_scatter_maps(hsym_.super, hsym_.rowptr, h_xk_, plan_.sc_used, d_Lk_, f == 1,
+                              sm.data(), err))
         return false;
-      e = cudaMalloc(&d_sc_maps_, sm.size());
-      if (e == cudaSuccess) e = cudaMemcpy(d_sc_maps_, sm.data(), sm.size(), cudaMemcpyHostToDevice);
+      void *&dst = f ? d_sc_maps16_ : d_sc_maps_;
+      e = cudaMalloc(&dst, sm.size());
+      if (e == cudaSuccess) e = cudaMemcpy(dst, sm.data(), sm.size(), cudaMemcpyHostToDevice);
       if (e != cudaSuccess) {
         err = std::string("scatter tensor maps: ") + cudaGetErrorString(e);
         return false;

@@ -140,7 +140,7 @@ struct Plan {
   double sc_flops = 0;               // executed flops of the tiles (128x128 blocks)
   int persist_smem = 0;
   int launches = 0;  // kernel launches per factorization
-  int launches_scatter = 0;  // the same in the split-TF32 mode with right-looking updates
+  int launches_scatter = 0;  // the same in the mixed modes with right-looking updates
   KernelStats work;  // algorithmic flops/bytes per kernel class
 };
 
@@ -272,7 +272,7 @@ class Engine {
   double *device_L() const { return dL_; }
   // kernel launches of one factorization in the given mode
   int launches_per_factor(int prec = 0) const {
-    return prec == 1 ? plan_.launches_scatter : plan_.launches;
+    return prec != 0 ? plan_.launches_scatter : plan_.launches;
   }
 
   // Adjoint (swc_adjoint.cu), on the current factor; device pointers, grad has one entry
@@ -345,7 +345,8 @@ class Engine {
   ScTile *d_sc_dense_ = nullptr;
   int64_t *d_sc_base_ = nullptr, *d_sc_coff_ = nullptr;
   int *d_sc_rel_ = nullptr, *d_sc_relidx_ = nullptr;
-  void *d_sc_maps_ = nullptr;                  // four tensor maps per supernode (over d_Lk_)
+  void *d_sc_maps_ = nullptr;                  // tensor maps of the mirror's planes (over
+  void *d_sc_maps16_ = nullptr;                //   d_Lk_): split-TF32 and BF16x3 layouts
   ScatterCols scatter_cols() const { return {d_sc_base_, d_sc_rel_, d_sc_coff_, d_sc_relidx_}; }
   bool use_graph_ = true;
   Tuning tuning_;
@@ -430,16 +431,17 @@ void launch_update_tc(const DevSym &S, const void *maps, const int4 *tasks, cons
 
 // Right-looking split-TF32 updates (swc_scatter_tc.cu): ScatterCols, ScTile above.
 bool scatter_tc_configure(std::string &err);
-// tensor maps over the K-major split mirror, 4 nsuper entries: [2 d], [2 d + 1] the hi and lo
-// planes of supernode d with 128-row boxes (used[d] & 1), [2 (nsuper + d)] and + 1 the same
-// with 64-row boxes (used[d] & 2)
+// tensor maps over the K-major split mirror (scatter_maps_count entries): plane p (TF32: hi,
+// lo; BF16x3: hi, mid, lo) of supernode d at [(box * planes + p) * nsuper + d], box 0 with
+// 128-row boxes (used[d] & 1), box 1 with 64-row boxes (used[d] & 2)
+size_t scatter_maps_count(int nsuper, bool bf16);
 bool build_scatter_maps(const std::vector<int> &super, const std::vector<int64_t> &rowptr,
                         const std::vector<int64_t> &xk, const std::vector<char> &used, float *Lk,
-                        void *maps_host, std::string &err);
+                        bool bf16, void *maps_host, std::string &err);
 // reserve: SMs left free for a kernel running at the same time (the diagonal-block kernel
-// of the dense steps)
+// of the dense steps); bf16: the mirror holds BF16x3 planes (else split-TF32)
 void launch_scatter_tc(const DevSym &S, const void *maps, const ScTile *tiles, int count,
-                       const ScatterCols &C, int reserve, cudaStream_t st);
+                       const ScatterCols &C, int reserve, bool bf16, cudaStream_t st);
 // Small contributions (a descendant whose rows from c0 number at most 128 and whose width
 // times those rows, rounded up to 32, is at most SC_SMALL_ELEMS): one CTA per (d, c0) task,
 // FP64 products from L on the CUDA cores, the same atomic scatter.

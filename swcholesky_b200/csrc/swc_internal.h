@@ -96,12 +96,12 @@ struct Tuning {
   int dense_dataflow = 0;                // dense steps of a wave: one dataflow launch (else
                                          // three launches per 64-column step)
   int dense_group = 4;                   // column blocks per grouped trailing update
-  int syrk_fp64 = 0;                     // split-TF32 mode: trailing SYRK steps in FP64
-                                         // (DMMA) instead of split-TF32 dense tiles of the
-                                         // scatter kernel (the BF16x3 mode keeps FP64)
+  int syrk_fp64 = 0;                     // mixed modes: trailing SYRK steps in FP64 (DMMA)
+                                         // instead of split dense tiles of the scatter
+                                         // kernel
   int tc_tma = 0;                        // split-TF32 tile-owner tcgen05 updates: stage
                                          // operands with TMA gather4 loads, not cp.async
-  int scatter = 1;                       // split-TF32 mode: right-looking updates (dense
+  int scatter = 1;                       // mixed modes: right-looking updates (dense
                                          // 128x128 tiles, FP64 atomic scatter) instead of
                                          // the tile-owner gather
 };

@@ -55,31 +55,49 @@ namespace swc {
 
 namespace {
 
-constexpr int SC_STAGES = 3;
 constexpr int SC_KCHUNK = 32;                 // K columns per stage
-constexpr int SC_OP = 128 * 128;              // bytes of one operand chunk (128 rows x 128 B)
-constexpr int SC_STAGE = 4 * SC_OP;           // A hi, A lo, B hi, B lo
-constexpr int SC_SMEM = SC_STAGES * SC_STAGE + 1024;   // + alignment slack
+constexpr int SC_MAX_STAGES = 4;
 constexpr int SC_EPI_WARPS = 16;              // epilogue: (row quarter, 32-column group)
 constexpr int SC_PRODUCER = 16, SC_MMA = 17, SC_TABLE = 18;   // warps of the other roles
 constexpr int SC_THREADS = 32 * 19;
 constexpr int SC_TMEM_COLS = 256;             // two 128-column FP32 accumulators
 constexpr unsigned long long SC_WAIT_NS = 2000000000ULL;
-// Instruction descriptor: D F32 (bit 4), A and B TF32 (2 at bits 7 and 10), K-major, N >> 3
-// at bit 17, M >> 4 at bit 24; M = 128, N = 128 or 64.
-__host__ __device__ constexpr uint32_t sc_idesc(uint32_t n) {
-  return (1u << 4) | (2u << 7) | (2u << 10) | ((n >> 3) << 17) | ((128u >> 4) << 24);
+// The two split formats (the mirror's format entry): per format the planes of a value, the
+// bytes of a 32-column row chunk (= its swizzle span: 128-byte swizzle for TF32, 64-byte for
+// bfloat16), the stages of the ring, the MMA kind's operand format and the products per K
+// step (TF32: K = 8, hi hi' + lo hi' + hi lo'; BF16x3: K = 16, the six products down to the
+// third order).  A stage holds the A planes, then the B planes, each 128 rows x ROW bytes.
+template <bool BF16>
+struct Sc {
+  static constexpr int PLANES = BF16 ? 3 : 2;
+  static constexpr int ROW = SC_KCHUNK * (BF16 ? 2 : 4);
+  static constexpr int OP = 128 * ROW;
+  static constexpr int STAGE = 2 * PLANES * OP;
+  static constexpr int STAGES = BF16 ? 4 : 3;
+  static constexpr int SBO = 8 * ROW;                 // bytes between 8-row groups
+  static constexpr uint64_t LAYOUT = BF16 ? 4 : 2;    // SWIZZLE_64B / SWIZZLE_128B
+  static constexpr uint32_t FMT = BF16 ? 1 : 2;       // BF16 / TF32 operands
+  static constexpr int KSTEP = BF16 ? 16 : 8;         // K of one MMA
+};
+constexpr int SC_SMEM = 3 * 4 * 128 * 128 + 1024;   // either format: 192 KB of stages + slack
+static_assert(Sc<false>::STAGES * Sc<false>::STAGE + 1024 <= SC_SMEM, "TF32 ring fits");
+static_assert(Sc<true>::STAGES * Sc<true>::STAGE + 1024 <= SC_SMEM, "BF16x3 ring fits");
+
+// Instruction descriptor: D F32 (bit 4), A and B format at bits 7 and 10 (TF32 2, BF16 1),
+// K-major, N >> 3 at bit 17, M >> 4 at bit 24; M = 128, N = 128 or 64.
+__host__ __device__ constexpr uint32_t sc_idesc(uint32_t fmt, uint32_t n) {
+  return (1u << 4) | (fmt << 7) | (fmt << 10) | ((n >> 3) << 17) | ((128u >> 4) << 24);
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-// K-major operand with the 128-byte swizzle: 8-row groups 1024 bytes apart, version 1,
-// layout type 2.
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
-  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
-         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+// K-major swizzled operand: 8-row groups sbo bytes apart, leading offset 16 (unused by the
+// swizzled K-major layouts), version 1, the layout type of the swizzle.
+__device__ __forceinline__ uint64_t sw_desc(uint32_t saddr, uint32_t sbo, uint64_t layout) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) |
+         ((uint64_t)1 << 46) | (layout << 61);
 }
 
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
@@ -153,13 +171,21 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map
       : "memory");
 }
 
-__device__ __forceinline__ void mma_tf32(uint32_t tmem, uint64_t adesc, uint64_t bdesc,
-                                         uint32_t idesc, uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
-          tmem),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+template <bool BF16>
+__device__ __forceinline__ void mma_split(uint32_t tmem, uint64_t adesc, uint64_t bdesc,
+                                          uint32_t idesc, uint32_t accumulate) {
+  if (BF16)
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+            tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+  else
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+            tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
 }
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
   asm volatile(
@@ -197,11 +223,14 @@ struct ScTable {
   int md, i0, j0, nslots;
 };
 
+template <bool BF16>
 __global__ void __launch_bounds__(SC_THREADS, 1)
     k_scatter_tc(DevSym S, const CUtensorMap *__restrict__ maps, const ScTile *__restrict__ tiles,
                  int count, ScatterCols C) {
+  using F = Sc<BF16>;
+  constexpr int NP = F::PLANES;
   extern __shared__ unsigned char sc_dyn[];
-  __shared__ __align__(8) uint64_t full_bar[SC_STAGES], empty_bar[SC_STAGES];
+  __shared__ __align__(8) uint64_t full_bar[SC_MAX_STAGES], empty_bar[SC_MAX_STAGES];
   __shared__ __align__(8) uint64_t accf_bar[2], acce_bar[2], tblf_bar[2], tble_bar[2], done_bar;
   __shared__ __align__(16) ScTable tbl[2];
   __shared__ uint32_t tmem_base;
@@ -216,7 +245,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
   }
   if (tid == 32 * SC_MMA) {
-    for (int s = 0; s < SC_STAGES; ++s) {
+    for (int s = 0; s < F::STAGES; ++s) {
       mbar_init(smem_u32(&full_bar[s]), 1);
       mbar_init(smem_u32(&empty_bar[s]), 1);
     }
@@ -238,39 +267,39 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
   if (warp == SC_PRODUCER) {
     // ------------------------------ TMA producer ------------------------------
     if (lane == 0) {
-      int stage = 0, armed[SC_STAGES];
+      int stage = 0, armed[SC_MAX_STAGES];
       uint32_t phase = 0;
-      for (int s = 0; s < SC_STAGES; ++s) armed[s] = 0;
+      for (int s = 0; s < SC_MAX_STAGES; ++s) armed[s] = 0;
       bool ok = true;
+      const int ns = S.nsuper;
       for (int t = blockIdx.x; t < count && ok; t += gridDim.x) {
         const ScTile tl = tiles[t];
-        const CUtensorMap *hi = maps + 2 * tl.d, *lo = hi + 1;
-        // B: 128-row boxes, or 64-row boxes for a tile of at most 64 columns
+        // maps: plane p of supernode d at [(box * NP + p) * nsuper + d], box 0: 128 rows,
+        // box 1: 64 rows (B of a tile of at most 64 columns)
         const bool narrow = tl.ncol <= 64;
-        const CUtensorMap *bhi = narrow ? maps + 2 * (S.nsuper + tl.d) : hi, *blo = bhi + 1;
+        const CUtensorMap *amap = maps + tl.d, *bmap = maps + (narrow ? NP : 0) * ns + tl.d;
         const bool diag = tl.i0 == tl.j0;   // B = the first ncol rows of A
-        const uint32_t bytes = 2 * SC_OP + (diag ? 0 : (narrow ? SC_OP : 2 * SC_OP));
+        const uint32_t bytes = NP * F::OP + (diag ? 0 : NP * (narrow ? F::OP / 2 : F::OP));
         for (int kc = 0; kc < tl.nk; ++kc) {
           if (!mbar_wait(smem_u32(&empty_bar[stage]), phase ^ 1u, &abort_flag, S.status)) {
             ok = false;
             break;
           }
           const uint32_t fb = smem_u32(&full_bar[stage]);
-          const uint32_t sa = sbase + stage * SC_STAGE;
+          const uint32_t sa = sbase + stage * F::STAGE;
           mbar_arrive_tx(fb, bytes);
           armed[stage] += 1;
           const int x = tl.k0 + kc * SC_KCHUNK;
-          tma_load_2d(sa, hi, fb, x, tl.i0);
-          tma_load_2d(sa + SC_OP, lo, fb, x, tl.i0);
-          if (!diag) {
-            tma_load_2d(sa + 2 * SC_OP, bhi, fb, x, tl.j0);
-            tma_load_2d(sa + 3 * SC_OP, blo, fb, x, tl.j0);
+#pragma unroll
+          for (int p = 0; p < NP; ++p) {
+            tma_load_2d(sa + p * F::OP, amap + p * ns, fb, x, tl.i0);
+            if (!diag) tma_load_2d(sa + (NP + p) * F::OP, bmap + p * ns, fb, x, tl.j0);
           }
-          if (++stage == SC_STAGES) { stage = 0; phase ^= 1u; }
+          if (++stage == F::STAGES) { stage = 0; phase ^= 1u; }
         }
       }
       // loads in flight land before the CTA leaves
-      for (int s = 0; s < SC_STAGES; ++s)
+      for (int s = 0; s < F::STAGES; ++s)
         if (armed[s] > 0) mbar_drain(smem_u32(&full_bar[s]), (uint32_t)(armed[s] - 1) & 1u, S.status);
     }
     __syncwarp();
@@ -283,7 +312,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
       for (int t = blockIdx.x; t < count && ok; t += gridDim.x) {
         const int i0 = tiles[t].i0, j0 = tiles[t].j0, nk = tiles[t].nk;
         const bool diag = i0 == j0;
-        const uint32_t idesc = sc_idesc(tiles[t].ncol <= 64 ? 64u : 128u);
+        const uint32_t idesc = sc_idesc(F::FMT, tiles[t].ncol <= 64 ? 64u : 128u);
         if (!mbar_wait(smem_u32(&acce_bar[buf]), accphase[buf] ^ 1u, &abort_flag, S.status)) break;
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
         const uint32_t dt = tmem + (uint32_t)buf * 128u;
@@ -293,17 +322,35 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
             break;
           }
           asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-          const uint32_t ah = sbase + stage * SC_STAGE, al = ah + SC_OP;
-          const uint32_t bh = diag ? ah : ah + 2 * SC_OP, bl = diag ? al : ah + 3 * SC_OP;
+          // plane p of A at a[p], of B at b[p] (B = A for a diagonal tile)
+          const uint32_t a0 = sbase + stage * F::STAGE;
+          uint32_t a[NP], b[NP];
 #pragma unroll
-          for (int kk = 0; kk < SC_KCHUNK / 8; ++kk) {
-            const uint32_t o = 32u * kk;   // 8 TF32 columns = 32 bytes along the swizzled row
-            mma_tf32(dt, sw128_desc(ah + o), sw128_desc(bh + o), idesc, (kc | kk) != 0);
-            mma_tf32(dt, sw128_desc(al + o), sw128_desc(bh + o), idesc, 1u);
-            mma_tf32(dt, sw128_desc(ah + o), sw128_desc(bl + o), idesc, 1u);
+          for (int p = 0; p < NP; ++p) {
+            a[p] = a0 + p * F::OP;
+            b[p] = diag ? a[p] : a0 + (NP + p) * F::OP;
+          }
+#pragma unroll
+          for (int kk = 0; kk < SC_KCHUNK / F::KSTEP; ++kk) {
+            const uint32_t o = 32u * kk;   // one MMA's K = 32 bytes along the swizzled row
+            auto mma = [&](int pa, int pb, uint32_t acc) {
+              mma_split<BF16>(dt, sw_desc(a[pa] + o, F::SBO, F::LAYOUT),
+                              sw_desc(b[pb] + o, F::SBO, F::LAYOUT), idesc, acc);
+            };
+            mma(0, 0, (kc | kk) != 0);   // hi hi'
+            if (BF16) {                  // planes hi, mid, lo
+              mma(0, 1, 1u);
+              mma(1, 0, 1u);
+              mma(1, 1, 1u);
+              mma(0, 2, 1u);
+              mma(2, 0, 1u);
+            } else {                     // planes hi, lo
+              mma(1, 0, 1u);
+              mma(0, 1, 1u);
+            }
           }
           mma_commit(smem_u32(&empty_bar[stage]));   // the stage is free once these are done
-          if (++stage == SC_STAGES) { stage = 0; phase ^= 1u; }
+          if (++stage == F::STAGES) { stage = 0; phase ^= 1u; }
         }
         if (!ok) break;
         mma_commit(smem_u32(&accf_bar[buf]));          // the tile's product: to the epilogue
@@ -534,8 +581,11 @@ EncodeTiled encode_fn() {
 }  // namespace
 
 bool scatter_tc_configure(std::string &err) {
-  cudaError_t e =
-      cudaFuncSetAttribute(k_scatter_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, SC_SMEM);
+  cudaError_t e = cudaFuncSetAttribute(k_scatter_tc<false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, SC_SMEM);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_scatter_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             SC_SMEM);
   if (e != cudaSuccess) {
     err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e);
     return false;
@@ -543,49 +593,58 @@ bool scatter_tc_configure(std::string &err) {
   return true;
 }
 
+size_t scatter_maps_count(int nsuper, bool bf16) { return (size_t)2 * (bf16 ? 3 : 2) * nsuper; }
+
 bool build_scatter_maps(const std::vector<int> &super, const std::vector<int64_t> &rowptr,
                         const std::vector<int64_t> &xk, const std::vector<char> &used, float *Lk,
-                        void *maps_host, std::string &err) {
+                        bool bf16, void *maps_host, std::string &err) {
   EncodeTiled enc = encode_fn();
   if (!enc) {
     err = "cuTensorMapEncodeTiled is not available from the driver";
     return false;
   }
   CUtensorMap *maps = static_cast<CUtensorMap *>(maps_host);
-  const int ns = (int)super.size() - 1;
-  for (int q = 0; q < 2 * ns; ++q) {
-    const int d = q % ns, rows = q < ns ? 128 : 64;
-    if (!(used[d] & (q < ns ? 1 : 2))) continue;
-    const uint64_t w = super[d + 1] - super[d], m = rowptr[d + 1] - rowptr[d];
-    const uint64_t wp = (uint64_t)kmirror_pitch_tf32((int)w);
-    const cuuint64_t dims[2] = {w, m};
-    const cuuint64_t strides[1] = {wp * sizeof(float)};
-    const cuuint32_t box[2] = {SC_KCHUNK, (cuuint32_t)rows};
-    const cuuint32_t estr[2] = {1, 1};
-    for (int p = 0; p < 2; ++p) {   // hi plane, lo plane (rows outside a plane read zeros)
-      CUresult r = enc(&maps[2 * q + p], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
-                       Lk + xk[d] + (int64_t)p * m * wp, dims, strides, box, estr,
-                       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                       CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-      if (r != CUDA_SUCCESS) {
-        err = "cuTensorMapEncodeTiled failed for supernode " + std::to_string(d) + " (code " +
-              std::to_string((int)r) + ")";
-        return false;
+  const int ns = (int)super.size() - 1, np = bf16 ? 3 : 2, esz = bf16 ? 2 : 4;
+  for (int box = 0; box < 2; ++box)
+    for (int d = 0; d < ns; ++d) {
+      if (!(used[d] & (box == 0 ? 1 : 2))) continue;
+      const uint64_t w = super[d + 1] - super[d], m = rowptr[d + 1] - rowptr[d];
+      const uint64_t wp = (uint64_t)(bf16 ? kmirror_pitch_bf16((int)w) : kmirror_pitch_tf32((int)w));
+      const cuuint64_t dims[2] = {w, m};
+      const cuuint64_t strides[1] = {wp * esz};
+      const cuuint32_t boxdim[2] = {SC_KCHUNK, (cuuint32_t)(box == 0 ? 128 : 64)};
+      const cuuint32_t estr[2] = {1, 1};
+      // planes hi, (mid,) lo of m rows each (rows outside a plane read zeros)
+      unsigned char *base = reinterpret_cast<unsigned char *>(Lk + xk[d]);
+      for (int p = 0; p < np; ++p) {
+        CUresult r = enc(&maps[(size_t)(box * np + p) * ns + d],
+                         bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                         2, base + (size_t)p * m * wp * esz, dims, strides, boxdim, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         bf16 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) {
+          err = "cuTensorMapEncodeTiled failed for supernode " + std::to_string(d) + " (code " +
+                std::to_string((int)r) + ")";
+          return false;
+        }
       }
     }
-  }
   return true;
 }
 
 void launch_scatter_tc(const DevSym &S, const void *maps, const ScTile *tiles, int count,
-                       const ScatterCols &C, int reserve, cudaStream_t st) {
+                       const ScatterCols &C, int reserve, bool bf16, cudaStream_t st) {
   if (count <= 0) return;
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int ctas = std::max(1, std::min(count, sms - reserve));
-  k_scatter_tc<<<ctas, SC_THREADS, SC_SMEM, st>>>(S, static_cast<const CUtensorMap *>(maps), tiles,
-                                                  count, C);
+  const CUtensorMap *m = static_cast<const CUtensorMap *>(maps);
+  if (bf16)
+    k_scatter_tc<true><<<ctas, SC_THREADS, SC_SMEM, st>>>(S, m, tiles, count, C);
+  else
+    k_scatter_tc<false><<<ctas, SC_THREADS, SC_SMEM, st>>>(S, m, tiles, count, C);
 }
 
 void launch_scatter_small(const DevSym &S, const int2 *tasks, int count, const ScatterCols &C,
