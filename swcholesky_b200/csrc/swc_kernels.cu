@@ -641,11 +641,11 @@ __global__ void __launch_bounds__(MT, 4) k_update_tiles(DevSym S, const int4 *ta
 
 // ---------------------------------------------------------------------------------------
 // Dense factorization of a tiled-class panel, blocked by 64 columns (right-looking):
-//   step j:  TRSM of the tiles below diagonal block j (k_trsm_step; its first row block's
-//            task also applies the update of diagonal tile j+1 by block j), then,
-//            concurrently, the trailing SYRK/GEMM update of the column blocks after j
-//            (k_syrk_step) and the POTRF + inverse of diagonal block j+1 (k_diag_step), so
-//            every diagonal block is factored before the next step's TRSM reads it.
+//   step j:  TRSM of the tiles below diagonal block j (k_trsm_step), then, concurrently,
+//            the trailing SYRK/GEMM update of the column blocks after j (k_syrk_step, which
+//            leaves out the next diagonal tile) and, for diagonal block j+1, its update by
+//            block j, POTRF and inverse (k_diag_step), so every diagonal block is factored
+//            before the next step's TRSM reads it.
 //   block 0 is factored by k_diag_step with step 0.
 
 // ---- one 64x64 diagonal block: POTRF and its inverse, blocked by 8 ----------------------
@@ -831,10 +831,14 @@ __device__ void trtri64_blocked(const double *D, double *E, double *W, int bw) {
 // NW warps (upd needs NW = 4: the tile accumulator's layout), diag_smem(NW) bytes of
 // dynamic shared memory: E, W (NW x 64), then D.
 constexpr int diag_smem(int nw) { return (E_ELEMS + nw * 64 + TB * DLD) * 8; }
+constexpr int diag_prev_smem(int nw) { return diag_smem(nw) + TB * DLD * 8; }   // + X
 constexpr int DIAG_SMEM = diag_smem(4);
 constexpr int DIAG_NW = 8;   // warps of the per-step diagonal-block kernel
 
-template <int NW>
+// PREV: the block still misses its update by column block c0/64 - 1 (the rows just above it
+// solved by the previous TRSM launch): it is applied here, on the tile in shared memory,
+// before the factorization (and to the panel rows below a narrower last block, in L).
+template <int NW, bool PREV = false>
 __device__ void factor_diag_block(const DevSym &S, int s, int c0, double *smem,
                                   const TileAcc *upd) {
   constexpr int NTH = 32 * NW;
@@ -862,6 +866,45 @@ __device__ void factor_diag_block(const DevSym &S, int s, int c0, double *smem,
     }
   }
   for (int e = tid; e < E_ELEMS; e += blockDim.x) E[e] = 0.0;
+  if (PREV) {
+    // X = rows c0.. of column block c0/64 - 1 (64 wide), [column][row] after D
+    double *Xs = D + TB * DLD;
+    const int nr = min(TB, m - c0);
+    for (int e0 = tid; e0 < TB * TB; e0 += 8 * NTH) {
+      double v[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int e = e0 + q * NTH, k = e >> 6, r = e & (TB - 1);
+        v[q] = r < nr ? P[(size_t)(c0 - TB + k) * m + c0 + r] : 0.0;
+      }
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int e = e0 + q * NTH;
+        Xs[(e >> 6) * DLD + (e & (TB - 1))] = v[q];
+      }
+    }
+    __syncthreads();
+    // tile -= X X^T over the lower 8x8 blocks (DMMA), block columns of the diagonal block only
+    const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, qq = lane & 3;
+    int blk = 0;
+    for (int bj = 0; bj < (bw + 7) / 8; ++bj)
+      for (int bi = bj; bi < TB / 8; ++bi, ++blk) {
+        if (blk % NW != warp) continue;
+        double acc[2] = {0.0, 0.0};
+#pragma unroll
+        for (int k0 = 0; k0 < TB; k0 += 8) mma8_abt(acc, Xs, 8 * bi, k0, Xs, 8 * bj, k0, false);
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int r = 8 * bi + g, c = 8 * bj + 2 * qq + e;
+          if (c >= bw) continue;
+          if (r < bw) {
+            if (r >= c) D[c * DLD + r] -= acc[e];
+          } else if (c0 + r < m) {   // a partial last block: panel rows below it, in L
+            P[(size_t)(c0 + c) * m + c0 + r] -= acc[e];
+          }
+        }
+      }
+  }
   if (upd) {
     __syncthreads();
 #pragma unroll
@@ -959,12 +1002,15 @@ __device__ void diag_task(const DevSym &S, int s, int step, double *smem) {
   }
 }
 
-// Per-step launches: one CTA per supernode of the list factors diagonal block `step`, whose
-// update by column block step-1 the TRSM launch of that step has applied.
+// Per-step launches: one CTA per supernode of the list factors diagonal block `step`, after
+// applying its update by column block step-1 (the last one it misses).
 __global__ void __launch_bounds__(DIAG_NW * 32) k_diag_step(DevSym S, const int *list, int count,
                                                            int step) {
   extern __shared__ double dyn[];
-  factor_diag_block<DIAG_NW>(S, list[blockIdx.x], step * TB, dyn, nullptr);
+  if (step > 0)
+    factor_diag_block<DIAG_NW, true>(S, list[blockIdx.x], step * TB, dyn, nullptr);
+  else
+    factor_diag_block<DIAG_NW, false>(S, list[blockIdx.x], 0, dyn, nullptr);
 }
 
 // task = (s, r0): B = L[r0:r0+64, blk] := B * L_blk^{-T} = B * T^T with T = L_blk^{-1},
@@ -1000,21 +1046,13 @@ __device__ void trsm_task(const DevSym &S, int s, int r0, int step, double *dyn)
   }
 }
 
-// TRSM tiles of step `step`.  The task of the first row block below the diagonal block
-// holds the rows of the next diagonal tile: after solving them it applies that tile's
-// update by this column block itself (FP64, the rows it just wrote, still on chip or in
-// L2), so the next diagonal block's kernel only factors and the chain of dependent
-// launches (TRSM -> diagonal block -> TRSM) does not re-read the column block.
+// TRSM tiles of step `step`, one product each; the next diagonal block's update by this
+// column block is applied by the diagonal-block kernel that factors it (on the tile in its
+// shared memory), so every TRSM task of the chain's launch takes one product.
 __global__ void __launch_bounds__(MT, 4) k_trsm_step(DevSym S, const int2 *tasks, int count,
                                                   int step) {
   extern __shared__ double dyn[];
-  const int s = tasks[blockIdx.x].x, r0 = tasks[blockIdx.x].y;
-  trsm_task(S, s, r0, step, dyn);
-  const int c0 = step * TB, w = S.super[s + 1] - S.super[s];
-  if (c0 + TB < w && r0 == c0 + TB) {
-    __syncthreads();   // the solved rows are in L (visible to the whole CTA)
-    syrk_tile(S, s, r0, r0, step, dyn);
-  }
+  trsm_task(S, tasks[blockIdx.x].x, tasks[blockIdx.x].y, step, dyn);
 }
 
 // Trailing update of a step: task = (s, r0, c0, product index) with c0 >= (step+1)*64,
@@ -1238,7 +1276,7 @@ bool kernels_configure(std::string &err) {
     e = cudaFuncSetAttribute(k_trsm_step, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * STAGE * 8);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_diag_step, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             diag_smem(DIAG_NW));
+                             diag_prev_smem(DIAG_NW));
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_syrk_step, cudaFuncAttributeMaxDynamicSharedMemorySize, SYRK_SMEM);
   if (e == cudaSuccess)
@@ -1290,7 +1328,8 @@ void launch_update_tiles(const DevSym &S, const int4 *tasks, const int *task_end
   if (count > 0) k_update_tiles<<<count, MT, UPD_SMEM, st>>>(S, tasks, task_end, pairs, count);
 }
 void launch_diag_step(const DevSym &S, const int *list, int count, int step, cudaStream_t st) {
-  if (count > 0) k_diag_step<<<count, DIAG_NW * 32, diag_smem(DIAG_NW), st>>>(S, list, count, step);
+  if (count > 0)
+    k_diag_step<<<count, DIAG_NW * 32, diag_prev_smem(DIAG_NW), st>>>(S, list, count, step);
 }
 void launch_trsm_step(const DevSym &S, const int2 *tasks, int count, int step, cudaStream_t st) {
   if (count > 0) k_trsm_step<<<count, MT, 2 * STAGE * 8, st>>>(S, tasks, count, step);

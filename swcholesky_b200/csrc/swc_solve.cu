@@ -393,126 +393,263 @@ __device__ __forceinline__ void stage_block(double *dst, const double *src, int 
 }
 template <int N>
 __device__ __forceinline__ void stage_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+// an empty cp.async group (keeps one group per ring step)
+__device__ __forceinline__ void stage_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 
 // Chain blocks stage the inverse of their diagonal block and the panel block of each
-// predecessor in shared memory before the predecessor's flag arrives (double buffer), so
-// the step that waits on the flag only reads x_c and multiplies from shared memory.
-constexpr int CHAIN_SMEM = 3 * TB * BLD * 8;
+// predecessor in shared memory before the predecessor's solution arrives (a ring of
+// CHAIN_NS buffers, CHAIN_NS - 1 blocks in flight: the last block of a long chain applies
+// every predecessor in turn, so its loop runs at the rate it can stream panel blocks), and
+// the step that waits only reads x_c and multiplies from shared memory.
+constexpr int CHAIN_NS = 4;
+constexpr int CHAIN_SMEM = (1 + CHAIN_NS) * TB * BLD * 8;
+
+// Chains launch in thread-block clusters of CHAIN_CL consecutive tasks.  A block publishes its
+// solution through global memory and a flag (for the blocks of later clusters and the next
+// level's kernels) and also writes it straight into the shared memory of the later blocks
+// of its supernode in its own cluster (distributed shared memory), arriving on their
+// mbarriers: a hop inside a cluster does not go through L2.  Slot j of a block receives the
+// solution of cluster rank j.  Every CTA of a cluster (tail padding included) passes a
+// cluster barrier after the mbarrier set-up and another before it exits, so no block leaves
+// while a remote write to it may be in flight.
+constexpr int CHAIN_CL = 8;
+struct ChainCluster {
+  double yin[CHAIN_CL][TB];
+  unsigned long long bar[CHAIN_CL];
+};
+
+__device__ __forceinline__ uint32_t chain_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;\n" ::
+                   : "memory");
+}
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+// address of the same shared-memory location in the CTA of cluster rank `rank`
+__device__ __forceinline__ uint32_t cluster_addr(const void *p, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(r) : "r"(smem_addr(p)), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void chain_cluster_init(ChainCluster &cc) {
+  if (threadIdx.x == 0) {
+    for (int j = 0; j < CHAIN_CL; ++j)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(&cc.bar[j])), "r"(TB)
+                   : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  cluster_sync_all();
+}
+// Thread t < 64 of the producer (cluster rank `me`) sends element t of its solution to every
+// later rank of its cluster that holds a block of the same supernode (ranks me+1 .. last).
+__device__ __forceinline__ void chain_send(ChainCluster &cc, int me, int last, double val) {
+  if (threadIdx.x >= TB) return;
+  for (int q = me + 1; q <= last; ++q) {
+    asm volatile("st.shared::cluster.f64 [%0], %1;\n" ::"r"(cluster_addr(&cc.yin[me][threadIdx.x], q)),
+                 "d"(val)
+                 : "memory");
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];\n" ::"r"(
+                     cluster_addr(&cc.bar[me], q))
+                 : "memory");
+  }
+}
+// Thread 0 waits (bounded) for slot j's phase; everyone waits at the barrier; false after a
+// timeout (its own, or one another block recorded).
+__device__ bool chain_recv(ChainCluster &cc, int j, int *status) {
+  __shared__ int ok;
+  if (threadIdx.x == 0) {
+    long long it = 0;
+    const long long budget = wait_budget(status);
+    ok = 1;
+    for (;;) {
+      uint32_t done;
+      asm volatile(
+          "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 P1, [%1], 0;\n\t"
+          "selp.b32 %0, 1, 0, P1;\n\t}\n"
+          : "=r"(done)
+          : "r"(smem_addr(&cc.bar[j]))
+          : "memory");
+      if (done) break;
+      if (++it > budget || ((it & 31) == 0 && *(volatile int *)&status[2])) {
+        atomicExch(&status[2], 1);
+        ok = 0;
+        break;
+      }
+    }
+  }
+  __syncthreads();
+  return ok != 0;
+}
 
 // task = (s, k); forward: y[f + 64k ..] := T_k (y[...] - contributions - sum_{c<k} L_kc x_c)
-__global__ void __launch_bounds__(ST) k_fwd_chain(DevSym S, const int2 *tasks, double *y,
-                                                  const double *contrib, const int *cptr,
-                                                  const int *cidx, int *flags, int epoch,
-                                                  int n, int64_t cstride) {
+// (tasks of a supernode consecutive, in increasing k; CTAs from `count` on are padding)
+__global__ void __launch_bounds__(ST) k_fwd_chain(DevSym S, const int2 *tasks, int count,
+                                                  double *y, const double *contrib,
+                                                  const int *cptr, const int *cidx, int *flags,
+                                                  int epoch, int n, int64_t cstride) {
   extern __shared__ double csm[];
-  double *Ts = csm, *Lb0 = csm + TB * BLD;   // Lb0 and Lb0 + TB * BLD: double buffer
+  double *Ts = csm, *Lb0 = csm + TB * BLD;   // ring: Lb0 + j * TB * BLD, j < CHAIN_NS
   __shared__ double v[TB], part[4][TB], xc[TB];
-  const int s = tasks[blockIdx.x].x, k = tasks[blockIdx.x].y;
-  const int tid = threadIdx.x, r = tid & (TB - 1), q = tid >> 6;
-  const int f = S.super[s], w = S.super[s + 1] - f;
-  const int m = (int)(S.rowptr[s + 1] - S.rowptr[s]);
-  const double *P = S.L + S.xptr[s];
-  const int r0 = k * TB, bw = min(TB, w - r0);
-  const int base = S.dinv_off[s];
-  const double *T = S.dinv + ((size_t)base + k) * (TB * TB);
-  stage_block(Ts, T, TB, TB, TB);                 // T(r, c) at Ts[c * BLD + r]
-  if (k > 0) stage_block(Lb0, P + r0, m, bw, TB); // L_k0(r, jj) at Lb0[jj * BLD + r]
-  // right-hand side of the block minus the descendants' contributions
-  if (tid < TB) {
-    double acc = 0.0;
-    if (tid < bw) {
-      const int j = f + r0 + tid;
-      acc = y[j];
-      for (int qq = cptr[j]; qq < cptr[j + 1]; ++qq) acc -= contrib[cidx[qq]];
+  __shared__ ChainCluster cc;
+  chain_cluster_init(cc);
+  const int me = (int)chain_rank();
+  if ((int)blockIdx.x < count) {
+    const int s = tasks[blockIdx.x].x, k = tasks[blockIdx.x].y;
+    const int tid = threadIdx.x, r = tid & (TB - 1), q = tid >> 6;
+    const int f = S.super[s], w = S.super[s + 1] - f;
+    const int m = (int)(S.rowptr[s + 1] - S.rowptr[s]);
+    const double *P = S.L + S.xptr[s];
+    const int r0 = k * TB, bw = min(TB, w - r0);
+    const int nb = (w + TB - 1) / TB;
+    const int base = S.dinv_off[s];
+    const double *T = S.dinv + ((size_t)base + k) * (TB * TB);
+    // predecessors c >= cfirst are in this cluster (rank me - (k - c)); the later ranks of
+    // the same supernode receive this block's solution
+    const int cfirst = k - me, last = me + min(nb - 1 - k, CHAIN_CL - 1 - me);
+    stage_block(Ts, T, TB, TB, TB);                 // T(r, c) at Ts[c * BLD + r]
+    // L_kc(r, jj) at Lb0[(c % CHAIN_NS) * TB * BLD + jj * BLD + r]; one cp.async group per c
+    for (int c = 0; c < CHAIN_NS - 1; ++c) {
+      if (c < k) stage_block(Lb0 + c * (TB * BLD), P + (size_t)c * TB * m + r0, m, bw, TB);
+      else stage_commit();
     }
-    v[tid] = acc;
-  }
-  for (int c = 0; c < k; ++c) {
-    const double *Lc = Lb0 + (c & 1) * (TB * BLD);
-    if (c + 1 < k) {
-      stage_block(Lb0 + ((c + 1) & 1) * (TB * BLD), P + (size_t)(c + 1) * TB * m + r0, m, bw, TB);
-      stage_wait<1>();
-    } else {
-      stage_wait<0>();
+    // right-hand side of the block minus the descendants' contributions
+    if (tid < TB) {
+      double acc = 0.0;
+      if (tid < bw) {
+        const int j = f + r0 + tid;
+        acc = y[j];
+        for (int qq = cptr[j]; qq < cptr[j + 1]; ++qq) acc -= contrib[cidx[qq]];
+      }
+      v[tid] = acc;
     }
-    if (!wait_flag(&flags[base + c], epoch, S.status)) break;   // ends with a barrier
-    if (tid < TB) xc[tid] = __ldcg(&y[f + c * TB + tid]);
-    __syncthreads();
-    double acc = 0.0;
+    bool ok = true;
+    for (int c = 0; c < k && ok; ++c) {
+      const double *Lc = Lb0 + (c % CHAIN_NS) * (TB * BLD);
+      const int cn = c + CHAIN_NS - 1;   // the block staged now, into the buffer freed last step
+      if (cn < k) stage_block(Lb0 + (cn % CHAIN_NS) * (TB * BLD), P + (size_t)cn * TB * m + r0, m, bw, TB);
+      else stage_commit();
+      stage_wait<CHAIN_NS - 1>();        // block c has landed
+      if (c >= cfirst) {   // from the cluster (ends with a barrier)
+        const int j = me - (k - c);
+        if (!chain_recv(cc, j, S.status)) { ok = false; break; }
+        if (tid < TB) xc[tid] = cc.yin[j][tid];
+      } else {             // from global memory (ends with a barrier)
+        if (!wait_flag(&flags[base + c], epoch, S.status)) { ok = false; break; }
+        if (tid < TB) xc[tid] = __ldcg(&y[f + c * TB + tid]);
+      }
+      __syncthreads();
+      double acc = 0.0;
 #pragma unroll
-    for (int jj = q * 16; jj < q * 16 + 16; ++jj) acc = fma(Lc[jj * BLD + r], xc[jj], acc);
-    part[q][r] = acc;
+      for (int jj = q * 16; jj < q * 16 + 16; ++jj) acc = fma(Lc[jj * BLD + r], xc[jj], acc);
+      part[q][r] = acc;
+      __syncthreads();
+      if (tid < TB) v[tid] -= (part[0][tid] + part[1][tid]) + (part[2][tid] + part[3][tid]);
+    }
+    stage_wait<0>();
     __syncthreads();
-    if (tid < TB) v[tid] -= (part[0][tid] + part[1][tid]) + (part[2][tid] + part[3][tid]);
+    if (ok) {
+      // x_k = T_k v
+      double acc = 0.0;
+#pragma unroll
+      for (int jj = q * 16; jj < q * 16 + 16; ++jj) acc = fma(Ts[jj * BLD + r], v[jj], acc);
+      part[q][r] = acc;
+      __syncthreads();
+      const double xk = (part[0][r] + part[1][r]) + (part[2][r] + part[3][r]);
+      // the cluster's later blocks first: each arrive releases only the thread's earlier
+      // stores, which then do not yet include the global one
+      chain_send(cc, me, last, tid < bw ? xk : 0.0);
+      if (tid < bw) y[f + r0 + tid] = xk;
+      __threadfence();
+      __syncthreads();
+      if (tid == 0) st_release(&flags[base + k], epoch);
+    }
   }
-  stage_wait<0>();
-  __syncthreads();
-  // x_k = T_k v
-  double acc = 0.0;
-#pragma unroll
-  for (int jj = q * 16; jj < q * 16 + 16; ++jj) acc = fma(Ts[jj * BLD + r], v[jj], acc);
-  part[q][r] = acc;
-  __syncthreads();
-  if (tid < bw) y[f + r0 + tid] = (part[0][tid] + part[1][tid]) + (part[2][tid] + part[3][tid]);
-  __threadfence();
-  __syncthreads();
-  if (tid == 0) st_release(&flags[base + k], epoch);
+  cluster_sync_all();
 }
 
 // task = (s, k) in decreasing k; backward: x[f + 64k ..] := T_k^T (x[...] - sum_{c>k} L_ck^T x_c)
-__global__ void __launch_bounds__(ST) k_bwd_chain(DevSym S, const int2 *tasks, double *x,
-                                                  int *flags, int epoch) {
+// (tasks of a supernode consecutive, in decreasing k; CTAs from `count` on are padding)
+__global__ void __launch_bounds__(ST) k_bwd_chain(DevSym S, const int2 *tasks, int count,
+                                                  double *x, int *flags, int epoch) {
   extern __shared__ double csm[];
-  double *Ts = csm, *Lb0 = csm + TB * BLD;
+  double *Ts = csm, *Lb0 = csm + TB * BLD;   // ring of CHAIN_NS buffers
   __shared__ double v[TB], part[4][TB], xc[TB];
-  const int s = tasks[blockIdx.x].x, k = tasks[blockIdx.x].y;
-  const int tid = threadIdx.x, i = tid & (TB - 1), q = tid >> 6;
-  const int f = S.super[s], w = S.super[s + 1] - f;
-  const int m = (int)(S.rowptr[s + 1] - S.rowptr[s]);
-  const double *P = S.L + S.xptr[s];
-  const int r0 = k * TB, bw = min(TB, w - r0);
-  const int nb = (w + TB - 1) / TB;
-  const int base = S.dinv_off[s];
-  const double *T = S.dinv + ((size_t)base + k) * (TB * TB);
-  // panel block (c, k): rows 64c + rr, columns r0 + i, staged as Lc[i * BLD + rr]
-  stage_block(Ts, T, TB, TB, TB);   // T(rr, i) at Ts[i * BLD + rr]
-  if (k + 1 < nb)
-    stage_block(Lb0, P + (size_t)r0 * m + (nb - 1) * TB, m, min(TB, w - (nb - 1) * TB), bw);
-  if (tid < TB) v[tid] = (tid < bw) ? x[f + r0 + tid] : 0.0;
-  int buf = 0;
-  for (int c = nb - 1; c > k; --c, buf ^= 1) {
-    const double *Lc = Lb0 + buf * (TB * BLD);
-    if (c - 1 > k) {
-      stage_block(Lb0 + (buf ^ 1) * (TB * BLD), P + (size_t)r0 * m + (c - 1) * TB, m,
-                  min(TB, w - (c - 1) * TB), bw);
-      stage_wait<1>();
-    } else {
-      stage_wait<0>();
+  __shared__ ChainCluster cc;
+  chain_cluster_init(cc);
+  const int me = (int)chain_rank();
+  if ((int)blockIdx.x < count) {
+    const int s = tasks[blockIdx.x].x, k = tasks[blockIdx.x].y;
+    const int tid = threadIdx.x, i = tid & (TB - 1), q = tid >> 6;
+    const int f = S.super[s], w = S.super[s + 1] - f;
+    const int m = (int)(S.rowptr[s + 1] - S.rowptr[s]);
+    const double *P = S.L + S.xptr[s];
+    const int r0 = k * TB, bw = min(TB, w - r0);
+    const int nb = (w + TB - 1) / TB;
+    const int base = S.dinv_off[s];
+    const double *T = S.dinv + ((size_t)base + k) * (TB * TB);
+    // successors c <= clast are in this cluster (rank me - (c - k)); the later ranks (lower
+    // k) of the same supernode receive this block's solution
+    const int clast = k + me, last = me + min(k, CHAIN_CL - 1 - me);
+    // panel block (c, k): rows 64c + rr, columns r0 + i, staged as Lc[i * BLD + rr]
+    stage_block(Ts, T, TB, TB, TB);   // T(rr, i) at Ts[i * BLD + rr]
+    // successor step t = nb - 1 - c (c = nb - 1 first): block (c, k) in buffer t % CHAIN_NS
+    auto stage_succ = [&](int t) {
+      const int c = nb - 1 - t;
+      if (c > k)
+        stage_block(Lb0 + (t % CHAIN_NS) * (TB * BLD), P + (size_t)r0 * m + c * TB, m,
+                    min(TB, w - c * TB), bw);
+      else
+        stage_commit();
+    };
+    for (int t = 0; t < CHAIN_NS - 1; ++t) stage_succ(t);
+    if (tid < TB) v[tid] = (tid < bw) ? x[f + r0 + tid] : 0.0;
+    bool ok = true;
+    for (int c = nb - 1; c > k; --c) {
+      const int t = nb - 1 - c;
+      const double *Lc = Lb0 + (t % CHAIN_NS) * (TB * BLD);
+      stage_succ(t + CHAIN_NS - 1);
+      stage_wait<CHAIN_NS - 1>();        // block (c, k) has landed
+      const int cw = min(TB, w - c * TB);
+      if (c <= clast) {   // from the cluster (ends with a barrier)
+        const int j = me - (c - k);
+        if (!chain_recv(cc, j, S.status)) { ok = false; break; }
+        if (tid < TB) xc[tid] = cc.yin[j][tid];
+      } else {            // from global memory (ends with a barrier)
+        if (!wait_flag(&flags[base + c], epoch, S.status)) { ok = false; break; }
+        if (tid < TB) xc[tid] = (tid < cw) ? __ldcg(&x[f + c * TB + tid]) : 0.0;
+      }
+      __syncthreads();
+      // v[i] -= sum_rr L(64c + rr, r0 + i) x_c[rr]
+      double acc = 0.0;
+#pragma unroll
+      for (int rr = q * 16; rr < q * 16 + 16; ++rr) acc = fma(Lc[i * BLD + rr], xc[rr], acc);
+      part[q][i] = acc;
+      __syncthreads();
+      if (tid < TB) v[tid] -= (part[0][tid] + part[1][tid]) + (part[2][tid] + part[3][tid]);
     }
-    if (!wait_flag(&flags[base + c], epoch, S.status)) break;
-    const int cw = min(TB, w - c * TB);
-    if (tid < TB) xc[tid] = (tid < cw) ? __ldcg(&x[f + c * TB + tid]) : 0.0;
+    stage_wait<0>();
     __syncthreads();
-    // v[i] -= sum_rr L(64c + rr, r0 + i) x_c[rr]
-    double acc = 0.0;
+    if (ok) {
+      // x_k[i] = sum_{rr >= i} T(rr, i) v[rr]
+      double acc = 0.0;
 #pragma unroll
-    for (int rr = q * 16; rr < q * 16 + 16; ++rr) acc = fma(Lc[i * BLD + rr], xc[rr], acc);
-    part[q][i] = acc;
-    __syncthreads();
-    if (tid < TB) v[tid] -= (part[0][tid] + part[1][tid]) + (part[2][tid] + part[3][tid]);
+      for (int rr = q * 16; rr < q * 16 + 16; ++rr) acc = fma(Ts[i * BLD + rr], v[rr], acc);
+      part[q][i] = acc;
+      __syncthreads();
+      const double xk = (part[0][i] + part[1][i]) + (part[2][i] + part[3][i]);
+      chain_send(cc, me, last, tid < bw ? xk : 0.0);   // before the global store (above)
+      if (tid < bw) x[f + r0 + tid] = xk;
+      __threadfence();
+      __syncthreads();
+      if (tid == 0) st_release(&flags[base + k], epoch);
+    }
   }
-  stage_wait<0>();
-  __syncthreads();
-  // x_k[i] = sum_{rr >= i} T(rr, i) v[rr]
-  double acc = 0.0;
-#pragma unroll
-  for (int rr = q * 16; rr < q * 16 + 16; ++rr) acc = fma(Ts[i * BLD + rr], v[rr], acc);
-  part[q][i] = acc;
-  __syncthreads();
-  if (tid < bw) x[f + r0 + tid] = (part[0][tid] + part[1][tid]) + (part[2][tid] + part[3][tid]);
-  __threadfence();
-  __syncthreads();
-  if (tid == 0) st_release(&flags[base + k], epoch);
+  cluster_sync_all();
 }
 
 // y = A x for the symmetric matrix held as full CSR (both triangles), nrhs vectors.
@@ -666,16 +803,36 @@ void launch_bwd_diag(const DevSym &S, const int *list, int count, int smem, doub
                      int nrhs, cudaStream_t st) {
   if (count > 0) k_bwd_diag<<<count, ST, smem, st>>>(S, list, x, n, nrhs);
 }
+// the chains' launch configuration: a grid of whole clusters of CHAIN_CL CTAs
+static cudaLaunchConfig_t chain_config(int count, cudaStream_t st, cudaLaunchAttribute *at) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)((count + CHAIN_CL - 1) / CHAIN_CL * CHAIN_CL));
+  cfg.blockDim = dim3(ST);
+  cfg.dynamicSmemBytes = CHAIN_SMEM;
+  cfg.stream = st;
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = CHAIN_CL;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cfg;
+}
 void launch_fwd_chain(const DevSym &S, const int2 *tasks, int count, double *y,
                       const double *contrib, const int *cptr, const int *cidx, int *flags,
                       int epoch, int n, int64_t cstride, cudaStream_t st) {
-  if (count > 0)
-    k_fwd_chain<<<count, ST, CHAIN_SMEM, st>>>(S, tasks, y, contrib, cptr, cidx, flags, epoch, n,
-                                               cstride);
+  if (count <= 0) return;
+  cudaLaunchAttribute at[1];
+  const cudaLaunchConfig_t cfg = chain_config(count, st, at);
+  cudaLaunchKernelEx(&cfg, k_fwd_chain, S, tasks, count, y, contrib, cptr, cidx, flags, epoch, n,
+                     cstride);
 }
 void launch_bwd_chain(const DevSym &S, const int2 *tasks, int count, double *x, int *flags,
                       int epoch, cudaStream_t st) {
-  if (count > 0) k_bwd_chain<<<count, ST, CHAIN_SMEM, st>>>(S, tasks, x, flags, epoch);
+  if (count <= 0) return;
+  cudaLaunchAttribute at[1];
+  const cudaLaunchConfig_t cfg = chain_config(count, st, at);
+  cudaLaunchKernelEx(&cfg, k_bwd_chain, S, tasks, count, x, flags, epoch);
 }
 void launch_spmv(int n, const int *rp, const int *ci, const double *val, const double *x,
                  double *y, int nrhs, cudaStream_t st) {
