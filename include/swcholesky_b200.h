@@ -90,7 +90,10 @@ void *swc_get_stream(swc_handle_t handle);
  * in the mixed modes, the descendant updates by the tile-owner gather kernel (split-TF32
  * operands staged by TMA gather4 loads, 6, or by cp.async, 7; BF16x3 by cp.async) instead
  * of the right-looking dense products with an FP64 atomic scatter, and the trailing SYRK
- * steps in FP64.  SWC_INVALID_INPUT for other values. */
+ * steps in FP64; 8 and 9: in the mixed modes, the right-looking products cut into tiles
+ * of at most 256 (8) or 128 (9) columns of K, each accumulated in FP32 on the tensor
+ * cores and summed in FP64 by the scatter (a more accurate factor for more atomic adds).
+ * SWC_INVALID_INPUT for other values. */
 int swc_set_plan(swc_handle_t handle, int plan);
 
 /* Poll budget of the handle's device-side waits: the persistent walks of the
@@ -188,7 +191,11 @@ int swc_profile(swc_handle_t handle, const double *values, int values_on_device,
 
 /* Host-only: validates the structure (as swc_analyze does) and describes the execution
  * plan (candidate `plan`, as swc_set_plan) without touching a GPU; for plan 4 the dataflow
- * task order is checked (every wait served by an earlier task) as at analysis.
+ * task order is checked (every wait served by an earlier task) as at analysis, and the
+ * tables of the mixed modes' right-looking updates are checked against a direct lookup
+ * (every scattered entry's address in L, each descendant's contribution covered once per
+ * column of K, the dense steps' trailing updates covering each column block once);
+ * SWC_INVALID_INPUT with the first violation in swc_last_error().
  * stats[0..19] = levels, kernel launches per factorization,
  * small-class supernodes, tiled-class supernodes, update tiles, update (tile, descendant)
  * pairs, TRSM tiles, SYRK tiles, then per kernel class (memset, small, assemble, update,

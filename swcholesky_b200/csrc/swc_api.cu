@@ -416,6 +416,8 @@ int swc_plan_stats(int n, const int *c, const int *r, const size_t *lC, const in
   if (!swc::build_plan(n, c, r, lc.data(), Ls, lip.data(), blockSet, supNo, prunePtr, pruneSet,
                        H, P, err, swc::plan_candidate(plan)))
     return fail(SWC_INVALID_INPUT, err);
+  if (!swc::check_scatter_plan(n, Ls, H, P, swc::plan_candidate(plan), err))
+    return fail(SWC_INVALID_INPUT, err);
   stats[0] = (double)P.waves.size();
   stats[1] = (double)P.launches;
   stats[2] = (double)P.small_list.size();

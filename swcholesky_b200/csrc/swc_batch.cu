@@ -112,11 +112,13 @@ Tuning plan_candidate(int k) {
     case 5: t.syrk_fp64 = 1; break;                      // mixed modes: FP64 SYRK steps
     case 6: t.scatter = 0; t.tc_tma = 1; break;          // mixed: tile-owner updates (TMA for TF32)
     case 7: t.scatter = 0; break;                        // mixed: tile-owner, cp.async
+    case 8: t.scatter_kmax = 256; break;                 // mixed: K cut into 256-column tiles
+    case 9: t.scatter_kmax = 128; break;                 // mixed: 128-column tiles
     default: break;
   }
   return t;
 }
-const int kNumPlans = 8;
+const int kNumPlans = 10;
 int num_plans() { return kNumPlans; }
 
 bool BatchState::set(int nm, const int *n, const int *c, const int *r, std::string &err) {

@@ -6,6 +6,8 @@
 #include <climits>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <tuple>
 
 #include "swc_engine.h"
 
@@ -617,9 +619,12 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
         small_by_wave[level[d] + 1].push_back(make_int2(d, c0));   // FP64 on the CUDA cores
         continue;
       }
+      const int kcut = T.scatter_kmax > 0 ? std::max(1, T.scatter_kmax / 32) : nk;
       for (int i0 = c0; i0 < md; i0 += 128)
         for (int j0 = c0; j0 <= i0; j0 += 128) {
-          by_wave[level[d] + 1].push_back(ScTile{d, i0, j0, nk, md, 0, 128, 0, P.sc_coff[d], 0});
+          for (int kb = 0; kb < nk; kb += kcut)
+            by_wave[level[d] + 1].push_back(
+                ScTile{d, i0, j0, std::min(kcut, nk - kb), md, kb * 32, 128, 0, P.sc_coff[d], 0});
           P.sc_flops += 2.0 * 128 * 128 * wd;
         }
       P.sc_used[d] |= 1;
@@ -732,6 +737,163 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
       const int ub = (int)(std::lower_bound(b, e, H.super[t + 1]) - b) + wd;
       H.upd_lbub[q] = make_int2(lb, ub);
     }
+  return true;
+}
+
+bool check_scatter_plan(int n, const int *Ls, const HostSym &H, const Plan &P, const Tuning &T,
+                        std::string &err) {
+  if (P.sc_coff.empty()) return true;
+  const std::vector<int> &super = H.super;
+  const int ns = (int)super.size() - 1;
+  std::vector<int> col2sup(n), level(ns, 0), wave_of(ns, -1);
+  for (int s = 0; s < ns; ++s)
+    for (int j = super[s]; j < super[s + 1]; ++j) col2sup[j] = s;
+  for (int s = 0; s < ns; ++s) {
+    const int w = super[s + 1] - super[s];
+    if (H.rowptr[s + 1] - H.rowptr[s] > w)
+      level[col2sup[Ls[H.rowptr[s] + w]]] = std::max(level[col2sup[Ls[H.rowptr[s] + w]]], level[s] + 1);
+  }
+  std::vector<char> tiled(ns, 0);
+  for (size_t lv = 0; lv < P.waves.size(); ++lv)
+    for (int k = P.waves[lv].big_off; k < P.waves[lv].big_off + P.waves[lv].big_cnt; ++k) {
+      tiled[P.big_list[k]] = 1;
+      wave_of[P.big_list[k]] = (int)lv;
+    }
+  auto fail = [&](const std::string &what, long long a, long long b) {
+    err = "scatter plan check: " + what + " (" + std::to_string(a) + ", " + std::to_string(b) + ")";
+    return false;
+  };
+  // 1. per descendant: the column table and the relative indices address, for every entry
+  //    (i, j), i >= j, from its first row with a tiled-class target, the entry of L a direct
+  //    lookup finds (rs[pos] == rd[i] in the target's sorted row list identifies it)
+  std::vector<int> first(ns, -1);
+  for (int d = 0; d < ns; ++d) {
+    const int wd = super[d + 1] - super[d];
+    const int md = (int)(H.rowptr[d + 1] - H.rowptr[d]);
+    const int *rd = Ls + H.rowptr[d];
+    int c0 = wd;
+    while (c0 < md && !tiled[col2sup[rd[c0]]]) ++c0;
+    if (c0 == md) continue;
+    first[d] = c0;
+    for (int j = c0; j < md; ++j) {
+      const int s = col2sup[rd[j]];
+      const int64_t base = P.sc_base[P.sc_coff[d] + j];
+      if (!tiled[s]) {
+        if (base != -1) return fail("small-class target with an address, descendant/column", d, j);
+        continue;
+      }
+      const int ms = (int)(H.rowptr[s + 1] - H.rowptr[s]);
+      if (base != H.xptr[s] + (int64_t)(rd[j] - super[s]) * ms)
+        return fail("column address, descendant/column", d, j);
+      const int *rs = Ls + H.rowptr[s];
+      const int64_t rel = P.sc_rel[P.sc_coff[d] + j];
+      for (int i = j; i < md; ++i) {
+        const int pos = P.sc_relidx[rel + i];
+        if (pos < 0 || pos >= ms || rs[pos] != rd[i]) return fail("relative index, descendant/row", d, i);
+      }
+    }
+  }
+  // 2. every descendant with a tiled-class target is handled once, in the level after its
+  //    own: by one CUDA-core task, or by tiles whose K ranges cover its width exactly once
+  //    for every 128 x 128 block of its lower triangle from that first row
+  std::vector<int> nsmall(ns, 0);
+  std::vector<std::vector<const ScTile *>> tiles_of(ns);
+  for (size_t lv = 0; lv < P.waves.size(); ++lv) {
+    const Wave &W = P.waves[lv];
+    for (int q = W.scs_off; q < W.scs_off + W.scs_cnt; ++q) {
+      const int d = P.sc_small[q].x;
+      if (level[d] + 1 != (int)lv || P.sc_small[q].y != first[d])
+        return fail("CUDA-core task level or first row, descendant/level", d, (long long)lv);
+      ++nsmall[d];
+    }
+    for (int t = W.sc_off; t < W.sc_off + W.sc_cnt; ++t) {
+      const ScTile &tl = P.sc_tiles[t];
+      if (tl.d < 0 || tl.d >= ns || level[tl.d] + 1 != (int)lv)
+        return fail("tile level, tile/level", t, (long long)lv);
+      tiles_of[tl.d].push_back(&tl);
+    }
+  }
+  for (int d = 0; d < ns; ++d) {
+    const int c0 = first[d];
+    const int wd = super[d + 1] - super[d];
+    const int md = (int)(H.rowptr[d + 1] - H.rowptr[d]);
+    const int nk = (wd + 31) / 32;
+    if (c0 < 0) {
+      if (nsmall[d] || !tiles_of[d].empty()) return fail("work for a descendant without tiled targets", d, 0);
+      continue;
+    }
+    if (nsmall[d] + (tiles_of[d].empty() ? 0 : 1) != 1) return fail("descendant handled twice or never", d, nsmall[d]);
+    if (nsmall[d]) continue;
+    const int nb = (md - c0 + 127) / 128;
+    std::vector<std::vector<std::pair<int, int>>> kr((size_t)nb * nb);
+    for (const ScTile *tl : tiles_of[d]) {
+      if (tl->md != md || tl->ncol != 128 || tl->dense || tl->co != P.sc_coff[d] ||
+          (tl->i0 - c0) % 128 || (tl->j0 - c0) % 128 || tl->j0 < c0 || tl->j0 > tl->i0 ||
+          tl->i0 >= md || tl->k0 % 32 || tl->nk <= 0)
+        return fail("tile fields, descendant/row", d, tl->i0);
+      kr[(size_t)((tl->i0 - c0) / 128) * nb + (tl->j0 - c0) / 128].push_back({tl->k0 / 32, tl->nk});
+    }
+    for (int bi = 0; bi < nb; ++bi)
+      for (int bj = 0; bj <= bi; ++bj) {
+        std::vector<std::pair<int, int>> &v = kr[(size_t)bi * nb + bj];
+        std::sort(v.begin(), v.end());
+        int at = 0;
+        for (const auto &p : v) {
+          if (p.first != at) return fail("K ranges of a tile leave a gap or overlap, descendant/block", d, bi);
+          at += p.second;
+        }
+        if (at != nk) return fail("K ranges of a tile do not cover the width, descendant/block", d, bi);
+      }
+  }
+  // 3. trailing updates of the dense steps: for every tiled supernode, column block C and K
+  //    block b < C, the rows that receive b tile [C*64 + 64, m) when b = C - 1 (the diagonal
+  //    tile gets that block from the diagonal-block kernel) and [C*64, m) otherwise, every
+  //    row exactly once, from the tiles of step b's group
+  const int G = std::max(1, T.dense_group);
+  std::map<std::tuple<int, int, int>, std::vector<std::pair<int, int>>> rows;   // (s, C, b)
+  for (size_t lv = 0; lv < P.waves.size(); ++lv) {
+    const Wave &W = P.waves[lv];
+    for (size_t j = 0; j < W.scd_off.size(); ++j)
+      for (int t = W.scd_off[j]; t < W.scd_off[j] + W.scd_cnt[j]; ++t) {
+        const ScTile &tl = P.sc_dense[t];
+        const int s = tl.d;
+        if (s < 0 || s >= ns || !tiled[s] || wave_of[s] != (int)lv) return fail("dense tile's supernode, tile", t, s);
+        const int w = super[s + 1] - super[s];
+        const int m = (int)(H.rowptr[s + 1] - H.rowptr[s]);
+        const int C = tl.j0 / TB;
+        const int b0 = tl.k0 / TB, b1 = (std::min(w, tl.k0 + 32 * tl.nk) + TB - 1) / TB;
+        if (!tl.dense || tl.md != m || tl.j0 % TB || tl.k0 % TB || tl.ncol != std::min(TB, w - tl.j0) ||
+            b1 - 1 != (int)j || C <= (int)j || tl.i0 < tl.j0 || tl.i0 >= m ||
+            tl.k0 + 32 * tl.nk < std::min(w, b1 * TB) || b1 - b0 > G)
+          return fail("dense tile fields, tile/step", t, (long long)j);
+        for (int b = b0; b < b1; ++b) rows[std::make_tuple(s, C, b)].push_back({tl.i0, std::min(m, tl.i0 + 128)});
+      }
+  }
+  for (int s = 0; s < ns; ++s) {
+    if (!tiled[s]) continue;
+    const int w = super[s + 1] - super[s];
+    const int m = (int)(H.rowptr[s + 1] - H.rowptr[s]);
+    for (int C = 1; C * TB < w; ++C)
+      for (int b = 0; b < C; ++b) {
+        const int lo = b == C - 1 ? C * TB + TB : C * TB;
+        auto it = rows.find(std::make_tuple(s, C, b));
+        if (lo >= m) {
+          if (it != rows.end()) return fail("dense rows below the supernode, supernode/block", s, C);
+          continue;
+        }
+        if (it == rows.end()) return fail("column block misses a K block, supernode/block", s, C);
+        std::vector<std::pair<int, int>> &v = it->second;
+        std::sort(v.begin(), v.end());
+        int at = lo;
+        for (const auto &p : v) {
+          if (p.first != at) return fail("dense rows leave a gap or overlap, supernode/block", s, C);
+          at = p.second;
+        }
+        if (at != m) return fail("dense rows do not reach the last row, supernode/block", s, C);
+        rows.erase(it);
+      }
+  }
+  if (!rows.empty()) return fail("dense tiles outside the lower column blocks", (long long)rows.size(), 0);
   return true;
 }
 

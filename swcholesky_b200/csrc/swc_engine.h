@@ -222,6 +222,14 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
                 const int *pruneSet, HostSym &H, Plan &P, std::string &err,
                 const Tuning &T = Tuning());
 
+// Host check of a plan's right-looking update tables (a no-op without them): every scattered
+// entry's address against a direct lookup in the target's row list, every descendant's
+// lower triangle covered once per column of K, every tile in the level after its
+// descendant's, every column block of the dense steps' trailing updates receiving each
+// earlier block once.  False with a message on the first violation.
+bool check_scatter_plan(int n, const int *Ls, const HostSym &H, const Plan &P, const Tuning &T,
+                        std::string &err);
+
 struct AdjointPlan;   // reverse-sweep schedule of the adjoint (swc_adjoint.cu)
 
 class Engine {

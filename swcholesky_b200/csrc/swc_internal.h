@@ -104,6 +104,10 @@ struct Tuning {
   int scatter = 1;                       // mixed modes: right-looking updates (dense
                                          // 128x128 tiles, FP64 atomic scatter) instead of
                                          // the tile-owner gather
+  int scatter_kmax = 0;                  // right-looking tiles: columns of K per tile (a
+                                         // multiple of 32; 0 = the descendant's width).
+                                         // Shorter FP32 accumulations, summed in FP64 by
+                                         // the scatter's atomic adds
 };
 
 }  // namespace swc

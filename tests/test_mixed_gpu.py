@@ -81,14 +81,17 @@ def test_stencil27_40_eight_rhs(cuda_ok, name, mode):
                                        (swc.SWC_MODE_MIXED_TF32X3, 5),
                                        (swc.SWC_MODE_MIXED_TF32X3, 6),
                                        (swc.SWC_MODE_MIXED_TF32X3, 7),
+                                       (swc.SWC_MODE_MIXED_TF32X3, 9),
                                        (swc.SWC_MODE_MIXED_BF16X3, 5),
-                                       (swc.SWC_MODE_MIXED_BF16X3, 7)])
+                                       (swc.SWC_MODE_MIXED_BF16X3, 7),
+                                       (swc.SWC_MODE_MIXED_BF16X3, 8)])
 def test_split_plan_variants(cuda_ok, mode, plan):
     """The split factors under each of their execution-plan variants (0: right-looking
     tcgen05 updates scattered by FP64 atomics, trailing SYRK steps as tcgen05 tiles; 5: the
     trailing SYRK steps in FP64; 6, 7: tile-owner tcgen05 updates staged with TMA
-    tile::gather4 loads or with cp.async) agree with the FP64 factor to FP32-class accuracy
-    and refine to the FP64 backward error."""
+    tile::gather4 loads or with cp.async; 8, 9: the right-looking products cut into tiles of
+    256 or 128 columns of K) agree with the FP64 factor to FP32-class accuracy and refine to
+    the FP64 backward error."""
     gs = load_sym("grid3d_24")
     A, _, _ = W.build("grid3d_24")
     P = W.assemble(A, gs["perm"], gs["super"])
