@@ -1487,8 +1487,10 @@ void Engine::run_solve(double *x, int nrhs) {
 
 // Forward then backward supernodal solve, level by level, with the contribution scratch
 // `contrib` (one double per off-diagonal row of L per right-hand side).  The chained blocks'
-// flags are cleared first, so the epochs of every solve are the same (2r + 1 forward, 2r + 2
-// backward for right-hand side r) and a graph of this sequence can be replayed.
+// counters are cleared first and every block takes part in every pass, in the order
+// forward r = 0 .. nrhs - 1, then backward r = 0 .. nrhs - 1, so the pass numbers (epochs
+// r + 1 forward, nrhs + r + 1 backward) are the same in every solve and a graph of this
+// sequence can be replayed.
 void Engine::run_solve_with(double *x, int nrhs, double *contrib) {
   cudaStream_t st = stream_;
   const SolvePlan &SP = splan_;
@@ -1506,7 +1508,7 @@ void Engine::run_solve_with(double *x, int nrhs, double *contrib) {
     for (int r = 0; r < nrhs; ++r)
       launch_fwd_chain(sym_, d_fchain_ + SP.chain_off[l], SP.chain_off[l + 1] - SP.chain_off[l],
                        x + (size_t)r * n_, contrib + (size_t)r * cs, d_cptr_, d_cidx_, d_flags_,
-                       base + 2 * r + 1, n_, cs, st);
+                       base + r + 1, n_, cs, st);
     launch_fwd_contrib(sym_, d_scontrib_ + SP.contrib_off[l], SP.contrib_off[l + 1] - SP.contrib_off[l],
                        SP.contrib_wide[l], x, contrib, n_, nrhs, cs, st);
   }
@@ -1519,7 +1521,7 @@ void Engine::run_solve_with(double *x, int nrhs, double *contrib) {
                     nrhs, st);
     for (int r = 0; r < nrhs; ++r)
       launch_bwd_chain(sym_, d_bchain_ + SP.chain_off[l], SP.chain_off[l + 1] - SP.chain_off[l],
-                       x + (size_t)r * n_, d_flags_, base + 2 * r + 2, st);
+                       x + (size_t)r * n_, d_flags_, base + nrhs + r + 1, st);
   }
 }
 

@@ -339,79 +339,92 @@ __global__ void __launch_bounds__(ST) k_bwd_diag(DevSym S, const int *list, doub
   }
 }
 
-// ---- chained dense solves with the diagonal block of a tiled-class supernode -----------
-// One CTA per 64-row block k of the diagonal block; block k consumes the solved blocks
-// c < k (forward) or c > k (backward) as they are published through per-block flags
-// (flag == epoch), and applies its own block through the stored inverse of the 64x64
-// diagonal block (DMMA-free GEMVs: the work per block is small and latency-bound).  All
-// CTAs of a chain are resident together (a few hundred at most) and only wait on CTAs with
-// a lower blockIdx, which the hardware dispatches first.  Waits are bounded: after the poll
-// budget in status[4] the CTA records a timeout in status[2] and stops waiting.
-
+// Per-block counters of the chained solves: each of a block's eight warps adds 1 (release)
+// once its rows of the block's solution are in global memory, so the solution of pass e
+// (the e-th chain launch that includes the block since the counters were cleared) is
+// complete when the counter reaches 8e.  Waits are
+// bounded: after the poll budget in status[4] a waiter records a timeout in status[2] and
+// stops waiting.
+constexpr int CHAIN_WARPS = ST / 32;
 __device__ __forceinline__ int ld_acquire(const int *p) {
   int v;
   asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(p));
   return v;
 }
-__device__ __forceinline__ void st_release(int *p, int v) {
-  asm volatile("st.release.gpu.global.s32 [%0], %1;\n" ::"l"(p), "r"(v));
+__device__ __forceinline__ void red_release_add(int *p, int v) {
+  asm volatile("red.release.gpu.global.add.s32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
 }
 
-// thread 0 polls, everyone waits at the barrier; returns false after a timeout (its own,
-// or one another block recorded: a block that gave up never publishes its flag)
-__device__ bool wait_flag(const int *flag, int val, int *status) {
-  __shared__ int ok;
-  if (threadIdx.x == 0) {
-    long long it = 0;
-    const long long budget = wait_budget(status);
-    ok = 1;
-    while (ld_acquire(flag) != val) {
-      if (++it > budget || ((it & 31) == 0 && *(volatile int *)&status[2])) {
-        atomicExch(&status[2], 1);
-        ok = 0;
-        break;
-      }
-      __nanosleep(100);
+// Lane u < nf polls the counter at flag + dir * u (no sleep between polls: a hop between
+// clusters is on the chain's critical path) until the first one has reached `target`;
+// returns how many consecutive counters from the first have reached it (1 .. nf), or 0
+// after a timeout (its own, or one another block recorded).  A batch is never held back
+// by a block that is not finished yet.
+__device__ int warp_wait_prefix(const int *flag, int dir, int nf, int target, int *status) {
+  const long long budget = wait_budget(status);
+  long long it = 0;
+  const int lane = threadIdx.x & 31;
+  bool mine = lane < nf && ld_acquire(flag + dir * lane) >= target;
+  int n = 0;
+  for (;;) {
+    const unsigned done = __ballot_sync(0xffffffffu, mine);
+    n = min(nf, __ffs(~done) - 1);
+    if (n > 0) break;
+    if (++it > budget || ((it & 31) == 0 && *(volatile int *)&status[2])) {
+      if (lane == 0) atomicExch(&status[2], 1);
+      break;
     }
+    if (lane < nf && !mine) mine = ld_acquire(flag + dir * lane) >= target;
   }
-  __syncthreads();
-  return ok != 0;
+  __syncwarp();   // the lanes' later loads are ordered after the polling lanes' acquires
+  return n;
 }
 
-// Shared staging of one 64x64 block of a panel (column-major source, leading dimension m):
-// dst[col * 65 + row] (padded), rows >= nr and columns >= nc zero-filled; 8-byte cp.async.
-constexpr int BLD = TB + 1;
-__device__ __forceinline__ void stage_block(double *dst, const double *src, int m, int nr, int nc) {
-  for (int e = threadIdx.x; e < TB * TB; e += ST) {
-    const int c = e >> 6, r = e & (TB - 1);
-    const bool in = r < nr && c < nc;
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst + c * BLD + r);
-    const double *g = in ? src + (size_t)c * m + r : src;
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(g), "r"(in ? 8 : 0));
-  }
-  asm volatile("cp.async.commit_group;\n" ::);
-}
 template <int N>
 __device__ __forceinline__ void stage_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 // an empty cp.async group (keeps one group per ring step)
 __device__ __forceinline__ void stage_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp8(double *dst, const double *src, bool in) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src), "r"(in ? 8 : 0));
+}
 
-// Chain blocks stage the inverse of their diagonal block and the panel block of each
-// predecessor in shared memory before the predecessor's solution arrives (a ring of
-// CHAIN_NS buffers, CHAIN_NS - 1 blocks in flight: the last block of a long chain applies
-// every predecessor in turn, so its loop runs at the rate it can stream panel blocks), and
-// the step that waits only reads x_c and multiplies from shared memory.
-constexpr int CHAIN_NS = 4;
-constexpr int CHAIN_SMEM = (1 + CHAIN_NS) * TB * BLD * 8;
+// ---- chained dense solves with the diagonal block of a tiled-class supernode -----------
+// One CTA per 64-row block k of the diagonal block; block k consumes the solved blocks
+// c < k (forward) or c > k (backward) as they arrive and applies its own block through the
+// stored inverse T_k of the 64x64 diagonal block.  All CTAs of a chain are resident
+// together (a few hundred at most) and only wait on CTAs with a lower blockIdx, which the
+// hardware dispatches first.
+//
+// Warp w owns rows 8w .. 8w + 7 of the block's right-hand side v: it stages its eight rows
+// of each predecessor's panel block in its own shared-memory ring (cp.async, CHAIN_NS
+// slots, CHAIN_NS - 1 blocks ahead), holds them and its rows of T_k in registers, and lane
+// l multiplies columns l and l + 32; a butterfly of shuffles sums the eight rows across
+// the lanes (row 8w + (l >> 2) in every lane of quad l >> 2).  No block barrier until the
+// last predecessor is applied; then one barrier hands v to every warp for x_k = T_k v.
+// The step that waits for a predecessor's solution therefore only reads it, sixteen FMAs
+// and nine shuffles.
+constexpr int CHAIN_NS = 5;
+constexpr int LW = TB + 1;                      // padded row of a staged block
+constexpr int CHAIN_SLOT = 8 * LW;              // one warp's eight rows
+// Predecessors outside the cluster come from global memory in batches of up to CHAIN_XB
+// finished blocks: their counters are polled together and their solutions loaded together
+// (a lane keeps the two elements it multiplies, in its warp's batch buffer), so a batch
+// costs two memory round trips instead of two per block.
+constexpr int CHAIN_XB = 8;
+constexpr int CHAIN_SMEM = (CHAIN_NS * CHAIN_SLOT + CHAIN_XB * TB) * CHAIN_WARPS * 8;
 
 // Chains launch in thread-block clusters of CHAIN_CL consecutive tasks.  A block publishes its
-// solution through global memory and a flag (for the blocks of later clusters and the next
-// level's kernels) and also writes it straight into the shared memory of the later blocks
-// of its supernode in its own cluster (distributed shared memory), arriving on their
-// mbarriers: a hop inside a cluster does not go through L2.  Slot j of a block receives the
-// solution of cluster rank j.  Every CTA of a cluster (tail padding included) passes a
-// cluster barrier after the mbarrier set-up and another before it exits, so no block leaves
-// while a remote write to it may be in flight.
+// solution through global memory and its counter (for the blocks of later clusters and the
+// next level's kernels) and also writes it straight into the shared memory of the later blocks
+// of its supernode in its own cluster (distributed shared memory) with st.async, whose
+// transaction bytes complete the receiver's mbarrier of that sender slot: a hop inside a
+// cluster neither goes through L2 nor waits for a release fence.  Slot j of a block
+// receives the solution of cluster rank j (64 doubles, 512 transaction bytes, armed at
+// set-up).  Every CTA of a cluster (tail padding included) passes a cluster barrier after
+// the mbarrier set-up and another before it exits, so no block leaves while a remote
+// write to it may be in flight.
 constexpr int CHAIN_CL = 8;
 struct ChainCluster {
   double yin[CHAIN_CL][TB];
@@ -438,135 +451,203 @@ __device__ __forceinline__ uint32_t cluster_addr(const void *p, uint32_t rank) {
 }
 __device__ __forceinline__ void chain_cluster_init(ChainCluster &cc) {
   if (threadIdx.x == 0) {
-    for (int j = 0; j < CHAIN_CL; ++j)
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(&cc.bar[j])), "r"(TB)
+    for (int j = 0; j < CHAIN_CL; ++j) {
+      const uint32_t b = smem_addr(&cc.bar[j]);
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(b) : "memory");
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(b), "r"(TB * 8)
                    : "memory");
+    }
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   cluster_sync_all();
 }
-// Thread t < 64 of the producer (cluster rank `me`) sends element t of its solution to every
-// later rank of its cluster that holds a block of the same supernode (ranks me+1 .. last).
-__device__ __forceinline__ void chain_send(ChainCluster &cc, int me, int last, double val) {
-  if (threadIdx.x >= TB) return;
-  for (int q = me + 1; q <= last; ++q) {
-    asm volatile("st.shared::cluster.f64 [%0], %1;\n" ::"r"(cluster_addr(&cc.yin[me][threadIdx.x], q)),
-                 "d"(val)
+// Lane l (holding element `row` of this block's solution when (l & 3) == 0; every lane of
+// quad l >> 2 holds it) sends it to the later ranks me+1 .. last of its cluster, the four
+// lanes of a quad to different ranks.
+__device__ __forceinline__ void chain_send(ChainCluster &cc, int me, int last, int row, double val) {
+  for (int q = me + 1 + (threadIdx.x & 3); q <= last; q += 4)
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.f64 [%0], %1, [%2];\n" ::"r"(
+                     cluster_addr(&cc.yin[me][row], q)),
+                 "d"(val), "r"(cluster_addr(&cc.bar[me], q))
                  : "memory");
-    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];\n" ::"r"(
-                     cluster_addr(&cc.bar[me], q))
-                 : "memory");
-  }
 }
-// Thread 0 waits (bounded) for slot j's phase; everyone waits at the barrier; false after a
-// timeout (its own, or one another block recorded).
-__device__ bool chain_recv(ChainCluster &cc, int j, int *status) {
-  __shared__ int ok;
-  if (threadIdx.x == 0) {
-    long long it = 0;
-    const long long budget = wait_budget(status);
-    ok = 1;
-    for (;;) {
-      uint32_t done;
-      asm volatile(
-          "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 P1, [%1], 0;\n\t"
-          "selp.b32 %0, 1, 0, P1;\n\t}\n"
-          : "=r"(done)
-          : "r"(smem_addr(&cc.bar[j]))
-          : "memory");
-      if (done) break;
-      if (++it > budget || ((it & 31) == 0 && *(volatile int *)&status[2])) {
-        atomicExch(&status[2], 1);
-        ok = 0;
-        break;
-      }
+// Every lane waits (bounded) for slot j's 512 bytes; false after a timeout (its own, or
+// one another block recorded) in any lane.
+__device__ bool warp_chain_recv(ChainCluster &cc, int j, int *status) {
+  const uint32_t b = smem_addr(&cc.bar[j]);
+  const long long budget = wait_budget(status);
+  long long it = 0;
+  int ok = 1;
+  for (;;) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 P1, [%1], 0;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(done)
+        : "r"(b)
+        : "memory");
+    if (done) break;
+    if (++it > budget || ((it & 31) == 0 && *(volatile int *)&status[2])) {
+      atomicExch(&status[2], 1);
+      ok = 0;
+      break;
     }
   }
-  __syncthreads();
-  return ok != 0;
+  return __all_sync(0xffffffffu, ok) != 0;
+}
+
+// Sum over the lanes of a[i] (this lane's part of row 8w + i): the total of row
+// 8w + ((lane >> 2) & 7), in every lane of the quad.
+__device__ __forceinline__ double warp_rows8(double (&a)[8], int lane) {
+  const unsigned F = 0xffffffffu;
+  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const double o = __shfl_xor_sync(F, b4 ? a[i] : a[i + 4], 16);
+    a[i] = (b4 ? a[i + 4] : a[i]) + o;
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const double o = __shfl_xor_sync(F, b3 ? a[i] : a[i + 2], 8);
+    a[i] = (b3 ? a[i + 2] : a[i]) + o;
+  }
+  {
+    const double o = __shfl_xor_sync(F, b2 ? a[0] : a[1], 4);
+    a[0] = (b2 ? a[1] : a[0]) + o;
+  }
+  a[0] += __shfl_xor_sync(F, a[0], 2);
+  a[0] += __shfl_xor_sync(F, a[0], 1);
+  return a[0];
 }
 
 // task = (s, k); forward: y[f + 64k ..] := T_k (y[...] - contributions - sum_{c<k} L_kc x_c)
-// (tasks of a supernode consecutive, in increasing k; CTAs from `count` on are padding)
-__global__ void __launch_bounds__(ST) k_fwd_chain(DevSym S, const int2 *tasks, int count,
-                                                  double *y, const double *contrib,
-                                                  const int *cptr, const int *cidx, int *flags,
-                                                  int epoch, int n, int64_t cstride) {
+// (tasks of a supernode consecutive, in increasing k; CTAs from `count` on are padding).
+// Warp w takes columns 8w .. 8w + 7 of every L_kc (eight contiguous 512-byte column pieces
+// of the panel, staged by the warp alone) and keeps its partial sums of all 64 rows (rows
+// l and l + 32 in lane l); the eight warps' partial sums meet once, after the last
+// predecessor, and x_k = T_k v is then formed with warp w owning rows 8w .. 8w + 7.
+__global__ void __launch_bounds__(ST, 1) k_fwd_chain(DevSym S, const int2 *tasks, int count,
+                                                     double *y, const double *contrib,
+                                                     const int *cptr, const int *cidx, int *flags,
+                                                     int epoch, int n, int64_t cstride) {
   extern __shared__ double csm[];
-  double *Ts = csm, *Lb0 = csm + TB * BLD;   // ring: Lb0 + j * TB * BLD, j < CHAIN_NS
-  __shared__ double v[TB], part[4][TB], xc[TB];
+  __shared__ double vs[TB], part[CHAIN_WARPS][TB];
   __shared__ ChainCluster cc;
   chain_cluster_init(cc);
   const int me = (int)chain_rank();
   if ((int)blockIdx.x < count) {
     const int s = tasks[blockIdx.x].x, k = tasks[blockIdx.x].y;
-    const int tid = threadIdx.x, r = tid & (TB - 1), q = tid >> 6;
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, w8 = wp * 8;
+    const int row = w8 + ((lane >> 2) & 7);   // the row of x_k this lane's sums belong to
     const int f = S.super[s], w = S.super[s + 1] - f;
     const int m = (int)(S.rowptr[s + 1] - S.rowptr[s]);
     const double *P = S.L + S.xptr[s];
     const int r0 = k * TB, bw = min(TB, w - r0);
     const int nb = (w + TB - 1) / TB;
     const int base = S.dinv_off[s];
-    const double *T = S.dinv + ((size_t)base + k) * (TB * TB);
+    const double *T = S.dinv + ((size_t)base + k) * (TB * TB);   // T(r, c) at T[c * 64 + r]
     // predecessors c >= cfirst are in this cluster (rank me - (k - c)); the later ranks of
     // the same supernode receive this block's solution
     const int cfirst = k - me, last = me + min(nb - 1 - k, CHAIN_CL - 1 - me);
-    stage_block(Ts, T, TB, TB, TB);                 // T(r, c) at Ts[c * BLD + r]
-    // L_kc(r, jj) at Lb0[(c % CHAIN_NS) * TB * BLD + jj * BLD + r]; one cp.async group per c
-    for (int c = 0; c < CHAIN_NS - 1; ++c) {
-      if (c < k) stage_block(Lb0 + c * (TB * BLD), P + (size_t)c * TB * m + r0, m, bw, TB);
-      else stage_commit();
-    }
-    // right-hand side of the block minus the descendants' contributions
-    if (tid < TB) {
-      double acc = 0.0;
-      if (tid < bw) {
-        const int j = f + r0 + tid;
-        acc = y[j];
-        for (int qq = cptr[j]; qq < cptr[j + 1]; ++qq) acc -= contrib[cidx[qq]];
+    double *ring = csm + wp * CHAIN_SLOT;   // slot j at ring + j * CHAIN_WARPS * CHAIN_SLOT
+    double *xw = csm + CHAIN_NS * CHAIN_WARPS * CHAIN_SLOT + wp * (CHAIN_XB * TB);
+    // this warp's columns of L_kc: element (r, 8w + q) = P[(64c + 8w + q) m + r0 + r] at
+    // [q * LW + r] (a warp instruction copies 32 consecutive rows of one column)
+    auto stage = [&](int c) {
+      if (c < k) {
+        double *d = ring + (c % CHAIN_NS) * CHAIN_WARPS * CHAIN_SLOT;
+        const double *src = P + (size_t)(c * TB + w8) * m + r0;
+#pragma unroll 4
+        for (int t = 0; t < 16; ++t) {
+          const int e = lane + 32 * t, q = e >> 6, r = e & (TB - 1);
+          const bool in = r < bw;
+          cp8(d + q * LW + r, in ? src + (size_t)q * m + r : src, in);
+        }
       }
-      v[tid] = acc;
-    }
-    bool ok = true;
-    for (int c = 0; c < k && ok; ++c) {
-      const double *Lc = Lb0 + (c % CHAIN_NS) * (TB * BLD);
-      const int cn = c + CHAIN_NS - 1;   // the block staged now, into the buffer freed last step
-      if (cn < k) stage_block(Lb0 + (cn % CHAIN_NS) * (TB * BLD), P + (size_t)cn * TB * m + r0, m, bw, TB);
-      else stage_commit();
-      stage_wait<CHAIN_NS - 1>();        // block c has landed
-      if (c >= cfirst) {   // from the cluster (ends with a barrier)
-        const int j = me - (k - c);
-        if (!chain_recv(cc, j, S.status)) { ok = false; break; }
-        if (tid < TB) xc[tid] = cc.yin[j][tid];
-      } else {             // from global memory (ends with a barrier)
-        if (!wait_flag(&flags[base + c], epoch, S.status)) { ok = false; break; }
-        if (tid < TB) xc[tid] = __ldcg(&y[f + c * TB + tid]);
-      }
-      __syncthreads();
-      double acc = 0.0;
+      stage_commit();
+    };
+    for (int c = 0; c < CHAIN_NS - 1; ++c) stage(c);
+    double tr[8][2];
 #pragma unroll
-      for (int jj = q * 16; jj < q * 16 + 16; ++jj) acc = fma(Lc[jj * BLD + r], xc[jj], acc);
-      part[q][r] = acc;
-      __syncthreads();
-      if (tid < TB) v[tid] -= (part[0][tid] + part[1][tid]) + (part[2][tid] + part[3][tid]);
+    for (int i = 0; i < 8; ++i) {
+      tr[i][0] = T[(size_t)lane * TB + w8 + i];
+      tr[i][1] = T[(size_t)(lane + 32) * TB + w8 + i];
+    }
+    // right-hand side minus the descendants' contributions (read after the last barrier)
+    if (threadIdx.x < TB) {
+      double v = 0.0;
+      if ((int)threadIdx.x < bw) {
+        const int j = f + r0 + threadIdx.x;
+        v = y[j];
+        for (int qq = cptr[j]; qq < cptr[j + 1]; ++qq) v -= contrib[cidx[qq]];
+      }
+      vs[threadIdx.x] = v;
+    }
+    double acc0 = 0.0, acc1 = 0.0;   // rows lane, lane + 32 over this warp's columns
+    bool ok = true;
+    int xb0 = 0, nbt = 0;            // the batch in xw: blocks xb0 .. xb0 + nbt - 1
+    for (int c = 0; c < k; ++c) {
+      stage(c + CHAIN_NS - 1);           // into the slot freed by step c - 1
+      stage_wait<CHAIN_NS - 1>();        // block c has landed (this lane's copies)
+      __syncwarp();
+      const double *Lc = ring + (c % CHAIN_NS) * CHAIN_WARPS * CHAIN_SLOT;
+      double lr[8][2];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        lr[q][0] = Lc[q * LW + lane];
+        lr[q][1] = Lc[q * LW + lane + 32];
+      }
+      __syncwarp();                      // the slot is refilled at step c + 1
+      const double *xc;                  // x_c(8w + q) at xc[q]
+      if (c >= cfirst) {   // from the cluster
+        const int j = me - (k - c);
+        if (!warp_chain_recv(cc, j, S.status)) { ok = false; break; }
+        xc = &cc.yin[j][w8];
+      } else {             // from global memory, a batch of finished blocks at a time
+        if (c >= xb0 + nbt) {
+          xb0 = c;
+          nbt = warp_wait_prefix(&flags[base + c], 1, min(CHAIN_XB, cfirst - c), CHAIN_WARPS * epoch,
+                                 S.status);
+          if (nbt == 0) { ok = false; break; }
+          // x_{c+u}(8w + q) into xw[u * 8 + q], lane = u * 8 + q (two rounds of four blocks)
+          const int q = lane & 7, u = lane >> 3;
+          const double a0 = u < nbt ? __ldcg(&y[f + (c + u) * TB + w8 + q]) : 0.0;
+          const double a1 = u + 4 < nbt ? __ldcg(&y[f + (c + u + 4) * TB + w8 + q]) : 0.0;
+          xw[lane] = a0;
+          xw[lane + 32] = a1;
+          __syncwarp();
+        }
+        xc = xw + (c - xb0) * 8;
+      }
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const double xq = xc[q];
+        acc0 = fma(lr[q][0], xq, acc0);
+        acc1 = fma(lr[q][1], xq, acc1);
+      }
+      __syncwarp();                      // xw is rewritten by the next batch
     }
     stage_wait<0>();
-    __syncthreads();
+    part[wp][lane] = acc0;
+    part[wp][lane + 32] = acc1;
+    ok = __syncthreads_and(ok) != 0;
     if (ok) {
-      // x_k = T_k v
-      double acc = 0.0;
+      // v(j) for j = lane, lane + 32; then x_k = T_k v
+      double x0 = vs[lane], x1 = vs[lane + 32];
 #pragma unroll
-      for (int jj = q * 16; jj < q * 16 + 16; ++jj) acc = fma(Ts[jj * BLD + r], v[jj], acc);
-      part[q][r] = acc;
-      __syncthreads();
-      const double xk = (part[0][r] + part[1][r]) + (part[2][r] + part[3][r]);
-      // the cluster's later blocks first: each arrive releases only the thread's earlier
-      // stores, which then do not yet include the global one
-      chain_send(cc, me, last, tid < bw ? xk : 0.0);
-      if (tid < bw) y[f + r0 + tid] = xk;
-      __threadfence();
-      __syncthreads();
-      if (tid == 0) st_release(&flags[base + k], epoch);
+      for (int g = 0; g < CHAIN_WARPS; ++g) {
+        x0 -= part[g][lane];
+        x1 -= part[g][lane + 32];
+      }
+      double a[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) a[i] = fma(tr[i][1], x1, tr[i][0] * x0);
+      const double xk = warp_rows8(a, lane);
+      // the cluster's later blocks first, then global memory and the counter
+      chain_send(cc, me, last, row, row < bw ? xk : 0.0);
+      if ((lane & 3) == 0 && row < bw) y[f + r0 + row] = xk;
+      __syncwarp();
+      if (lane == 0) red_release_add(&flags[base + k], 1);
     }
   }
   cluster_sync_all();
@@ -574,79 +655,118 @@ __global__ void __launch_bounds__(ST) k_fwd_chain(DevSym S, const int2 *tasks, i
 
 // task = (s, k) in decreasing k; backward: x[f + 64k ..] := T_k^T (x[...] - sum_{c>k} L_ck^T x_c)
 // (tasks of a supernode consecutive, in decreasing k; CTAs from `count` on are padding)
-__global__ void __launch_bounds__(ST) k_bwd_chain(DevSym S, const int2 *tasks, int count,
+__global__ void __launch_bounds__(ST, 1) k_bwd_chain(DevSym S, const int2 *tasks, int count,
                                                   double *x, int *flags, int epoch) {
   extern __shared__ double csm[];
-  double *Ts = csm, *Lb0 = csm + TB * BLD;   // ring of CHAIN_NS buffers
-  __shared__ double v[TB], part[4][TB], xc[TB];
+  __shared__ double vs[TB];
   __shared__ ChainCluster cc;
   chain_cluster_init(cc);
   const int me = (int)chain_rank();
   if ((int)blockIdx.x < count) {
     const int s = tasks[blockIdx.x].x, k = tasks[blockIdx.x].y;
-    const int tid = threadIdx.x, i = tid & (TB - 1), q = tid >> 6;
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, w8 = wp * 8;
+    const int row = w8 + ((lane >> 2) & 7);
     const int f = S.super[s], w = S.super[s + 1] - f;
     const int m = (int)(S.rowptr[s + 1] - S.rowptr[s]);
     const double *P = S.L + S.xptr[s];
     const int r0 = k * TB, bw = min(TB, w - r0);
     const int nb = (w + TB - 1) / TB;
     const int base = S.dinv_off[s];
-    const double *T = S.dinv + ((size_t)base + k) * (TB * TB);
+    const double *T = S.dinv + ((size_t)base + k) * (TB * TB);   // T(r, c) at T[c * 64 + r]
     // successors c <= clast are in this cluster (rank me - (c - k)); the later ranks (lower
     // k) of the same supernode receive this block's solution
     const int clast = k + me, last = me + min(k, CHAIN_CL - 1 - me);
-    // panel block (c, k): rows 64c + rr, columns r0 + i, staged as Lc[i * BLD + rr]
-    stage_block(Ts, T, TB, TB, TB);   // T(rr, i) at Ts[i * BLD + rr]
-    // successor step t = nb - 1 - c (c = nb - 1 first): block (c, k) in buffer t % CHAIN_NS
-    auto stage_succ = [&](int t) {
+    double *ring = csm + wp * CHAIN_SLOT;
+    double *xw = csm + CHAIN_NS * CHAIN_WARPS * CHAIN_SLOT + wp * (CHAIN_XB * TB);
+    // successor step t = nb - 1 - c (c = nb - 1 first); this warp's columns of block (c, k):
+    // element (i, rr) = P[(r0 + w8 + i) m + 64c + rr] at [i * LW + rr]
+    auto stage = [&](int t) {
       const int c = nb - 1 - t;
-      if (c > k)
-        stage_block(Lb0 + (t % CHAIN_NS) * (TB * BLD), P + (size_t)r0 * m + c * TB, m,
-                    min(TB, w - c * TB), bw);
-      else
-        stage_commit();
+      if (c > k) {
+        double *d = ring + (t % CHAIN_NS) * CHAIN_WARPS * CHAIN_SLOT;
+        const int cw = min(TB, w - c * TB);
+        const double *src = P + (size_t)(r0 + w8) * m + c * TB;
+#pragma unroll 4
+        for (int u = 0; u < 16; ++u) {
+          const int e = lane + 32 * u, i = e >> 6, rr = e & 63;
+          const bool in = w8 + i < bw && rr < cw;
+          cp8(d + i * LW + rr, in ? src + (size_t)i * m + rr : src, in);
+        }
+      }
+      stage_commit();
     };
-    for (int t = 0; t < CHAIN_NS - 1; ++t) stage_succ(t);
-    if (tid < TB) v[tid] = (tid < bw) ? x[f + r0 + tid] : 0.0;
+    for (int t = 0; t < CHAIN_NS - 1; ++t) stage(t);
+    double tr[8][2];   // T(rr, w8 + i) for rr = lane, lane + 32
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      tr[i][0] = T[(size_t)(w8 + i) * TB + lane];
+      tr[i][1] = T[(size_t)(w8 + i) * TB + lane + 32];
+    }
+    double v = (row < bw) ? x[f + r0 + row] : 0.0;
     bool ok = true;
+    int xb0 = nb, nbt = 0;               // the batch in xw: blocks xb0, .., xb0 - nbt + 1
     for (int c = nb - 1; c > k; --c) {
       const int t = nb - 1 - c;
-      const double *Lc = Lb0 + (t % CHAIN_NS) * (TB * BLD);
-      stage_succ(t + CHAIN_NS - 1);
-      stage_wait<CHAIN_NS - 1>();        // block (c, k) has landed
-      const int cw = min(TB, w - c * TB);
-      if (c <= clast) {   // from the cluster (ends with a barrier)
-        const int j = me - (c - k);
-        if (!chain_recv(cc, j, S.status)) { ok = false; break; }
-        if (tid < TB) xc[tid] = cc.yin[j][tid];
-      } else {            // from global memory (ends with a barrier)
-        if (!wait_flag(&flags[base + c], epoch, S.status)) { ok = false; break; }
-        if (tid < TB) xc[tid] = (tid < cw) ? __ldcg(&x[f + c * TB + tid]) : 0.0;
-      }
-      __syncthreads();
-      // v[i] -= sum_rr L(64c + rr, r0 + i) x_c[rr]
-      double acc = 0.0;
+      stage(t + CHAIN_NS - 1);
+      stage_wait<CHAIN_NS - 1>();        // block (c, k) has landed (this lane's copies)
+      __syncwarp();
+      const double *Lc = ring + (t % CHAIN_NS) * CHAIN_WARPS * CHAIN_SLOT;
+      double lr[8][2];
 #pragma unroll
-      for (int rr = q * 16; rr < q * 16 + 16; ++rr) acc = fma(Lc[i * BLD + rr], xc[rr], acc);
-      part[q][i] = acc;
-      __syncthreads();
-      if (tid < TB) v[tid] -= (part[0][tid] + part[1][tid]) + (part[2][tid] + part[3][tid]);
+      for (int i = 0; i < 8; ++i) {
+        lr[i][0] = Lc[i * LW + lane];
+        lr[i][1] = Lc[i * LW + lane + 32];
+      }
+      __syncwarp();
+      double x0, x1;
+      if (c <= clast) {   // from the cluster
+        const int j = me - (c - k);
+        if (!warp_chain_recv(cc, j, S.status)) { ok = false; break; }
+        x0 = cc.yin[j][lane];
+        x1 = cc.yin[j][lane + 32];
+      } else {            // from global memory, a batch of blocks c, c - 1, .. at a time
+        if (c <= xb0 - nbt) {
+          xb0 = c;                         // blocks c, c - 1, .., c - nbt + 1
+          nbt = warp_wait_prefix(&flags[base + c], -1, min(CHAIN_XB, c - clast), CHAIN_WARPS * epoch,
+                                 S.status);
+          if (nbt == 0) { ok = false; break; }
+          double t2[CHAIN_XB][2];
+#pragma unroll
+          for (int u = 0; u < CHAIN_XB; ++u)
+            if (u < nbt) {
+              const int cu = c - u, cwu = min(TB, w - cu * TB);
+              t2[u][0] = lane < cwu ? __ldcg(&x[f + cu * TB + lane]) : 0.0;
+              t2[u][1] = lane + 32 < cwu ? __ldcg(&x[f + cu * TB + lane + 32]) : 0.0;
+            }
+#pragma unroll
+          for (int u = 0; u < CHAIN_XB; ++u)
+            if (u < nbt) {
+              xw[u * TB + lane] = t2[u][0];
+              xw[u * TB + lane + 32] = t2[u][1];
+            }
+        }
+        x0 = xw[(xb0 - c) * TB + lane];   // written by this lane
+        x1 = xw[(xb0 - c) * TB + lane + 32];
+      }
+      double a[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) a[i] = fma(lr[i][1], x1, lr[i][0] * x0);
+      v -= warp_rows8(a, lane);
     }
     stage_wait<0>();
-    __syncthreads();
+    if ((lane & 3) == 0) vs[row] = v;
+    ok = __syncthreads_and(ok) != 0;
     if (ok) {
-      // x_k[i] = sum_{rr >= i} T(rr, i) v[rr]
-      double acc = 0.0;
+      // x_k[i] = sum_rr T(rr, i) v[rr]
+      const double x0 = vs[lane], x1 = vs[lane + 32];
+      double a[8];
 #pragma unroll
-      for (int rr = q * 16; rr < q * 16 + 16; ++rr) acc = fma(Ts[i * BLD + rr], v[rr], acc);
-      part[q][i] = acc;
-      __syncthreads();
-      const double xk = (part[0][i] + part[1][i]) + (part[2][i] + part[3][i]);
-      chain_send(cc, me, last, tid < bw ? xk : 0.0);   // before the global store (above)
-      if (tid < bw) x[f + r0 + tid] = xk;
-      __threadfence();
-      __syncthreads();
-      if (tid == 0) st_release(&flags[base + k], epoch);
+      for (int i = 0; i < 8; ++i) a[i] = fma(tr[i][1], x1, tr[i][0] * x0);
+      const double xk = warp_rows8(a, lane);
+      chain_send(cc, me, last, row, row < bw ? xk : 0.0);
+      if ((lane & 3) == 0 && row < bw) x[f + r0 + row] = xk;
+      __syncwarp();
+      if (lane == 0) red_release_add(&flags[base + k], 1);
     }
   }
   cluster_sync_all();
