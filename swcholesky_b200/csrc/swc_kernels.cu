@@ -654,7 +654,9 @@ __global__ void __launch_bounds__(MT, 4) k_update_tiles(DevSym S, const int4 *ta
 // array with leading dimension DLD; E (the inverse, lower triangular) holds only its 36
 // lower 8x8 blocks, packed: block (bi, bk), bi >= bk, at (bi (bi + 1) / 2 + bk) * 64, each
 // block column-major.  128 threads (4 warps).
-constexpr int DLD = TB + 1;
+// DLD = 68: the 8x8 DMMA operand loads (lane 4g + kq reads row g, column kq of a block)
+// hit 16 different bank pairs per half warp (68 = 4 mod 16); 65 gave four-way conflicts.
+constexpr int DLD = TB + 4;
 constexpr int E_ELEMS = 36 * 64;
 
 __device__ __forceinline__ int eix(int r, int c) {
@@ -688,41 +690,43 @@ __device__ __forceinline__ void store8(const double (&c)[2], double *X, int r0, 
 }
 
 // Warp-level Cholesky of the 8x8 diagonal block kb of D and its inverse into E (same
-// position).  Lane 4r + q holds row r, columns 2q and 2q+1; the scaled pivot column reaches
-// the other lanes by shuffles (no shared-memory round trip).
+// position).  Every lane factors the whole block in registers (broadcast loads of its 36
+// entries), so the chain of pivots is one reciprocal square root, one product and one
+// FMA per column with no shuffle on it; lane j < 8 then forms column j of the inverse by
+// forward substitution.
 __device__ void potrf8_inv8(double *D, double *E, int kb, const DevSym &S, int gcol0, int bw,
                             bool report) {
-  const unsigned FULL = 0xffffffffu;
-  const int lane = threadIdx.x & 31, r = lane >> 2, q = lane & 3, k0 = 8 * kb;
-  double x0 = (2 * q <= r) ? D[(k0 + 2 * q) * DLD + k0 + r] : 0.0;
-  double x1 = (2 * q + 1 <= r) ? D[(k0 + 2 * q + 1) * DLD + k0 + r] : 0.0;
-  double rd_row = 0.0;   // 1 / L(r, r)
+  const int lane = threadIdx.x & 31, k0 = 8 * kb;
+  double a[8][8];
 #pragma unroll
-  for (int c = 0; c < 8; ++c) {
-    const int qc = c >> 1;
-    const bool odd = c & 1;
-    const double piv = __shfl_sync(FULL, odd ? x1 : x0, 4 * c + qc);
-    const double inv = rsqrt(piv), dsq = piv * inv;
-    if (report && lane == 0 && k0 + c < bw && !(piv > 0.0))
-      atomicMin(&S.status[0], gcol0 + k0 + c + 1);
-    if (q == qc && r >= c) {
-      const double v = (r == c) ? dsq : (odd ? x1 : x0) * inv;
-      if (odd) x1 = v; else x0 = v;
-    }
-    if (r == c) rd_row = inv;
-    const double lrc = __shfl_sync(FULL, odd ? x1 : x0, 4 * r + qc);
-    const double l0 = __shfl_sync(FULL, odd ? x1 : x0, 8 * q + qc);
-    const double l1 = __shfl_sync(FULL, odd ? x1 : x0, 8 * q + 4 + qc);
-    if (2 * q > c && 2 * q <= r) x0 = fma(-lrc, l0, x0);
-    if (2 * q + 1 > c && 2 * q + 1 <= r) x1 = fma(-lrc, l1, x1);
+  for (int j = 0; j < 8; ++j)
+#pragma unroll
+    for (int i = j; i < 8; ++i) a[i][j] = D[(k0 + j) * DLD + k0 + i];
+  double rinv[8];
+  int bad = 8;   // first column with a pivot <= 0 or NaN (reported after the chain)
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const double piv = a[j][j];
+    const double inv = rsqrt(piv);
+    if (!(piv > 0.0) && j < bad) bad = j;
+    rinv[j] = inv;
+    a[j][j] = piv * inv;
+#pragma unroll
+    for (int i = j + 1; i < 8; ++i) a[i][j] *= inv;
+    // the next pivot first
+#pragma unroll
+    for (int k = j + 1; k < 8; ++k)
+#pragma unroll
+      for (int i = k; i < 8; ++i) a[i][k] = fma(-a[i][j], a[k][j], a[i][k]);
   }
-  if (2 * q <= r) D[(k0 + 2 * q) * DLD + k0 + r] = x0;
-  if (2 * q + 1 <= r) D[(k0 + 2 * q + 1) * DLD + k0 + r] = x1;
-  double rd[8];
+  if (report && lane == 0 && bad < 8 && k0 + bad < bw) atomicMin(&S.status[0], gcol0 + k0 + bad + 1);
+  // every lane stores the same 36 values (one write per address; no lane-dependent index
+  // into a[][], which would move the array to local memory)
 #pragma unroll
-  for (int i = 0; i < 8; ++i) rd[i] = __shfl_sync(FULL, rd_row, 4 * i);
-  __syncwarp();
-  // lane j < 8: column j of the inverse by forward substitution, 1/L(i,i) = rd[i]
+  for (int j = 0; j < 8; ++j)
+#pragma unroll
+    for (int i = j; i < 8; ++i) D[(k0 + j) * DLD + k0 + i] = a[i][j];
+  // lane j < 8: column j of the inverse, 1/L(i,i) = rinv[i]
   const int j = lane & 7;
   double t[8];
 #pragma unroll
@@ -730,8 +734,8 @@ __device__ void potrf8_inv8(double *D, double *E, int kb, const DevSym &S, int g
     double sacc = 0.0;
 #pragma unroll
     for (int k = 0; k < i; ++k)
-      if (k >= j) sacc = fma(D[(k0 + k) * DLD + k0 + i], t[k], sacc);
-    t[i] = (i < j) ? 0.0 : ((i == j) ? rd[i] : -sacc * rd[i]);
+      if (k >= j) sacc = fma(a[i][k], t[k], sacc);
+    t[i] = (i < j) ? 0.0 : ((i == j) ? rinv[i] : -sacc * rinv[i]);
   }
   if (lane < 8) {
 #pragma unroll
@@ -774,16 +778,31 @@ __device__ void potrf64_blocked(double *D, double *E, int bw, const DevSym &S, i
       __syncwarp();
       potrf8_inv8(D, E, nb, S, gcol0, bw, true);
     } else {
-      int q = 0;
-      for (int jb = kb + 1; jb < nbk; ++jb)
-        for (int ib = jb; ib < nbk; ++ib) {
-          if (ib == kb + 1) continue;   // (kb+1, kb+1) belongs to warp 0
-          if ((q++ % (NW - 1)) != warp - 1) continue;
-          double c[2];
-          load8(c, D, 8 * ib, 8 * jb);
-          mma8_abt(c, D, 8 * ib, 8 * kb, D, 8 * jb, 8 * kb, true);
-          store8(c, D, 8 * ib, 8 * jb, ib == jb);
-        }
+      // blocks (ib, jb), kb < jb <= ib < nbk, except (kb+1, kb+1), in column order; warp
+      // w > 0 takes the blocks w - 1, w - 1 + (NW - 1), .. and runs them interleaved
+      // (independent DMMA chains: their latency, not their issue, bounds a short chain)
+      constexpr int MAXT = (27 + NW - 2) / (NW - 1);
+      const int nrem = nbk - kb - 1;                       // block rows/columns left
+      const int ntot = nrem * (nrem + 1) / 2 - 1;
+      double c[MAXT][2];
+      int bi[MAXT], bj[MAXT];
+#pragma unroll
+      for (int t = 0; t < MAXT; ++t) {
+        int idx = warp - 1 + (NW - 1) * t;
+        if (idx >= ntot) idx = -1;  // an unused slot: block (kb+1, kb+1), nothing stored
+        idx += 1;                   // skip (kb+1, kb+1), the first block of the order
+        int jj = 0;
+        while (idx >= nrem - jj) { idx -= nrem - jj; ++jj; }
+        bj[t] = 8 * (kb + 1 + jj);
+        bi[t] = bj[t] + 8 * idx;
+        load8(c[t], D, bi[t], bj[t]);
+      }
+#pragma unroll
+      for (int t = 0; t < MAXT; ++t)
+        if (warp - 1 + (NW - 1) * t < ntot) mma8_abt(c[t], D, bi[t], 8 * kb, D, bj[t], 8 * kb, true);
+#pragma unroll
+      for (int t = 0; t < MAXT; ++t)
+        if (warp - 1 + (NW - 1) * t < ntot) store8(c[t], D, bi[t], bj[t], bi[t] == bj[t]);
     }
     __syncthreads();
   }
@@ -850,60 +869,65 @@ __device__ void factor_diag_block(const DevSym &S, int s, int c0, double *smem,
   double *P = S.L + S.xptr[s];
   const int bw = min(TB, w - c0);
   __syncthreads();
-  // eight loads in flight per thread before the shared stores
+  // the tile and, with PREV, X = rows c0.. of column block c0/64 - 1 (64 wide, [column][row]
+  // after D): eight loads of each in flight per thread before the shared stores
+  double *Xs = D + TB * DLD;
+  const int nr = min(TB, m - c0);
   for (int e0 = tid; e0 < TB * TB; e0 += 8 * NTH) {
-    double v[8];
+    double v[8], xv[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
       const int e = e0 + q * NTH, c = e >> 6, r = e & (TB - 1);
       if (c < bw && r < bw) v[q] = (!upd && r >= c) ? P[(size_t)(c0 + c) * m + c0 + r] : 0.0;
       else v[q] = (r == c) ? 1.0 : 0.0;
+      if (PREV) xv[q] = r < nr ? P[(size_t)(c0 - TB + c) * m + c0 + r] : 0.0;
     }
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
       const int e = e0 + q * NTH;
       D[(e >> 6) * DLD + (e & (TB - 1))] = v[q];
+      if (PREV) Xs[(e >> 6) * DLD + (e & (TB - 1))] = xv[q];
     }
   }
   for (int e = tid; e < E_ELEMS; e += blockDim.x) E[e] = 0.0;
   if (PREV) {
-    // X = rows c0.. of column block c0/64 - 1 (64 wide), [column][row] after D
-    double *Xs = D + TB * DLD;
-    const int nr = min(TB, m - c0);
-    for (int e0 = tid; e0 < TB * TB; e0 += 8 * NTH) {
-      double v[8];
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const int e = e0 + q * NTH, k = e >> 6, r = e & (TB - 1);
-        v[q] = r < nr ? P[(size_t)(c0 - TB + k) * m + c0 + r] : 0.0;
-      }
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const int e = e0 + q * NTH;
-        Xs[(e >> 6) * DLD + (e & (TB - 1))] = v[q];
-      }
-    }
     __syncthreads();
-    // tile -= X X^T over the lower 8x8 blocks (DMMA), block columns of the diagonal block only
+    // tile -= X X^T over the lower 8x8 blocks (DMMA), block columns of the diagonal block
+    // only.  Blocks in column order (column bj holds 8 - bj of them); warp w takes blocks
+    // w, w + NW, .. and runs their DMMA chains interleaved (independent accumulators).
+    constexpr int MAXB = (36 + NW - 1) / NW;
     const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, qq = lane & 3;
-    int blk = 0;
-    for (int bj = 0; bj < (bw + 7) / 8; ++bj)
-      for (int bi = bj; bi < TB / 8; ++bi, ++blk) {
-        if (blk % NW != warp) continue;
-        double acc[2] = {0.0, 0.0};
+    const int nbj = (bw + 7) / 8, nblk = 8 * nbj - nbj * (nbj - 1) / 2;
+    double acc[MAXB][2];
+    int ar[MAXB], br[MAXB];
 #pragma unroll
-        for (int k0 = 0; k0 < TB; k0 += 8) mma8_abt(acc, Xs, 8 * bi, k0, Xs, 8 * bj, k0, false);
+    for (int q = 0; q < MAXB; ++q) {
+      acc[q][0] = acc[q][1] = 0.0;
+      int blk = warp + NW * q, bj = 0;
+      if (blk >= nblk) blk = 0;   // unused slot: a valid block, its result dropped below
+      while (blk >= 8 - bj) { blk -= 8 - bj; ++bj; }
+      ar[q] = 8 * (bj + blk);
+      br[q] = 8 * bj;
+    }
 #pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          const int r = 8 * bi + g, c = 8 * bj + 2 * qq + e;
-          if (c >= bw) continue;
-          if (r < bw) {
-            if (r >= c) D[c * DLD + r] -= acc[e];
-          } else if (c0 + r < m) {   // a partial last block: panel rows below it, in L
-            P[(size_t)(c0 + c) * m + c0 + r] -= acc[e];
-          }
+    for (int k0 = 0; k0 < TB; k0 += 8)
+#pragma unroll
+      for (int q = 0; q < MAXB; ++q)
+        if (warp + NW * q < nblk) mma8_abt(acc[q], Xs, ar[q], k0, Xs, br[q], k0, false);
+#pragma unroll
+    for (int q = 0; q < MAXB; ++q) {
+      if (warp + NW * q >= nblk) continue;
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int r = ar[q] + g, c = br[q] + 2 * qq + e;
+        if (c >= bw) continue;
+        if (r < bw) {
+          if (r >= c) D[c * DLD + r] -= acc[q][e];
+        } else if (c0 + r < m) {   // a partial last block: panel rows below it, in L
+          P[(size_t)(c0 + c) * m + c0 + r] -= acc[q][e];
         }
       }
+    }
   }
   if (upd) {
     __syncthreads();
