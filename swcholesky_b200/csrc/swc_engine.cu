@@ -950,7 +950,17 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
       SP.chain_off.push_back((int)SP.fchain.size());
       SP.contrib_off.push_back((int)SP.contrib_tasks.size());
       SP.gather_off.push_back((int)SP.gather_tasks.size());
-      std::vector<int2> narrow;
+      std::vector<int2> narrow, wide;
+      // 128-row tasks of 8 warps for the wide supernodes only when the level has enough of
+      // them to fill the GPU; otherwise 32-row tasks of 32 warps (more, shorter CTAs)
+      int64_t n128 = 0;
+      for (int s : bylev[l]) {
+        const int w = super[s + 1] - super[s];
+        const int64_t m = rowptr[s + 1] - rowptr[s];
+        if (w > SOLVE_NARROW_W && (H.dinv_off[s] >= 0 || !(warp_level[l] && warp_size_ok(s))))
+          n128 += (m - w + SOLVE_CONTRIB_WIDE_ROWS - 1) / SOLVE_CONTRIB_WIDE_ROWS;
+      }
+      const bool wide_level = n128 >= SOLVE_CONTRIB_WIDE_MIN;
       for (int s : bylev[l]) {
         const int w = super[s + 1] - super[s];
         const int m = (int)(rowptr[s + 1] - rowptr[s]);
@@ -964,12 +974,18 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
         } else {
           SP.list.push_back(s);
         }
-        for (int r0 = w; r0 < m; r0 += SOLVE_CONTRIB_ROWS)
-          (w > SOLVE_NARROW_W ? SP.contrib_tasks : narrow).push_back(make_int2(s, r0));
+        if (w > SOLVE_CONTRIB_BIG_W || (w > SOLVE_NARROW_W && !wide_level))
+          for (int r0 = w; r0 < m; r0 += SOLVE_CONTRIB_ROWS) SP.contrib_tasks.push_back(make_int2(s, r0));
+        else if (w > SOLVE_NARROW_W)
+          for (int r0 = w; r0 < m; r0 += SOLVE_CONTRIB_WIDE_ROWS) wide.push_back(make_int2(s, r0));
+        else
+          for (int r0 = w; r0 < m; r0 += SOLVE_CONTRIB_ROWS) narrow.push_back(make_int2(s, r0));
         if (m > w)
           for (int j0 = 0; j0 < w; j0 += SOLVE_GATHER_COLS) SP.gather_tasks.push_back(make_int2(s, j0));
       }
-      SP.contrib_wide.push_back((int)SP.contrib_tasks.size() - SP.contrib_off.back());
+      SP.contrib_big.push_back((int)SP.contrib_tasks.size() - SP.contrib_off.back());
+      SP.contrib_wide.push_back((int)wide.size());
+      SP.contrib_tasks.insert(SP.contrib_tasks.end(), wide.begin(), wide.end());
       SP.contrib_tasks.insert(SP.contrib_tasks.end(), narrow.begin(), narrow.end());
     }
     SP.level_off.push_back((int)SP.list.size());
@@ -1510,7 +1526,7 @@ void Engine::run_solve_with(double *x, int nrhs, double *contrib) {
                        x + (size_t)r * n_, contrib + (size_t)r * cs, d_cptr_, d_cidx_, d_flags_,
                        base + r + 1, n_, cs, st);
     launch_fwd_contrib(sym_, d_scontrib_ + SP.contrib_off[l], SP.contrib_off[l + 1] - SP.contrib_off[l],
-                       SP.contrib_wide[l], x, contrib, n_, nrhs, cs, st);
+                       SP.contrib_big[l], SP.contrib_wide[l], x, contrib, n_, nrhs, cs, st);
   }
   for (int l = nl - 1; l >= 0; --l) {
     launch_bwd_gather(sym_, d_sgather_ + SP.gather_off[l], SP.gather_off[l + 1] - SP.gather_off[l],

@@ -150,7 +150,7 @@ bool solve_configure(int max_w, std::string &err);
 void launch_fwd_diag(const DevSym &S, const int *list, int count, int smem, double *y,
                      const double *contrib, const int *cptr, const int *cidx, int n, int nrhs,
                      int64_t cstride, cudaStream_t st);
-void launch_fwd_contrib(const DevSym &S, const int2 *tasks, int count, int nwide,
+void launch_fwd_contrib(const DevSym &S, const int2 *tasks, int count, int nbig, int nwide,
                         const double *y, double *contrib, int n, int nrhs, int64_t cstride,
                         cudaStream_t st);
 void launch_bwd_gather(const DevSym &S, const int2 *tasks, int count, double *x, int n, int nrhs,
@@ -188,8 +188,9 @@ struct SolvePlan {
   std::vector<int> warp_list;       //   warp_list[warp_off[l] .. warp_off[l+1])
   std::vector<int> chain_off;       // (s, block) tasks of the tiled class in level l:
   std::vector<int2> fchain, bchain; //   forward (increasing block) / backward (decreasing)
-  std::vector<int> contrib_off;     // (s, r0) tasks of level l: contrib_wide[l] tasks of
-  std::vector<int> contrib_wide;    //   wide supernodes (a CTA each), then narrow ones (a warp)
+  std::vector<int> contrib_off;     // (s, r0) tasks of level l: contrib_big[l] tasks of very
+  std::vector<int> contrib_big;     //   wide supernodes, contrib_wide[l] of wide ones (a CTA
+  std::vector<int> contrib_wide;    //   each), then narrow ones (a warp)
   std::vector<int2> contrib_tasks;
   std::vector<int> gather_off;      // (s, j0) tasks of level l
   std::vector<int2> gather_tasks;

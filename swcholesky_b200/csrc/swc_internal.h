@@ -58,6 +58,9 @@ constexpr int TB = 64;
 // Task shapes of the solve's streaming kernels: rows of an off-diagonal block per forward
 // contribution task, columns per backward gather task.
 constexpr int SOLVE_CONTRIB_ROWS = 32;
+constexpr int SOLVE_CONTRIB_WIDE_ROWS = 128;   // rows of a wide supernode's contribution task
+constexpr int SOLVE_CONTRIB_BIG_W = 512;       // wider: 32-row tasks of 32 warps each
+constexpr int SOLVE_CONTRIB_WIDE_MIN = 300;    // 128-row tasks only on levels with this many
 constexpr int SOLVE_GATHER_COLS = 16;
 constexpr int SOLVE_NARROW_W = 64;   // contribution tasks of supernodes this narrow: a warp each
 // Supernodes of the small class at most this wide, with at most SOLVE_WARP_ROWS rows below

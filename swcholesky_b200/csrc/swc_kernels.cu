@@ -118,6 +118,38 @@ __device__ __forceinline__ void store_mirror_panel(const DevSym &S, int s, int m
   }
 }
 
+// An nr x nc block of the panel (rows r0.., columns c0..), staged in shared memory as
+// X[c * ld + r], into the mirror: consecutive threads write consecutive columns of a mirror
+// row (the rows are K-major), so every warp store is one contiguous piece of a plane.
+__device__ __forceinline__ void store_mirror_block(const DevSym &S, int s, int m, int w, int r0,
+                                                   int c0, int nr, int nc, const double *X,
+                                                   int ld, int t, int nt) {
+  float *base = reinterpret_cast<float *>(S.Lf) + S.xk[s];
+  if (S.xk[S.nsuper] == 0) {
+    const int wp = kmirror_pitch_tf32(w);
+    float *hi = base, *lo = hi + (size_t)m * wp;
+    for (int e = t; e < TB * TB; e += nt) {
+      const int r = e >> 6, c = e & (TB - 1);
+      if (r >= nr || c >= nc) continue;
+      const float2 v = split_tf32(X[c * ld + r]);
+      hi[(size_t)(r0 + r) * wp + c0 + c] = v.x;
+      lo[(size_t)(r0 + r) * wp + c0 + c] = v.y;
+    }
+  } else {
+    const int wq = kmirror_pitch_bf16(w);
+    unsigned short *hi = reinterpret_cast<unsigned short *>(base);
+    unsigned short *mid = hi + (size_t)m * wq, *lo = mid + (size_t)m * wq;
+    for (int e = t; e < TB * TB; e += nt) {
+      const int r = e >> 6, c = e & (TB - 1);
+      if (r >= nr || c >= nc) continue;
+      const Bf16x3 v = split_bf16x3(X[c * ld + r]);
+      hi[(size_t)(r0 + r) * wq + c0 + c] = v.hi;
+      mid[(size_t)(r0 + r) * wq + c0 + c] = v.mid;
+      lo[(size_t)(r0 + r) * wq + c0 + c] = v.lo;
+    }
+  }
+}
+
 // The same for one warp, out of line (keeps the warp-per-supernode kernel's registers).
 __device__ __noinline__ void store_mirror_panel_warp(const DevSym &S, int s, int m, int w,
                                                      const double *P) {
@@ -1053,21 +1085,23 @@ __device__ void trsm_task(const DevSym &S, int s, int r0, int step, double *dyn)
   acc.zero();
   // X[r][c] = sum_k B[r][k] T(c, k); operand element (row c, column k) = T[k * 64 + c]
   dmma_tile_product(P + (size_t)c0 * m + r0, m, nr, T, TB, bw, bw, dyn, acc);
+  // through shared memory (the staging area), so the stores of L (column-major) and of
+  // the mirror (K-major rows) are both contiguous per warp
+  constexpr int XLD = TB + 1;
+  static_assert(TB * XLD <= 2 * STAGE, "result tile fits the staging area");
+  __syncthreads();   // every warp is done with the stages
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int r = acc_row(i);
-    if (r >= nr) continue;
+  for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j)
 #pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const int c = acc_col(j, e);
-        if (c < bw) {
-          P[(size_t)(c0 + c) * m + r0 + r] = acc.v[i][j][e];
-          if (S.Lf) store_mirror(S, s, m, w, r0 + r, c0 + c, acc.v[i][j][e]);
-        }
-      }
+      for (int e = 0; e < 2; ++e) dyn[acc_col(j, e) * XLD + acc_row(i)] = acc.v[i][j][e];
+  __syncthreads();
+  for (int e = threadIdx.x; e < TB * TB; e += blockDim.x) {
+    const int c = e >> 6, r = e & (TB - 1);
+    if (r < nr && c < bw) P[(size_t)(c0 + c) * m + r0 + r] = dyn[c * XLD + r];
   }
+  if (S.Lf) store_mirror_block(S, s, m, w, r0, c0, nr, bw, dyn, XLD, threadIdx.x, blockDim.x);
 }
 
 // TRSM tiles of step `step`, one product each; the next diagonal block's update by this

@@ -79,15 +79,56 @@ __global__ void __launch_bounds__(ST) k_fwd_diag(DevSym S, const int *list, doub
   }
 }
 
-// task = (s, r0): rows r0..r0+31 of supernode s's off-diagonal block (r0 >= w); warp q
-// (lane = row) sums the columns k = q (mod CQ) with four loads in flight per lane, and the
-// CQ partial sums meet in shared memory in a fixed order.  32-row tasks and 1024 threads
-// keep enough loads in flight to stream the panel from HBM when a level holds only a few
-// wide supernodes.
-constexpr int CR = SOLVE_CONTRIB_ROWS, CT = 1024, CQ = CT / CR;
-static_assert(CR == 32, "a warp covers the rows of a task");
-// Tasks of narrow supernodes (w <= SOLVE_NARROW_W) come after the nwide wide ones, one
-// warp each (lane = row, all w columns in the warp), CQ per CTA.
+// Contribution tasks.  Very wide supernodes (w > SOLVE_CONTRIB_BIG_W; few of them, each a
+// long row of work): task = (s, r0), 32 rows, one CTA of 32 warps, warp q summing the
+// columns k = q (mod 32) with four loads in flight, so a level of one or two such
+// supernodes still spreads over the GPU.  Wide supernodes (w > SOLVE_NARROW_W): task = (s, r0), rows
+// r0 .. r0 + SOLVE_CONTRIB_WIDE_ROWS - 1 of the off-diagonal block (r0 >= w), one CTA of CW
+// warps: warp q sums the columns k = q (mod CW), lane l the rows r0 + l + 32 t (t < 4), with
+// four columns unrolled (sixteen loads in flight per lane, each warp load 32 consecutive
+// rows of a column), and the CW partial sums meet in shared memory in a fixed order.
+// Narrow supernodes: task = (s, r0), 32 rows, one warp (lane = row, all w columns), CW per
+// CTA after the nwide wide tasks.
+constexpr int CR = SOLVE_CONTRIB_ROWS, CRW = SOLVE_CONTRIB_WIDE_ROWS, CW = 8, CT = 32 * CW;
+constexpr int CTB = 1024, CQB = CTB / CR;
+__global__ void __launch_bounds__(CTB) k_fwd_contrib_big(DevSym S, const int2 *tasks,
+                                                        const double *y, double *contrib, int n,
+                                                        int nrhs, int64_t cstride) {
+  __shared__ double part[CQB][CR];
+  const int s = tasks[blockIdx.x].x, r0 = tasks[blockIdx.x].y;
+  const int f = S.super[s], w = S.super[s + 1] - f;
+  const int64_t rb = S.rowptr[s];
+  const int m = (int)(S.rowptr[s + 1] - rb);
+  const double *Ls_s = S.L + S.xptr[s];
+  const int r = threadIdx.x & (CR - 1), q = threadIdx.x / CR;
+  const int a = r0 + r;
+  for (int rhs = 0; rhs < nrhs; ++rhs) {
+    const double *yr = y + (size_t)rhs * n + f;
+    double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
+    if (a < m) {
+      const double *col = Ls_s + a;
+      int k = q;
+      for (; k + 3 * CQB < w; k += 4 * CQB) {
+        acc0 = fma(col[(size_t)k * m], yr[k], acc0);
+        acc1 = fma(col[(size_t)(k + CQB) * m], yr[k + CQB], acc1);
+        acc2 = fma(col[(size_t)(k + 2 * CQB) * m], yr[k + 2 * CQB], acc2);
+        acc3 = fma(col[(size_t)(k + 3 * CQB) * m], yr[k + 3 * CQB], acc3);
+      }
+      for (; k < w; k += CQB) acc0 = fma(col[(size_t)k * m], yr[k], acc0);
+    }
+    part[q][r] = (acc0 + acc1) + (acc2 + acc3);
+    __syncthreads();
+    if (q == 0 && a < m) {
+      double t = 0.0;
+#pragma unroll
+      for (int g = 0; g < CQB; ++g) t += part[g][r];
+      contrib[(size_t)rhs * cstride + (rb - f) + (a - w)] = t;
+    }
+    __syncthreads();
+  }
+}
+
+static_assert(CR == 32 && CRW == 4 * CR, "a lane covers four rows of a wide task");
 __device__ void fwd_contrib_narrow(const DevSym &S, int2 task, const double *y, double *contrib,
                                    int n, int nrhs, int64_t cstride) {
   const int s = task.x, r0 = task.y, lane = threadIdx.x & 31;
@@ -115,9 +156,9 @@ __device__ void fwd_contrib_narrow(const DevSym &S, int2 task, const double *y, 
 __global__ void __launch_bounds__(CT) k_fwd_contrib(DevSym S, const int2 *tasks, int count,
                                                     int nwide, const double *y, double *contrib,
                                                     int n, int nrhs, int64_t cstride) {
-  __shared__ double part[CQ][CR];
+  __shared__ double part[CW][CRW];
   if ((int)blockIdx.x >= nwide) {
-    const int t = nwide + ((int)blockIdx.x - nwide) * CQ + (int)(threadIdx.x >> 5);
+    const int t = nwide + ((int)blockIdx.x - nwide) * CW + (int)(threadIdx.x >> 5);
     if (t < count) fwd_contrib_narrow(S, tasks[t], y, contrib, n, nrhs, cstride);
     return;
   }
@@ -126,29 +167,51 @@ __global__ void __launch_bounds__(CT) k_fwd_contrib(DevSym S, const int2 *tasks,
   const int64_t rb = S.rowptr[s];
   const int m = (int)(S.rowptr[s + 1] - rb);
   const double *Ls_s = S.L + S.xptr[s];
-  const int r = threadIdx.x & (CR - 1), q = threadIdx.x / CR;
-  const int a = r0 + r;
+  const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
+  // rows of this lane (rows past the panel read row r0 and are dropped)
+  int ra[4];
+  bool in[4];
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    ra[t] = r0 + lane + 32 * t;
+    in[t] = ra[t] < m;
+    if (!in[t]) ra[t] = r0;
+  }
   for (int rhs = 0; rhs < nrhs; ++rhs) {
     const double *yr = y + (size_t)rhs * n + f;
-    double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
-    if (a < m) {
-      const double *col = Ls_s + a;
-      int k = q;
-      for (; k + 3 * CQ < w; k += 4 * CQ) {
-        acc0 = fma(col[(size_t)k * m], yr[k], acc0);
-        acc1 = fma(col[(size_t)(k + CQ) * m], yr[k + CQ], acc1);
-        acc2 = fma(col[(size_t)(k + 2 * CQ) * m], yr[k + 2 * CQ], acc2);
-        acc3 = fma(col[(size_t)(k + 3 * CQ) * m], yr[k + 3 * CQ], acc3);
-      }
-      for (; k < w; k += CQ) acc0 = fma(col[(size_t)k * m], yr[k], acc0);
-    }
-    part[q][r] = (acc0 + acc1) + (acc2 + acc3);
-    __syncthreads();
-    if (q == 0 && a < m) {
-      double t = 0.0;
+    double acc[4][2];
 #pragma unroll
-      for (int g = 0; g < CQ; ++g) t += part[g][r];
-      contrib[(size_t)rhs * cstride + (rb - f) + (a - w)] = t;
+    for (int t = 0; t < 4; ++t) acc[t][0] = acc[t][1] = 0.0;
+    int k = q;
+    for (; k + 3 * CW < w; k += 4 * CW) {
+      const double y0 = yr[k], y1 = yr[k + CW], y2 = yr[k + 2 * CW], y3 = yr[k + 3 * CW];
+      const double *c0 = Ls_s + (size_t)k * m, *c1 = c0 + (size_t)CW * m;
+      const double *c2 = c1 + (size_t)CW * m, *c3 = c2 + (size_t)CW * m;
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        acc[t][0] = fma(c0[ra[t]], y0, acc[t][0]);
+        acc[t][1] = fma(c1[ra[t]], y1, acc[t][1]);
+        acc[t][0] = fma(c2[ra[t]], y2, acc[t][0]);
+        acc[t][1] = fma(c3[ra[t]], y3, acc[t][1]);
+      }
+    }
+    for (; k < w; k += CW) {
+      const double yk = yr[k];
+      const double *ck = Ls_s + (size_t)k * m;
+#pragma unroll
+      for (int t = 0; t < 4; ++t) acc[t][0] = fma(ck[ra[t]], yk, acc[t][0]);
+    }
+#pragma unroll
+    for (int t = 0; t < 4; ++t) part[q][lane + 32 * t] = acc[t][0] + acc[t][1];
+    __syncthreads();
+    if (threadIdx.x < CRW) {
+      const int a = r0 + (int)threadIdx.x;
+      if (a < m) {
+        double t = 0.0;
+#pragma unroll
+        for (int g = 0; g < CW; ++g) t += part[g][threadIdx.x];
+        contrib[(size_t)rhs * cstride + (rb - f) + (a - w)] = t;
+      }
     }
     __syncthreads();
   }
@@ -897,10 +960,13 @@ void launch_fwd_diag(const DevSym &S, const int *list, int count, int smem, doub
   if (count > 0)
     k_fwd_diag<<<count, ST, smem, st>>>(S, list, y, contrib, cptr, cidx, n, nrhs, cstride);
 }
-void launch_fwd_contrib(const DevSym &S, const int2 *tasks, int count, int nwide,
+void launch_fwd_contrib(const DevSym &S, const int2 *tasks, int count, int nbig, int nwide,
                         const double *y, double *contrib, int n, int nrhs, int64_t cstride,
                         cudaStream_t st) {
-  const int blocks = nwide + (count - nwide + CQ - 1) / CQ;
+  if (nbig > 0) k_fwd_contrib_big<<<nbig, CTB, 0, st>>>(S, tasks, y, contrib, n, nrhs, cstride);
+  tasks += nbig;
+  count -= nbig;
+  const int blocks = nwide + (count - nwide + CW - 1) / CW;
   if (count > 0)
     k_fwd_contrib<<<blocks, CT, 0, st>>>(S, tasks, count, nwide, y, contrib, n, nrhs, cstride);
 }
