@@ -736,20 +736,28 @@ __device__ void potrf8_inv8(double *D, double *E, int kb, const DevSym &S, int g
     for (int i = j; i < 8; ++i) a[i][j] = D[(k0 + j) * DLD + k0 + i];
   double rinv[8];
   int bad = 8;   // first column with a pivot <= 0 or NaN (reported after the chain)
+  double inv = rsqrt(a[0][0]);
 #pragma unroll
   for (int j = 0; j < 8; ++j) {
     const double piv = a[j][j];
-    const double inv = rsqrt(piv);
     if (!(piv > 0.0) && j < bad) bad = j;
     rinv[j] = inv;
     a[j][j] = piv * inv;
+    // the chain first: the next pivot and its reciprocal square root, issued before the
+    // rest of the column's update, which runs under its latency
+    if (j + 1 < 8) {
+      a[j + 1][j] *= inv;
+      a[j + 1][j + 1] = fma(-a[j + 1][j], a[j + 1][j], a[j + 1][j + 1]);
+    }
+    const double inv_next = (j + 1 < 8) ? rsqrt(a[j + 1][j + 1]) : 0.0;
 #pragma unroll
-    for (int i = j + 1; i < 8; ++i) a[i][j] *= inv;
-    // the next pivot first
+    for (int i = j + 2; i < 8; ++i) a[i][j] *= inv;
 #pragma unroll
     for (int k = j + 1; k < 8; ++k)
 #pragma unroll
-      for (int i = k; i < 8; ++i) a[i][k] = fma(-a[i][j], a[k][j], a[i][k]);
+      for (int i = k; i < 8; ++i)
+        if (!(k == j + 1 && i == j + 1)) a[i][k] = fma(-a[i][j], a[k][j], a[i][k]);
+    inv = inv_next;
   }
   if (report && lane == 0 && bad < 8 && k0 + bad < bw) atomicMin(&S.status[0], gcol0 + k0 + bad + 1);
   // every lane stores the same 36 values (one write per address; no lane-dependent index
