@@ -817,18 +817,22 @@ __device__ void potrf64_blocked(double *D, double *E, int bw, const DevSym &S, i
       store8(c, D, 8 * nb, 8 * nb, true);
       __syncwarp();
       potrf8_inv8(D, E, nb, S, gcol0, bw, true);
-    } else {
-      // blocks (ib, jb), kb < jb <= ib < nbk, except (kb+1, kb+1), in column order; warp
-      // w > 0 takes the blocks w - 1, w - 1 + (NW - 1), .. and runs them interleaved
-      // (independent DMMA chains: their latency, not their issue, bounds a short chain)
-      constexpr int MAXT = (27 + NW - 2) / (NW - 1);
+    } else if ((warp & 3) != 0) {
+      // blocks (ib, jb), kb < jb <= ib < nbk, except (kb+1, kb+1), in column order; the
+      // warps that do not share warp 0's scheduler (warp % 4 != 0: NU of them, rank u) take
+      // the blocks u, u + NU, .. and run them interleaved (independent DMMA chains: their
+      // latency, not their issue, bounds a short chain); warp 0's chain of pivots keeps its
+      // scheduler to itself
+      constexpr int NU = NW - NW / 4;
+      constexpr int MAXT = (27 + NU - 1) / NU;
+      const int u = warp - 1 - (warp >> 2);
       const int nrem = nbk - kb - 1;                       // block rows/columns left
       const int ntot = nrem * (nrem + 1) / 2 - 1;
       double c[MAXT][2];
       int bi[MAXT], bj[MAXT];
 #pragma unroll
       for (int t = 0; t < MAXT; ++t) {
-        int idx = warp - 1 + (NW - 1) * t;
+        int idx = u + NU * t;
         if (idx >= ntot) idx = -1;  // an unused slot: block (kb+1, kb+1), nothing stored
         idx += 1;                   // skip (kb+1, kb+1), the first block of the order
         int jj = 0;
@@ -839,10 +843,10 @@ __device__ void potrf64_blocked(double *D, double *E, int bw, const DevSym &S, i
       }
 #pragma unroll
       for (int t = 0; t < MAXT; ++t)
-        if (warp - 1 + (NW - 1) * t < ntot) mma8_abt(c[t], D, bi[t], 8 * kb, D, bj[t], 8 * kb, true);
+        if (u + NU * t < ntot) mma8_abt(c[t], D, bi[t], 8 * kb, D, bj[t], 8 * kb, true);
 #pragma unroll
       for (int t = 0; t < MAXT; ++t)
-        if (warp - 1 + (NW - 1) * t < ntot) store8(c[t], D, bi[t], bj[t], bi[t] == bj[t]);
+        if (u + NU * t < ntot) store8(c[t], D, bi[t], bj[t], bi[t] == bj[t]);
     }
     __syncthreads();
   }
