@@ -461,14 +461,16 @@ __device__ __forceinline__ void cp8(double *dst, const double *src, bool in) {
 // hardware dispatches first.
 //
 // Warp w owns rows 8w .. 8w + 7 of the block's right-hand side v: it stages its eight rows
-// of each predecessor's panel block in its own shared-memory ring (cp.async, CHAIN_NS
-// slots, CHAIN_NS - 1 blocks ahead), holds them and its rows of T_k in registers, and lane
+// of each predecessor's panel block in its own shared-memory ring (cp.async, NS slots,
+// NS - 1 blocks ahead), holds them and its rows of T_k in registers, and lane
 // l multiplies columns l and l + 32; a butterfly of shuffles sums the eight rows across
 // the lanes (row 8w + (l >> 2) in every lane of quad l >> 2).  No block barrier until the
 // last predecessor is applied; then one barrier hands v to every warp for x_k = T_k v.
 // The step that waits for a predecessor's solution therefore only reads it, sixteen FMAs
 // and nine shuffles.
-constexpr int CHAIN_NS = 5;
+// Ring depth: CHAIN_NS_BIG for launches that fit the GPU at one CTA per SM (long chains:
+// deep prefetch), CHAIN_NS_SMALL (two CTAs per SM) for levels of many short chains.
+constexpr int CHAIN_NS_BIG = 5, CHAIN_NS_SMALL = 2;
 constexpr int LW = TB + 1;                      // padded row of a staged block
 constexpr int CHAIN_SLOT = 8 * LW;              // one warp's eight rows
 // Predecessors outside the cluster come from global memory in batches of up to CHAIN_XB
@@ -476,7 +478,10 @@ constexpr int CHAIN_SLOT = 8 * LW;              // one warp's eight rows
 // (a lane keeps the two elements it multiplies, in its warp's batch buffer), so a batch
 // costs two memory round trips instead of two per block.
 constexpr int CHAIN_XB = 8;
-constexpr int CHAIN_SMEM = (CHAIN_NS * CHAIN_SLOT + CHAIN_XB * TB) * CHAIN_WARPS * 8;
+// dynamic shared memory: the ring, then each warp's batch buffer (forward: x_c(8w .. 8w+7)
+// of up to eight blocks; backward: whole x_c of up to CHAIN_XB blocks)
+constexpr int CHAIN_XW_FWD = TB, CHAIN_XW_BWD = CHAIN_XB * TB;
+constexpr int chain_smem(int ns, int xw) { return (ns * CHAIN_SLOT + xw) * CHAIN_WARPS * 8; }
 
 // Chains launch in thread-block clusters of CHAIN_CL consecutive tasks.  A block publishes its
 // solution through global memory and its counter (for the blocks of later clusters and the
@@ -589,7 +594,8 @@ __device__ __forceinline__ double warp_rows8(double (&a)[8], int lane) {
 // of the panel, staged by the warp alone) and keeps its partial sums of all 64 rows (rows
 // l and l + 32 in lane l); the eight warps' partial sums meet once, after the last
 // predecessor, and x_k = T_k v is then formed with warp w owning rows 8w .. 8w + 7.
-__global__ void __launch_bounds__(ST, 1) k_fwd_chain(DevSym S, const int2 *tasks, int count,
+template <int NS>
+__global__ void __launch_bounds__(ST, NS == CHAIN_NS_SMALL ? 2 : 1) k_fwd_chain(DevSym S, const int2 *tasks, int count,
                                                      double *y, const double *contrib,
                                                      const int *cptr, const int *cidx, int *flags,
                                                      int epoch, int n, int64_t cstride) {
@@ -613,12 +619,12 @@ __global__ void __launch_bounds__(ST, 1) k_fwd_chain(DevSym S, const int2 *tasks
     // the same supernode receive this block's solution
     const int cfirst = k - me, last = me + min(nb - 1 - k, CHAIN_CL - 1 - me);
     double *ring = csm + wp * CHAIN_SLOT;   // slot j at ring + j * CHAIN_WARPS * CHAIN_SLOT
-    double *xw = csm + CHAIN_NS * CHAIN_WARPS * CHAIN_SLOT + wp * (CHAIN_XB * TB);
+    double *xw = csm + NS * CHAIN_WARPS * CHAIN_SLOT + wp * CHAIN_XW_FWD;
     // this warp's columns of L_kc: element (r, 8w + q) = P[(64c + 8w + q) m + r0 + r] at
     // [q * LW + r] (a warp instruction copies 32 consecutive rows of one column)
     auto stage = [&](int c) {
       if (c < k) {
-        double *d = ring + (c % CHAIN_NS) * CHAIN_WARPS * CHAIN_SLOT;
+        double *d = ring + (c % NS) * CHAIN_WARPS * CHAIN_SLOT;
         const double *src = P + (size_t)(c * TB + w8) * m + r0;
 #pragma unroll 4
         for (int t = 0; t < 16; ++t) {
@@ -629,7 +635,7 @@ __global__ void __launch_bounds__(ST, 1) k_fwd_chain(DevSym S, const int2 *tasks
       }
       stage_commit();
     };
-    for (int c = 0; c < CHAIN_NS - 1; ++c) stage(c);
+    for (int c = 0; c < NS - 1; ++c) stage(c);
     double tr[8][2];
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
@@ -650,10 +656,10 @@ __global__ void __launch_bounds__(ST, 1) k_fwd_chain(DevSym S, const int2 *tasks
     bool ok = true;
     int xb0 = 0, nbt = 0;            // the batch in xw: blocks xb0 .. xb0 + nbt - 1
     for (int c = 0; c < k; ++c) {
-      stage(c + CHAIN_NS - 1);           // into the slot freed by step c - 1
-      stage_wait<CHAIN_NS - 1>();        // block c has landed (this lane's copies)
+      stage(c + NS - 1);                 // into the slot freed by step c - 1
+      stage_wait<NS - 1>();              // block c has landed (this lane's copies)
       __syncwarp();
-      const double *Lc = ring + (c % CHAIN_NS) * CHAIN_WARPS * CHAIN_SLOT;
+      const double *Lc = ring + (c % NS) * CHAIN_WARPS * CHAIN_SLOT;
       double lr[8][2];
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
@@ -718,7 +724,8 @@ __global__ void __launch_bounds__(ST, 1) k_fwd_chain(DevSym S, const int2 *tasks
 
 // task = (s, k) in decreasing k; backward: x[f + 64k ..] := T_k^T (x[...] - sum_{c>k} L_ck^T x_c)
 // (tasks of a supernode consecutive, in decreasing k; CTAs from `count` on are padding)
-__global__ void __launch_bounds__(ST, 1) k_bwd_chain(DevSym S, const int2 *tasks, int count,
+template <int NS>
+__global__ void __launch_bounds__(ST, NS == CHAIN_NS_SMALL ? 2 : 1) k_bwd_chain(DevSym S, const int2 *tasks, int count,
                                                   double *x, int *flags, int epoch) {
   extern __shared__ double csm[];
   __shared__ double vs[TB];
@@ -740,13 +747,13 @@ __global__ void __launch_bounds__(ST, 1) k_bwd_chain(DevSym S, const int2 *tasks
     // k) of the same supernode receive this block's solution
     const int clast = k + me, last = me + min(k, CHAIN_CL - 1 - me);
     double *ring = csm + wp * CHAIN_SLOT;
-    double *xw = csm + CHAIN_NS * CHAIN_WARPS * CHAIN_SLOT + wp * (CHAIN_XB * TB);
+    double *xw = csm + NS * CHAIN_WARPS * CHAIN_SLOT + wp * CHAIN_XW_BWD;
     // successor step t = nb - 1 - c (c = nb - 1 first); this warp's columns of block (c, k):
     // element (i, rr) = P[(r0 + w8 + i) m + 64c + rr] at [i * LW + rr]
     auto stage = [&](int t) {
       const int c = nb - 1 - t;
       if (c > k) {
-        double *d = ring + (t % CHAIN_NS) * CHAIN_WARPS * CHAIN_SLOT;
+        double *d = ring + (t % NS) * CHAIN_WARPS * CHAIN_SLOT;
         const int cw = min(TB, w - c * TB);
         const double *src = P + (size_t)(r0 + w8) * m + c * TB;
 #pragma unroll 4
@@ -758,7 +765,7 @@ __global__ void __launch_bounds__(ST, 1) k_bwd_chain(DevSym S, const int2 *tasks
       }
       stage_commit();
     };
-    for (int t = 0; t < CHAIN_NS - 1; ++t) stage(t);
+    for (int t = 0; t < NS - 1; ++t) stage(t);
     double tr[8][2];   // T(rr, w8 + i) for rr = lane, lane + 32
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
@@ -770,10 +777,10 @@ __global__ void __launch_bounds__(ST, 1) k_bwd_chain(DevSym S, const int2 *tasks
     int xb0 = nb, nbt = 0;               // the batch in xw: blocks xb0, .., xb0 - nbt + 1
     for (int c = nb - 1; c > k; --c) {
       const int t = nb - 1 - c;
-      stage(t + CHAIN_NS - 1);
-      stage_wait<CHAIN_NS - 1>();        // block (c, k) has landed (this lane's copies)
+      stage(t + NS - 1);
+      stage_wait<NS - 1>();              // block (c, k) has landed (this lane's copies)
       __syncwarp();
-      const double *Lc = ring + (t % CHAIN_NS) * CHAIN_WARPS * CHAIN_SLOT;
+      const double *Lc = ring + (t % NS) * CHAIN_WARPS * CHAIN_SLOT;
       double lr[8][2];
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
@@ -934,6 +941,11 @@ __global__ void k_norms_final(const double *part, double *out) {
 
 }  // namespace
 
+// the chains' grids: whole clusters of CHAIN_CL CTAs; launches that fit the SMs at one CTA
+// each take the deep ring
+static int g_num_sms = 148;
+static int chain_grid(int count) { return (count + CHAIN_CL - 1) / CHAIN_CL * CHAIN_CL; }
+
 bool solve_configure(int max_w, std::string &err) {
   size_t smem = sizeof(double) * (size_t)(max_w > 0 ? max_w : 1);
   if (smem > 220 * 1024) {
@@ -942,9 +954,22 @@ bool solve_configure(int max_w, std::string &err) {
   }
   cudaError_t e = cudaFuncSetAttribute(k_fwd_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_fwd_chain, cudaFuncAttributeMaxDynamicSharedMemorySize, CHAIN_SMEM);
+    e = cudaFuncSetAttribute(k_fwd_chain<CHAIN_NS_BIG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             chain_smem(CHAIN_NS_BIG, CHAIN_XW_FWD));
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_bwd_chain, cudaFuncAttributeMaxDynamicSharedMemorySize, CHAIN_SMEM);
+    e = cudaFuncSetAttribute(k_fwd_chain<CHAIN_NS_SMALL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             chain_smem(CHAIN_NS_SMALL, CHAIN_XW_FWD));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_bwd_chain<CHAIN_NS_BIG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             chain_smem(CHAIN_NS_BIG, CHAIN_XW_BWD));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_bwd_chain<CHAIN_NS_SMALL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             chain_smem(CHAIN_NS_SMALL, CHAIN_XW_BWD));
+  if (e == cudaSuccess) {
+    int dev = 0;
+    e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+  }
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_bwd_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) {
@@ -990,11 +1015,12 @@ void launch_bwd_diag(const DevSym &S, const int *list, int count, int smem, doub
   if (count > 0) k_bwd_diag<<<count, ST, smem, st>>>(S, list, x, n, nrhs);
 }
 // the chains' launch configuration: a grid of whole clusters of CHAIN_CL CTAs
-static cudaLaunchConfig_t chain_config(int count, cudaStream_t st, cudaLaunchAttribute *at) {
+static cudaLaunchConfig_t chain_config(int count, int smem, cudaStream_t st,
+                                       cudaLaunchAttribute *at) {
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)((count + CHAIN_CL - 1) / CHAIN_CL * CHAIN_CL));
+  cfg.gridDim = dim3((unsigned)chain_grid(count));
   cfg.blockDim = dim3(ST);
-  cfg.dynamicSmemBytes = CHAIN_SMEM;
+  cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   at[0].id = cudaLaunchAttributeClusterDimension;
   at[0].val.clusterDim.x = CHAIN_CL;
@@ -1009,16 +1035,27 @@ void launch_fwd_chain(const DevSym &S, const int2 *tasks, int count, double *y,
                       int epoch, int n, int64_t cstride, cudaStream_t st) {
   if (count <= 0) return;
   cudaLaunchAttribute at[1];
-  const cudaLaunchConfig_t cfg = chain_config(count, st, at);
-  cudaLaunchKernelEx(&cfg, k_fwd_chain, S, tasks, count, y, contrib, cptr, cidx, flags, epoch, n,
-                     cstride);
+  if (chain_grid(count) <= g_num_sms) {
+    const cudaLaunchConfig_t cfg = chain_config(count, chain_smem(CHAIN_NS_BIG, CHAIN_XW_FWD), st, at);
+    cudaLaunchKernelEx(&cfg, k_fwd_chain<CHAIN_NS_BIG>, S, tasks, count, y, contrib, cptr, cidx,
+                       flags, epoch, n, cstride);
+  } else {
+    const cudaLaunchConfig_t cfg = chain_config(count, chain_smem(CHAIN_NS_SMALL, CHAIN_XW_FWD), st, at);
+    cudaLaunchKernelEx(&cfg, k_fwd_chain<CHAIN_NS_SMALL>, S, tasks, count, y, contrib, cptr, cidx,
+                       flags, epoch, n, cstride);
+  }
 }
 void launch_bwd_chain(const DevSym &S, const int2 *tasks, int count, double *x, int *flags,
                       int epoch, cudaStream_t st) {
   if (count <= 0) return;
   cudaLaunchAttribute at[1];
-  const cudaLaunchConfig_t cfg = chain_config(count, st, at);
-  cudaLaunchKernelEx(&cfg, k_bwd_chain, S, tasks, count, x, flags, epoch);
+  if (chain_grid(count) <= g_num_sms) {
+    const cudaLaunchConfig_t cfg = chain_config(count, chain_smem(CHAIN_NS_BIG, CHAIN_XW_BWD), st, at);
+    cudaLaunchKernelEx(&cfg, k_bwd_chain<CHAIN_NS_BIG>, S, tasks, count, x, flags, epoch);
+  } else {
+    const cudaLaunchConfig_t cfg = chain_config(count, chain_smem(CHAIN_NS_SMALL, CHAIN_XW_BWD), st, at);
+    cudaLaunchKernelEx(&cfg, k_bwd_chain<CHAIN_NS_SMALL>, S, tasks, count, x, flags, epoch);
+  }
 }
 void launch_spmv(int n, const int *rp, const int *ci, const double *val, const double *x,
                  double *y, int nrhs, cudaStream_t st) {
