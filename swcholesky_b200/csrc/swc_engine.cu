@@ -134,6 +134,9 @@ Engine::Engine(int device) : device_(device) {
   cudaStreamCreateWithFlags(&aux_stream_, cudaStreamNonBlocking);
   cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming);
   cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming);
+  cudaStreamCreateWithFlags(&small_stream_, cudaStreamNonBlocking);
+  cudaEventCreateWithFlags(&ev_sfork_, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&ev_sjoin_, cudaEventDisableTiming);
   cudaMallocHost(&h_status_, kStatusWords * sizeof(int));
 }
 
@@ -146,6 +149,9 @@ Engine::~Engine() {
   if (aux_stream_) cudaStreamDestroy(aux_stream_);
   if (ev_fork_) cudaEventDestroy(ev_fork_);
   if (ev_join_) cudaEventDestroy(ev_join_);
+  if (small_stream_) cudaStreamDestroy(small_stream_);
+  if (ev_sfork_) cudaEventDestroy(ev_sfork_);
+  if (ev_sjoin_) cudaEventDestroy(ev_sjoin_);
 }
 
 void Engine::release() {
@@ -1202,9 +1208,21 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec
     mark(-1, 1);
   }
   for (const Wave &W : plan_.waves) {
-    mark(K_SMALL, W.small_cnt);
-    launch_factor_small(sym_, d_upd_lbub_, d_small_ + W.small_off, W.small_cnt, W.small_smem, st);
-    mark(-1, W.small_cnt);
+    // the wave's small supernodes read only earlier waves' panels and write only their own,
+    // so they run beside the wave's tiled work (updates and dense steps) on a second
+    // stream, joined before the next wave (whose updates and supernodes read them)
+    const bool side = !prof && W.small_cnt > 0 && W.big_cnt > 0;
+    if (side) {
+      cudaEventRecord(ev_sfork_, st);
+      cudaStreamWaitEvent(small_stream_, ev_sfork_, 0);
+      launch_factor_small(sym_, d_upd_lbub_, d_small_ + W.small_off, W.small_cnt, W.small_smem,
+                          small_stream_);
+      cudaEventRecord(ev_sjoin_, small_stream_);
+    } else {
+      mark(K_SMALL, W.small_cnt);
+      launch_factor_small(sym_, d_upd_lbub_, d_small_ + W.small_off, W.small_cnt, W.small_smem, st);
+      mark(-1, W.small_cnt);
+    }
     if (scatter) {
       mark(K_UPDATE, W.scs_cnt);
       launch_scatter_small(sym_, d_sc_small_ + W.scs_off, W.scs_cnt, sc_cols, st);
@@ -1233,6 +1251,7 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec
                            d_dense_toff_, d_dense_ver_ + plan_.waves.size(), d_dense_ver_ + wave,
                            st);
       mark(-1, 1);
+      if (side) cudaStreamWaitEvent(st, ev_sjoin_, 0);
       continue;
     }
     mark(K_PANEL, W.big_cnt);
@@ -1262,6 +1281,7 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec
         syrk(W, (int)j);
       }
     }
+    if (side) cudaStreamWaitEvent(st, ev_sjoin_, 0);
   }
 }
 

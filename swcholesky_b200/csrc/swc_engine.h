@@ -337,6 +337,8 @@ class Engine {
   int64_t dense_ver_len_ = 0;
   cudaStream_t aux_stream_ = nullptr;          // second branch of each dense step
   cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
+  cudaStream_t small_stream_ = nullptr;        // a wave's small supernodes, beside its tiled work
+  cudaEvent_t ev_sfork_ = nullptr, ev_sjoin_ = nullptr;
   int2 *d_asm_ = nullptr, *d_panel_ = nullptr;
   int4 *d_upd_tasks_ = nullptr, *d_syrk_ = nullptr, *d_pairs_ = nullptr;
   int *d_upd_end_ = nullptr;
