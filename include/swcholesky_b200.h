@@ -81,9 +81,11 @@ int swc_destroy(swc_handle_t handle);
 int swc_set_stream(swc_handle_t handle, void *stream);
 void *swc_get_stream(swc_handle_t handle);
 /* Execution plan used by the next swc_analyze / swc_batch_analyze on the handle: one of
- * the candidates swc_batch_autotune tries.  0: default; 1: persistent small-supernode
- * walk up to 100 KB of shared memory per supernode; 2: no persistent walk (one launch per
- * level); 3: smaller small-class limits (more tiled supernodes); 4: the dense
+ * the candidates swc_batch_autotune tries.  0: default (supernodes of at most 1,024 rows
+ * and 4,096 panel entries in the small class, persistent walk up to 24 KB of shared memory
+ * per supernode); 1: persistent small-supernode walk up to 100 KB; 2: no persistent walk
+ * (one launch per level); 3: larger small-class limits (2,048 rows, 12,288 entries, walk up
+ * to 48 KB: fewer tiled supernodes); 4: the dense
  * factorization of each level's tiled supernodes as one persistent dataflow launch
  * instead of three launches per 64-column step; 5: in the mixed modes, the trailing SYRK
  * steps of the dense factorization in FP64 (DMMA) instead of split tcgen05 tiles; 6 and 7:

@@ -104,10 +104,14 @@ const int kNumPartitions = sizeof(kPartitions) / sizeof(kPartitions[0]);
 Tuning plan_candidate(int k) {
   Tuning t;
   switch (k) {
-    case 0: break;                                       // defaults: persistent <= 48 KB
+    case 0: break;                                       // defaults: persistent <= 24 KB
     case 1: t.persist_max_smem = 100 * 1024; break;      // bigger supernodes in the walk
     case 2: t.persist = 0; break;                        // level-by-level launches only
-    case 3: t.small_max_elems = 4096; t.small_max_m = 1024; break;   // more tiled supernodes
+    case 3:                                              // fewer tiled supernodes
+      t.small_max_elems = SMALL_MAX_ELEMS;
+      t.small_max_m = SMALL_MAX_M;
+      t.persist_max_smem = 48 * 1024;
+      break;
     case 4: t.dense_dataflow = 1; break;                 // dense steps as one dataflow launch
     case 5: t.syrk_fp64 = 1; break;                      // mixed modes: FP64 SYRK steps
     case 6: t.scatter = 0; t.tc_tma = 1; break;          // mixed: tile-owner updates (TMA for TF32)

@@ -90,12 +90,16 @@ static_assert(SMALL_SLAB >= SMALL_MAX_M && TINY_SLAB >= TINY_M, "a slab holds on
 
 // Execution-plan parameters (defaults above; the batched path's autotuner varies them).
 struct Tuning {
-  int small_max_w = SMALL_MAX_W;         // size-class limits, at most the constants above
-  int small_max_m = SMALL_MAX_M;
-  int small_max_elems = SMALL_MAX_ELEMS;
+  // size-class limits, at most the constants above.  Supernodes above 1,024 rows or 4,096
+  // panel entries go through the tiled path: their updates then come from the descendants'
+  // tiles over the whole GPU, where a CTA per supernode would walk a long descendant list
+  // alone (grid3d_60: the split-TF32 factor 9.7 -> 9.3 ms)
+  int small_max_w = SMALL_MAX_W;
+  int small_max_m = 1024;
+  int small_max_elems = 4096;
   int tiny = 1;                          // bottom tiny supernodes: one warp each, one launch
   int persist = 1;                       // bottom small supernodes in one persistent launch
-  int persist_max_smem = 48 * 1024;      // shared-memory cap of a persistent supernode (bytes)
+  int persist_max_smem = 24 * 1024;      // shared-memory cap of a persistent supernode (bytes)
   int dense_dataflow = 0;                // dense steps of a wave: one dataflow launch (else
                                          // three launches per 64-column step)
   int dense_group = 4;                   // column blocks per grouped trailing update
