@@ -135,6 +135,8 @@ Engine::Engine(int device) : device_(device) {
   cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming);
   cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming);
   cudaStreamCreateWithFlags(&small_stream_, cudaStreamNonBlocking);
+  cudaStreamCreateWithFlags(&grp_stream_, cudaStreamNonBlocking);
+  for (int k = 0; k < 2; ++k) cudaEventCreateWithFlags(&ev_grp_[k], cudaEventDisableTiming);
   cudaEventCreateWithFlags(&ev_sfork_, cudaEventDisableTiming);
   cudaEventCreateWithFlags(&ev_sjoin_, cudaEventDisableTiming);
   cudaMallocHost(&h_status_, kStatusWords * sizeof(int));
@@ -150,6 +152,9 @@ Engine::~Engine() {
   if (ev_fork_) cudaEventDestroy(ev_fork_);
   if (ev_join_) cudaEventDestroy(ev_join_);
   if (small_stream_) cudaStreamDestroy(small_stream_);
+  if (grp_stream_) cudaStreamDestroy(grp_stream_);
+  for (int k = 0; k < 2; ++k)
+    if (ev_grp_[k]) cudaEventDestroy(ev_grp_[k]);
   if (ev_sfork_) cudaEventDestroy(ev_sfork_);
   if (ev_sjoin_) cudaEventDestroy(ev_sjoin_);
 }
@@ -492,6 +497,7 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
       W.syrk_off.push_back((int)P.syrk_tasks.size());
       W.diag_off.push_back((int)P.diag_list.size());
       W.scd_off.push_back((int)P.sc_dense.size());
+      std::vector<ScTile> grouped;   // after the step's next-column tiles
       for (int s : big) {
         int w = super[s + 1] - super[s];
         int m = (int)(rowptr[s + 1] - rowptr[s]);
@@ -513,8 +519,9 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
           if (T.scatter) {   // the same update as 128-row x one-column-block dense tiles
             const int kc = c0 + bw - first * TB;
             for (int r0 = cc == c0 + TB ? cc + TB : cc; r0 < m; r0 += 128)
-              P.sc_dense.push_back(ScTile{s, r0, cc, (kc + 31) / 32, m, first * TB,
-                                          std::min(TB, w - cc), 1, 0, 0});
+              (C == j + 1 ? P.sc_dense : grouped)
+                  .push_back(ScTile{s, r0, cc, (kc + 31) / 32, m, first * TB,
+                                    std::min(TB, w - cc), 1, 0, 0});
           }
           for (int r0 = cc; r0 < m; r0 += TB)
             if (!(cc == c0 + TB && r0 == cc)) {   // next diagonal tile: the TRSM task's update
@@ -531,6 +538,8 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
       W.panel_cnt.push_back((int)P.panel_tasks.size() - W.panel_off.back());
       W.syrk_cnt.push_back((int)P.syrk_tasks.size() - W.syrk_off.back());
       W.diag_cnt.push_back((int)P.diag_list.size() - W.diag_off.back());
+      W.scd_nc.push_back((int)P.sc_dense.size() - W.scd_off.back());
+      P.sc_dense.insert(P.sc_dense.end(), grouped.begin(), grouped.end());
       W.scd_cnt.push_back((int)P.sc_dense.size() - W.scd_off.back());
     }
     launches += (W.small_cnt > 0) + (W.asm_cnt > 0) + (W.upd_cnt > 0);
@@ -1261,7 +1270,27 @@ void Engine::launch_all(std::vector<std::pair<int, cudaEvent_t>> *prof, int prec
       mark(K_PANEL, W.panel_cnt[j]);
       launch_trsm_step(sym_, d_panel_ + W.panel_off[j], W.panel_cnt[j], (int)j, st);
       mark(-1, W.panel_cnt[j]);
-      if (prof) {
+      if (syrk_tc && !prof) {
+        // look-ahead: the step's trailing update split in two.  Column block j+1 (the next
+        // TRSM reads it) on this stream; the grouped updates of the later columns on a third
+        // stream, where they may run on beside the next TRSM: only the diagonal block two
+        // steps on (the next iteration's diagonal-block launch) waits for them
+        cudaEventRecord(ev_fork_, st);
+        if (W.diag_cnt[j] > 0) {
+          cudaStreamWaitEvent(aux_stream_, ev_fork_, 0);
+          if (j > 0) cudaStreamWaitEvent(aux_stream_, ev_grp_[(j - 1) & 1], 0);
+          launch_diag_step(sym_, d_diag_ + W.diag_off[j], W.diag_cnt[j], (int)j + 1, aux_stream_);
+          cudaEventRecord(ev_join_, aux_stream_);
+        }
+        const int nc = W.scd_nc[j];
+        cudaStreamWaitEvent(grp_stream_, ev_fork_, 0);
+        launch_scatter_tc(sym_, sc_maps, d_sc_dense_ + W.scd_off[j] + nc, W.scd_cnt[j] - nc,
+                          scatter_cols(), tuning_.grouped_reserve, bf16, grp_stream_);
+        cudaEventRecord(ev_grp_[j & 1], grp_stream_);
+        launch_scatter_tc(sym_, sc_maps, d_sc_dense_ + W.scd_off[j], nc, scatter_cols(), 2, bf16, st);
+        if (W.diag_cnt[j] > 0) cudaStreamWaitEvent(st, ev_join_, 0);
+        if (j + 1 == W.panel_off.size()) cudaStreamWaitEvent(st, ev_grp_[j & 1], 0);
+      } else if (prof) {
         // profiled runs keep one stream so every launch is bracketed by its own events
         mark(K_PANEL, W.diag_cnt[j]);
         launch_diag_step(sym_, d_diag_ + W.diag_off[j], W.diag_cnt[j], (int)j + 1, st);

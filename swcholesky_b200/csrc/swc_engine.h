@@ -91,7 +91,8 @@ struct Wave {
   std::vector<int> panel_off, panel_cnt;  // per column block step: TRSM tiles
   std::vector<int> syrk_off, syrk_cnt;
   std::vector<int> diag_off, diag_cnt;    // per step j: supernodes whose block j+1 exists
-  std::vector<int> scd_off, scd_cnt;      // per step j: the trailing updates as dense tiles
+  std::vector<int> scd_off, scd_cnt;      // per step j: the trailing updates as dense tiles,
+  std::vector<int> scd_nc;                //   the first scd_nc of them for column block j+1
                                           // (split-TF32 mode)
   int dense_off = 0, dense_cnt = 0;       // dataflow tasks of the dense factorization
   int dense_ctas = 0;
@@ -339,6 +340,8 @@ class Engine {
   cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
   cudaStream_t small_stream_ = nullptr;        // a wave's small supernodes, beside its tiled work
   cudaEvent_t ev_sfork_ = nullptr, ev_sjoin_ = nullptr;
+  cudaStream_t grp_stream_ = nullptr;          // grouped trailing updates of the dense steps
+  cudaEvent_t ev_grp_[2] = {nullptr, nullptr};
   int2 *d_asm_ = nullptr, *d_panel_ = nullptr;
   int4 *d_upd_tasks_ = nullptr, *d_syrk_ = nullptr, *d_pairs_ = nullptr;
   int *d_upd_end_ = nullptr;

@@ -103,6 +103,8 @@ struct Tuning {
   int dense_dataflow = 0;                // dense steps of a wave: one dataflow launch (else
                                          // three launches per 64-column step)
   int dense_group = 4;                   // column blocks per grouped trailing update
+  int grouped_reserve = 48;              // mixed modes: SMs the grouped trailing updates
+                                         // leave to the next TRSM and diagonal block
   int syrk_fp64 = 0;                     // mixed modes: trailing SYRK steps in FP64 (DMMA)
                                          // instead of split dense tiles of the scatter
                                          // kernel
