@@ -881,6 +881,10 @@ bool check_scatter_plan(int n, const int *Ls, const HostSym &H, const Plan &P, c
             b1 - 1 != (int)j || C <= (int)j || tl.i0 < tl.j0 || tl.i0 >= m ||
             tl.k0 + 32 * tl.nk < std::min(w, b1 * TB) || b1 - b0 > G)
           return fail("dense tile fields, tile/step", t, (long long)j);
+        // the step's next-column tiles (the next TRSM's column, launched on the chain's
+        // stream) come first, then the grouped ones (launched beside the next steps)
+        if ((t - W.scd_off[j] < W.scd_nc[j]) != (C == (int)j + 1))
+          return fail("next-column and grouped dense tiles out of order, tile/step", t, (long long)j);
         for (int b = b0; b < b1; ++b) rows[std::make_tuple(s, C, b)].push_back({tl.i0, std::min(m, tl.i0 + 128)});
       }
   }

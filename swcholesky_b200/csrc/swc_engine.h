@@ -228,7 +228,8 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
 // entry's address against a direct lookup in the target's row list, every descendant's
 // lower triangle covered once per column of K, every tile in the level after its
 // descendant's, every column block of the dense steps' trailing updates receiving each
-// earlier block once.  False with a message on the first violation.
+// earlier block once, each step's next-column tiles ahead of its grouped ones.  False with
+// a message on the first violation.
 bool check_scatter_plan(int n, const int *Ls, const HostSym &H, const Plan &P, const Tuning &T,
                         std::string &err);
 

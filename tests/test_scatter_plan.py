@@ -8,7 +8,8 @@ every scattered entry's address with a direct lookup in the target's row list, a
 that each descendant's lower triangle is covered once per column of K (also when the plan
 cuts K into 256- or 128-column tiles), that every tile runs in the level after its
 descendant's, and that the dense steps' trailing-update tiles give every column block each
-earlier column block exactly once."""
+earlier column block exactly once, each step's next-column tiles (launched on the chain's
+stream) ahead of its grouped ones (launched beside the following steps)."""
 import pytest
 
 from conftest import load_sym
