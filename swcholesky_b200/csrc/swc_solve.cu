@@ -843,18 +843,23 @@ __global__ void __launch_bounds__(ST, NS == CHAIN_NS_SMALL ? 2 : 1) k_bwd_chain(
 }
 
 // y = A x for the symmetric matrix held as full CSR (both triangles), nrhs vectors.
-__global__ void k_spmv(int n, const int *rp, const int *ci, const double *val, const double *x,
-                       double *y, int nrhs) {
-  const int row = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
-  if (row >= n) return;
+__global__ void __launch_bounds__(256) k_spmv(int n, const int *rp, const int *ci,
+                                              const double *val, const double *x, double *y,
+                                              int nrhs) {
+  // eight lanes per row (rows of a stencil matrix hold 7 to 81 entries: a warp per row
+  // left most lanes idle), 32 rows per CTA; the eight partial sums meet by shuffles
+  const int row = blockIdx.x * 32 + (int)(threadIdx.x >> 3);
+  const int sub = threadIdx.x & 7;
+  const bool ok = row < n;
+  const int p0 = ok ? rp[row] : 0, p1 = ok ? rp[row + 1] : 0;
   for (int r = 0; r < nrhs; ++r) {
     const double *xr = x + (size_t)r * n;
     double acc = 0.0;
-    for (int p = rp[row] + lane; p < rp[row + 1]; p += 32) acc = fma(val[p], xr[ci[p]], acc);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) y[(size_t)r * n + row] = acc;
+    for (int p = p0 + sub; p < p1; p += 8) acc = fma(val[p], xr[ci[p]], acc);
+    acc += __shfl_xor_sync(0xffffffffu, acc, 4);
+    acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+    acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+    if (ok && sub == 0) y[(size_t)r * n + row] = acc;
   }
 }
 
@@ -1059,8 +1064,7 @@ void launch_bwd_chain(const DevSym &S, const int2 *tasks, int count, double *x, 
 }
 void launch_spmv(int n, const int *rp, const int *ci, const double *val, const double *x,
                  double *y, int nrhs, cudaStream_t st) {
-  const int warps = 8;
-  k_spmv<<<(n + warps - 1) / warps, warps * 32, 0, st>>>(n, rp, ci, val, x, y, nrhs);
+  k_spmv<<<(n + 31) / 32, 256, 0, st>>>(n, rp, ci, val, x, y, nrhs);
 }
 void launch_gather_vals(int nnz, const int *map, const double *ax, double *val, cudaStream_t st) {
   if (nnz > 0) k_gather_vals<<<(nnz + 255) / 256, 256, 0, st>>>(nnz, map, ax, val);
