@@ -674,10 +674,13 @@ __global__ void __launch_bounds__(MT, 4) k_update_tiles(DevSym S, const int4 *ta
 // ---------------------------------------------------------------------------------------
 // Dense factorization of a tiled-class panel, blocked by 64 columns (right-looking):
 //   step j:  TRSM of the tiles below diagonal block j (k_trsm_step), then, concurrently,
-//            the trailing SYRK/GEMM update of the column blocks after j (k_syrk_step, which
-//            leaves out the next diagonal tile) and, for diagonal block j+1, its update by
-//            block j, POTRF and inverse (k_diag_step), so every diagonal block is factored
-//            before the next step's TRSM reads it.
+//            the trailing SYRK/GEMM update of the column blocks after j (k_syrk_step in
+//            FP64, dense tiles of the split scatter kernel in the mixed modes; it leaves out
+//            the next diagonal tile) and, for diagonal block j+1, its update by block j,
+//            POTRF and inverse (k_diag_step), so every diagonal block is factored before the
+//            next step's TRSM reads it.  In the mixed modes the trailing update is launched
+//            in two parts: column block j+1 (read by the next TRSM) on the chain's stream,
+//            the grouped updates of the later column blocks on a stream of their own.
 //   block 0 is factored by k_diag_step with step 0.
 
 // ---- one 64x64 diagonal block: POTRF and its inverse, blocked by 8 ----------------------
