@@ -196,7 +196,10 @@ int swc_profile(swc_handle_t handle, const double *values, int values_on_device,
  * task order is checked (every wait served by an earlier task) as at analysis, and the
  * tables of the mixed modes' right-looking updates are checked against a direct lookup
  * (every scattered entry's address in L, each descendant's contribution covered once per
- * column of K, the dense steps' trailing updates covering each column block once);
+ * column of K, the dense steps' trailing updates covering each column block once), and
+ * so are the solves' task lists (every supernode solved once, after its children; every
+ * off-diagonal row in one forward contribution task, every 16-column group in one backward
+ * gather task, each contribution listed once under its column);
  * SWC_INVALID_INPUT with the first violation in swc_last_error().
  * stats[0..19] = levels, kernel launches per factorization,
  * small-class supernodes, tiled-class supernodes, update tiles, update (tile, descendant)

@@ -418,6 +418,9 @@ int swc_plan_stats(int n, const int *c, const int *r, const size_t *lC, const in
     return fail(SWC_INVALID_INPUT, err);
   if (!swc::check_scatter_plan(n, Ls, H, P, swc::plan_candidate(plan), err))
     return fail(SWC_INVALID_INPUT, err);
+  swc::SolvePlan SP;
+  swc::build_solve_plan(n, Ls, H, SP);
+  if (!swc::check_solve_plan(n, Ls, H, SP, err)) return fail(SWC_INVALID_INPUT, err);
   stats[0] = (double)P.waves.size();
   stats[1] = (double)P.launches;
   stats[2] = (double)P.small_list.size();

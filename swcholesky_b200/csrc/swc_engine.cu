@@ -916,6 +916,260 @@ bool check_scatter_plan(int n, const int *Ls, const HostSym &H, const Plan &P, c
   return true;
 }
 
+// Per-level task lists of the supernodal solves (no device work).
+void build_solve_plan(int n, const int *Ls, const HostSym &H, SolvePlan &SP) {
+  const int supNo = (int)H.super.size() - 1;
+  const std::vector<int> &super = H.super;
+  const std::vector<int64_t> &rowptr = H.rowptr;
+  const int64_t nls = H.nls;
+  SP = SolvePlan();
+  std::vector<int> lev(supNo, 0);
+  int nl = 0;
+  std::vector<int> col2sup(n);
+  for (int s = 0; s < supNo; ++s)
+    for (int j = super[s]; j < super[s + 1]; ++j) col2sup[j] = s;
+  for (int s = 0; s < supNo; ++s) {
+    const int w = super[s + 1] - super[s];
+    const int64_t m = rowptr[s + 1] - rowptr[s];
+    nl = std::max(nl, lev[s] + 1);
+    if (m > w) {
+      const int p = col2sup[Ls[rowptr[s] + w]];
+      lev[p] = std::max(lev[p], lev[s] + 1);
+    }
+    SP.max_w = std::max(SP.max_w, w);
+  }
+  std::vector<std::vector<int>> bylev(nl);
+  for (int s = 0; s < supNo; ++s) bylev[lev[s]].push_back(s);
+  auto warp_size_ok = [&](int s) {
+    const int w = super[s + 1] - super[s];
+    const int64_t m = rowptr[s + 1] - rowptr[s];
+    return H.dinv_off[s] < 0 && w <= SOLVE_WARP_W && m - w <= SOLVE_WARP_ROWS;
+  };
+  std::vector<int> warp_level(nl, 0);
+  for (int l = 0; l < nl; ++l) {
+    int cnt = 0;
+    for (int s : bylev[l]) cnt += warp_size_ok(s);
+    warp_level[l] = cnt >= SOLVE_WARP_LEVEL_MIN;
+  }
+  for (int l = 0; l < nl; ++l) {
+    SP.level_off.push_back((int)SP.list.size());
+    SP.warp_off.push_back((int)SP.warp_list.size());
+    SP.chain_off.push_back((int)SP.fchain.size());
+    SP.contrib_off.push_back((int)SP.contrib_tasks.size());
+    SP.gather_off.push_back((int)SP.gather_tasks.size());
+    std::vector<int2> narrow, wide;
+    // 128-row tasks of 8 warps for the wide supernodes only when the level has enough of
+    // them to fill the GPU; otherwise 32-row tasks of 32 warps (more, shorter CTAs)
+    int64_t n128 = 0;
+    for (int s : bylev[l]) {
+      const int w = super[s + 1] - super[s];
+      const int64_t m = rowptr[s + 1] - rowptr[s];
+      if (w > SOLVE_NARROW_W && (H.dinv_off[s] >= 0 || !(warp_level[l] && warp_size_ok(s))))
+        n128 += (m - w + SOLVE_CONTRIB_WIDE_ROWS - 1) / SOLVE_CONTRIB_WIDE_ROWS;
+    }
+    const bool wide_level = n128 >= SOLVE_CONTRIB_WIDE_MIN;
+    for (int s : bylev[l]) {
+      const int w = super[s + 1] - super[s];
+      const int m = (int)(rowptr[s + 1] - rowptr[s]);
+      if (H.dinv_off[s] >= 0) {   // tiled class: chained solves through the block inverses
+        const int nb = (w + TB - 1) / TB;
+        for (int k = 0; k < nb; ++k) SP.fchain.push_back(make_int2(s, k));
+        for (int k = nb - 1; k >= 0; --k) SP.bchain.push_back(make_int2(s, k));
+      } else if (warp_level[l] && warp_size_ok(s)) {
+        SP.warp_list.push_back(s);   // its contributions and gathers are done by the warp
+        continue;
+      } else {
+        SP.list.push_back(s);
+      }
+      if (w > SOLVE_CONTRIB_BIG_W || (w > SOLVE_NARROW_W && !wide_level))
+        for (int r0 = w; r0 < m; r0 += SOLVE_CONTRIB_ROWS) SP.contrib_tasks.push_back(make_int2(s, r0));
+      else if (w > SOLVE_NARROW_W)
+        for (int r0 = w; r0 < m; r0 += SOLVE_CONTRIB_WIDE_ROWS) wide.push_back(make_int2(s, r0));
+      else
+        for (int r0 = w; r0 < m; r0 += SOLVE_CONTRIB_ROWS) narrow.push_back(make_int2(s, r0));
+      if (m > w)
+        for (int j0 = 0; j0 < w; j0 += SOLVE_GATHER_COLS) SP.gather_tasks.push_back(make_int2(s, j0));
+    }
+    SP.contrib_big.push_back((int)SP.contrib_tasks.size() - SP.contrib_off.back());
+    SP.contrib_wide.push_back((int)wide.size());
+    SP.contrib_tasks.insert(SP.contrib_tasks.end(), wide.begin(), wide.end());
+    SP.contrib_tasks.insert(SP.contrib_tasks.end(), narrow.begin(), narrow.end());
+  }
+  SP.level_off.push_back((int)SP.list.size());
+  SP.warp_off.push_back((int)SP.warp_list.size());
+  SP.chain_off.push_back((int)SP.fchain.size());
+  SP.contrib_off.push_back((int)SP.contrib_tasks.size());
+  SP.gather_off.push_back((int)SP.gather_tasks.size());
+  SP.contrib_len = nls - n;
+  // column contribution lists: off-diagonal row a of supernode d (a >= w_d) feeds column
+  // Ls[a] through contribution (rowptr[d] - super[d]) + (a - w_d)
+  SP.cptr.assign(n + 1, 0);
+  for (int d = 0; d < supNo; ++d) {
+    const int w = super[d + 1] - super[d];
+    for (int64_t q = rowptr[d] + w; q < rowptr[d + 1]; ++q) SP.cptr[Ls[q] + 1]++;
+  }
+  for (int j = 0; j < n; ++j) SP.cptr[j + 1] += SP.cptr[j];
+  SP.cidx.resize(SP.cptr[n]);
+  std::vector<int> fillc(SP.cptr.begin(), SP.cptr.end() - 1);
+  for (int d = 0; d < supNo; ++d) {
+    const int w = super[d + 1] - super[d];
+    for (int64_t q = rowptr[d] + w; q < rowptr[d + 1]; ++q)
+      SP.cidx[fillc[Ls[q]]++] = (int)((rowptr[d] - super[d]) + (q - rowptr[d] - w));
+  }
+}
+
+// The streaming tasks of a solve plan whose supernodes sit in `level` (by_warp: solved by
+// one warp, which does its own contributions and gathers): forward contribution tasks cover
+// each off-diagonal row once, backward gather tasks each 16-column group once, and the
+// per-column contribution lists name each contribution once, under the row it belongs to.
+static bool check_solve_tasks(int n, const int *Ls, const HostSym &H, const SolvePlan &SP,
+                              const std::vector<int> &level, const std::vector<char> &by_warp,
+                              std::string &err) {
+  const int supNo = (int)H.super.size() - 1;
+  const std::vector<int> &super = H.super;
+  const std::vector<int64_t> &rowptr = H.rowptr;
+  const int nl = (int)SP.level_off.size() - 1;
+  const int64_t clen = SP.contrib_len;
+  auto bad = [&](const std::string &m) {
+    err = "solve plan: " + m;
+    return false;
+  };
+  std::vector<char> row_done(std::max<int64_t>(clen, 1), 0);
+  std::vector<char> col_done(n, 0);
+  for (int l = 0; l < nl; ++l) {
+    const int t0 = SP.contrib_off[l], t1 = SP.contrib_off[l + 1];
+    const int nbig = SP.contrib_big[l], nwide = SP.contrib_wide[l];
+    if (nbig < 0 || nwide < 0 || nbig + nwide > t1 - t0) return bad("contribution classes");
+    for (int k = t0; k < t1; ++k) {
+      const int s = SP.contrib_tasks[k].x, r0 = SP.contrib_tasks[k].y;
+      if (s < 0 || s >= supNo || level[s] != l || by_warp[s])
+        return bad("contribution task of a supernode not solved by a CTA in its level");
+      const int w = super[s + 1] - super[s];
+      const int m = (int)(rowptr[s + 1] - rowptr[s]);
+      const int span = (k - t0 >= nbig && k - t0 < nbig + nwide) ? SOLVE_CONTRIB_WIDE_ROWS
+                                                                 : SOLVE_CONTRIB_ROWS;
+      if (r0 < w || r0 >= m || (r0 - w) % span != 0) return bad("contribution rows misaligned");
+      for (int a = r0; a < std::min(m, r0 + span); ++a) {
+        const int64_t idx = (rowptr[s] - super[s]) + (a - w);
+        if (row_done[idx]) return bad("an off-diagonal row in two contribution tasks");
+        row_done[idx] = 1;
+      }
+    }
+    for (int k = SP.gather_off[l]; k < SP.gather_off[l + 1]; ++k) {
+      const int s = SP.gather_tasks[k].x, j0 = SP.gather_tasks[k].y;
+      if (s < 0 || s >= supNo || level[s] != l || by_warp[s])
+        return bad("gather task of a supernode not solved by a CTA in its level");
+      const int w = super[s + 1] - super[s];
+      if (rowptr[s + 1] - rowptr[s] == w || j0 < 0 || j0 >= w || j0 % SOLVE_GATHER_COLS != 0)
+        return bad("gather columns misaligned");
+      if (col_done[super[s] + j0]) return bad("a column group in two gather tasks");
+      col_done[super[s] + j0] = 1;
+    }
+  }
+  // coverage, and the contribution lists: row of each contribution
+  std::vector<int> row_of(std::max<int64_t>(clen, 1), -1);
+  for (int s = 0; s < supNo; ++s) {
+    const int w = super[s + 1] - super[s];
+    const int m = (int)(rowptr[s + 1] - rowptr[s]);
+    for (int a = w; a < m; ++a) {
+      const int64_t idx = (rowptr[s] - super[s]) + (a - w);
+      row_of[idx] = Ls[rowptr[s] + a];
+      if (!by_warp[s] && !row_done[idx]) return bad("an off-diagonal row in no contribution task");
+    }
+    if (by_warp[s] || m == w) continue;
+    for (int j0 = 0; j0 < w; j0 += SOLVE_GATHER_COLS)
+      if (!col_done[super[s] + j0]) return bad("a column group in no gather task");
+  }
+  if ((int64_t)SP.cptr.size() != n + 1 || SP.cptr[0] != 0 || SP.cptr[n] != clen ||
+      (int64_t)SP.cidx.size() != clen)
+    return bad("contribution lists of the wrong size");
+  std::fill(row_done.begin(), row_done.end(), 0);
+  for (int j = 0; j < n; ++j) {
+    if (SP.cptr[j + 1] < SP.cptr[j]) return bad("contribution list pointers decrease");
+    for (int q = SP.cptr[j]; q < SP.cptr[j + 1]; ++q) {
+      const int idx = SP.cidx[q];
+      if (idx < 0 || idx >= clen || row_done[idx] || row_of[idx] != j)
+        return bad("column " + std::to_string(j) + "'s contribution list");
+      row_done[idx] = 1;
+    }
+  }
+  return true;
+}
+
+bool check_solve_plan(int n, const int *Ls, const HostSym &H, const SolvePlan &SP,
+                      std::string &err) {
+  const int supNo = (int)H.super.size() - 1;
+  const std::vector<int> &super = H.super;
+  const std::vector<int64_t> &rowptr = H.rowptr;
+  const int nl = (int)SP.level_off.size() - 1;
+  auto bad = [&](const std::string &m) {
+    err = "solve plan: " + m;
+    return false;
+  };
+  if (nl < 0 || (int)SP.warp_off.size() != nl + 1 || (int)SP.chain_off.size() != nl + 1 ||
+      (int)SP.contrib_off.size() != nl + 1 || (int)SP.gather_off.size() != nl + 1 ||
+      (int)SP.contrib_big.size() != nl || (int)SP.contrib_wide.size() != nl ||
+      SP.fchain.size() != SP.bchain.size())
+    return bad("per-level offsets of unequal length");
+  if (SP.contrib_len != H.nls - n) return bad("contribution length");
+  // every supernode in exactly one level, by exactly one kind of task
+  std::vector<int> level(supNo, -1);
+  std::vector<char> by_warp(supNo, 0);
+  auto place = [&](int s, int l) {
+    if (s < 0 || s >= supNo) return false;
+    if (level[s] >= 0 && level[s] != l) return false;
+    level[s] = l;
+    return true;
+  };
+  for (int l = 0; l < nl; ++l) {
+    for (int k = SP.level_off[l]; k < SP.level_off[l + 1]; ++k) {
+      const int s = SP.list[k];
+      if (!place(s, l) || H.dinv_off[s] >= 0) return bad("small supernode misplaced");
+    }
+    for (int k = SP.warp_off[l]; k < SP.warp_off[l + 1]; ++k) {
+      const int s = SP.warp_list[k];
+      if (!place(s, l) || H.dinv_off[s] >= 0) return bad("warp supernode misplaced");
+      const int w = super[s + 1] - super[s];
+      if (w > SOLVE_WARP_W || rowptr[s + 1] - rowptr[s] - w > SOLVE_WARP_ROWS)
+        return bad("supernode too large for one warp");
+      by_warp[s] = 1;
+    }
+    // chained blocks: one per 64 columns, forward increasing, backward decreasing
+    const int c0 = SP.chain_off[l], c1 = SP.chain_off[l + 1];
+    for (int k = c0; k < c1;) {
+      const int s = SP.fchain[k].x;
+      if (!place(s, l) || H.dinv_off[s] < 0) return bad("chained supernode misplaced");
+      const int nb = (super[s + 1] - super[s] + TB - 1) / TB;
+      if (k + nb > c1) return bad("chain cut short");
+      for (int b = 0; b < nb; ++b)
+        if (SP.fchain[k + b].x != s || SP.fchain[k + b].y != b ||
+            SP.bchain[k + b].x != s || SP.bchain[k + b].y != nb - 1 - b)
+          return bad("chain blocks out of order");
+      k += nb;
+    }
+  }
+  std::vector<int> col2sup(n);
+  for (int s = 0; s < supNo; ++s)
+    for (int j = super[s]; j < super[s + 1]; ++j) col2sup[j] = s;
+  std::vector<int> seen(supNo, 0);
+  for (int l = 0; l < nl; ++l) {
+    for (int k = SP.level_off[l]; k < SP.level_off[l + 1]; ++k) seen[SP.list[k]]++;
+    for (int k = SP.warp_off[l]; k < SP.warp_off[l + 1]; ++k) seen[SP.warp_list[k]]++;
+    for (int k = SP.chain_off[l]; k < SP.chain_off[l + 1]; ++k)
+      if (SP.fchain[k].y == 0) seen[SP.fchain[k].x]++;
+  }
+  for (int s = 0; s < supNo; ++s) {
+    if (seen[s] != 1) return bad("supernode " + std::to_string(s) + " solved " +
+                                 std::to_string(seen[s]) + " times");
+    const int w = super[s + 1] - super[s];
+    if (rowptr[s + 1] - rowptr[s] > w) {
+      const int p = col2sup[Ls[rowptr[s] + w]];   // the parent: first off-diagonal row's
+      if (level[p] <= level[s]) return bad("a parent not in a later level");
+    }
+  }
+  return check_solve_tasks(n, Ls, H, SP, level, by_warp, err);
+}
+
 bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const int *Ls,
                      const int64_t *Li_ptr, const int *blockSet, int supNo,
                      const int *prunePtr, const int *pruneSet, std::string &err) {
@@ -934,101 +1188,7 @@ bool Engine::analyze(int n, const int *c, const int *r, const int64_t *lC, const
 
   // ---- solve plan: levels of the supernodal etree, per-level task lists ----
   SolvePlan SP;
-  {
-    std::vector<int> lev(supNo, 0);
-    int nl = 0;
-    std::vector<int> col2sup(n);
-    for (int s = 0; s < supNo; ++s)
-      for (int j = super[s]; j < super[s + 1]; ++j) col2sup[j] = s;
-    for (int s = 0; s < supNo; ++s) {
-      const int w = super[s + 1] - super[s];
-      const int64_t m = rowptr[s + 1] - rowptr[s];
-      nl = std::max(nl, lev[s] + 1);
-      if (m > w) {
-        const int p = col2sup[Ls[rowptr[s] + w]];
-        lev[p] = std::max(lev[p], lev[s] + 1);
-      }
-      SP.max_w = std::max(SP.max_w, w);
-    }
-    std::vector<std::vector<int>> bylev(nl);
-    for (int s = 0; s < supNo; ++s) bylev[lev[s]].push_back(s);
-    auto warp_size_ok = [&](int s) {
-      const int w = super[s + 1] - super[s];
-      const int64_t m = rowptr[s + 1] - rowptr[s];
-      return H.dinv_off[s] < 0 && w <= SOLVE_WARP_W && m - w <= SOLVE_WARP_ROWS;
-    };
-    std::vector<int> warp_level(nl, 0);
-    for (int l = 0; l < nl; ++l) {
-      int cnt = 0;
-      for (int s : bylev[l]) cnt += warp_size_ok(s);
-      warp_level[l] = cnt >= SOLVE_WARP_LEVEL_MIN;
-    }
-    for (int l = 0; l < nl; ++l) {
-      SP.level_off.push_back((int)SP.list.size());
-      SP.warp_off.push_back((int)SP.warp_list.size());
-      SP.chain_off.push_back((int)SP.fchain.size());
-      SP.contrib_off.push_back((int)SP.contrib_tasks.size());
-      SP.gather_off.push_back((int)SP.gather_tasks.size());
-      std::vector<int2> narrow, wide;
-      // 128-row tasks of 8 warps for the wide supernodes only when the level has enough of
-      // them to fill the GPU; otherwise 32-row tasks of 32 warps (more, shorter CTAs)
-      int64_t n128 = 0;
-      for (int s : bylev[l]) {
-        const int w = super[s + 1] - super[s];
-        const int64_t m = rowptr[s + 1] - rowptr[s];
-        if (w > SOLVE_NARROW_W && (H.dinv_off[s] >= 0 || !(warp_level[l] && warp_size_ok(s))))
-          n128 += (m - w + SOLVE_CONTRIB_WIDE_ROWS - 1) / SOLVE_CONTRIB_WIDE_ROWS;
-      }
-      const bool wide_level = n128 >= SOLVE_CONTRIB_WIDE_MIN;
-      for (int s : bylev[l]) {
-        const int w = super[s + 1] - super[s];
-        const int m = (int)(rowptr[s + 1] - rowptr[s]);
-        if (H.dinv_off[s] >= 0) {   // tiled class: chained solves through the block inverses
-          const int nb = (w + TB - 1) / TB;
-          for (int k = 0; k < nb; ++k) SP.fchain.push_back(make_int2(s, k));
-          for (int k = nb - 1; k >= 0; --k) SP.bchain.push_back(make_int2(s, k));
-        } else if (warp_level[l] && warp_size_ok(s)) {
-          SP.warp_list.push_back(s);   // its contributions and gathers are done by the warp
-          continue;
-        } else {
-          SP.list.push_back(s);
-        }
-        if (w > SOLVE_CONTRIB_BIG_W || (w > SOLVE_NARROW_W && !wide_level))
-          for (int r0 = w; r0 < m; r0 += SOLVE_CONTRIB_ROWS) SP.contrib_tasks.push_back(make_int2(s, r0));
-        else if (w > SOLVE_NARROW_W)
-          for (int r0 = w; r0 < m; r0 += SOLVE_CONTRIB_WIDE_ROWS) wide.push_back(make_int2(s, r0));
-        else
-          for (int r0 = w; r0 < m; r0 += SOLVE_CONTRIB_ROWS) narrow.push_back(make_int2(s, r0));
-        if (m > w)
-          for (int j0 = 0; j0 < w; j0 += SOLVE_GATHER_COLS) SP.gather_tasks.push_back(make_int2(s, j0));
-      }
-      SP.contrib_big.push_back((int)SP.contrib_tasks.size() - SP.contrib_off.back());
-      SP.contrib_wide.push_back((int)wide.size());
-      SP.contrib_tasks.insert(SP.contrib_tasks.end(), wide.begin(), wide.end());
-      SP.contrib_tasks.insert(SP.contrib_tasks.end(), narrow.begin(), narrow.end());
-    }
-    SP.level_off.push_back((int)SP.list.size());
-    SP.warp_off.push_back((int)SP.warp_list.size());
-    SP.chain_off.push_back((int)SP.fchain.size());
-    SP.contrib_off.push_back((int)SP.contrib_tasks.size());
-    SP.gather_off.push_back((int)SP.gather_tasks.size());
-    SP.contrib_len = nls - n;
-    // column contribution lists: off-diagonal row a of supernode d (a >= w_d) feeds column
-    // Ls[a] through contribution (rowptr[d] - super[d]) + (a - w_d)
-    SP.cptr.assign(n + 1, 0);
-    for (int d = 0; d < supNo; ++d) {
-      const int w = super[d + 1] - super[d];
-      for (int64_t q = rowptr[d] + w; q < rowptr[d + 1]; ++q) SP.cptr[Ls[q] + 1]++;
-    }
-    for (int j = 0; j < n; ++j) SP.cptr[j + 1] += SP.cptr[j];
-    SP.cidx.resize(SP.cptr[n]);
-    std::vector<int> fillc(SP.cptr.begin(), SP.cptr.end() - 1);
-    for (int d = 0; d < supNo; ++d) {
-      const int w = super[d + 1] - super[d];
-      for (int64_t q = rowptr[d] + w; q < rowptr[d + 1]; ++q)
-        SP.cidx[fillc[Ls[q]]++] = (int)((rowptr[d] - super[d]) + (q - rowptr[d] - w));
-    }
-  }
+  build_solve_plan(n, Ls, H, SP);
   if (!solve_configure(SP.max_w, err)) return false;
   // ---- full CSR of the symmetric matrix for residuals: entry -> index into A2 values ----
   std::vector<int> csr_rp(n + 1, 0), csr_ci, csr_map;

@@ -233,6 +233,19 @@ bool build_plan(int n, const int *c, const int *r, const int64_t *lC, const int 
 bool check_scatter_plan(int n, const int *Ls, const HostSym &H, const Plan &P, const Tuning &T,
                         std::string &err);
 
+// Per-level task lists of the supernodal solves (no device work).
+void build_solve_plan(int n, const int *Ls, const HostSym &H, SolvePlan &SP);
+
+// Host check of a solve plan: every supernode solved once (by its CTA or its warp, or, in
+// the tiled class, by one chained block per 64 columns, forward in increasing and backward
+// in decreasing block order), in a level after the levels of its children; every
+// off-diagonal row of a supernode not solved by a warp in exactly one forward contribution
+// task of its level, and each of its 16-column groups in exactly one backward gather task;
+// every column's contribution list naming exactly the contributions of the rows equal to
+// it.  False with a message on the first violation.
+bool check_solve_plan(int n, const int *Ls, const HostSym &H, const SolvePlan &SP,
+                      std::string &err);
+
 struct AdjointPlan;   // reverse-sweep schedule of the adjoint (swc_adjoint.cu)
 
 class Engine {
